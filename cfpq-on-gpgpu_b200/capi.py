@@ -1,0 +1,286 @@
+"""ctypes binding of libcfpq_b200.so (the C ABI declared in include/cfpq_b200.h).
+
+Used by the tests, bench.py and the Python query helpers.  The library is
+the product; this module only marshals arguments.  Loading fails loudly when
+the shared library has not been built -- there is no fallback implementation.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Iterable, Sequence
+
+import numpy as np
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG_DIR, "lib", "libcfpq_b200.so")
+
+OK = 0
+ERR_INVALID, ERR_CUDA, ERR_OOM, ERR_UNSUPPORTED, ERR_TIMEOUT, ERR_IO = 1, 2, 3, 4, 5, 6
+
+VARIANT_AUTO, VARIANT_PLAIN, VARIANT_LOP3, VARIANT_M4R, VARIANT_TC = 0, 1, 2, 3, 4
+VARIANTS = {"auto": 0, "plain": 1, "lop3": 2, "m4r": 3, "tc": 4}
+DRIVER_ENGINE, DRIVER_WORKLIST = 0, 1
+
+# Every entry point declared in include/cfpq_b200.h.
+EXPORTED = (
+    "cfpq_abi_version", "cfpq_last_error", "cfpq_ctx_create", "cfpq_ctx_destroy", "cfpq_ctx_synchronize",
+    "cfpq_ctx_num_sms", "cfpq_matrix_create", "cfpq_matrix_destroy", "cfpq_matrix_size", "cfpq_matrix_set_bits",
+    "cfpq_matrix_set_bits_device", "cfpq_load_edges", "cfpq_matrix_set_diagonal", "cfpq_matrix_clear",
+    "cfpq_matrix_copy", "cfpq_matrix_upload_rows", "cfpq_matrix_download_rows", "cfpq_matrix_hash_count",
+    "cfpq_matrix_count", "cfpq_hash_count_many", "cfpq_add_mul", "cfpq_closure", "cfpq_closure_batch",
+    "cfpq_product_log",
+)
+
+
+class CfpqError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"cfpq error {code}: {message}")
+        self.code = code
+
+
+class Rule(ctypes.Structure):
+    _fields_ = [("head", ctypes.c_uint32), ("body1", ctypes.c_uint32), ("body2", ctypes.c_uint32)]
+
+
+class ClosureOpts(ctypes.Structure):
+    _fields_ = [("driver", ctypes.c_int32), ("variant", ctypes.c_int32), ("max_iterations", ctypes.c_int32),
+                ("use_graph", ctypes.c_int32), ("log_products", ctypes.c_int32), ("reserved", ctypes.c_int32 * 3)]
+
+
+class ClosureStats(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_uint32), ("reserved0", ctypes.c_uint32), ("products", ctypes.c_uint64),
+                ("tile_triples", ctypes.c_uint64), ("work_items", ctypes.c_uint64),
+                ("dense_bitops", ctypes.c_uint64), ("device_ms", ctypes.c_double),
+                ("kernel_launches", ctypes.c_uint64), ("variant_items", ctypes.c_uint64 * 5)]
+
+    def as_dict(self) -> dict:
+        d = {k: getattr(self, k) for k, _ in self._fields_ if not k.startswith("reserved")}
+        d["variant_items"] = list(self.variant_items)
+        return d
+
+
+class Query(ctypes.Structure):
+    _fields_ = [("rules", ctypes.POINTER(Rule)), ("nrules", ctypes.c_size_t),
+                ("mats", ctypes.POINTER(ctypes.c_void_p)), ("nmats", ctypes.c_size_t)]
+
+
+class ProductRecord(ctypes.Structure):
+    _fields_ = [("iteration", ctypes.c_uint32), ("query", ctypes.c_uint32), ("rule", ctypes.c_uint32),
+                ("term", ctypes.c_uint32), ("n", ctypes.c_uint32), ("variant", ctypes.c_uint32),
+                ("p_tiles", ctypes.c_uint64), ("q_tiles", ctypes.c_uint64), ("c_tiles", ctypes.c_uint64),
+                ("tile_triples", ctypes.c_uint64), ("usec", ctypes.c_float), ("reserved", ctypes.c_float)]
+
+
+_lib = None
+
+
+def load_library(path: str | None = None) -> ctypes.CDLL:
+    """Load libcfpq_b200.so and declare the C signatures (cached)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise FileNotFoundError(f"{p} is not built; run `make -C cfpq-on-gpgpu_b200` (or __graft_entry__.build())")
+    lib = ctypes.CDLL(p)
+    vp, u32, u64, sz, i32 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_size_t, ctypes.c_int
+    P = ctypes.POINTER
+    sigs = {
+        "cfpq_abi_version": ([], i32),
+        "cfpq_last_error": ([], ctypes.c_char_p),
+        "cfpq_ctx_create": ([i32, P(vp)], i32),
+        "cfpq_ctx_destroy": ([vp], i32),
+        "cfpq_ctx_synchronize": ([vp], i32),
+        "cfpq_ctx_num_sms": ([vp], i32),
+        "cfpq_matrix_create": ([vp, u32, P(vp)], i32),
+        "cfpq_matrix_destroy": ([vp, vp], i32),
+        "cfpq_matrix_size": ([vp], u32),
+        "cfpq_matrix_set_bits": ([vp, vp, vp, vp, sz], i32),
+        "cfpq_matrix_set_bits_device": ([vp, vp, vp, vp, sz], i32),
+        "cfpq_load_edges": ([vp, P(vp), sz, vp, vp, vp, sz, vp, vp, u32], i32),
+        "cfpq_matrix_set_diagonal": ([vp, vp], i32),
+        "cfpq_matrix_clear": ([vp, vp], i32),
+        "cfpq_matrix_copy": ([vp, vp, vp], i32),
+        "cfpq_matrix_upload_rows": ([vp, vp, vp], i32),
+        "cfpq_matrix_download_rows": ([vp, vp, vp], i32),
+        "cfpq_matrix_hash_count": ([vp, vp, P(u64), P(u64)], i32),
+        "cfpq_matrix_count": ([vp, vp, P(u64)], i32),
+        "cfpq_hash_count_many": ([vp, P(vp), sz, P(u64), P(u64)], i32),
+        "cfpq_add_mul": ([vp, vp, vp, vp, i32, P(i32)], i32),
+        "cfpq_closure": ([vp, P(Rule), sz, P(vp), sz, P(ClosureOpts), P(ClosureStats)], i32),
+        "cfpq_closure_batch": ([vp, P(Query), sz, P(ClosureOpts), P(ClosureStats), P(u32),
+                                P(ctypes.c_double)], i32),
+        "cfpq_product_log": ([vp, P(ProductRecord), sz], sz),
+    }
+    for name, (args, res) in sigs.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = res
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def _check(lib, rc: int) -> None:
+    if rc != OK:
+        raise CfpqError(rc, lib.cfpq_last_error().decode(errors="replace"))
+
+
+def _ptr(a: np.ndarray) -> ctypes.c_void_p:
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+class Matrix:
+    """An n x n Boolean matrix resident on the device."""
+
+    def __init__(self, ctx: "Context", n: int):
+        self.ctx, self.n = ctx, int(n)
+        h = ctypes.c_void_p()
+        _check(ctx.lib, ctx.lib.cfpq_matrix_create(ctx.handle, self.n, ctypes.byref(h)))
+        self.handle = h
+
+    @property
+    def words_per_row(self) -> int:
+        return (self.n + 63) // 64
+
+    def set_bits(self, rows: Iterable[int], cols: Iterable[int]) -> None:
+        r = np.ascontiguousarray(np.asarray(rows, dtype=np.uint32))
+        c = np.ascontiguousarray(np.asarray(cols, dtype=np.uint32))
+        if r.shape != c.shape:
+            raise ValueError("rows and cols differ in length")
+        _check(self.ctx.lib, self.ctx.lib.cfpq_matrix_set_bits(self.ctx.handle, self.handle, _ptr(r), _ptr(c), r.size))
+
+    def set_diagonal(self) -> None:
+        _check(self.ctx.lib, self.ctx.lib.cfpq_matrix_set_diagonal(self.ctx.handle, self.handle))
+
+    def clear(self) -> None:
+        _check(self.ctx.lib, self.ctx.lib.cfpq_matrix_clear(self.ctx.handle, self.handle))
+
+    def copy_from(self, other: "Matrix") -> None:
+        _check(self.ctx.lib, self.ctx.lib.cfpq_matrix_copy(self.ctx.handle, self.handle, other.handle))
+
+    def upload_rows(self, rows: np.ndarray) -> None:
+        a = np.ascontiguousarray(rows, dtype=np.uint64)
+        if a.size != self.n * self.words_per_row:
+            raise ValueError(f"expected {self.n * self.words_per_row} words, got {a.size}")
+        _check(self.ctx.lib, self.ctx.lib.cfpq_matrix_upload_rows(self.ctx.handle, self.handle, _ptr(a)))
+
+    def download_rows(self) -> np.ndarray:
+        a = np.zeros((self.n, self.words_per_row), dtype=np.uint64)
+        if self.n:
+            _check(self.ctx.lib, self.ctx.lib.cfpq_matrix_download_rows(self.ctx.handle, self.handle, _ptr(a)))
+        return a
+
+    def hash_count(self) -> tuple[int, int]:
+        h, c = ctypes.c_uint64(), ctypes.c_uint64()
+        _check(self.ctx.lib, self.ctx.lib.cfpq_matrix_hash_count(self.ctx.handle, self.handle, ctypes.byref(h),
+                                                                 ctypes.byref(c)))
+        return int(h.value), int(c.value)
+
+    def destroy(self) -> None:
+        if self.handle:
+            _check(self.ctx.lib, self.ctx.lib.cfpq_matrix_destroy(self.ctx.handle, self.handle))
+            self.handle = None
+
+
+class Context:
+    """A device context (one CUDA stream and the engine's scratch state)."""
+
+    def __init__(self, device: int = 0, lib: ctypes.CDLL | None = None):
+        self.lib = lib or load_library()
+        h = ctypes.c_void_p()
+        _check(self.lib, self.lib.cfpq_ctx_create(int(device), ctypes.byref(h)))
+        self.handle = h
+        self.device = device
+
+    def close(self) -> None:
+        if self.handle:
+            _check(self.lib, self.lib.cfpq_ctx_destroy(self.handle))
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def num_sms(self) -> int:
+        return self.lib.cfpq_ctx_num_sms(self.handle)
+
+    def synchronize(self) -> None:
+        _check(self.lib, self.lib.cfpq_ctx_synchronize(self.handle))
+
+    def matrix(self, n: int) -> Matrix:
+        return Matrix(self, n)
+
+    def add_mul(self, c: Matrix, a: Matrix, b: Matrix, variant: int | str = VARIANT_AUTO) -> bool:
+        v = VARIANTS[variant] if isinstance(variant, str) else int(variant)
+        ch = ctypes.c_int()
+        _check(self.lib, self.lib.cfpq_add_mul(self.handle, c.handle, a.handle, b.handle, v, ctypes.byref(ch)))
+        return bool(ch.value)
+
+    @staticmethod
+    def _opts(driver, variant, use_graph, max_iterations, log_products) -> ClosureOpts:
+        o = ClosureOpts()
+        o.driver = {"engine": DRIVER_ENGINE, "worklist": DRIVER_WORKLIST}.get(driver, driver)
+        o.variant = VARIANTS[variant] if isinstance(variant, str) else int(variant)
+        o.use_graph = int(use_graph)
+        o.max_iterations = int(max_iterations)
+        o.log_products = int(log_products)
+        return o
+
+    def closure(self, rules: Sequence[tuple[int, int, int]], mats: Sequence[Matrix], driver="engine",
+                variant="auto", use_graph: bool = True, max_iterations: int = 0, log_products: bool = False) -> dict:
+        rs = (Rule * max(len(rules), 1))(*[Rule(*map(int, r)) for r in rules])
+        hs = (ctypes.c_void_p * max(len(mats), 1))(*[m.handle for m in mats])
+        o = self._opts(driver, variant, use_graph, max_iterations, log_products)
+        st = ClosureStats()
+        _check(self.lib, self.lib.cfpq_closure(self.handle, rs, len(rules), hs, len(mats), ctypes.byref(o),
+                                               ctypes.byref(st)))
+        return st.as_dict()
+
+    def closure_batch(self, queries: Sequence[tuple[Sequence[tuple[int, int, int]], Sequence[Matrix]]],
+                      variant="auto", use_graph: bool = True, max_iterations: int = 0):
+        keep = []
+        qs = (Query * max(len(queries), 1))()
+        for i, (rules, mats) in enumerate(queries):
+            rs = (Rule * max(len(rules), 1))(*[Rule(*map(int, r)) for r in rules])
+            hs = (ctypes.c_void_p * max(len(mats), 1))(*[m.handle for m in mats])
+            keep += [rs, hs]
+            qs[i].rules = ctypes.cast(rs, ctypes.POINTER(Rule))
+            qs[i].nrules = len(rules)
+            qs[i].mats = ctypes.cast(hs, ctypes.POINTER(ctypes.c_void_p))
+            qs[i].nmats = len(mats)
+        o = self._opts("engine", variant, use_graph, max_iterations, False)
+        st = ClosureStats()
+        iters = np.zeros(max(len(queries), 1), dtype=np.uint32)
+        done = np.zeros(max(len(queries), 1), dtype=np.float64)
+        _check(self.lib, self.lib.cfpq_closure_batch(
+            self.handle, qs, len(queries), ctypes.byref(o), ctypes.byref(st),
+            iters.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
+            done.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return st.as_dict(), iters[:len(queries)], done[:len(queries)]
+
+    def load_edges(self, mats: Sequence[Matrix], src: np.ndarray, label: np.ndarray, dst: np.ndarray,
+                   label_offsets: np.ndarray, label_mats: np.ndarray) -> None:
+        s = np.ascontiguousarray(src, dtype=np.uint32)
+        l = np.ascontiguousarray(label, dtype=np.uint32)
+        d = np.ascontiguousarray(dst, dtype=np.uint32)
+        off = np.ascontiguousarray(label_offsets, dtype=np.uint32)
+        lm = np.ascontiguousarray(label_mats, dtype=np.uint32)
+        if lm.size == 0:
+            lm = np.zeros(1, dtype=np.uint32)
+        hs = (ctypes.c_void_p * max(len(mats), 1))(*[m.handle for m in mats])
+        _check(self.lib, self.lib.cfpq_load_edges(self.handle, hs, len(mats), _ptr(s), _ptr(l), _ptr(d), s.size,
+                                                  _ptr(off), _ptr(lm), off.size - 1))
+
+    def hash_count_many(self, mats: Sequence[Matrix]) -> list[tuple[int, int]]:
+        if not mats:
+            return []
+        hs = (ctypes.c_void_p * len(mats))(*[m.handle for m in mats])
+        h = (ctypes.c_uint64 * len(mats))()
+        c = (ctypes.c_uint64 * len(mats))()
+        _check(self.lib, self.lib.cfpq_hash_count_many(self.handle, hs, len(mats), h, c))
+        return [(int(h[i]), int(c[i])) for i in range(len(mats))]

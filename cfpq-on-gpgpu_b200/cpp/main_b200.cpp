@@ -1,0 +1,29 @@
+// b200GPU: drop-in executable with the reference mains' contract
+// (m4ri/main.cpp:7-15, cuda/naive-gpu/main.cpp:6-14, harness
+// test_utils/runners.py:22-30):
+//   b200GPU <grammar> <graph> <answer-file>
+// prints "total_ms algo_ms" on stdout and writes one "name hash count" line per
+// nonterminal to the answer file; nothing on stderr on success.
+#include <iostream>
+
+#include "cfpq/B200Matrix.h"
+#include "cfpq/Grammar.h"
+#include "cfpq/Graph.h"
+
+int main(int argc, char *argv[]) {
+    if (argc < 4) {
+        std::cerr << "usage: " << argv[0] << " <grammar> <graph> <answer-file>\n";
+        return 2;
+    }
+    try {
+        Grammar grammar = Grammar(argv[1]);
+        Graph graph = Graph(argv[2]);
+        auto times = grammar.intersection_with_graph<B200Matrix, B200MatricesEnv>(graph);
+        std::cout << times.first << ' ' << times.second << std::endl;
+        grammar.print_results(argv[3]);
+    } catch (const std::exception &e) {
+        std::cerr << "b200GPU: " << e.what() << '\n';
+        return 1;
+    }
+    return 0;
+}

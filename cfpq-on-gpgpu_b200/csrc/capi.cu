@@ -1,0 +1,966 @@
+// C ABI of libcfpq_b200.so (declared in include/cfpq_b200.h).
+//
+// Host runtime: context (device, stream, scratch buffers, delta-matrix pool,
+// cached CUDA graph), matrices, product entry point and the two closure
+// drivers:
+//   ENGINE   -- semi-naive iterations resident on the device.  Iteration t
+//               runs, for every rule C -> A B, the product terms
+//               dA_{t-1} * B and A * dB_{t-1} (d = bits added in the previous
+//               iteration; in the first iteration dA = A and only the first
+//               term runs).  New bits of C go to C and to dC_t.  The loop ends
+//               after an iteration without new bits.  Every bit of the least
+//               fixpoint is produced because each pair (A bit, B bit) meets in
+//               the iteration after the later of the two appeared.  Iterations
+//               are plan -> product -> advance -> iter_end kernels, either
+//               launched from a host loop that checks the flag every few
+//               iterations or captured once as the body of a CUDA-graph while
+//               node whose condition the iter_end kernel sets on the device.
+//   WORKLIST -- the reference loop (cfpq-cpp/Grammar.h:58-69): one add_mul at
+//               a time with the changed flag read back after each product.
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <deque>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "cfpq_b200.h"
+#include "launch.h"
+
+using namespace cfpq;
+
+// ---------------------------------------------------------------------------
+// errors
+
+static thread_local std::string g_last_error;
+
+static int set_error(int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+#define CUDA_TRY(call)                                                                                \
+    do {                                                                                              \
+        cudaError_t e_ = (call);                                                                      \
+        if (e_ != cudaSuccess)                                                                        \
+            return set_error(e_ == cudaErrorMemoryAllocation ? CFPQ_ERR_OOM : CFPQ_ERR_CUDA,          \
+                             "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__);    \
+    } while (0)
+
+#define TRY(call)                   \
+    do {                            \
+        int r_ = (call);            \
+        if (r_ != CFPQ_OK) return r_; \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// types
+
+namespace {
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    int ensure(size_t bytes) {
+        if (bytes <= cap) return CFPQ_OK;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        size_t want = std::max<size_t>(bytes, 256);
+        want = (want + 4095) & ~(size_t)4095;
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            return set_error(CFPQ_ERR_OOM, "device allocation of %zu bytes failed: %s", want, cudaGetErrorString(e));
+        }
+        cap = want;
+        return CFPQ_OK;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+    template <class T> T *as() const { return reinterpret_cast<T *>(p); }
+};
+
+struct PowTables {
+    uint32_t *d_pow11 = nullptr;
+    uint32_t *d_pow13 = nullptr;
+};
+
+struct GraphCache {
+    cudaGraphExec_t exec = nullptr;
+    cudaGraph_t graph = nullptr;
+    std::vector<uint64_t> key;
+    void release() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+        key.clear();
+    }
+};
+
+}  // namespace
+
+struct cfpq_matrix {
+    cfpq_ctx *ctx;
+    DevMat d;
+};
+
+struct cfpq_ctx {
+    int device = 0;
+    int num_sms = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // small device scratch
+    IterState *d_st = nullptr;
+    uint32_t *d_flag = nullptr;
+    unsigned long long *d_hash = nullptr;  // 2 per matrix for hash_count_many
+    size_t d_hash_cap = 0;
+    uint32_t *d_bad = nullptr;
+    // pinned host scratch
+    IterState *h_st = nullptr;
+    uint32_t *h_flag = nullptr;
+    unsigned long long *h_hash = nullptr;
+    size_t h_hash_cap = 0;
+    // growable device scratch
+    DevBuf stage, items, prods, slots, qtrack, prod_seen, mats_desc, edge_buf;
+    std::unordered_map<uint32_t, PowTables> pow;
+    std::vector<cfpq_matrix *> pool;  // zeroed spare matrices (deltas, alias copies)
+    GraphCache gcache;
+    int lop3_grid = 0;
+    std::vector<cfpq_product_record> log;
+};
+
+// ---------------------------------------------------------------------------
+// helpers
+
+static inline uint32_t tiles_for(uint32_t n) { return (n + 63) / 64; }
+
+static int alloc_devmat(uint32_t n, DevMat *d) {
+    memset(d, 0, sizeof(*d));
+    d->n = n;
+    d->T = tiles_for(n);
+    d->ow = (d->T + 31) / 32;
+    if (d->T == 0) return CFPQ_OK;
+    const size_t bits_bytes = (size_t)d->T * d->T * 512;
+    const size_t occ_bytes = (size_t)d->T * d->ow * 4;
+    cudaError_t e = cudaMalloc(&d->bits, bits_bytes);
+    if (e != cudaSuccess)
+        return set_error(CFPQ_ERR_OOM, "cannot allocate %zu bytes for a %u x %u matrix: %s", bits_bytes, n, n,
+                         cudaGetErrorString(e));
+    e = cudaMalloc(&d->occ, occ_bytes);
+    if (e != cudaSuccess) {
+        cudaFree(d->bits);
+        d->bits = nullptr;
+        return set_error(CFPQ_ERR_OOM, "cannot allocate occupancy bitmap: %s", cudaGetErrorString(e));
+    }
+    return CFPQ_OK;
+}
+
+static void free_devmat(DevMat *d) {
+    if (d->bits) cudaFree(d->bits);
+    if (d->occ) cudaFree(d->occ);
+    d->bits = nullptr;
+    d->occ = nullptr;
+}
+
+static int use_device(cfpq_ctx *ctx) {
+    if (!ctx) return set_error(CFPQ_ERR_INVALID, "null context");
+    CUDA_TRY(cudaSetDevice(ctx->device));
+    return CFPQ_OK;
+}
+
+// Take a zeroed matrix of size n from the pool (or allocate one).
+static int pool_take(cfpq_ctx *ctx, uint32_t n, cfpq_matrix **out) {
+    for (size_t i = 0; i < ctx->pool.size(); ++i) {
+        if (ctx->pool[i]->d.n == n) {
+            *out = ctx->pool[i];
+            ctx->pool.erase(ctx->pool.begin() + i);
+            return CFPQ_OK;
+        }
+    }
+    cfpq_matrix *m = new cfpq_matrix();
+    m->ctx = ctx;
+    int rc = alloc_devmat(n, &m->d);
+    if (rc != CFPQ_OK) {
+        delete m;
+        return rc;
+    }
+    cudaError_t e = launch_clear_matrix(m->d, ctx->stream);
+    if (e != cudaSuccess) {
+        free_devmat(&m->d);
+        delete m;
+        return set_error(CFPQ_ERR_CUDA, "clear: %s", cudaGetErrorString(e));
+    }
+    *out = m;
+    return CFPQ_OK;
+}
+
+// Return a matrix to the pool; `dirty` matrices are cleared first.
+static int pool_give(cfpq_ctx *ctx, cfpq_matrix *m, bool dirty) {
+    if (dirty) CUDA_TRY(launch_clear_matrix(m->d, ctx->stream));
+    ctx->pool.push_back(m);
+    return CFPQ_OK;
+}
+
+static int get_pow_tables(cfpq_ctx *ctx, uint32_t n, PowTables *out) {
+    auto it = ctx->pow.find(n);
+    if (it != ctx->pow.end()) {
+        *out = it->second;
+        return CFPQ_OK;
+    }
+    const uint32_t np = tiles_for(n) * 64;
+    std::vector<uint32_t> p11(np ? np : 1, 0), p13(np ? np : 1, 0);
+    const uint64_t mod = 1000000007ULL;
+    uint64_t a = 1, b = 1;
+    for (int64_t c = (int64_t)n - 1; c >= 0; --c) {  // 11^(n-1-c), 13^(n-1-r)
+        p11[c] = (uint32_t)a;
+        p13[c] = (uint32_t)b;
+        a = a * 11 % mod;
+        b = b * 13 % mod;
+    }
+    PowTables t;
+    CUDA_TRY(cudaMalloc(&t.d_pow11, p11.size() * 4));
+    CUDA_TRY(cudaMalloc(&t.d_pow13, p13.size() * 4));
+    CUDA_TRY(cudaMemcpy(t.d_pow11, p11.data(), p11.size() * 4, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(t.d_pow13, p13.data(), p13.size() * 4, cudaMemcpyHostToDevice));
+    ctx->pow[n] = t;
+    *out = t;
+    return CFPQ_OK;
+}
+
+static int sync_and_check(cfpq_ctx *ctx) {
+    CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return CFPQ_OK;
+}
+
+// ---------------------------------------------------------------------------
+// context
+
+extern "C" int cfpq_abi_version(void) { return CFPQ_B200_ABI_VERSION; }
+
+extern "C" const char *cfpq_last_error(void) { return g_last_error.c_str(); }
+
+extern "C" int cfpq_ctx_create(int device, cfpq_ctx **out) {
+    if (!out) return set_error(CFPQ_ERR_INVALID, "null output pointer");
+    *out = nullptr;
+    int ndev = 0;
+    CUDA_TRY(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) return set_error(CFPQ_ERR_INVALID, "device %d out of range (%d devices)", device, ndev);
+    CUDA_TRY(cudaSetDevice(device));
+    cfpq_ctx *c = new cfpq_ctx();
+    c->device = device;
+    cudaDeviceProp prop;
+    CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+    if (prop.major < 10) {
+        delete c;
+        return set_error(CFPQ_ERR_UNSUPPORTED, "device %d is sm_%d%d; this library is built for sm_100a", device,
+                         prop.major, prop.minor);
+    }
+    c->num_sms = prop.multiProcessorCount;
+    CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    CUDA_TRY(cudaEventCreate(&c->ev0));
+    CUDA_TRY(cudaEventCreate(&c->ev1));
+    CUDA_TRY(cudaMalloc(&c->d_st, sizeof(IterState)));
+    CUDA_TRY(cudaMalloc(&c->d_flag, 64));
+    CUDA_TRY(cudaMalloc(&c->d_bad, 64));
+    CUDA_TRY(cudaMallocHost(&c->h_st, sizeof(IterState)));
+    CUDA_TRY(cudaMallocHost(&c->h_flag, 64));
+    c->lop3_grid = c->num_sms * product_lop3_blocks_per_sm();
+    *out = c;
+    return CFPQ_OK;
+}
+
+extern "C" int cfpq_ctx_destroy(cfpq_ctx *ctx) {
+    if (!ctx) return CFPQ_OK;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    ctx->gcache.release();
+    for (auto *m : ctx->pool) {
+        free_devmat(&m->d);
+        delete m;
+    }
+    for (auto &kv : ctx->pow) {
+        cudaFree(kv.second.d_pow11);
+        cudaFree(kv.second.d_pow13);
+    }
+    for (DevBuf *b : {&ctx->stage, &ctx->items, &ctx->prods, &ctx->slots, &ctx->qtrack, &ctx->prod_seen,
+                      &ctx->mats_desc, &ctx->edge_buf})
+        b->release();
+    cudaFree(ctx->d_st);
+    cudaFree(ctx->d_flag);
+    cudaFree(ctx->d_bad);
+    if (ctx->d_hash) cudaFree(ctx->d_hash);
+    cudaFreeHost(ctx->h_st);
+    cudaFreeHost(ctx->h_flag);
+    if (ctx->h_hash) cudaFreeHost(ctx->h_hash);
+    cudaEventDestroy(ctx->ev0);
+    cudaEventDestroy(ctx->ev1);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return CFPQ_OK;
+}
+
+extern "C" int cfpq_ctx_synchronize(cfpq_ctx *ctx) {
+    TRY(use_device(ctx));
+    return sync_and_check(ctx);
+}
+
+extern "C" int cfpq_ctx_num_sms(const cfpq_ctx *ctx) { return ctx ? ctx->num_sms : 0; }
+
+// ---------------------------------------------------------------------------
+// matrices
+
+extern "C" int cfpq_matrix_create(cfpq_ctx *ctx, uint32_t n, cfpq_matrix **out) {
+    TRY(use_device(ctx));
+    if (!out) return set_error(CFPQ_ERR_INVALID, "null output pointer");
+    if (tiles_for(n) > (uint32_t)product_lop3_max_tiles())
+        return set_error(CFPQ_ERR_UNSUPPORTED, "n = %u exceeds the supported maximum %d", n,
+                         product_lop3_max_tiles() * 64);
+    cfpq_matrix *m = new cfpq_matrix();
+    m->ctx = ctx;
+    int rc = alloc_devmat(n, &m->d);
+    if (rc != CFPQ_OK) {
+        delete m;
+        return rc;
+    }
+    cudaError_t e = launch_clear_matrix(m->d, ctx->stream);
+    if (e != cudaSuccess) {
+        free_devmat(&m->d);
+        delete m;
+        return set_error(CFPQ_ERR_CUDA, "clear: %s", cudaGetErrorString(e));
+    }
+    *out = m;
+    return CFPQ_OK;
+}
+
+extern "C" int cfpq_matrix_destroy(cfpq_ctx *ctx, cfpq_matrix *m) {
+    if (!m) return CFPQ_OK;
+    TRY(use_device(ctx));
+    cudaStreamSynchronize(ctx->stream);
+    free_devmat(&m->d);
+    delete m;
+    return CFPQ_OK;
+}
+
+extern "C" uint32_t cfpq_matrix_size(const cfpq_matrix *m) { return m ? m->d.n : 0; }
+
+static int check_bad(cfpq_ctx *ctx, const char *what) {
+    uint32_t bad = 0;
+    CUDA_TRY(cudaMemcpyAsync(ctx->h_flag, ctx->d_bad, 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    bad = ctx->h_flag[0];
+    if (bad) return set_error(CFPQ_ERR_INVALID, "%s: %u coordinates out of range", what, bad);
+    return CFPQ_OK;
+}
+
+extern "C" int cfpq_matrix_set_bits(cfpq_ctx *ctx, cfpq_matrix *m, const uint32_t *rows, const uint32_t *cols,
+                                    size_t count) {
+    TRY(use_device(ctx));
+    if (!m || (count && (!rows || !cols))) return set_error(CFPQ_ERR_INVALID, "null argument");
+    if (count == 0) return CFPQ_OK;
+    TRY(ctx->stage.ensure(count * 8));
+    uint32_t *dr = ctx->stage.as<uint32_t>(), *dc = dr + count;
+    CUDA_TRY(cudaMemcpyAsync(dr, rows, count * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(cudaMemcpyAsync(dc, cols, count * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(cudaMemsetAsync(ctx->d_bad, 0, 4, ctx->stream));
+    CUDA_TRY(launch_set_bits(m->d, dr, dc, count, ctx->d_bad, ctx->stream));
+    return check_bad(ctx, "cfpq_matrix_set_bits");
+}
+
+extern "C" int cfpq_matrix_set_bits_device(cfpq_ctx *ctx, cfpq_matrix *m, const uint32_t *d_rows,
+                                           const uint32_t *d_cols, size_t count) {
+    TRY(use_device(ctx));
+    if (!m || (count && (!d_rows || !d_cols))) return set_error(CFPQ_ERR_INVALID, "null argument");
+    CUDA_TRY(cudaMemsetAsync(ctx->d_bad, 0, 4, ctx->stream));
+    CUDA_TRY(launch_set_bits(m->d, d_rows, d_cols, count, ctx->d_bad, ctx->stream));
+    return check_bad(ctx, "cfpq_matrix_set_bits_device");
+}
+
+extern "C" int cfpq_load_edges(cfpq_ctx *ctx, cfpq_matrix *const *mats, size_t nmats, const uint32_t *from,
+                               const uint32_t *label, const uint32_t *to, size_t nedges,
+                               const uint32_t *label_offsets, const uint32_t *label_mats, uint32_t nlabels) {
+    TRY(use_device(ctx));
+    if ((nmats && !mats) || (nedges && (!from || !label || !to)) || (nlabels && (!label_offsets)))
+        return set_error(CFPQ_ERR_INVALID, "null argument");
+    if (nedges == 0 || nlabels == 0) return CFPQ_OK;
+    const uint32_t nlm = label_offsets[nlabels];
+    for (uint32_t l = 0; l < nlabels; ++l)
+        if (label_offsets[l] > label_offsets[l + 1]) return set_error(CFPQ_ERR_INVALID, "label_offsets not sorted");
+    if (nlm && !label_mats) return set_error(CFPQ_ERR_INVALID, "null label_mats");
+    std::vector<DevMat> descs(nmats);
+    for (size_t i = 0; i < nmats; ++i) {
+        if (!mats[i]) return set_error(CFPQ_ERR_INVALID, "null matrix %zu", i);
+        descs[i] = mats[i]->d;
+    }
+    for (uint32_t j = 0; j < nlm; ++j)
+        if (label_mats[j] >= nmats) return set_error(CFPQ_ERR_INVALID, "label_mats[%u] out of range", j);
+    // one staging block: descs | from | label | to | offsets | label_mats
+    const size_t bd = nmats * sizeof(DevMat);
+    const size_t be = nedges * 4;
+    const size_t bo = (size_t)(nlabels + 1) * 4;
+    const size_t bl = (size_t)(nlm ? nlm : 1) * 4;
+    auto up = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    TRY(ctx->edge_buf.ensure(up(bd) + 3 * up(be) + up(bo) + up(bl)));
+    char *base = ctx->edge_buf.as<char>();
+    DevMat *d_desc = reinterpret_cast<DevMat *>(base);
+    uint32_t *d_from = reinterpret_cast<uint32_t *>(base + up(bd));
+    uint32_t *d_label = reinterpret_cast<uint32_t *>(base + up(bd) + up(be));
+    uint32_t *d_to = reinterpret_cast<uint32_t *>(base + up(bd) + 2 * up(be));
+    uint32_t *d_off = reinterpret_cast<uint32_t *>(base + up(bd) + 3 * up(be));
+    uint32_t *d_lm = reinterpret_cast<uint32_t *>(base + up(bd) + 3 * up(be) + up(bo));
+    CUDA_TRY(cudaMemcpyAsync(d_desc, descs.data(), bd, cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(cudaMemcpyAsync(d_from, from, be, cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(cudaMemcpyAsync(d_label, label, be, cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(cudaMemcpyAsync(d_to, to, be, cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(cudaMemcpyAsync(d_off, label_offsets, bo, cudaMemcpyHostToDevice, ctx->stream));
+    if (nlm) CUDA_TRY(cudaMemcpyAsync(d_lm, label_mats, (size_t)nlm * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(cudaMemsetAsync(ctx->d_bad, 0, 4, ctx->stream));
+    CUDA_TRY(launch_load_edges(d_desc, d_from, d_label, d_to, nedges, d_off, d_lm, nlabels, ctx->d_bad, ctx->stream));
+    return check_bad(ctx, "cfpq_load_edges");
+}
+
+extern "C" int cfpq_matrix_set_diagonal(cfpq_ctx *ctx, cfpq_matrix *m) {
+    TRY(use_device(ctx));
+    if (!m) return set_error(CFPQ_ERR_INVALID, "null matrix");
+    CUDA_TRY(launch_set_diag(m->d, ctx->stream));
+    return CFPQ_OK;
+}
+
+extern "C" int cfpq_matrix_clear(cfpq_ctx *ctx, cfpq_matrix *m) {
+    TRY(use_device(ctx));
+    if (!m) return set_error(CFPQ_ERR_INVALID, "null matrix");
+    CUDA_TRY(launch_clear_matrix(m->d, ctx->stream));
+    return CFPQ_OK;
+}
+
+extern "C" int cfpq_matrix_copy(cfpq_ctx *ctx, cfpq_matrix *dst, const cfpq_matrix *src) {
+    TRY(use_device(ctx));
+    if (!dst || !src) return set_error(CFPQ_ERR_INVALID, "null matrix");
+    if (dst->d.n != src->d.n) return set_error(CFPQ_ERR_INVALID, "size mismatch %u vs %u", dst->d.n, src->d.n);
+    if (dst == src) return CFPQ_OK;
+    CUDA_TRY(launch_copy_matrix(dst->d, src->d, ctx->stream));
+    return CFPQ_OK;
+}
+
+extern "C" int cfpq_matrix_upload_rows(cfpq_ctx *ctx, cfpq_matrix *m, const uint64_t *host_rows) {
+    TRY(use_device(ctx));
+    if (!m || (!host_rows && m->d.n)) return set_error(CFPQ_ERR_INVALID, "null argument");
+    if (m->d.n == 0) return CFPQ_OK;
+    const size_t words = (size_t)m->d.n * m->d.T;
+    TRY(ctx->stage.ensure(words * 8));
+    CUDA_TRY(cudaMemcpyAsync(ctx->stage.p, host_rows, words * 8, cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(launch_rows_to_tiles(m->d, ctx->stage.as<uint64_t>(), ctx->stream));
+    return sync_and_check(ctx);
+}
+
+extern "C" int cfpq_matrix_download_rows(cfpq_ctx *ctx, const cfpq_matrix *m, uint64_t *host_rows) {
+    TRY(use_device(ctx));
+    if (!m || (!host_rows && m->d.n)) return set_error(CFPQ_ERR_INVALID, "null argument");
+    if (m->d.n == 0) return CFPQ_OK;
+    const size_t words = (size_t)m->d.n * m->d.T;
+    TRY(ctx->stage.ensure(words * 8));
+    CUDA_TRY(launch_tiles_to_rows(m->d, ctx->stage.as<uint64_t>(), ctx->stream));
+    CUDA_TRY(cudaMemcpyAsync(host_rows, ctx->stage.p, words * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    return sync_and_check(ctx);
+}
+
+static int ensure_hash_buffers(cfpq_ctx *ctx, size_t nm) {
+    if (ctx->d_hash_cap < nm) {
+        if (ctx->d_hash) cudaFree(ctx->d_hash);
+        if (ctx->h_hash) cudaFreeHost(ctx->h_hash);
+        ctx->d_hash = nullptr;
+        ctx->h_hash = nullptr;
+        ctx->d_hash_cap = ctx->h_hash_cap = 0;
+        CUDA_TRY(cudaMalloc(&ctx->d_hash, nm * 2 * sizeof(unsigned long long)));
+        CUDA_TRY(cudaMallocHost(&ctx->h_hash, nm * 2 * sizeof(unsigned long long)));
+        ctx->d_hash_cap = ctx->h_hash_cap = nm;
+    }
+    return CFPQ_OK;
+}
+
+extern "C" int cfpq_hash_count_many(cfpq_ctx *ctx, cfpq_matrix *const *mats, size_t nmats, uint64_t *hashes,
+                                    uint64_t *counts) {
+    TRY(use_device(ctx));
+    if (nmats && (!mats || !hashes || !counts)) return set_error(CFPQ_ERR_INVALID, "null argument");
+    if (nmats == 0) return CFPQ_OK;
+    TRY(ensure_hash_buffers(ctx, nmats));
+    for (size_t i = 0; i < nmats; ++i) {
+        if (!mats[i]) return set_error(CFPQ_ERR_INVALID, "null matrix %zu", i);
+        PowTables pt;
+        TRY(get_pow_tables(ctx, mats[i]->d.n, &pt));
+        CUDA_TRY(launch_hash_count(mats[i]->d, pt.d_pow11, pt.d_pow13, ctx->d_hash + 2 * i, ctx->stream));
+    }
+    CUDA_TRY(cudaMemcpyAsync(ctx->h_hash, ctx->d_hash, nmats * 2 * sizeof(unsigned long long),
+                             cudaMemcpyDeviceToHost, ctx->stream));
+    TRY(sync_and_check(ctx));
+    for (size_t i = 0; i < nmats; ++i) {
+        hashes[i] = ctx->h_hash[2 * i] % 1000000007ULL;
+        counts[i] = ctx->h_hash[2 * i + 1];
+    }
+    return CFPQ_OK;
+}
+
+extern "C" int cfpq_matrix_hash_count(cfpq_ctx *ctx, const cfpq_matrix *m, uint64_t *hash, uint64_t *count) {
+    if (!m || !hash || !count) return set_error(CFPQ_ERR_INVALID, "null argument");
+    cfpq_matrix *mm = const_cast<cfpq_matrix *>(m);
+    return cfpq_hash_count_many(ctx, &mm, 1, hash, count);
+}
+
+extern "C" int cfpq_matrix_count(cfpq_ctx *ctx, const cfpq_matrix *m, uint64_t *count) {
+    uint64_t h = 0;
+    return cfpq_matrix_hash_count(ctx, m, &h, count);
+}
+
+// ---------------------------------------------------------------------------
+// one product (add_mul)
+
+static int read_flag(cfpq_ctx *ctx, uint32_t *dflag, int *changed) {
+    CUDA_TRY(cudaMemcpyAsync(ctx->h_flag, dflag, 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    *changed = ctx->h_flag[0] != 0;
+    return CFPQ_OK;
+}
+
+// Enqueue c |= a * b with the tiled LOP3 kernel (operands must not alias c).
+static int enqueue_tiled_product(cfpq_ctx *ctx, const DevMat &a, const DevMat &b, const DevMat &c) {
+    const uint32_t T = a.T;
+    const int tpb = product_lop3_tiles_per_block();
+    MatSlot hs[3];
+    memset(hs, 0, sizeof(hs));
+    hs[0].cur = a;
+    hs[1].cur = b;
+    hs[2].cur = c;
+    ProdDesc pd;
+    memset(&pd, 0, sizeof(pd));
+    pd.head = 2;
+    pd.pslot = 0;
+    pd.qslot = 1;
+    pd.T = T;
+    pd.n = a.n;
+    const size_t cap = (size_t)T * ((T + tpb - 1) / tpb);
+    TRY(ctx->slots.ensure(sizeof(hs)));
+    TRY(ctx->prods.ensure(sizeof(pd)));
+    TRY(ctx->items.ensure(std::max<size_t>(cap, 1) * 8));
+    IterState st;
+    memset(&st, 0, sizeof(st));
+    st.iter = 1;
+    st.active = 1;
+    *ctx->h_st = st;
+    CUDA_TRY(cudaMemcpyAsync(ctx->slots.p, hs, sizeof(hs), cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(cudaMemcpyAsync(ctx->prods.p, &pd, sizeof(pd), cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(cudaMemcpyAsync(ctx->d_st, ctx->h_st, sizeof(IterState), cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(launch_plan(ctx->prods.as<ProdDesc>(), 1, 0, T, ctx->slots.as<MatSlot>(), ctx->d_st,
+                         ctx->items.as<uint64_t>(), tpb, nullptr, ctx->stream));
+    CUDA_TRY(launch_product_lop3(ctx->prods.as<ProdDesc>(), ctx->slots.as<MatSlot>(), ctx->d_st,
+                                 ctx->items.as<uint64_t>(), nullptr, ctx->lop3_grid, ctx->stream));
+    return CFPQ_OK;
+}
+
+extern "C" int cfpq_add_mul(cfpq_ctx *ctx, cfpq_matrix *c, const cfpq_matrix *a, const cfpq_matrix *b, int variant,
+                            int *changed) {
+    TRY(use_device(ctx));
+    if (!c || !a || !b || !changed) return set_error(CFPQ_ERR_INVALID, "null argument");
+    if (a->d.n != c->d.n || b->d.n != c->d.n)
+        return set_error(CFPQ_ERR_INVALID, "size mismatch (%u, %u, %u)", c->d.n, a->d.n, b->d.n);
+    *changed = 0;
+    if (c->d.n == 0) return CFPQ_OK;
+    if (variant == CFPQ_VARIANT_AUTO) variant = CFPQ_VARIANT_LOP3;
+    const bool alias = (a == c) || (b == c);
+    if (variant == CFPQ_VARIANT_PLAIN) {
+        CUDA_TRY(cudaMemsetAsync(ctx->d_flag, 0, 4, ctx->stream));
+        if (alias) {
+            cfpq_matrix *tmp = nullptr;
+            TRY(pool_take(ctx, c->d.n, &tmp));
+            CUDA_TRY(launch_plain_product(a->d, b->d, tmp->d, 1, ctx->d_flag, ctx->stream));
+            CUDA_TRY(launch_merge_or(c->d, tmp->d, ctx->d_flag, ctx->stream));
+            TRY(pool_give(ctx, tmp, true));
+        } else {
+            CUDA_TRY(launch_plain_product(a->d, b->d, c->d, 0, ctx->d_flag, ctx->stream));
+        }
+        return read_flag(ctx, ctx->d_flag, changed);
+    }
+    if (variant != CFPQ_VARIANT_LOP3)
+        return set_error(CFPQ_ERR_UNSUPPORTED, "variant %d is not available for add_mul", variant);
+    // Snapshot semantics: operands that alias c are read from a copy.
+    cfpq_matrix *ca = nullptr, *cb = nullptr;
+    DevMat da = a->d, db = b->d;
+    if (a == c) {
+        TRY(pool_take(ctx, c->d.n, &ca));
+        CUDA_TRY(launch_copy_matrix(ca->d, a->d, ctx->stream));
+        da = ca->d;
+    }
+    if (b == c) {
+        if (a == b) {
+            db = da;
+        } else {
+            TRY(pool_take(ctx, c->d.n, &cb));
+            CUDA_TRY(launch_copy_matrix(cb->d, b->d, ctx->stream));
+            db = cb->d;
+        }
+    }
+    TRY(enqueue_tiled_product(ctx, da, db, c->d));
+    CUDA_TRY(cudaMemcpyAsync(ctx->h_st, ctx->d_st, sizeof(IterState), cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    if (ca) TRY(pool_give(ctx, ca, true));
+    if (cb) TRY(pool_give(ctx, cb, true));
+    if (ctx->h_st->error) return set_error(CFPQ_ERR_TIMEOUT, "a bounded device wait gave up (product kernel)");
+    *changed = ctx->h_st->changed != 0;
+    return CFPQ_OK;
+}
+
+// ---------------------------------------------------------------------------
+// closure
+
+namespace {
+
+struct QueryIn {
+    const cfpq_rule *rules;
+    size_t nrules;
+    cfpq_matrix *const *mats;
+    size_t nmats;
+};
+
+struct ClosurePlan {
+    std::vector<MatSlot> slots;
+    std::vector<ProdDesc> prods;
+    std::vector<cfpq_matrix *> deltas;
+    uint32_t slot_rows = 0, prod_rows = 0;
+    size_t item_cap = 0;
+};
+
+}  // namespace
+
+static int validate_query(const QueryIn &q, size_t qi) {
+    if (q.nmats && !q.mats) return set_error(CFPQ_ERR_INVALID, "query %zu: null matrix array", qi);
+    if (q.nrules && !q.rules) return set_error(CFPQ_ERR_INVALID, "query %zu: null rule array", qi);
+    uint32_t n = 0;
+    for (size_t i = 0; i < q.nmats; ++i) {
+        if (!q.mats[i]) return set_error(CFPQ_ERR_INVALID, "query %zu: null matrix %zu", qi, i);
+        if (i == 0) n = q.mats[i]->d.n;
+        if (q.mats[i]->d.n != n)
+            return set_error(CFPQ_ERR_INVALID, "query %zu: matrices of different sizes (%u vs %u)", qi, n,
+                             q.mats[i]->d.n);
+        for (size_t j = 0; j < i; ++j)
+            if (q.mats[j] == q.mats[i])
+                return set_error(CFPQ_ERR_INVALID, "query %zu: matrix %zu repeated at %zu", qi, i, j);
+    }
+    for (size_t r = 0; r < q.nrules; ++r) {
+        const cfpq_rule &ru = q.rules[r];
+        if (ru.head >= q.nmats || ru.body1 >= q.nmats || ru.body2 >= q.nmats)
+            return set_error(CFPQ_ERR_INVALID, "query %zu: rule %zu refers to a matrix out of range", qi, r);
+    }
+    return CFPQ_OK;
+}
+
+static int build_plan(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, int variant, ClosurePlan *pl) {
+    const int tpb = product_lop3_tiles_per_block();
+    for (size_t qi = 0; qi < qs.size(); ++qi) {
+        const QueryIn &q = qs[qi];
+        const uint32_t base = (uint32_t)pl->slots.size();
+        for (size_t i = 0; i < q.nmats; ++i) {
+            MatSlot s;
+            memset(&s, 0, sizeof(s));
+            s.cur = q.mats[i]->d;
+            s.query = (uint32_t)qi;
+            s.row_start = pl->slot_rows;
+            for (int k = 0; k < 2; ++k) {
+                cfpq_matrix *dm = nullptr;
+                TRY(pool_take(ctx, s.cur.n, &dm));
+                pl->deltas.push_back(dm);
+                s.dlt[k] = dm->d;
+            }
+            pl->slot_rows += s.cur.T;
+            pl->slots.push_back(s);
+        }
+        if (q.nmats == 0) continue;
+        const uint32_t T = q.mats[0]->d.T, n = q.mats[0]->d.n;
+        if (T == 0) continue;
+        for (size_t r = 0; r < q.nrules; ++r) {
+            for (uint8_t term = 0; term < 2; ++term) {
+                ProdDesc pd;
+                memset(&pd, 0, sizeof(pd));
+                pd.head = base + q.rules[r].head;
+                pd.pslot = base + q.rules[r].body1;
+                pd.qslot = base + q.rules[r].body2;
+                pd.p_delta = term == 0;
+                pd.q_delta = term == 1;
+                pd.term = term;
+                pd.variant = (uint8_t)variant;
+                pd.query = (uint32_t)qi;
+                pd.rule = (uint32_t)r;
+                pd.T = T;
+                pd.n = n;
+                pd.row_start = pl->prod_rows;
+                pl->prod_rows += T;
+                pl->item_cap += (size_t)T * ((T + tpb - 1) / tpb);
+                pl->prods.push_back(pd);
+            }
+        }
+    }
+    return CFPQ_OK;
+}
+
+static int enqueue_iteration(cfpq_ctx *ctx, const ClosurePlan &pl, const QueryTrack &qt,
+                             cudaGraphConditionalHandle handle, int use_handle) {
+    const int tpb = product_lop3_tiles_per_block();
+    CUDA_TRY(launch_plan(ctx->prods.as<ProdDesc>(), (uint32_t)pl.prods.size(), 0, pl.prod_rows,
+                         ctx->slots.as<MatSlot>(), ctx->d_st, ctx->items.as<uint64_t>(), tpb,
+                         ctx->prod_seen.as<uint32_t>(), ctx->stream));
+    CUDA_TRY(launch_product_lop3(ctx->prods.as<ProdDesc>(), ctx->slots.as<MatSlot>(), ctx->d_st,
+                                 ctx->items.as<uint64_t>(), qt.changed, ctx->lop3_grid, ctx->stream));
+    CUDA_TRY(launch_advance(ctx->slots.as<MatSlot>(), (uint32_t)pl.slots.size(), pl.slot_rows, ctx->d_st,
+                            ctx->stream));
+    CUDA_TRY(launch_iter_end(ctx->d_st, qt, handle, use_handle, ctx->stream));
+    return CFPQ_OK;
+}
+
+// Build (or reuse) the CUDA graph: one while node whose body is one iteration.
+static int get_loop_graph(cfpq_ctx *ctx, const ClosurePlan &pl, const QueryTrack &qt, cudaGraphExec_t *out) {
+    std::vector<uint64_t> key = {(uint64_t)(uintptr_t)ctx->prods.p,  (uint64_t)pl.prods.size(),
+                                 (uint64_t)pl.prod_rows,              (uint64_t)(uintptr_t)ctx->slots.p,
+                                 (uint64_t)pl.slots.size(),           (uint64_t)pl.slot_rows,
+                                 (uint64_t)(uintptr_t)ctx->items.p,   (uint64_t)(uintptr_t)ctx->prod_seen.p,
+                                 (uint64_t)(uintptr_t)qt.changed,     (uint64_t)(uintptr_t)qt.last_iter,
+                                 (uint64_t)(uintptr_t)qt.done_ns,     (uint64_t)ctx->lop3_grid};
+    if (ctx->gcache.exec && ctx->gcache.key == key) {
+        *out = ctx->gcache.exec;
+        return CFPQ_OK;
+    }
+    ctx->gcache.release();
+    cudaGraph_t graph = nullptr;
+    CUDA_TRY(cudaGraphCreate(&graph, 0));
+    cudaGraphConditionalHandle handle;
+    CUDA_TRY(cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = handle;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    CUDA_TRY(cudaGraphAddNode(&node, graph, nullptr, 0, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    CUDA_TRY(cudaStreamBeginCaptureToGraph(ctx->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    int rc = enqueue_iteration(ctx, pl, qt, handle, 1);
+    cudaGraph_t captured = nullptr;
+    cudaError_t e = cudaStreamEndCapture(ctx->stream, &captured);
+    if (rc != CFPQ_OK) {
+        cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        return set_error(CFPQ_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+    }
+    cudaGraphExec_t exec = nullptr;
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        return set_error(CFPQ_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
+    }
+    ctx->gcache.graph = graph;
+    ctx->gcache.exec = exec;
+    ctx->gcache.key = key;
+    *out = exec;
+    return CFPQ_OK;
+}
+
+static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_closure_opts &o,
+                      cfpq_closure_stats *stats, uint32_t *iters_out, double *done_ms_out) {
+    for (size_t qi = 0; qi < qs.size(); ++qi) TRY(validate_query(qs[qi], qi));
+    ClosurePlan pl;
+    int rc = build_plan(ctx, qs, o.variant, &pl);
+    auto give_back = [&](bool dirty) {
+        for (auto *m : pl.deltas) pool_give(ctx, m, dirty);
+        pl.deltas.clear();
+    };
+    if (rc != CFPQ_OK) {
+        give_back(false);
+        return rc;
+    }
+    const size_t nq = qs.size();
+    if (pl.prods.empty()) {
+        give_back(false);
+        if (stats) memset(stats, 0, sizeof(*stats));
+        for (size_t q = 0; q < nq; ++q) {
+            if (iters_out) iters_out[q] = 0;
+            if (done_ms_out) done_ms_out[q] = 0;
+        }
+        return CFPQ_OK;
+    }
+    // device tables
+    TRY(ctx->slots.ensure(pl.slots.size() * sizeof(MatSlot)));
+    TRY(ctx->prods.ensure(pl.prods.size() * sizeof(ProdDesc)));
+    TRY(ctx->items.ensure(std::max<size_t>(pl.item_cap, 1) * 8));
+    TRY(ctx->prod_seen.ensure(pl.prods.size() * 4));
+    const size_t qbytes = nq * (4 + 4 + 8) + 64;
+    TRY(ctx->qtrack.ensure(qbytes));
+    QueryTrack qt;
+    qt.done_ns = ctx->qtrack.as<unsigned long long>();
+    qt.changed = reinterpret_cast<uint32_t *>(qt.done_ns + nq);
+    qt.last_iter = qt.changed + nq;
+    CUDA_TRY(cudaMemcpyAsync(ctx->slots.p, pl.slots.data(), pl.slots.size() * sizeof(MatSlot),
+                             cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(cudaMemcpyAsync(ctx->prods.p, pl.prods.data(), pl.prods.size() * sizeof(ProdDesc),
+                             cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(cudaMemsetAsync(ctx->prod_seen.p, 0, pl.prods.size() * 4, ctx->stream));
+    CUDA_TRY(cudaMemsetAsync(ctx->qtrack.p, 0, qbytes, ctx->stream));
+    IterState st;
+    memset(&st, 0, sizeof(st));
+    st.active = 1;
+    st.max_iter = o.max_iterations > 0 ? (uint32_t)o.max_iterations : 0;
+    st.nqueries = (uint32_t)nq;
+    *ctx->h_st = st;
+    CUDA_TRY(cudaMemcpyAsync(ctx->d_st, ctx->h_st, sizeof(IterState), cudaMemcpyHostToDevice, ctx->stream));
+
+    cudaGraphExec_t exec = nullptr;
+    if (o.use_graph) TRY(get_loop_graph(ctx, pl, qt, &exec));
+
+    CUDA_TRY(launch_mark_start(ctx->d_st, ctx->stream));
+    CUDA_TRY(cudaEventRecord(ctx->ev0, ctx->stream));
+    if (exec) {
+        CUDA_TRY(cudaGraphLaunch(exec, ctx->stream));
+    } else {
+        // Host loop: check the device flag every `batch` iterations; surplus
+        // iterations after convergence are no-ops.
+        const int batch = 4;
+        uint32_t launched = 0;
+        for (;;) {
+            for (int k = 0; k < batch; ++k) TRY(enqueue_iteration(ctx, pl, qt, 0, 0));
+            launched += batch;
+            CUDA_TRY(cudaMemcpyAsync(ctx->h_st, ctx->d_st, sizeof(IterState), cudaMemcpyDeviceToHost, ctx->stream));
+            CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+            if (!ctx->h_st->active) break;
+            if (launched > (1u << 24)) return set_error(CFPQ_ERR_CUDA, "closure did not converge");
+        }
+    }
+    CUDA_TRY(cudaEventRecord(ctx->ev1, ctx->stream));
+    CUDA_TRY(cudaMemcpyAsync(ctx->h_st, ctx->d_st, sizeof(IterState), cudaMemcpyDeviceToHost, ctx->stream));
+    std::vector<unsigned long long> h_done(nq);
+    std::vector<uint32_t> h_last(nq);
+    CUDA_TRY(cudaMemcpyAsync(h_done.data(), qt.done_ns, nq * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(cudaMemcpyAsync(h_last.data(), qt.last_iter, nq * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    float ms = 0;
+    CUDA_TRY(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    const IterState &hs = *ctx->h_st;
+    const bool converged = hs.last_changed == 0;
+    give_back(!converged);
+    if (hs.error) return set_error(CFPQ_ERR_TIMEOUT, "a bounded device wait gave up during the closure");
+    if (stats) {
+        memset(stats, 0, sizeof(*stats));
+        stats->iterations = hs.iter;
+        stats->products = hs.products;
+        stats->tile_triples = hs.tile_triples;
+        stats->work_items = hs.items_total;
+        stats->dense_bitops = hs.dense_bitops;
+        stats->device_ms = ms;
+        stats->kernel_launches = (uint64_t)hs.iter * 4 + 1;
+        stats->variant_items[CFPQ_VARIANT_LOP3] = hs.items_total;
+    }
+    for (size_t q = 0; q < nq; ++q) {
+        if (iters_out) iters_out[q] = h_last[q];
+        if (done_ms_out) done_ms_out[q] = h_last[q] ? (double)(h_done[q] - hs.t_start_ns) / 1e6 : 0.0;
+    }
+    return CFPQ_OK;
+}
+
+static int run_worklist(cfpq_ctx *ctx, const QueryIn &q, const cfpq_closure_opts &o, cfpq_closure_stats *stats) {
+    TRY(validate_query(q, 0));
+    const size_t nr = q.nrules;
+    std::vector<std::vector<uint32_t>> users(q.nmats);
+    for (size_t r = 0; r < nr; ++r) {
+        users[q.rules[r].body1].push_back((uint32_t)r);
+        users[q.rules[r].body2].push_back((uint32_t)r);
+    }
+    std::deque<uint32_t> queue;
+    std::vector<char> queued(nr, 1);
+    for (size_t r = 0; r < nr; ++r) queue.push_back((uint32_t)r);
+    const int variant = o.variant == CFPQ_VARIANT_AUTO ? CFPQ_VARIANT_LOP3 : o.variant;
+    uint64_t products = 0;
+    CUDA_TRY(cudaEventRecord(ctx->ev0, ctx->stream));
+    while (!queue.empty()) {
+        const uint32_t r = queue.front();
+        queue.pop_front();
+        queued[r] = 0;
+        const cfpq_rule &ru = q.rules[r];
+        int changed = 0;
+        TRY(cfpq_add_mul(ctx, q.mats[ru.head], q.mats[ru.body1], q.mats[ru.body2], variant, &changed));
+        ++products;
+        if (changed) {
+            for (uint32_t u : users[ru.head])
+                if (!queued[u]) {
+                    queued[u] = 1;
+                    queue.push_back(u);
+                }
+        }
+        if (o.max_iterations > 0 && products >= (uint64_t)o.max_iterations) break;
+    }
+    CUDA_TRY(cudaEventRecord(ctx->ev1, ctx->stream));
+    CUDA_TRY(cudaEventSynchronize(ctx->ev1));
+    float ms = 0;
+    CUDA_TRY(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    if (stats) {
+        memset(stats, 0, sizeof(*stats));
+        stats->products = products;
+        const uint64_t n = q.nmats ? q.mats[0]->d.n : 0;
+        stats->dense_bitops = products * n * n * n;
+        stats->device_ms = ms;
+        stats->kernel_launches = products;
+    }
+    return CFPQ_OK;
+}
+
+static cfpq_closure_opts default_opts() {
+    cfpq_closure_opts o;
+    memset(&o, 0, sizeof(o));
+    o.driver = CFPQ_DRIVER_ENGINE;
+    o.variant = CFPQ_VARIANT_AUTO;
+    o.use_graph = 1;
+    return o;
+}
+
+extern "C" int cfpq_closure(cfpq_ctx *ctx, const cfpq_rule *rules, size_t nrules, cfpq_matrix *const *mats,
+                            size_t nmats, const cfpq_closure_opts *opts, cfpq_closure_stats *stats) {
+    TRY(use_device(ctx));
+    const cfpq_closure_opts o = opts ? *opts : default_opts();
+    QueryIn q{rules, nrules, mats, nmats};
+    if (o.driver == CFPQ_DRIVER_WORKLIST) return run_worklist(ctx, q, o, stats);
+    if (o.driver != CFPQ_DRIVER_ENGINE) return set_error(CFPQ_ERR_INVALID, "unknown driver %d", o.driver);
+    if (o.variant != CFPQ_VARIANT_AUTO && o.variant != CFPQ_VARIANT_LOP3)
+        return set_error(CFPQ_ERR_UNSUPPORTED, "variant %d is not available in the engine driver", o.variant);
+    std::vector<QueryIn> qs{q};
+    return run_engine(ctx, qs, o, stats, nullptr, nullptr);
+}
+
+extern "C" int cfpq_closure_batch(cfpq_ctx *ctx, const cfpq_query *queries, size_t nqueries,
+                                  const cfpq_closure_opts *opts, cfpq_closure_stats *stats, uint32_t *iterations_out,
+                                  double *done_ms_out) {
+    TRY(use_device(ctx));
+    if (nqueries && !queries) return set_error(CFPQ_ERR_INVALID, "null query array");
+    const cfpq_closure_opts o = opts ? *opts : default_opts();
+    if (o.driver != CFPQ_DRIVER_ENGINE) return set_error(CFPQ_ERR_INVALID, "batched closure needs the engine driver");
+    if (o.variant != CFPQ_VARIANT_AUTO && o.variant != CFPQ_VARIANT_LOP3)
+        return set_error(CFPQ_ERR_UNSUPPORTED, "variant %d is not available in the engine driver", o.variant);
+    std::vector<QueryIn> qs;
+    qs.reserve(nqueries);
+    for (size_t i = 0; i < nqueries; ++i) qs.push_back({queries[i].rules, queries[i].nrules, queries[i].mats, queries[i].nmats});
+    return run_engine(ctx, qs, o, stats, iterations_out, done_ms_out);
+}
+
+extern "C" size_t cfpq_product_log(cfpq_ctx *ctx, cfpq_product_record *out, size_t cap) {
+    if (!ctx) return 0;
+    const size_t n = ctx->log.size();
+    if (out) memcpy(out, ctx->log.data(), std::min(n, cap) * sizeof(cfpq_product_record));
+    return n;
+}

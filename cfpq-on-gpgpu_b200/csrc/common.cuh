@@ -1,0 +1,164 @@
+// Internal definitions shared by the CUDA sources of libcfpq_b200.so.
+//
+// Device matrix layout ("tiled bits"): an n x n Boolean matrix is padded to
+// np = ceil(n/64)*64 and split into T x T tiles of 64 x 64 bits, T = np/64.
+// Tile (ti, tj) is 64 consecutive uint64 words at word offset (ti*T + tj)*64;
+// word r of the tile holds row ti*64 + r, columns tj*64 .. tj*64+63, column
+// tj*64 + b at bit b.  A tile is 512 contiguous bytes, so a block of tiles along
+// a tile-row is one contiguous range that a single bulk copy can stage.
+//
+// Occupancy bitmap: one bit per tile, row ti of the bitmap is `ow` uint32
+// words (ow = ceil(T/32)), tile (ti, tj) at bit tj % 32 of word ti*ow + tj/32.
+// Invariant at every API boundary and at every kernel boundary of the closure:
+// a tile that holds a set bit has its occupancy bit set.  (A set occupancy bit
+// does not promise a non-zero tile.)  Bits of padding rows/columns (>= n) are
+// always zero.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace cfpq {
+
+constexpr int kTileBits = 64;   // tile side
+constexpr int kTileWords = 64;  // uint64 words per tile
+
+struct DevMat {
+    uint64_t *bits;   // T*T*64 words
+    uint32_t *occ;    // T*ow words
+    uint32_t T;       // tiles per side
+    uint32_t ow;      // occupancy words per tile-row
+    uint32_t n;       // logical size
+    uint32_t pad;
+};
+
+// One nonterminal matrix of a closure: the current matrix and two delta
+// buffers used alternately (bits added in the previous / current iteration).
+struct MatSlot {
+    DevMat cur;
+    DevMat dlt[2];
+    uint32_t query;
+    uint32_t row_start;  // prefix sum of T over slots (advance grid mapping)
+};
+
+// One product term of a closure iteration: C |= P * Q, new bits also into the
+// head's "next" delta.  Operands are slots; p_delta / q_delta select the
+// slot's previous-iteration delta instead of its current matrix.
+struct ProdDesc {
+    uint32_t head, pslot, qslot;
+    uint8_t p_delta, q_delta, term, variant;
+    uint32_t query, rule;
+    uint32_t T;
+    uint32_t n;
+    uint32_t row_start;  // prefix sum of T over products (plan grid mapping)
+};
+
+// Device-resident iteration state of a closure (one per context).
+struct IterState {
+    uint32_t iter;          // iteration index (parity selects delta buffers)
+    uint32_t item_count;    // work items written by the plan kernel
+    uint32_t item_next;     // work-stealing counter of the product kernel
+    uint32_t changed;       // set when any new bit appeared in this iteration
+    uint32_t last_changed;  // copy of `changed` at the end of the iteration
+    uint32_t error;         // nonzero: a bounded wait gave up (cfpq_status)
+    uint32_t max_iter;      // 0 = unbounded
+    uint32_t active;        // loop condition mirror (1 while iterating)
+    uint32_t nqueries;
+    uint32_t pad;
+    unsigned long long tile_triples;
+    unsigned long long items_total;
+    unsigned long long products;      // non-empty product terms over all iterations
+    unsigned long long dense_bitops;  // sum of n^3 over those products
+    unsigned long long t_start_ns;    // %globaltimer at the first plan
+    unsigned long long items_by_variant[5];
+};
+
+// Per-query bookkeeping of a batched closure (device arrays of nqueries).
+struct QueryTrack {
+    uint32_t *changed;              // set by product kernels in the current iteration
+    uint32_t *last_iter;            // last iteration (1-based) in which the query changed
+    unsigned long long *done_ns;    // %globaltimer at the end of that iteration
+};
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+#ifdef __CUDA_ARCH__
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+#else
+    return 0;
+#endif
+}
+
+// Work item: (product index, output tile-row, output tile-column block).
+__host__ __device__ inline uint64_t make_item(uint32_t p, uint32_t ti, uint32_t tjb) {
+    return ((uint64_t)p << 40) | ((uint64_t)ti << 20) | (uint64_t)tjb;
+}
+__host__ __device__ inline uint32_t item_prod(uint64_t it) { return (uint32_t)(it >> 40); }
+__host__ __device__ inline uint32_t item_ti(uint64_t it) { return (uint32_t)((it >> 20) & 0xFFFFF); }
+__host__ __device__ inline uint32_t item_tjb(uint64_t it) { return (uint32_t)(it & 0xFFFFF); }
+
+__host__ __device__ inline size_t tile_offset(uint32_t T, uint32_t ti, uint32_t tj) {
+    return ((size_t)ti * T + tj) * kTileWords;
+}
+
+#ifdef __CUDACC__
+
+// ---- mbarrier + bulk copy (TMA engine, 1D) helpers -------------------------
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// Bulk copy of `bytes` (multiple of 16, both addresses 16-byte aligned) from
+// global to this CTA's shared memory, completing on `bar`.
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t phase) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(phase)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait: each try_wait suspends for a hardware-defined time slice; the
+// iteration limit bounds the wait to well under a minute.  Returns false when
+// the limit is hit.
+constexpr uint32_t kWaitLimit = 1u << 22;
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t phase) {
+    for (uint32_t i = 0; i < kWaitLimit; ++i)
+        if (mbar_try_wait(bar, phase)) return true;
+    return false;
+}
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31; }
+
+#endif  // __CUDACC__
+
+}  // namespace cfpq

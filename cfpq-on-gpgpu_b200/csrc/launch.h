@@ -1,0 +1,50 @@
+// Host-side launch wrappers for the kernels of libcfpq_b200.so.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace cfpq {
+
+// Layout / initialisation
+cudaError_t launch_set_bits(const DevMat &m, const uint32_t *d_rows, const uint32_t *d_cols, size_t count,
+                            uint32_t *d_bad, cudaStream_t s);
+cudaError_t launch_load_edges(const DevMat *d_mats, const uint32_t *d_from, const uint32_t *d_label,
+                              const uint32_t *d_to, size_t ne, const uint32_t *d_off, const uint32_t *d_lm,
+                              uint32_t nlabels, uint32_t *d_bad, cudaStream_t s);
+cudaError_t launch_set_diag(const DevMat &m, cudaStream_t s);
+cudaError_t launch_occ_rebuild(const DevMat &m, cudaStream_t s);
+cudaError_t launch_rows_to_tiles(const DevMat &m, const uint64_t *d_rows, cudaStream_t s);
+cudaError_t launch_tiles_to_rows(const DevMat &m, uint64_t *d_rows, cudaStream_t s);
+cudaError_t launch_copy_matrix(const DevMat &dst, const DevMat &src, cudaStream_t s);
+cudaError_t launch_clear_matrix(const DevMat &m, cudaStream_t s);
+
+// Result hash / count (cfpq-cpp/Grammar.cpp:81-100 on the device)
+cudaError_t launch_hash_count(const DevMat &m, const uint32_t *d_pow11, const uint32_t *d_pow13,
+                              unsigned long long *d_out, cudaStream_t s);
+
+// Plain dense product (variant PLAIN): mode 0 ORs into c and sets *d_flag on
+// change; mode 1 writes the product into c (c must not alias a or b).
+cudaError_t launch_plain_product(const DevMat &a, const DevMat &b, const DevMat &c, int mode, uint32_t *d_flag,
+                                 cudaStream_t s);
+// dst |= src, *d_flag set on change.
+cudaError_t launch_merge_or(const DevMat &dst, const DevMat &src, uint32_t *d_flag, cudaStream_t s);
+
+// Closure iteration
+cudaError_t launch_plan(const ProdDesc *d_prods, uint32_t nprods, uint32_t row_begin, uint32_t row_end,
+                        const MatSlot *d_slots, IterState *d_st, uint64_t *d_items, int tiles_per_block,
+                        uint32_t *d_prod_seen, cudaStream_t s);
+cudaError_t launch_product_lop3(const ProdDesc *d_prods, const MatSlot *d_slots, IterState *d_st,
+                                const uint64_t *d_items, uint32_t *d_qchanged, int grid, cudaStream_t s);
+int product_lop3_tiles_per_block();
+int product_lop3_max_tiles();
+int product_lop3_blocks_per_sm();
+cudaError_t launch_advance(const MatSlot *d_slots, uint32_t nslots, uint32_t total_rows, IterState *d_st,
+                           cudaStream_t s);
+cudaError_t launch_mark_start(IterState *d_st, cudaStream_t s);
+cudaError_t launch_iter_end(IterState *d_st, const QueryTrack &qt, cudaGraphConditionalHandle handle, int use_handle,
+                            cudaStream_t s);
+
+}  // namespace cfpq

@@ -1,0 +1,231 @@
+/*
+ * cfpq_b200.h -- C ABI of the B200 CFPQ closure engine (libcfpq_b200.so).
+ *
+ * The reference crosses from its C++ driver to the GPU through C++ namespaces
+ * (gpu_lib:: in cuda/naive-gpu/Multiplication.h:7-28, gpu_m4ri:: in
+ * cuda/methodOf4RusBooleanSemiringGpu/gpuMemoryManagement.h:7-33 and
+ * methodOf4RusBooleanSemiringGpu.h:53-54) behind the Matrix / MatricesEnv
+ * plug-in interface (cfpq-cpp/Matrix.h:7-37).  This header replaces that
+ * boundary with plain C entry points: opaque handles, plain pointers and sizes,
+ * integer status codes.  Each entry point names the reference function it
+ * replaces.
+ *
+ * Matrices are n x n Boolean matrices that live on the device for their whole
+ * life.  The host exchange format ("row bits") is row-major, ceil(n/64) 64-bit
+ * words per row, column c of a row at bit c % 64 of word c / 64 (LSB first).
+ *
+ * Errors: every entry point returns CFPQ_OK (0) or a cfpq_status code and never
+ * exits the process or writes to stderr (the reference prints and calls exit(),
+ * cuda/naive-gpu/Multiplication.cu:10-17).  cfpq_last_error() returns a
+ * description of the last failure on the calling thread.
+ *
+ * Threading: a context may be used by one host thread at a time.  All work of
+ * a context is issued on its own CUDA stream.
+ */
+#ifndef CFPQ_B200_H
+#define CFPQ_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CFPQ_B200_ABI_VERSION 1
+
+typedef enum cfpq_status {
+    CFPQ_OK = 0,
+    CFPQ_ERR_INVALID = 1,      /* bad argument (null handle, index out of range, size mismatch) */
+    CFPQ_ERR_CUDA = 2,         /* a CUDA runtime call or a kernel failed */
+    CFPQ_ERR_OOM = 3,          /* device or pinned host allocation failed */
+    CFPQ_ERR_UNSUPPORTED = 4,  /* requested variant or size not supported */
+    CFPQ_ERR_TIMEOUT = 5,      /* a bounded device-side wait gave up */
+    CFPQ_ERR_IO = 6            /* a file could not be read or written */
+} cfpq_status;
+
+/* Product variants (kernels) for one rule product C |= A * B. */
+typedef enum cfpq_variant {
+    CFPQ_VARIANT_AUTO = 0,   /* the engine's selector picks per product */
+    CFPQ_VARIANT_PLAIN = 1,  /* dense word-level kernel, no tiles, no skipping */
+    CFPQ_VARIANT_LOP3 = 2,   /* tiled word-level AND/OR kernel with bulk-copy staged panels */
+    CFPQ_VARIANT_M4R = 3,    /* Four Russians with 8-bit lookup tables in shared memory */
+    CFPQ_VARIANT_TC = 4      /* exact tensor-core product (0/1 operands, int accumulators > 0) */
+} cfpq_variant;
+
+/* Closure drivers. */
+typedef enum cfpq_driver {
+    CFPQ_DRIVER_ENGINE = 0,   /* device-resident semi-naive iterations, tile skipping,
+                                 no host round trip per iteration */
+    CFPQ_DRIVER_WORKLIST = 1  /* the reference's host worklist (cfpq-cpp/Grammar.h:58-69):
+                                 one add_mul at a time, changed flag read back each time */
+} cfpq_driver;
+
+typedef struct cfpq_ctx cfpq_ctx;
+typedef struct cfpq_matrix cfpq_matrix;
+
+/* One CNF binary rule head -> body1 body2, as indices into the matrix array
+ * passed to cfpq_closure (the reference's rules vector, cfpq-cpp/Grammar.h:98). */
+typedef struct cfpq_rule {
+    uint32_t head;
+    uint32_t body1;
+    uint32_t body2;
+} cfpq_rule;
+
+typedef struct cfpq_closure_opts {
+    int32_t driver;          /* cfpq_driver */
+    int32_t variant;         /* cfpq_variant used for every product, or AUTO */
+    int32_t max_iterations;  /* 0 = until the fixpoint */
+    int32_t use_graph;       /* 1 = run the iteration loop as one CUDA graph with a
+                                device-side while condition (ENGINE driver only) */
+    int32_t log_products;    /* 1 = record a per-product timing log (see cfpq_product_log) */
+    int32_t reserved[3];
+} cfpq_closure_opts;
+
+typedef struct cfpq_closure_stats {
+    uint32_t iterations;        /* ENGINE: device iterations run; WORKLIST: 0 */
+    uint32_t reserved0;
+    uint64_t products;          /* rule products launched (ENGINE: non-empty product terms) */
+    uint64_t tile_triples;      /* 64x64x64 bit tile products executed */
+    uint64_t work_items;        /* output blocks processed by product kernels */
+    uint64_t dense_bitops;      /* sum over products of n^3 (dense-equivalent bit-MACs) */
+    double device_ms;           /* device time of the closure (CUDA events) */
+    uint64_t kernel_launches;   /* kernels launched by this call */
+    uint64_t variant_items[5];  /* work items per cfpq_variant */
+} cfpq_closure_stats;
+
+/* ---- context ------------------------------------------------------------ */
+
+/* Replaces the implicit per-process CUDA state of the reference backends
+ * (static gpuMatrix::N / tmp_matrix, cuda/naive-gpu/GpuMatrix.h:15-16;
+ * MethodOf4RusMatricesEnv, methodOf4RusBooleanSemiringMatrix.h:11-26). */
+int cfpq_ctx_create(int device, cfpq_ctx **out);
+int cfpq_ctx_destroy(cfpq_ctx *ctx);
+/* Waits for all work issued on the context's stream. */
+int cfpq_ctx_synchronize(cfpq_ctx *ctx);
+/* Number of SMs of the context's device. */
+int cfpq_ctx_num_sms(const cfpq_ctx *ctx);
+/* Description of the last error on this thread ("" if none). */
+const char *cfpq_last_error(void);
+/* Library ABI version (CFPQ_B200_ABI_VERSION). */
+int cfpq_abi_version(void);
+
+/* ---- matrices ----------------------------------------------------------- */
+
+/* Allocates a zero n x n matrix on the device.  Replaces
+ * gpu_lib::device_matrix_alloc + host_matrix_calloc
+ * (cuda/naive-gpu/Multiplication.cu:103-119) and
+ * gpu_m4ri::allocate_matrix_device (gpuMemoryManagement.cu:51-55). */
+int cfpq_matrix_create(cfpq_ctx *ctx, uint32_t n, cfpq_matrix **out);
+int cfpq_matrix_destroy(cfpq_ctx *ctx, cfpq_matrix *m);
+uint32_t cfpq_matrix_size(const cfpq_matrix *m);
+
+/* Sets bits (rows[i], cols[i]) from host arrays; the arrays are copied to the
+ * device and scattered there.  Replaces the per-bit Matrix::set_bit calls of the
+ * driver's initialisation (cfpq-cpp/Grammar.h:41-45, gpuMatrix::set_bit
+ * cuda/naive-gpu/GpuMatrix.cpp:15-18) followed by the H2D transfer of
+ * environment_preprocessing (cuda/naive-gpu/GpuMatrix.cpp:56-64). */
+int cfpq_matrix_set_bits(cfpq_ctx *ctx, cfpq_matrix *m, const uint32_t *rows,
+                         const uint32_t *cols, size_t count);
+/* Same, with the coordinate arrays already in device memory. */
+int cfpq_matrix_set_bits_device(cfpq_ctx *ctx, cfpq_matrix *m, const uint32_t *d_rows,
+                                const uint32_t *d_cols, size_t count);
+/* Initialises all nonterminal matrices of a query from its edge list in one
+ * host->device copy and one scatter kernel: edge e (from[e], label[e], to[e])
+ * sets bit (from[e], to[e]) in every matrix listed for its label, where the
+ * matrices of label l are label_mats[label_offsets[l] .. label_offsets[l+1]-1]
+ * (indices into mats).  Labels >= nlabels are ignored, like graph labels that
+ * no terminal rule derives.  Replaces the edge loop of
+ * Grammar::intersection_with_graph (cfpq-cpp/Grammar.h:41-45) and the H2D
+ * upload of environment_preprocessing (cuda/naive-gpu/GpuMatrix.cpp:56-64). */
+int cfpq_load_edges(cfpq_ctx *ctx, cfpq_matrix *const *mats, size_t nmats, const uint32_t *from,
+                    const uint32_t *label, const uint32_t *to, size_t nedges, const uint32_t *label_offsets,
+                    const uint32_t *label_mats, uint32_t nlabels);
+/* Sets the diagonal (epsilon nonterminals, cfpq-cpp/Grammar.h:47-51). */
+int cfpq_matrix_set_diagonal(cfpq_ctx *ctx, cfpq_matrix *m);
+/* Clears all bits. */
+int cfpq_matrix_clear(cfpq_ctx *ctx, cfpq_matrix *m);
+/* Copies all bits of src into dst (same n). */
+int cfpq_matrix_copy(cfpq_ctx *ctx, cfpq_matrix *dst, const cfpq_matrix *src);
+
+/* Host row-bits exchange: n * ceil(n/64) words.  Replaces
+ * gpu_lib::cpu_to_gpu_transfer_async / gpu_to_cpu_transfer_async
+ * (cuda/naive-gpu/Multiplication.cu:125-131) and the host mirror that
+ * Matrix::get_bit reads (cuda/naive-gpu/GpuMatrix.cpp:20-23). */
+int cfpq_matrix_upload_rows(cfpq_ctx *ctx, cfpq_matrix *m, const uint64_t *host_rows);
+int cfpq_matrix_download_rows(cfpq_ctx *ctx, const cfpq_matrix *m, uint64_t *host_rows);
+
+/* Reference result line for one matrix: the polynomial row hash (bases 11 and
+ * 13 modulo 1e9+7) and the number of set bits, computed on the device.
+ * Replaces the O(n^2) get_bit loop of Grammar::print_results
+ * (cfpq-cpp/Grammar.cpp:81-100). */
+int cfpq_matrix_hash_count(cfpq_ctx *ctx, const cfpq_matrix *m, uint64_t *hash,
+                           uint64_t *count);
+/* Number of set bits only. */
+int cfpq_matrix_count(cfpq_ctx *ctx, const cfpq_matrix *m, uint64_t *count);
+/* hash/count of several matrices with one synchronisation. */
+int cfpq_hash_count_many(cfpq_ctx *ctx, cfpq_matrix *const *mats, size_t nmats, uint64_t *hashes,
+                         uint64_t *counts);
+
+/* ---- products and closure ----------------------------------------------- */
+
+/* c |= a * b over the Boolean semiring; *changed = 1 if any bit of c changed.
+ * a and/or b may be c: the product then uses their values from before the
+ * call.  Replaces Matrix::add_mul (cfpq-cpp/Matrix.h:17) as implemented by
+ * gpu_lib::matrix_product_add_wrapper (cuda/naive-gpu/Multiplication.cu:145-166)
+ * and gpu_m4ri::wrapper_method_of_4rus_bool_semiring
+ * (cuda/methodOf4RusBooleanSemiringGpu/methodOf4RusBooleanSemiringGpu.cu:133-178).
+ * Synchronous: returns after the product is done and the flag is read. */
+int cfpq_add_mul(cfpq_ctx *ctx, cfpq_matrix *c, const cfpq_matrix *a, const cfpq_matrix *b,
+                 int variant, int *changed);
+
+/* Runs the whole fixpoint "mats[head] |= mats[body1] * mats[body2] for every
+ * rule until nothing changes" on the device.  Replaces the worklist loop of
+ * Grammar::intersection_with_graph (cfpq-cpp/Grammar.h:58-69).  All matrices
+ * must have the same n.  opts and stats may be NULL. */
+int cfpq_closure(cfpq_ctx *ctx, const cfpq_rule *rules, size_t nrules, cfpq_matrix *const *mats,
+                 size_t nmats, const cfpq_closure_opts *opts, cfpq_closure_stats *stats);
+
+/* One independent query of a batch: its rules index into its own matrices. */
+typedef struct cfpq_query {
+    const cfpq_rule *rules;
+    size_t nrules;
+    cfpq_matrix *const *mats;
+    size_t nmats;
+} cfpq_query;
+
+/* Closes many independent queries (matrices of different n allowed) together:
+ * every iteration runs the products of all unfinished queries in one grouped
+ * launch.  iterations_out[q] (optional) receives the iteration after which
+ * query q stopped changing, done_ms_out[q] (optional) the device time from the
+ * start of the batch until the end of that iteration.  No reference
+ * counterpart (the reference runs one query per process, runners.py:22-30). */
+int cfpq_closure_batch(cfpq_ctx *ctx, const cfpq_query *queries, size_t nqueries,
+                       const cfpq_closure_opts *opts, cfpq_closure_stats *stats,
+                       uint32_t *iterations_out, double *done_ms_out);
+
+/* Per-product log of the last cfpq_closure / cfpq_closure_batch call with
+ * opts->log_products = 1: one record per work-item group.  Returns the number
+ * of records available; copies at most cap records.  No reference
+ * counterpart (the reference only times the whole closure, Grammar.h:53-80). */
+typedef struct cfpq_product_record {
+    uint32_t iteration;
+    uint32_t query;
+    uint32_t rule;
+    uint32_t term;          /* 0: delta(body1) * body2, 1: body1 * delta(body2) */
+    uint32_t n;
+    uint32_t variant;
+    uint64_t p_tiles;       /* occupied tiles of the left operand */
+    uint64_t q_tiles;       /* occupied tiles of the right operand */
+    uint64_t c_tiles;       /* occupied tiles of the head before the product */
+    uint64_t tile_triples;  /* tile products executed */
+    float usec;             /* device time of the product (CUDA events) */
+    float reserved;
+} cfpq_product_record;
+size_t cfpq_product_log(cfpq_ctx *ctx, cfpq_product_record *out, size_t cap);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CFPQ_B200_H */

@@ -1,0 +1,234 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle.
+
+Bit-exact comparisons: whole matrices (row bits), changed flags and the
+reference result lines (name, hash, count)."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [1, 2, 63, 64, 65, 127, 130, 257, 640, 1000, 1100]
+
+
+def rand_rows(rng, n, density):
+    wpr = (n + 63) // 64
+    bits = rng.random((n, wpr * 64)) < density
+    bits[:, n:] = False
+    return np.packbits(bits, axis=1, bitorder="little").view(np.uint64).reshape(n, wpr).copy()
+
+
+def upload(ctx, n, rows):
+    m = ctx.matrix(n)
+    m.upload_rows(rows)
+    return m
+
+
+@pytest.mark.parametrize("variant", ["plain", "lop3"])
+@pytest.mark.parametrize("n", SIZES)
+def test_add_mul_random(ctx, oracle, variant, n):
+    rng = np.random.default_rng(n * 7 + len(variant))
+    for density in (0.002, 0.05, 0.4):
+        a, b, c = (rand_rows(rng, n, d) for d in (density, density, density / 2))
+        ma, mb, mc = upload(ctx, n, a), upload(ctx, n, b), upload(ctx, n, c)
+        exp = c.copy()
+        ch_exp = oracle.add_mul(exp, a, b, n, oracle.NAIVE, 1)
+        ch = ctx.add_mul(mc, ma, mb, variant)
+        got = mc.download_rows()
+        assert np.array_equal(got, exp), f"n={n} density={density}"
+        assert ch == ch_exp
+        # a second identical product cannot change anything
+        assert ctx.add_mul(mc, ma, mb, variant) is False
+        for m in (ma, mb, mc):
+            m.destroy()
+
+
+@pytest.mark.parametrize("variant", ["plain", "lop3"])
+@pytest.mark.parametrize("alias", ["a", "b", "ab"])
+def test_add_mul_aliasing(ctx, oracle, variant, alias):
+    n = 200
+    rng = np.random.default_rng(11)
+    a, b, c = rand_rows(rng, n, 0.03), rand_rows(rng, n, 0.03), rand_rows(rng, n, 0.03)
+    mc = upload(ctx, n, c)
+    if alias == "a":
+        ma, mb = mc, upload(ctx, n, b)
+        exp = c.copy()
+        ch_exp = oracle.add_mul(exp, c.copy(), b, n)
+    elif alias == "b":
+        ma, mb = upload(ctx, n, a), mc
+        exp = c.copy()
+        ch_exp = oracle.add_mul(exp, a, c.copy(), n)
+    else:
+        ma = mb = mc
+        exp = c.copy()
+        ch_exp = oracle.add_mul(exp, c.copy(), c.copy(), n)
+    ch = ctx.add_mul(mc, ma, mb, variant)
+    assert np.array_equal(mc.download_rows(), exp)
+    assert ch == ch_exp
+
+
+@pytest.mark.parametrize("n", [1, 64, 65, 300, 1024])
+def test_hash_count(ctx, oracle, n):
+    rng = np.random.default_rng(n)
+    for density in (0.0, 0.01, 0.5, 1.0):
+        rows = rand_rows(rng, n, density)
+        m = upload(ctx, n, rows)
+        assert m.hash_count() == oracle.hash_count(rows, n)
+        m.destroy()
+
+
+def test_upload_download_roundtrip(ctx):
+    rng = np.random.default_rng(3)
+    for n in (1, 64, 77, 1000):
+        rows = rand_rows(rng, n, 0.3)
+        m = upload(ctx, n, rows)
+        assert np.array_equal(m.download_rows(), rows)
+        m.destroy()
+
+
+def test_set_bits_and_diagonal(ctx, oracle):
+    n = 333
+    rng = np.random.default_rng(5)
+    r = rng.integers(0, n, 500)
+    c = rng.integers(0, n, 500)
+    m = ctx.matrix(n)
+    m.set_bits(r, c)
+    m.set_diagonal()
+    exp = np.zeros((n, (n + 63) // 64), dtype=np.uint64)
+    for i, j in list(zip(r, c)) + [(i, i) for i in range(n)]:
+        exp[i, j // 64] |= np.uint64(1) << np.uint64(j % 64)
+    assert np.array_equal(m.download_rows(), exp)
+    m.destroy()
+
+
+def test_set_bits_out_of_range_is_an_error(ctx, pkg):
+    m = ctx.matrix(10)
+    with pytest.raises(pkg.capi.CfpqError) as e:
+        m.set_bits([1, 10], [2, 3])
+    assert e.value.code == pkg.capi.ERR_INVALID
+    m.destroy()
+
+
+def _write(wl, tmp_path):
+    gp, rp = str(tmp_path / "grammar.txt"), str(tmp_path / "graph.txt")
+    wl.write(gp, rp)
+    return gp, rp
+
+
+def _oracle_run(oracle, gp, rp):
+    with oracle.Problem(gp, rp) as p:
+        p.closure(oracle.M4RM, 0)
+        return p.results(), [p.matrix(i) for i in range(len(p.names))], p.names
+
+
+def _check_query(ctx, pkg, oracle, wl, tmp_path, **kw):
+    gp, rp = _write(wl, tmp_path)
+    exp_lines, exp_mats, names = _oracle_run(oracle, gp, rp)
+    q = pkg.query.PreparedQuery(ctx, wl.grammar, wl.graph)
+    try:
+        res = q.run(**kw)
+        assert res.lines == exp_lines
+        assert q.grammar.nonterminals == names
+        for i, m in enumerate(q.mats):
+            assert np.array_equal(m.download_rows(), exp_mats[i]), names[i]
+        return res
+    finally:
+        q.close()
+
+
+@pytest.mark.parametrize("kw", [dict(driver="engine", use_graph=True), dict(driver="engine", use_graph=False),
+                                dict(driver="worklist", variant="plain"),
+                                dict(driver="worklist", variant="lop3")])
+def test_closure_brackets_full_size(ctx, pkg, oracle, tmp_path, kw):
+    wl = pkg.workloads.brackets_query()  # N=1024, 4096 edges
+    res = _check_query(ctx, pkg, oracle, wl, tmp_path, **kw)
+    if kw["driver"] == "engine":
+        assert res.stats["iterations"] > 1
+
+
+@pytest.mark.parametrize("n,seed", [(512, 3), (2048, 4), (8192, 1)])
+def test_closure_same_generation(ctx, pkg, oracle, tmp_path, n, seed):
+    wl = pkg.workloads.ontology_query(n, seed)
+    _check_query(ctx, pkg, oracle, wl, tmp_path)
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_closure_random_cnf(ctx, pkg, oracle, tmp_path, seed):
+    labels = ["x", "y", "z"]
+    g = pkg.workloads.uniform_graph(700, 1400, labels, seed)
+    gram = pkg.workloads.random_cnf(8, 20, labels, seed)
+    wl = pkg.workloads.Workload("random_cnf", gram, g, {})
+    _check_query(ctx, pkg, oracle, wl, tmp_path)
+
+
+def test_closure_epsilon_and_self_loops(ctx, pkg, oracle, tmp_path):
+    gram = "S\nS S S\nS A S\nA a\nB S B\nB b\n"
+    g = pkg.workloads.uniform_graph(150, 200, ["a", "b"], 9)
+    wl = pkg.workloads.Workload("eps", gram, g, {})
+    _check_query(ctx, pkg, oracle, wl, tmp_path)
+
+
+def test_closure_repeated_runs_are_identical(ctx, pkg, oracle, tmp_path):
+    wl = pkg.workloads.ontology_query(1024, 5)
+    gp, rp = _write(wl, tmp_path)
+    exp_lines, _, _ = _oracle_run(oracle, gp, rp)
+    q = pkg.query.PreparedQuery(ctx, wl.grammar, wl.graph)
+    try:
+        for _ in range(3):
+            assert q.run().lines == exp_lines
+    finally:
+        q.close()
+
+
+def test_batch_matches_single_queries(ctx, pkg, oracle, tmp_path):
+    wls = [w for w in pkg.workloads.batch_queries(24, seed=5, n_min=64, n_max=900)]
+    qs, exps = [], []
+    for i, wl in enumerate(wls):
+        d = tmp_path / f"q{i}"
+        d.mkdir()
+        gp, rp = _write(wl, d)
+        exps.append(_oracle_run(oracle, gp, rp)[0])
+        q = pkg.query.PreparedQuery(ctx, wl.grammar, wl.graph)
+        q.load()
+        qs.append(q)
+    stats, iters, done = ctx.closure_batch([(q.grammar.rules, q.mats) for q in qs])
+    try:
+        for q, exp in zip(qs, exps):
+            got = dict(zip(q.grammar.nonterminals, ctx.hash_count_many(q.mats)))
+            assert got == exp
+        assert stats["iterations"] >= int(iters.max())
+        assert (done >= 0).all()
+    finally:
+        for q in qs:
+            q.close()
+
+
+def test_b200gpu_executable(pkg, oracle, tmp_path):
+    exe = os.path.join(os.path.dirname(pkg.capi.LIB_PATH), "..", "bin", "b200GPU")
+    wl = pkg.workloads.brackets_query(n=512, nedges=2048, seed=3)
+    gp, rp = _write(wl, tmp_path)
+    exp, _, _ = _oracle_run(oracle, gp, rp)
+    for env in ({}, {"CFPQ_DRIVER": "worklist", "CFPQ_VARIANT": "plain"}):
+        got, (total, algo) = oracle.run_executable(exe, gp, rp, env={**os.environ, **env})
+        assert got == exp
+        assert total >= algo >= 0
+
+
+@pytest.mark.parametrize("exe", ["naiveGPU", "m4riGPU"])
+def test_reference_gpu_backends_agree(pkg, oracle, tmp_path, exe):
+    """The reference's own CUDA backends (built from its sources for sm_100a)
+    give the same answers as the oracle on inputs whose rules never alias
+    head and body (the reference naive backend's aliased path reads an
+    uninitialised temporary, cuda/naive-gpu/Multiplication.cu:151-158)."""
+    path = oracle.ref_executable(exe)
+    if path is None:
+        pytest.skip(f"oracle/_ref/{exe} not built")
+    for wl in (pkg.workloads.brackets_query(), pkg.workloads.ontology_query(2048, 2)):
+        d = tmp_path / wl.name
+        d.mkdir()
+        gp, rp = _write(wl, d)
+        exp, _, _ = _oracle_run(oracle, gp, rp)
+        got, _ = oracle.run_executable(path, gp, rp)
+        assert got == exp
