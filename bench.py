@@ -1,0 +1,379 @@
+#!/usr/bin/env python
+"""CFPQ closure benchmark on B200.
+
+Workload (one step = one whole CFPQ query on one GPU): the same-generation
+query on a seeded ontology-like graph, N = 8192 vertices, 4 labels
+(subClassOf, type and their inverses), mean out-degree ~3, subClassOf DAG of
+depth <= 12, CNF grammar with 7 nonterminals and 6 binary rules.  Synthetic
+data (the reference's RDF datasets are not available).
+
+  value  closures/s with the edge list resident in HBM: every step clears the
+         nonterminal matrices, scatters the edges on the device and runs the
+         closure to its fixpoint (CUDA-graph loop); device time from CUDA
+         events on the library's stream; L2 flushed (256 MiB write) between
+         steps; max over ranks.
+  e2e    the same through the C ABI from pinned host buffers: H2D of the edge
+         list, closure, and the D2H of the result lines (hash, count per
+         nonterminal) inside the timed region.
+
+Multi-GPU (torchrun): one process per GPU, each closes its own seeded query
+(query-partitioned replicas, weak scaling, no data-path collective).
+
+--impl reference times the reference's CPU path on the host cores: the
+reference's own m4riCPU driver (cfpq-cpp + m4ri backend sources) linked with
+the restated libm4ri subset (oracle/_ref/m4riCPU), all host threads.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_VERTICES = 8192
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-profile", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks() -> dict:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return {"hbm_gbs": d.get("hbm_gbs", 6650.0), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def committed_traffic() -> dict:
+    """ncu DRAM traffic per launch of the product kernel, scaled to the bench
+    workload (profiles/traffic.json, written from an ncu capture)."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return {}
+
+
+def reference_arm(args, world, rank):
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle  # reference / oracle executables only
+
+    pkg = importlib.import_module("cfpq-on-gpgpu_b200")
+    wl = pkg.workloads.ontology_query(N_VERTICES, args.seed)
+    exe = oracle.ref_executable("m4riCPU")
+    threads = os.cpu_count() or 1
+    env = {**os.environ, "OMP_NUM_THREADS": str(threads)}
+    with tempfile.TemporaryDirectory() as d:
+        gp, rp = os.path.join(d, "grammar.txt"), os.path.join(d, "graph.txt")
+        wl.write(gp, rp)
+        if exe is None:
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/m4riCPU not built"}))
+            return
+        times = []
+        for i in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            _, (total, algo) = oracle.run_executable(exe, gp, rp, env=env)
+            dt = time.perf_counter() - t0
+            if i >= args.warmup:
+                times.append(algo / 1e3 if algo > 0 else dt)
+    total_s = sum(times)
+    value = len(times) / total_s
+    line = {
+        "impl": "reference", "metric": "CFPQ closure throughput (same-generation query, N=8192)",
+        "value": value, "unit": "closures/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total_s / len(times), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u64 (bit-packed Boolean)", "data": "synthetic",
+        "config": {"workload": "same_generation_ontology_n8192", "n": N_VERTICES, "seed": args.seed,
+                   "edges": wl.graph.nedges},
+        "cpu_baseline": {"value": value, "unit": "closures/s", "cores": threads, "kind": "reference",
+                         "sample": f"{len(times)} full closures of the workload (algorithm time printed by "
+                                   "the reference m4riCPU main, restated libm4ri M4RM, OpenMP)"},
+        "e2e": {"value": value, "unit": "closures/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def cpu_baseline(wl, budget_s=12.0) -> dict:
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    exe = oracle.ref_executable("m4riCPU")
+    threads = os.cpu_count() or 1
+    with tempfile.TemporaryDirectory() as d:
+        gp, rp = os.path.join(d, "grammar.txt"), os.path.join(d, "graph.txt")
+        wl.write(gp, rp)
+        times, answer = [], None
+        t_start = time.perf_counter()
+        while time.perf_counter() - t_start < budget_s or not times:
+            if exe:
+                answer, (_, algo) = oracle.run_executable(exe, gp, rp,
+                                                          env={**os.environ, "OMP_NUM_THREADS": str(threads)})
+                times.append(max(algo, 1) / 1e3)
+            else:
+                with oracle.Problem(gp, rp) as p:
+                    times.append(p.closure(oracle.M4RM, threads) / 1e3)
+                    answer = p.results()
+            if len(times) >= 50:
+                break
+    kind = "reference" if exe else "port"
+    return {"value": len(times) / sum(times), "unit": "closures/s", "cores": threads, "kind": kind,
+            "sample": f"{len(times)} full closures of the same workload, algorithm time, "
+                      f"{'reference m4riCPU main + restated libm4ri' if exe else 'oracle M4RM port'}",
+            "answer": answer}
+
+
+def ours_arm(args, world, rank, local):
+    import numpy as np
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+
+        dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                    device_id=torch.device("cuda", local))
+        dist = dist_mod
+    pkg = importlib.import_module("cfpq-on-gpgpu_b200")
+    capi, query = pkg.capi, pkg.query
+    wl = pkg.workloads.ontology_query(N_VERTICES, args.seed + rank)
+    grammar, graph = wl.grammar, wl.graph
+    ctx = capi.Context(local)
+    q = query.PreparedQuery(ctx, grammar, graph)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    # device-resident edge list (value) and pinned host copy (e2e)
+    d_src = torch.from_numpy(graph.src.view(np.int32)).cuda()
+    d_lab = torch.from_numpy(graph.label.view(np.int32)).cuda()
+    d_dst = torch.from_numpy(graph.dst.view(np.int32)).cuda()
+    h_src = torch.from_numpy(graph.src.view(np.int32)).pin_memory().numpy().view(np.uint32)
+    h_lab = torch.from_numpy(graph.label.view(np.int32)).pin_memory().numpy().view(np.uint32)
+    h_dst = torch.from_numpy(graph.dst.view(np.int32)).pin_memory().numpy().view(np.uint32)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > 126 MB L2
+
+    launches = {"n": 0}
+
+    def step_value():
+        for m in q.mats:
+            m.clear()
+        ctx.load_edges_device(q.mats, d_src.data_ptr(), d_lab.data_ptr(), d_dst.data_ptr(), graph.nedges,
+                              q.off, q.lm)
+        for e in grammar.epsilon:
+            q.mats[e].set_diagonal()
+        st = ctx.closure(grammar.rules, q.mats, use_graph=True)
+        launches["n"] += 1 + len(grammar.epsilon) + st["kernel_launches"]
+        return st
+
+    def step_e2e():
+        for m in q.mats:
+            m.clear()
+        ctx.load_edges(q.mats, h_src, h_lab, h_dst, q.off, q.lm)
+        for e in grammar.epsilon:
+            q.mats[e].set_diagonal()
+        st = ctx.closure(grammar.rules, q.mats, use_graph=True)
+        return st, ctx.hash_count_many(q.mats)
+
+    def timed(fn, k):
+        times, last = [], None
+        for _ in range(k):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            last = fn()
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+            flush.zero_()
+            torch.cuda.synchronize()
+        return times, last
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # correctness gate on this rank's instance: device result == host result of the first closure
+    for _ in range(args.warmup):
+        step_value()
+    barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    launches["n"] = 0
+    times, st = timed(step_value, args.steps)
+    clocks = sampler.stop()
+    barrier()
+    total_ms = max_over_ranks(sum(times))
+    gpu_launches = launches["n"]
+    value = world * args.steps / (total_ms / 1e3)
+
+    # end to end through the C ABI with host buffers
+    for _ in range(max(1, args.warmup // 2)):
+        step_e2e()
+    barrier()
+    e2e_times, (st_e2e, lines) = timed(step_e2e, args.steps)
+    barrier()
+    e2e_total = max_over_ranks(sum(e2e_times))
+    e2e_value = world * args.steps / (e2e_total / 1e3)
+    h2d = 3 * 4 * graph.nedges + 4 * (q.off.size + q.lm.size)
+    d2h = 16 * len(q.mats)
+
+    # per-kernel device times (instrumented pass: every launch bracketed by events)
+    roofline, prof = None, None
+    if not args.no_profile:
+        for m in q.mats:
+            m.clear()
+        ctx.load_edges_device(q.mats, d_src.data_ptr(), d_lab.data_ptr(), d_dst.data_ptr(), graph.nedges,
+                              q.off, q.lm)
+        pst = ctx.closure(grammar.rules, q.mats, use_graph=False, log_products=capi.LOG_KERNELS)
+        prof = ctx.kernel_profile()
+        peaks = measured_peaks()
+        kern = {"product": prof["product_ms"], "plan": prof["plan_ms"], "advance": prof["advance_ms"],
+                "iter_end": prof["iter_end_ms"]}
+        launches_p = max(1, prof["product_launches"])
+        avg_ms = prof["product_ms"] / launches_p
+        alg_bytes = (pst["bytes_staged"] + 16 * pst["out_words"] + 8 * pst["new_words"]) / launches_p
+        achieved = alg_bytes / (avg_ms / 1e3) / 1e9 if avg_ms > 0 else 0.0
+        tr = committed_traffic().get("product_bytes_per_launch")
+        roofline = {"kernel": "k_product_lop3", "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
+                    "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": tr,
+                    "peak_source": peaks["source"], "avg_launch_ms": avg_ms,
+                    "algorithmic_bytes_per_launch": alg_bytes,
+                    "kernel_ms": kern, "dominant": max(kern, key=kern.get)}
+
+    out = None
+    if rank == 0:
+        out = {
+            "metric": "CFPQ closure throughput (same-generation query, N=8192)",
+            "value": value, "unit": "closures/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64 (bit-packed Boolean)",
+            "data": "synthetic (seeded ontology-like graph, MT19937)",
+            "config": {"workload": "same_generation_ontology_n8192", "n": N_VERTICES, "edges": graph.nedges,
+                       "nonterminals": len(grammar.nonterminals), "rules": len(grammar.rules),
+                       "seed": args.seed, "l2": "flushed between steps (256 MiB write)",
+                       "parallelism": f"query-partitioned x{world}"},
+            "clocks": clocks,
+            "e2e": {"value": e2e_value, "unit": "closures/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": gpu_launches,
+            "roofline": roofline,
+            "closure": {"iterations": st["iterations"], "products": st["products"], "work_items": st["work_items"],
+                        "tile_triples": st["tile_triples"], "device_ms_last": st["device_ms"],
+                        "dense_equiv_gbitops": st["dense_bitops"] / (total_ms / args.steps / 1e3) / 1e9,
+                        "result": {k: list(v) for k, v in zip(grammar.nonterminals, lines)}},
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            cb = cpu_baseline(wl)
+            answer = cb.pop("answer")
+            out["cpu_baseline"] = cb
+            out["closure"]["parity_vs_cpu"] = answer == {k: tuple(v) for k, v in zip(grammar.nonterminals, lines)}
+        print(json.dumps(out))
+    q.close()
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse_args()
+    world, rank, local = dist_env()
+    if args.impl == "reference":
+        reference_arm(args, world, rank)
+        return
+    ours_arm(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

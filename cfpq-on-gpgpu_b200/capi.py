@@ -29,7 +29,9 @@ EXPORTED = (
     "cfpq_matrix_set_bits_device", "cfpq_load_edges", "cfpq_matrix_set_diagonal", "cfpq_matrix_clear",
     "cfpq_matrix_copy", "cfpq_matrix_upload_rows", "cfpq_matrix_download_rows", "cfpq_matrix_hash_count",
     "cfpq_matrix_count", "cfpq_hash_count_many", "cfpq_add_mul", "cfpq_closure", "cfpq_closure_batch",
-    "cfpq_product_log",
+    "cfpq_product_log", "cfpq_last_kernel_profile", "cfpq_ctx_stream", "cfpq_load_edges_device",
+    "cfpq_matrix_tile_stats", "cfpq_order_create", "cfpq_order_destroy", "cfpq_order_suggest",
+    "cfpq_matrix_create_ordered",
 )
 
 
@@ -52,12 +54,26 @@ class ClosureStats(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_uint32), ("reserved0", ctypes.c_uint32), ("products", ctypes.c_uint64),
                 ("tile_triples", ctypes.c_uint64), ("work_items", ctypes.c_uint64),
                 ("dense_bitops", ctypes.c_uint64), ("device_ms", ctypes.c_double),
-                ("kernel_launches", ctypes.c_uint64), ("variant_items", ctypes.c_uint64 * 5)]
+                ("kernel_launches", ctypes.c_uint64), ("variant_items", ctypes.c_uint64 * 5),
+                ("bytes_staged", ctypes.c_uint64), ("out_words", ctypes.c_uint64), ("new_words", ctypes.c_uint64)]
 
     def as_dict(self) -> dict:
         d = {k: getattr(self, k) for k, _ in self._fields_ if not k.startswith("reserved")}
         d["variant_items"] = list(self.variant_items)
         return d
+
+
+class KernelProfile(ctypes.Structure):
+    _fields_ = [("plan_ms", ctypes.c_double), ("product_ms", ctypes.c_double), ("advance_ms", ctypes.c_double),
+                ("iter_end_ms", ctypes.c_double), ("plan_launches", ctypes.c_uint64),
+                ("product_launches", ctypes.c_uint64), ("advance_launches", ctypes.c_uint64),
+                ("iter_end_launches", ctypes.c_uint64)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+LOG_KERNELS, LOG_PRODUCTS = 1, 2
 
 
 class Query(ctypes.Structure):
@@ -112,6 +128,14 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "cfpq_closure_batch": ([vp, P(Query), sz, P(ClosureOpts), P(ClosureStats), P(u32),
                                 P(ctypes.c_double)], i32),
         "cfpq_product_log": ([vp, P(ProductRecord), sz], sz),
+        "cfpq_last_kernel_profile": ([vp, P(KernelProfile)], i32),
+        "cfpq_ctx_stream": ([vp], vp),
+        "cfpq_matrix_tile_stats": ([vp, vp, vp, vp], i32),
+        "cfpq_order_create": ([vp, u32, vp, P(vp)], i32),
+        "cfpq_order_destroy": ([vp, vp], i32),
+        "cfpq_order_suggest": ([u32, vp, vp, vp, sz, vp], i32),
+        "cfpq_matrix_create_ordered": ([vp, u32, vp, P(vp)], i32),
+        "cfpq_load_edges_device": ([vp, P(vp), sz, vp, vp, vp, sz, vp, vp, u32], i32),
     }
     for name, (args, res) in sigs.items():
         f = getattr(lib, name)
@@ -131,13 +155,42 @@ def _ptr(a: np.ndarray) -> ctypes.c_void_p:
     return ctypes.c_void_p(a.ctypes.data)
 
 
+def suggest_order(n: int, src: np.ndarray, label: np.ndarray, dst: np.ndarray, lib=None) -> np.ndarray:
+    """Vertex relabeling suggested by the library's heuristic (perm[v] = internal id)."""
+    lib = lib or load_library()
+    s = np.ascontiguousarray(src, dtype=np.uint32)
+    l = np.ascontiguousarray(label, dtype=np.uint32)
+    d = np.ascontiguousarray(dst, dtype=np.uint32)
+    perm = np.zeros(max(int(n), 1), dtype=np.uint32)
+    _check(lib, lib.cfpq_order_suggest(int(n), _ptr(s), _ptr(l), _ptr(d), s.size, _ptr(perm)))
+    return perm[:int(n)]
+
+
+class Order:
+    """A vertex relabeling shared by the matrices of one query."""
+
+    def __init__(self, ctx: "Context", perm: np.ndarray):
+        self.ctx = ctx
+        self.perm = np.ascontiguousarray(perm, dtype=np.uint32)
+        self.n = int(self.perm.size)
+        h = ctypes.c_void_p()
+        _check(ctx.lib, ctx.lib.cfpq_order_create(ctx.handle, self.n, _ptr(self.perm), ctypes.byref(h)))
+        self.handle = h
+
+    def destroy(self) -> None:
+        if self.handle:
+            _check(self.ctx.lib, self.ctx.lib.cfpq_order_destroy(self.ctx.handle, self.handle))
+            self.handle = None
+
+
 class Matrix:
     """An n x n Boolean matrix resident on the device."""
 
-    def __init__(self, ctx: "Context", n: int):
-        self.ctx, self.n = ctx, int(n)
+    def __init__(self, ctx: "Context", n: int, order: Order | None = None):
+        self.ctx, self.n, self.order = ctx, int(n), order
         h = ctypes.c_void_p()
-        _check(ctx.lib, ctx.lib.cfpq_matrix_create(ctx.handle, self.n, ctypes.byref(h)))
+        _check(ctx.lib, ctx.lib.cfpq_matrix_create_ordered(ctx.handle, self.n, order.handle if order else None,
+                                                           ctypes.byref(h)))
         self.handle = h
 
     @property
@@ -171,6 +224,16 @@ class Matrix:
         if self.n:
             _check(self.ctx.lib, self.ctx.lib.cfpq_matrix_download_rows(self.ctx.handle, self.handle, _ptr(a)))
         return a
+
+    def tile_stats(self) -> tuple[np.ndarray, np.ndarray]:
+        """(occupancy bitmap [T, ceil(T/32)] uint32, tile populations [T, T] uint32)."""
+        T = (self.n + 63) // 64
+        occ = np.zeros((T, (T + 31) // 32), dtype=np.uint32)
+        nnz = np.zeros((T, T), dtype=np.uint32)
+        if T:
+            _check(self.ctx.lib, self.ctx.lib.cfpq_matrix_tile_stats(self.ctx.handle, self.handle, _ptr(occ),
+                                                                     _ptr(nnz)))
+        return occ, nnz
 
     def hash_count(self) -> tuple[int, int]:
         h, c = ctypes.c_uint64(), ctypes.c_uint64()
@@ -212,8 +275,11 @@ class Context:
     def synchronize(self) -> None:
         _check(self.lib, self.lib.cfpq_ctx_synchronize(self.handle))
 
-    def matrix(self, n: int) -> Matrix:
-        return Matrix(self, n)
+    def matrix(self, n: int, order: Order | None = None) -> Matrix:
+        return Matrix(self, n, order)
+
+    def order(self, perm: np.ndarray) -> Order:
+        return Order(self, perm)
 
     def add_mul(self, c: Matrix, a: Matrix, b: Matrix, variant: int | str = VARIANT_AUTO) -> bool:
         v = VARIANTS[variant] if isinstance(variant, str) else int(variant)
@@ -275,6 +341,28 @@ class Context:
         hs = (ctypes.c_void_p * max(len(mats), 1))(*[m.handle for m in mats])
         _check(self.lib, self.lib.cfpq_load_edges(self.handle, hs, len(mats), _ptr(s), _ptr(l), _ptr(d), s.size,
                                                   _ptr(off), _ptr(lm), off.size - 1))
+
+    @property
+    def stream(self) -> int:
+        """The context's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""
+        return int(self.lib.cfpq_ctx_stream(self.handle) or 0)
+
+    def load_edges_device(self, mats: Sequence[Matrix], d_src: int, d_label: int, d_dst: int, nedges: int,
+                          label_offsets: np.ndarray, label_mats: np.ndarray) -> None:
+        """Edge scatter from device-resident arrays (device pointers as ints)."""
+        off = np.ascontiguousarray(label_offsets, dtype=np.uint32)
+        lm = np.ascontiguousarray(label_mats, dtype=np.uint32)
+        if lm.size == 0:
+            lm = np.zeros(1, dtype=np.uint32)
+        hs = (ctypes.c_void_p * max(len(mats), 1))(*[m.handle for m in mats])
+        _check(self.lib, self.lib.cfpq_load_edges_device(self.handle, hs, len(mats), ctypes.c_void_p(d_src),
+                                                         ctypes.c_void_p(d_label), ctypes.c_void_p(d_dst),
+                                                         int(nedges), _ptr(off), _ptr(lm), off.size - 1))
+
+    def kernel_profile(self) -> dict:
+        p = KernelProfile()
+        _check(self.lib, self.lib.cfpq_last_kernel_profile(self.handle, ctypes.byref(p)))
+        return p.as_dict()
 
     def hash_count_many(self, mats: Sequence[Matrix]) -> list[tuple[int, int]]:
         if not mats:

@@ -111,9 +111,16 @@ struct GraphCache {
 
 }  // namespace
 
+struct cfpq_order {
+    uint32_t n = 0;
+    uint32_t *d_perm = nullptr;
+    PowTables pow;  // hash powers indexed by internal id
+};
+
 struct cfpq_matrix {
     cfpq_ctx *ctx;
     DevMat d;
+    cfpq_order *order = nullptr;
 };
 
 struct cfpq_ctx {
@@ -139,12 +146,24 @@ struct cfpq_ctx {
     GraphCache gcache;
     int lop3_grid = 0;
     std::vector<cfpq_product_record> log;
+    cudaEvent_t kev[5] = {};
+    cfpq_kernel_profile prof = {};
+    void *h_small = nullptr;
+    size_t h_small_cap = 0;
 };
 
 // ---------------------------------------------------------------------------
 // helpers
 
 static inline uint32_t tiles_for(uint32_t n) { return (n + 63) / 64; }
+
+// Upper bound of the work items one product term can emit per iteration:
+// tile-rows x column blocks x inner-dimension groups.
+static inline size_t item_capacity(uint32_t T, int tpb) {
+    const uint32_t ow = (T + 31) / 32;
+    const uint32_t groups = (ow + kgroup_words(ow) - 1) / kgroup_words(ow);
+    return (size_t)T * ((T + tpb - 1) / tpb) * groups;
+}
 
 static int alloc_devmat(uint32_t n, DevMat *d) {
     memset(d, 0, sizeof(*d));
@@ -159,10 +178,14 @@ static int alloc_devmat(uint32_t n, DevMat *d) {
         return set_error(CFPQ_ERR_OOM, "cannot allocate %zu bytes for a %u x %u matrix: %s", bits_bytes, n, n,
                          cudaGetErrorString(e));
     e = cudaMalloc(&d->occ, occ_bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&d->nnz, (size_t)d->T * d->T * 4);
     if (e != cudaSuccess) {
         cudaFree(d->bits);
+        if (d->occ) cudaFree(d->occ);
         d->bits = nullptr;
-        return set_error(CFPQ_ERR_OOM, "cannot allocate occupancy bitmap: %s", cudaGetErrorString(e));
+        d->occ = nullptr;
+        d->nnz = nullptr;
+        return set_error(CFPQ_ERR_OOM, "cannot allocate tile statistics: %s", cudaGetErrorString(e));
     }
     return CFPQ_OK;
 }
@@ -170,8 +193,10 @@ static int alloc_devmat(uint32_t n, DevMat *d) {
 static void free_devmat(DevMat *d) {
     if (d->bits) cudaFree(d->bits);
     if (d->occ) cudaFree(d->occ);
+    if (d->nnz) cudaFree(d->nnz);
     d->bits = nullptr;
     d->occ = nullptr;
+    d->nnz = nullptr;
 }
 
 static int use_device(cfpq_ctx *ctx) {
@@ -213,29 +238,83 @@ static int pool_give(cfpq_ctx *ctx, cfpq_matrix *m, bool dirty) {
     return CFPQ_OK;
 }
 
-static int get_pow_tables(cfpq_ctx *ctx, uint32_t n, PowTables *out) {
+// Hash power tables for vertex ids 0..n-1 stored at internal index perm[v]
+// (identity when perm is null): pow11[perm[c]] = 11^(n-1-c),
+// pow13[perm[r]] = 13^(n-1-r) modulo 1e9+7 (cfpq-cpp/Grammar.cpp:12-14).
+static int make_pow_tables(uint32_t n, const uint32_t *perm, PowTables *t) {
+    const uint32_t np = tiles_for(n) * 64;
+    std::vector<uint32_t> p11(np ? np : 1, 0), p13(np ? np : 1, 0);
+    const uint64_t mod = 1000000007ULL;
+    uint64_t a = 1, b = 1;
+    for (int64_t c = (int64_t)n - 1; c >= 0; --c) {
+        const uint32_t at = perm ? perm[c] : (uint32_t)c;
+        p11[at] = (uint32_t)a;
+        p13[at] = (uint32_t)b;
+        a = a * 11 % mod;
+        b = b * 13 % mod;
+    }
+    CUDA_TRY(cudaMalloc(&t->d_pow11, p11.size() * 4));
+    CUDA_TRY(cudaMalloc(&t->d_pow13, p13.size() * 4));
+    CUDA_TRY(cudaMemcpy(t->d_pow11, p11.data(), p11.size() * 4, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(t->d_pow13, p13.data(), p13.size() * 4, cudaMemcpyHostToDevice));
+    return CFPQ_OK;
+}
+
+static int get_pow_tables(cfpq_ctx *ctx, const cfpq_matrix *m, PowTables *out) {
+    if (m->order) {
+        *out = m->order->pow;
+        return CFPQ_OK;
+    }
+    const uint32_t n = m->d.n;
     auto it = ctx->pow.find(n);
     if (it != ctx->pow.end()) {
         *out = it->second;
         return CFPQ_OK;
     }
-    const uint32_t np = tiles_for(n) * 64;
-    std::vector<uint32_t> p11(np ? np : 1, 0), p13(np ? np : 1, 0);
-    const uint64_t mod = 1000000007ULL;
-    uint64_t a = 1, b = 1;
-    for (int64_t c = (int64_t)n - 1; c >= 0; --c) {  // 11^(n-1-c), 13^(n-1-r)
-        p11[c] = (uint32_t)a;
-        p13[c] = (uint32_t)b;
-        a = a * 11 % mod;
-        b = b * 13 % mod;
-    }
     PowTables t;
-    CUDA_TRY(cudaMalloc(&t.d_pow11, p11.size() * 4));
-    CUDA_TRY(cudaMalloc(&t.d_pow13, p13.size() * 4));
-    CUDA_TRY(cudaMemcpy(t.d_pow11, p11.data(), p11.size() * 4, cudaMemcpyHostToDevice));
-    CUDA_TRY(cudaMemcpy(t.d_pow13, p13.data(), p13.size() * 4, cudaMemcpyHostToDevice));
+    TRY(make_pow_tables(n, nullptr, &t));
     ctx->pow[n] = t;
     *out = t;
+    return CFPQ_OK;
+}
+
+extern "C" int cfpq_order_create(cfpq_ctx *ctx, uint32_t n, const uint32_t *perm, cfpq_order **out) {
+    TRY(use_device(ctx));
+    if (!out || (n && !perm)) return set_error(CFPQ_ERR_INVALID, "null argument");
+    std::vector<char> seen(n, 0);
+    for (uint32_t v = 0; v < n; ++v) {
+        if (perm[v] >= n || seen[perm[v]]) return set_error(CFPQ_ERR_INVALID, "perm is not a permutation of 0..%u", n - 1);
+        seen[perm[v]] = 1;
+    }
+    cfpq_order *o = new cfpq_order();
+    o->n = n;
+    if (n) {
+        cudaError_t e = cudaMalloc(&o->d_perm, (size_t)n * 4);
+        if (e == cudaSuccess) e = cudaMemcpy(o->d_perm, perm, (size_t)n * 4, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            if (o->d_perm) cudaFree(o->d_perm);
+            delete o;
+            return set_error(CFPQ_ERR_CUDA, "order upload: %s", cudaGetErrorString(e));
+        }
+    }
+    int rc = make_pow_tables(n, n ? perm : nullptr, &o->pow);
+    if (rc != CFPQ_OK) {
+        if (o->d_perm) cudaFree(o->d_perm);
+        delete o;
+        return rc;
+    }
+    *out = o;
+    return CFPQ_OK;
+}
+
+extern "C" int cfpq_order_destroy(cfpq_ctx *ctx, cfpq_order *order) {
+    if (!order) return CFPQ_OK;
+    TRY(use_device(ctx));
+    cudaStreamSynchronize(ctx->stream);
+    if (order->d_perm) cudaFree(order->d_perm);
+    if (order->pow.d_pow11) cudaFree(order->pow.d_pow11);
+    if (order->pow.d_pow13) cudaFree(order->pow.d_pow13);
+    delete order;
     return CFPQ_OK;
 }
 
@@ -271,6 +350,7 @@ extern "C" int cfpq_ctx_create(int device, cfpq_ctx **out) {
     CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     CUDA_TRY(cudaEventCreate(&c->ev0));
     CUDA_TRY(cudaEventCreate(&c->ev1));
+    for (auto &e : c->kev) CUDA_TRY(cudaEventCreate(&e));
     CUDA_TRY(cudaMalloc(&c->d_st, sizeof(IterState)));
     CUDA_TRY(cudaMalloc(&c->d_flag, 64));
     CUDA_TRY(cudaMalloc(&c->d_bad, 64));
@@ -304,8 +384,10 @@ extern "C" int cfpq_ctx_destroy(cfpq_ctx *ctx) {
     cudaFreeHost(ctx->h_st);
     cudaFreeHost(ctx->h_flag);
     if (ctx->h_hash) cudaFreeHost(ctx->h_hash);
+    if (ctx->h_small) cudaFreeHost(ctx->h_small);
     cudaEventDestroy(ctx->ev0);
     cudaEventDestroy(ctx->ev1);
+    for (auto &e : ctx->kev) cudaEventDestroy(e);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     return CFPQ_OK;
@@ -322,14 +404,21 @@ extern "C" int cfpq_ctx_num_sms(const cfpq_ctx *ctx) { return ctx ? ctx->num_sms
 // matrices
 
 extern "C" int cfpq_matrix_create(cfpq_ctx *ctx, uint32_t n, cfpq_matrix **out) {
+    return cfpq_matrix_create_ordered(ctx, n, nullptr, out);
+}
+
+extern "C" int cfpq_matrix_create_ordered(cfpq_ctx *ctx, uint32_t n, cfpq_order *order, cfpq_matrix **out) {
     TRY(use_device(ctx));
     if (!out) return set_error(CFPQ_ERR_INVALID, "null output pointer");
+    if (order && order->n != n) return set_error(CFPQ_ERR_INVALID, "order is for %u vertices, matrix has %u", order->n, n);
     if (tiles_for(n) > (uint32_t)product_lop3_max_tiles())
         return set_error(CFPQ_ERR_UNSUPPORTED, "n = %u exceeds the supported maximum %d", n,
                          product_lop3_max_tiles() * 64);
     cfpq_matrix *m = new cfpq_matrix();
     m->ctx = ctx;
+    m->order = order;
     int rc = alloc_devmat(n, &m->d);
+    m->d.perm = order ? order->d_perm : nullptr;
     if (rc != CFPQ_OK) {
         delete m;
         return rc;
@@ -387,9 +476,29 @@ extern "C" int cfpq_matrix_set_bits_device(cfpq_ctx *ctx, cfpq_matrix *m, const 
     return check_bad(ctx, "cfpq_matrix_set_bits_device");
 }
 
+static int load_edges_impl(cfpq_ctx *ctx, cfpq_matrix *const *mats, size_t nmats, const uint32_t *from,
+                           const uint32_t *label, const uint32_t *to, size_t nedges, const uint32_t *label_offsets,
+                           const uint32_t *label_mats, uint32_t nlabels, bool on_device);
+
 extern "C" int cfpq_load_edges(cfpq_ctx *ctx, cfpq_matrix *const *mats, size_t nmats, const uint32_t *from,
                                const uint32_t *label, const uint32_t *to, size_t nedges,
                                const uint32_t *label_offsets, const uint32_t *label_mats, uint32_t nlabels) {
+    TRY(load_edges_impl(ctx, mats, nmats, from, label, to, nedges, label_offsets, label_mats, nlabels, false));
+    return check_bad(ctx, "cfpq_load_edges");
+}
+
+extern "C" int cfpq_load_edges_device(cfpq_ctx *ctx, cfpq_matrix *const *mats, size_t nmats, const uint32_t *d_from,
+                                      const uint32_t *d_label, const uint32_t *d_to, size_t nedges,
+                                      const uint32_t *label_offsets, const uint32_t *label_mats, uint32_t nlabels) {
+    return load_edges_impl(ctx, mats, nmats, d_from, d_label, d_to, nedges, label_offsets, label_mats, nlabels,
+                           true);
+}
+
+extern "C" void *cfpq_ctx_stream(const cfpq_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+static int load_edges_impl(cfpq_ctx *ctx, cfpq_matrix *const *mats, size_t nmats, const uint32_t *from,
+                           const uint32_t *label, const uint32_t *to, size_t nedges, const uint32_t *label_offsets,
+                           const uint32_t *label_mats, uint32_t nlabels, bool on_device) {
     TRY(use_device(ctx));
     if ((nmats && !mats) || (nedges && (!from || !label || !to)) || (nlabels && (!label_offsets)))
         return set_error(CFPQ_ERR_INVALID, "null argument");
@@ -419,15 +528,36 @@ extern "C" int cfpq_load_edges(cfpq_ctx *ctx, cfpq_matrix *const *mats, size_t n
     uint32_t *d_to = reinterpret_cast<uint32_t *>(base + up(bd) + 2 * up(be));
     uint32_t *d_off = reinterpret_cast<uint32_t *>(base + up(bd) + 3 * up(be));
     uint32_t *d_lm = reinterpret_cast<uint32_t *>(base + up(bd) + 3 * up(be) + up(bo));
-    CUDA_TRY(cudaMemcpyAsync(d_desc, descs.data(), bd, cudaMemcpyHostToDevice, ctx->stream));
-    CUDA_TRY(cudaMemcpyAsync(d_from, from, be, cudaMemcpyHostToDevice, ctx->stream));
-    CUDA_TRY(cudaMemcpyAsync(d_label, label, be, cudaMemcpyHostToDevice, ctx->stream));
-    CUDA_TRY(cudaMemcpyAsync(d_to, to, be, cudaMemcpyHostToDevice, ctx->stream));
-    CUDA_TRY(cudaMemcpyAsync(d_off, label_offsets, bo, cudaMemcpyHostToDevice, ctx->stream));
-    if (nlm) CUDA_TRY(cudaMemcpyAsync(d_lm, label_mats, (size_t)nlm * 4, cudaMemcpyHostToDevice, ctx->stream));
+    // Small tables go through a pinned host block (copied with the call, so the
+    // caller's arrays are free on return and the copy is truly asynchronous).
+    const size_t small = up(bd) + up(bo) + up(bl);
+    if (ctx->h_small_cap < small) {
+        if (ctx->h_small) cudaFreeHost(ctx->h_small);
+        ctx->h_small = nullptr;
+        ctx->h_small_cap = 0;
+        CUDA_TRY(cudaMallocHost(&ctx->h_small, small));
+        ctx->h_small_cap = small;
+    }
+    CUDA_TRY(cudaStreamSynchronize(ctx->stream));  // previous user of h_small done
+    char *hs = reinterpret_cast<char *>(ctx->h_small);
+    memcpy(hs, descs.data(), bd);
+    memcpy(hs + up(bd), label_offsets, bo);
+    if (nlm) memcpy(hs + up(bd) + up(bo), label_mats, (size_t)nlm * 4);
+    CUDA_TRY(cudaMemcpyAsync(d_desc, hs, bd, cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(cudaMemcpyAsync(d_off, hs + up(bd), bo, cudaMemcpyHostToDevice, ctx->stream));
+    if (nlm) CUDA_TRY(cudaMemcpyAsync(d_lm, hs + up(bd) + up(bo), (size_t)nlm * 4, cudaMemcpyHostToDevice, ctx->stream));
+    if (on_device) {
+        d_from = const_cast<uint32_t *>(from);
+        d_label = const_cast<uint32_t *>(label);
+        d_to = const_cast<uint32_t *>(to);
+    } else {
+        CUDA_TRY(cudaMemcpyAsync(d_from, from, be, cudaMemcpyHostToDevice, ctx->stream));
+        CUDA_TRY(cudaMemcpyAsync(d_label, label, be, cudaMemcpyHostToDevice, ctx->stream));
+        CUDA_TRY(cudaMemcpyAsync(d_to, to, be, cudaMemcpyHostToDevice, ctx->stream));
+    }
     CUDA_TRY(cudaMemsetAsync(ctx->d_bad, 0, 4, ctx->stream));
     CUDA_TRY(launch_load_edges(d_desc, d_from, d_label, d_to, nedges, d_off, d_lm, nlabels, ctx->d_bad, ctx->stream));
-    return check_bad(ctx, "cfpq_load_edges");
+    return CFPQ_OK;
 }
 
 extern "C" int cfpq_matrix_set_diagonal(cfpq_ctx *ctx, cfpq_matrix *m) {
@@ -448,6 +578,7 @@ extern "C" int cfpq_matrix_copy(cfpq_ctx *ctx, cfpq_matrix *dst, const cfpq_matr
     TRY(use_device(ctx));
     if (!dst || !src) return set_error(CFPQ_ERR_INVALID, "null matrix");
     if (dst->d.n != src->d.n) return set_error(CFPQ_ERR_INVALID, "size mismatch %u vs %u", dst->d.n, src->d.n);
+    if (dst->order != src->order) return set_error(CFPQ_ERR_INVALID, "matrices have different vertex orders");
     if (dst == src) return CFPQ_OK;
     CUDA_TRY(launch_copy_matrix(dst->d, src->d, ctx->stream));
     return CFPQ_OK;
@@ -475,6 +606,17 @@ extern "C" int cfpq_matrix_download_rows(cfpq_ctx *ctx, const cfpq_matrix *m, ui
     return sync_and_check(ctx);
 }
 
+extern "C" int cfpq_matrix_tile_stats(cfpq_ctx *ctx, const cfpq_matrix *m, uint32_t *occ_out, uint32_t *nnz_out) {
+    TRY(use_device(ctx));
+    if (!m) return set_error(CFPQ_ERR_INVALID, "null matrix");
+    if (m->d.T == 0) return CFPQ_OK;
+    if (occ_out)
+        CUDA_TRY(cudaMemcpyAsync(occ_out, m->d.occ, (size_t)m->d.T * m->d.ow * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    if (nnz_out)
+        CUDA_TRY(cudaMemcpyAsync(nnz_out, m->d.nnz, (size_t)m->d.T * m->d.T * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    return sync_and_check(ctx);
+}
+
 static int ensure_hash_buffers(cfpq_ctx *ctx, size_t nm) {
     if (ctx->d_hash_cap < nm) {
         if (ctx->d_hash) cudaFree(ctx->d_hash);
@@ -498,7 +640,7 @@ extern "C" int cfpq_hash_count_many(cfpq_ctx *ctx, cfpq_matrix *const *mats, siz
     for (size_t i = 0; i < nmats; ++i) {
         if (!mats[i]) return set_error(CFPQ_ERR_INVALID, "null matrix %zu", i);
         PowTables pt;
-        TRY(get_pow_tables(ctx, mats[i]->d.n, &pt));
+        TRY(get_pow_tables(ctx, mats[i], &pt));
         CUDA_TRY(launch_hash_count(mats[i]->d, pt.d_pow11, pt.d_pow13, ctx->d_hash + 2 * i, ctx->stream));
     }
     CUDA_TRY(cudaMemcpyAsync(ctx->h_hash, ctx->d_hash, nmats * 2 * sizeof(unsigned long long),
@@ -548,7 +690,7 @@ static int enqueue_tiled_product(cfpq_ctx *ctx, const DevMat &a, const DevMat &b
     pd.qslot = 1;
     pd.T = T;
     pd.n = a.n;
-    const size_t cap = (size_t)T * ((T + tpb - 1) / tpb);
+    const size_t cap = item_capacity(T, tpb);
     TRY(ctx->slots.ensure(sizeof(hs)));
     TRY(ctx->prods.ensure(sizeof(pd)));
     TRY(ctx->items.ensure(std::max<size_t>(cap, 1) * 8));
@@ -573,6 +715,8 @@ extern "C" int cfpq_add_mul(cfpq_ctx *ctx, cfpq_matrix *c, const cfpq_matrix *a,
     if (!c || !a || !b || !changed) return set_error(CFPQ_ERR_INVALID, "null argument");
     if (a->d.n != c->d.n || b->d.n != c->d.n)
         return set_error(CFPQ_ERR_INVALID, "size mismatch (%u, %u, %u)", c->d.n, a->d.n, b->d.n);
+    if (a->order != c->order || b->order != c->order)
+        return set_error(CFPQ_ERR_INVALID, "operands have different vertex orders");
     *changed = 0;
     if (c->d.n == 0) return CFPQ_OK;
     if (variant == CFPQ_VARIANT_AUTO) variant = CFPQ_VARIANT_LOP3;
@@ -651,6 +795,8 @@ static int validate_query(const QueryIn &q, size_t qi) {
         if (q.mats[i]->d.n != n)
             return set_error(CFPQ_ERR_INVALID, "query %zu: matrices of different sizes (%u vs %u)", qi, n,
                              q.mats[i]->d.n);
+        if (q.mats[i]->order != q.mats[0]->order)
+            return set_error(CFPQ_ERR_INVALID, "query %zu: matrices with different vertex orders", qi);
         for (size_t j = 0; j < i; ++j)
             if (q.mats[j] == q.mats[i])
                 return set_error(CFPQ_ERR_INVALID, "query %zu: matrix %zu repeated at %zu", qi, i, j);
@@ -703,7 +849,7 @@ static int build_plan(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, int variant
                 pd.n = n;
                 pd.row_start = pl->prod_rows;
                 pl->prod_rows += T;
-                pl->item_cap += (size_t)T * ((T + tpb - 1) / tpb);
+                pl->item_cap += item_capacity(T, tpb);
                 pl->prods.push_back(pd);
             }
         }
@@ -722,6 +868,45 @@ static int enqueue_iteration(cfpq_ctx *ctx, const ClosurePlan &pl, const QueryTr
     CUDA_TRY(launch_advance(ctx->slots.as<MatSlot>(), (uint32_t)pl.slots.size(), pl.slot_rows, ctx->d_st,
                             ctx->stream));
     CUDA_TRY(launch_iter_end(ctx->d_st, qt, handle, use_handle, ctx->stream));
+    return CFPQ_OK;
+}
+
+// One iteration with every kernel bracketed by events (profiling mode).
+static int enqueue_iteration_timed(cfpq_ctx *ctx, const ClosurePlan &pl, const QueryTrack &qt) {
+    const int tpb = product_lop3_tiles_per_block();
+    cudaStream_t s = ctx->stream;
+    CUDA_TRY(cudaEventRecord(ctx->kev[0], s));
+    CUDA_TRY(launch_plan(ctx->prods.as<ProdDesc>(), (uint32_t)pl.prods.size(), 0, pl.prod_rows,
+                         ctx->slots.as<MatSlot>(), ctx->d_st, ctx->items.as<uint64_t>(), tpb,
+                         ctx->prod_seen.as<uint32_t>(), s));
+    CUDA_TRY(cudaEventRecord(ctx->kev[1], s));
+    CUDA_TRY(launch_product_lop3(ctx->prods.as<ProdDesc>(), ctx->slots.as<MatSlot>(), ctx->d_st,
+                                 ctx->items.as<uint64_t>(), qt.changed, ctx->lop3_grid, s));
+    CUDA_TRY(cudaEventRecord(ctx->kev[2], s));
+    CUDA_TRY(launch_advance(ctx->slots.as<MatSlot>(), (uint32_t)pl.slots.size(), pl.slot_rows, ctx->d_st, s));
+    CUDA_TRY(cudaEventRecord(ctx->kev[3], s));
+    CUDA_TRY(launch_iter_end(ctx->d_st, qt, 0, 0, s));
+    CUDA_TRY(cudaEventRecord(ctx->kev[4], s));
+    return CFPQ_OK;
+}
+
+static int accumulate_kernel_times(cfpq_ctx *ctx) {
+    float t[4];
+    for (int i = 0; i < 4; ++i) CUDA_TRY(cudaEventElapsedTime(&t[i], ctx->kev[i], ctx->kev[i + 1]));
+    ctx->prof.plan_ms += t[0];
+    ctx->prof.product_ms += t[1];
+    ctx->prof.advance_ms += t[2];
+    ctx->prof.iter_end_ms += t[3];
+    ctx->prof.plan_launches++;
+    ctx->prof.product_launches++;
+    ctx->prof.advance_launches++;
+    ctx->prof.iter_end_launches++;
+    return CFPQ_OK;
+}
+
+extern "C" int cfpq_last_kernel_profile(cfpq_ctx *ctx, cfpq_kernel_profile *out) {
+    if (!ctx || !out) return set_error(CFPQ_ERR_INVALID, "null argument");
+    *out = ctx->prof;
     return CFPQ_OK;
 }
 
@@ -823,12 +1008,23 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
     *ctx->h_st = st;
     CUDA_TRY(cudaMemcpyAsync(ctx->d_st, ctx->h_st, sizeof(IterState), cudaMemcpyHostToDevice, ctx->stream));
 
+    const bool timed = (o.log_products & CFPQ_LOG_KERNELS) != 0;
     cudaGraphExec_t exec = nullptr;
-    if (o.use_graph) TRY(get_loop_graph(ctx, pl, qt, &exec));
+    if (o.use_graph && !timed) TRY(get_loop_graph(ctx, pl, qt, &exec));
+    if (timed) memset(&ctx->prof, 0, sizeof(ctx->prof));
 
     CUDA_TRY(launch_mark_start(ctx->d_st, ctx->stream));
     CUDA_TRY(cudaEventRecord(ctx->ev0, ctx->stream));
-    if (exec) {
+    if (timed) {
+        for (uint32_t it = 0;; ++it) {
+            TRY(enqueue_iteration_timed(ctx, pl, qt));
+            CUDA_TRY(cudaMemcpyAsync(ctx->h_st, ctx->d_st, sizeof(IterState), cudaMemcpyDeviceToHost, ctx->stream));
+            CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+            TRY(accumulate_kernel_times(ctx));
+            if (!ctx->h_st->active) break;
+            if (it > (1u << 24)) return set_error(CFPQ_ERR_CUDA, "closure did not converge");
+        }
+    } else if (exec) {
         CUDA_TRY(cudaGraphLaunch(exec, ctx->stream));
     } else {
         // Host loop: check the device flag every `batch` iterations; surplus
@@ -867,6 +1063,9 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
         stats->device_ms = ms;
         stats->kernel_launches = (uint64_t)hs.iter * 4 + 1;
         stats->variant_items[CFPQ_VARIANT_LOP3] = hs.items_total;
+        stats->bytes_staged = hs.bytes_staged;
+        stats->out_words = hs.out_words;
+        stats->new_words = hs.new_words;
     }
     for (size_t q = 0; q < nq; ++q) {
         if (iters_out) iters_out[q] = h_last[q];

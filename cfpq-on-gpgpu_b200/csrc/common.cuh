@@ -13,6 +13,11 @@
 // a tile that holds a set bit has its occupancy bit set.  (A set occupancy bit
 // does not promise a non-zero tile.)  Bits of padding rows/columns (>= n) are
 // always zero.
+//
+// Tile population: nnz[ti*T + tj] counts the set bits of tile (ti, tj).  It is
+// exact at API boundaries and at the kernel boundaries of the closure; product
+// kernels only use it to choose between the dense and the sparse inner loop,
+// never to decide which bits exist.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -26,6 +31,8 @@ constexpr int kTileWords = 64;  // uint64 words per tile
 struct DevMat {
     uint64_t *bits;   // T*T*64 words
     uint32_t *occ;    // T*ow words
+    uint32_t *nnz;    // T*T tile populations
+    const uint32_t *perm;  // vertex order: internal index of vertex v (null = identity)
     uint32_t T;       // tiles per side
     uint32_t ow;      // occupancy words per tile-row
     uint32_t n;       // logical size
@@ -71,6 +78,9 @@ struct IterState {
     unsigned long long dense_bitops;  // sum of n^3 over those products
     unsigned long long t_start_ns;    // %globaltimer at the first plan
     unsigned long long items_by_variant[5];
+    unsigned long long bytes_staged;  // operand bytes copied global -> shared by product kernels
+    unsigned long long out_words;     // non-zero accumulator words merged into heads
+    unsigned long long new_words;     // words that received new bits
 };
 
 // Per-query bookkeeping of a batched closure (device arrays of nqueries).
@@ -90,13 +100,26 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
 #endif
 }
 
-// Work item: (product index, output tile-row, output tile-column block).
-__host__ __device__ inline uint64_t make_item(uint32_t p, uint32_t ti, uint32_t tjb) {
-    return ((uint64_t)p << 40) | ((uint64_t)ti << 20) | (uint64_t)tjb;
+// Work item: (product, output tile-row ti, output tile-column block tjb,
+// inner-dimension word kw = k-tiles 32*kw .. 32*kw+31).  Items of the same
+// output block with different kw are independent: their partial products are
+// OR-ed into the head atomically.  Fields: p 21 bits, ti 15, tjb 12, kw 12
+// (n <= 2^21).
+__host__ __device__ inline uint64_t make_item(uint32_t p, uint32_t ti, uint32_t tjb, uint32_t kw) {
+    return ((uint64_t)p << 39) | ((uint64_t)ti << 24) | ((uint64_t)tjb << 12) | (uint64_t)kw;
 }
-__host__ __device__ inline uint32_t item_prod(uint64_t it) { return (uint32_t)(it >> 40); }
-__host__ __device__ inline uint32_t item_ti(uint64_t it) { return (uint32_t)((it >> 20) & 0xFFFFF); }
-__host__ __device__ inline uint32_t item_tjb(uint64_t it) { return (uint32_t)(it & 0xFFFFF); }
+__host__ __device__ inline uint32_t item_prod(uint64_t it) { return (uint32_t)(it >> 39); }
+__host__ __device__ inline uint32_t item_ti(uint64_t it) { return (uint32_t)((it >> 24) & 0x7FFF); }
+__host__ __device__ inline uint32_t item_tjb(uint64_t it) { return (uint32_t)((it >> 12) & 0xFFF); }
+__host__ __device__ inline uint32_t item_kw(uint64_t it) { return (uint32_t)(it & 0xFFF); }
+
+// The inner dimension of an output block is split into at most kKSplit groups
+// of consecutive occupancy words; item kw = group index.
+constexpr uint32_t kKSplit = 4;
+__host__ __device__ inline uint32_t kgroup_words(uint32_t ow) {
+    const uint32_t g = (ow + kKSplit - 1) / kKSplit;
+    return g ? g : 1;
+}
 
 __host__ __device__ inline size_t tile_offset(uint32_t T, uint32_t ti, uint32_t tj) {
     return ((size_t)ti * T + tj) * kTileWords;

@@ -6,43 +6,55 @@
 // tiles 4w..4w+3 of the block, lane l owns rows 2l and 2l+1, so every thread
 // keeps 2 rows x 4 tiles x 64 bits = 16 uint32 accumulators.
 //
-// Inner dimension: the CTA walks the k-tiles tk whose P tile (ti, tk) is
-// occupied and whose Q tiles (tk, block) are not all empty (the list is built
-// once per item by warp 0).  For each tk one elected thread stages the P tile
-// (512 B) and the kBJ Q tiles (kBJ*512 B, one contiguous range in the tiled
-// layout) into shared memory with bulk copies (cp.async.bulk, the TMA engine)
-// completing on an mbarrier; two stages double-buffer the staging.  A warp
-// whose 4 Q tiles are all empty skips the k-tile.
-//
-// Inner loop per row and inner index k: mask = -(P[row] bit k) (2 ALU ops),
-// then acc |= mask & Q[k] for 8 uint32 words (one LOP3 each).  Q rows k, k+1 of
-// a tile come in one 16-byte shared load that every lane of the warp reads at
-// the same address (broadcast).
+// Inner dimension: warp 0 lists the k-tiles tk whose P tile (ti, tk) is
+// occupied and whose Q tiles (tk, block) are not all empty, and sorts them by
+// the population of the P tile:
+//   dense  (population > kSparseMax): one elected thread stages the P tile
+//          (512 B) and the kBJ Q tiles (kBJ*512 B, one contiguous range of the
+//          tiled layout) into shared memory with bulk copies (cp.async.bulk,
+//          the TMA engine) completing on an mbarrier, double-buffered.  Per row
+//          and inner index k: mask = -(P[row] bit k) (2 ALU ops), then
+//          acc |= mask & Q[k] on 8 uint32 words (one LOP3 each); Q rows k, k+1
+//          of a tile come in one 16-byte shared load that all lanes of the
+//          warp read at the same address (broadcast).
+//   sparse (population <= kSparseMax): nothing is staged.  The (k-tile, row)
+//          pairs of all sparse k-tiles are spread over the CTA's 128 threads
+//          (4 pairs in flight per thread); a thread walks the set bits k of
+//          its P row word and ORs the Q words of row k of the occupied tiles,
+//          read straight from L2, into a shared-memory accumulator with shared
+//          atomics.  Latency is hidden by the number of independent pairs, not
+//          by a per-warp chain over k-tiles.
+// A warp whose 4 Q tiles are all empty skips a dense k-tile.
 //
 // Epilogue: for each non-zero accumulator word, new = acc & ~old via a 64-bit
 // atomicOr (several products of one iteration may write the same head); new
-// bits also go to the head's next-delta matrix D, and the occupancy bits of
-// the touched tiles of C and D are set.  Concurrent reads of matrices that
-// other CTAs are OR-ing into are safe: every bit only ever goes 0 -> 1, so a
-// read sees a subset of the final and a superset of the iteration-start value.
+// bits also go to the head's next-delta matrix D; occupancy bits and tile
+// populations of C and D are updated.  Concurrent reads of matrices that other
+// CTAs are OR-ing into are safe: every bit only goes 0 -> 1, so a read sees a
+// subset of the final value and a superset of the iteration-start value.
 #include "launch.h"
 
 namespace cfpq {
 
 namespace {
 
-constexpr int kBJ = 16;          // output tiles per work item (1024 columns)
-constexpr int kThreads = 128;    // 4 warps
-constexpr int kMaxTiles = 2048;  // k-list capacity (n <= 131072)
+constexpr int kBJ = 16;            // output tiles per work item (1024 columns)
+constexpr int kThreads = 128;      // 4 warps
+constexpr int kMaxTiles = 2048;    // k-list capacity (n <= 131072)
+constexpr uint32_t kSparseMax = 96;  // P-tile population up to which the sparse loop runs
 constexpr unsigned kFull = 0xffffffffu;
 
 struct __align__(128) Lop3Smem {
     uint64_t q[2][kBJ * 64];     // 2 x 8 KiB
     uint64_t p[2][64];           // 2 x 512 B
+    unsigned long long sacc[kBJ * 64];  // sparse-phase accumulator [tile][row], 8 KiB
     uint64_t bar[2];
-    uint16_t ktile[kMaxTiles];   // k-list: tile index
-    uint16_t kmask[kMaxTiles];   // k-list: occupancy of the kBJ Q tiles
-    uint32_t nk;
+    uint16_t dtile[kMaxTiles];   // dense k-list: tile index
+    uint16_t dmask[kMaxTiles];   //               occupancy of the kBJ Q tiles
+    uint16_t stile[kMaxTiles];   // sparse k-list
+    uint16_t smask[kMaxTiles];
+    uint16_t cand[kMaxTiles];    // occupied P tiles of the item's tile-row
+    uint32_t nc, nd, ns;
     uint32_t item;
 };
 
@@ -54,6 +66,10 @@ __device__ __forceinline__ DevMat resolve_operand(const MatSlot &s, uint8_t use_
 __device__ __forceinline__ uint32_t bitmask(uint32_t word, int b) {
     // all-ones if bit b of word is set, else zero
     return (uint32_t)((int32_t)(word << (31 - b)) >> 31);
+}
+
+__device__ __forceinline__ uint64_t ld_cg(const uint64_t *p) {
+    return __ldcg(reinterpret_cast<const unsigned long long *>(p));
 }
 
 __global__ void __launch_bounds__(kThreads, 4)
@@ -72,7 +88,7 @@ __global__ void __launch_bounds__(kThreads, 4)
     uint32_t phase = 0;  // bit s = next parity to wait for on stage s
     const uint32_t iter = st->iter;
     const uint32_t nitems = st->item_count;
-    unsigned long long triples = 0;
+    unsigned long long triples = 0, staged = 0, outw = 0, neww = 0;
     bool timed_out = false;
 
     for (;;) {
@@ -82,7 +98,7 @@ __global__ void __launch_bounds__(kThreads, 4)
         if (idx >= nitems) break;
         const uint64_t it = items[idx];
         const ProdDesc pd = prods[item_prod(it)];
-        const uint32_t ti = item_ti(it), tjb = item_tjb(it);
+        const uint32_t ti = item_ti(it), tjb = item_tjb(it), kw = item_kw(it);
         const DevMat P = resolve_operand(slots[pd.pslot], pd.p_delta, iter);
         const DevMat Q = resolve_operand(slots[pd.qslot], pd.q_delta, iter);
         const DevMat C = slots[pd.head].cur;
@@ -92,55 +108,77 @@ __global__ void __launch_bounds__(kThreads, 4)
         const uint32_t nblk = min((uint32_t)kBJ, T - tj0);
         const uint32_t qword = tj0 >> 5, qshift = tj0 & 31;
 
-        // ---- k-list: tk with occP(ti,tk) and a non-empty Q block (warp 0) ----
+        // ---- k-lists: warp 0 compacts the occupied P tiles of row ti into a
+        // candidate list, then all threads classify candidates in parallel ----
         if (warp == 0) {
-            uint32_t nk = 0;
+            uint32_t nc = 0;
             const uint32_t *prow = P.occ + (size_t)ti * ow;
-            for (uint32_t base = 0; base < ow; base += 32) {
-                uint32_t bits = (base + lane < ow) ? prow[base + lane] : 0u;
-                while (__any_sync(kFull, bits != 0)) {
-                    const bool has = bits != 0;
-                    uint32_t tk = 0, mask = 0;
-                    if (has) {
-                        tk = (base + lane) * 32 + (__ffs(bits) - 1);
-                        bits &= bits - 1;
-                        mask = (Q.occ[(size_t)tk * ow + qword] >> qshift) & ((1u << kBJ) - 1);
-                    }
-                    const unsigned ball = __ballot_sync(kFull, mask != 0);
-                    if (mask) {
-                        const uint32_t pos = nk + __popc(ball & ((1u << lane) - 1));
-                        S.ktile[pos] = (uint16_t)tk;
-                        S.kmask[pos] = (uint16_t)mask;
-                    }
-                    nk += __popc(ball);
+            const uint32_t G = kgroup_words(ow);
+            const uint32_t w_begin = kw * G, w_end = min(ow, w_begin + G);
+            for (uint32_t base = w_begin; base < w_end; base += 32) {
+                uint32_t bits = (base + lane < w_end) ? prow[base + lane] : 0u;
+                const uint32_t cnt = __popc(bits);
+                uint32_t pre = cnt;  // inclusive scan over lanes
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t v = __shfl_up_sync(kFull, pre, o);
+                    if (lane >= (uint32_t)o) pre += v;
                 }
+                uint32_t pos = nc + pre - cnt;
+                while (bits) {
+                    S.cand[pos++] = (uint16_t)((base + lane) * 32 + (__ffs(bits) - 1));
+                    bits &= bits - 1;
+                }
+                nc += __shfl_sync(kFull, pre, 31);
             }
-            if (lane == 0) S.nk = nk;
+            if (lane == 0) {
+                S.nc = nc;
+                S.nd = 0;
+                S.ns = 0;
+            }
         }
         __syncthreads();
-        const uint32_t nk = S.nk;
+        for (uint32_t c = tid; c < S.nc; c += kThreads) {
+            const uint32_t tk = S.cand[c];
+            const uint32_t mask = (Q.occ[(size_t)tk * ow + qword] >> qshift) & ((1u << kBJ) - 1);
+            if (!mask) continue;
+            triples += __popc(mask);
+            if (P.nnz[(size_t)ti * T + tk] > kSparseMax) {
+                const uint32_t pos = atomicAdd(&S.nd, 1u);
+                S.dtile[pos] = (uint16_t)tk;
+                S.dmask[pos] = (uint16_t)mask;
+            } else {
+                const uint32_t pos = atomicAdd(&S.ns, 1u);
+                S.stile[pos] = (uint16_t)tk;
+                S.smask[pos] = (uint16_t)mask;
+            }
+        }
+        __syncthreads();
+        const uint32_t nd = S.nd, ns = S.ns;
 
         uint2 acc0[4], acc1[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) acc0[j] = acc1[j] = make_uint2(0, 0);
 
+        // ---- dense k-tiles: staged panels, LOP3 inner loop ----
         auto issue = [&](uint32_t e, uint32_t stage) {
-            const uint32_t tk = S.ktile[e];
+            const uint32_t tk = S.dtile[e];
             fence_proxy_async_smem();
             mbar_arrive_expect_tx(&S.bar[stage], 512u + nblk * 512u);
             bulk_g2s(S.p[stage], P.bits + tile_offset(T, ti, tk), 512u, &S.bar[stage]);
             bulk_g2s(S.q[stage], Q.bits + tile_offset(T, tk, tj0), nblk * 512u, &S.bar[stage]);
         };
-
-        if (tid == 0 && nk > 0) issue(0, 0);
+        if (tid == 0 && nd > 0) {
+            issue(0, 0);
+            staged += (unsigned long long)nd * (512u + nblk * 512u);
+        }
         uint32_t stage = 0;
-        for (uint32_t e = 0; e < nk; ++e) {
-            if (tid == 0 && e + 1 < nk) issue(e + 1, stage ^ 1);
-            if (!mbar_wait_bounded(&S.bar[stage], (phase >> stage) & 1u)) timed_out = true;
+        for (uint32_t e = 0; e < nd; ++e) {
+            if (tid == 0 && e + 1 < nd) issue(e + 1, stage ^ 1);
+            if (!timed_out && !mbar_wait_bounded(&S.bar[stage], (phase >> stage) & 1u)) timed_out = true;
             phase ^= 1u << stage;
-            const uint32_t wmask = ((uint32_t)S.kmask[e] >> (4 * warp)) & 0xFu;
+            const uint32_t wmask = ((uint32_t)S.dmask[e] >> (4 * warp)) & 0xFu;
             if (wmask && !timed_out) {
-                triples += (lane == 0) ? __popc(wmask) : 0;
                 const uint4 pp = *reinterpret_cast<const uint4 *>(&S.p[stage][2 * lane]);
                 const uint64_t *q = &S.q[stage][(4 * warp) * 64];
 #pragma unroll
@@ -160,8 +198,53 @@ __global__ void __launch_bounds__(kThreads, 4)
                     }
                 }
             }
-            __syncthreads();
+            // all threads are done with this stage before it is refilled; a
+            // timeout anywhere in the CTA stops every later wait
+            timed_out = __syncthreads_or(timed_out) != 0;
             stage ^= 1;
+        }
+
+        // ---- sparse k-tiles: (k-tile, row) pairs over all threads ----
+        if (ns > 0) {
+            for (uint32_t i = tid; i < kBJ * 64; i += kThreads) S.sacc[i] = 0ULL;
+            __syncthreads();
+            const uint32_t units = ns * 64;
+            for (uint32_t u0 = tid; u0 < units; u0 += 4 * kThreads) {
+                uint64_t pw[4];
+#pragma unroll
+                for (int g = 0; g < 4; ++g) {
+                    const uint32_t u = u0 + g * kThreads;
+                    pw[g] = u < units ? ld_cg(P.bits + tile_offset(T, ti, S.stile[u >> 6]) + (u & 63)) : 0ULL;
+                }
+#pragma unroll
+                for (int g = 0; g < 4; ++g) {
+                    uint64_t x = pw[g];
+                    if (!x) continue;
+                    const uint32_t u = u0 + g * kThreads;
+                    const uint32_t e = u >> 6, r = u & 63;
+                    const uint32_t mask = S.smask[e];
+                    const uint64_t *qb = Q.bits + tile_offset(T, S.stile[e], tj0);
+                    while (x) {
+                        const int k = __ffsll((long long)x) - 1;
+                        x &= x - 1;
+                        uint64_t qv[kBJ];
+#pragma unroll
+                        for (int j = 0; j < kBJ; ++j) qv[j] = ((mask >> j) & 1u) ? ld_cg(qb + j * 64 + k) : 0ULL;
+#pragma unroll
+                        for (int j = 0; j < kBJ; ++j)
+                            if (qv[j]) atomicOr(&S.sacc[j * 64 + r], (unsigned long long)qv[j]);
+                    }
+                }
+            }
+            __syncthreads();
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const uint4 s = *reinterpret_cast<const uint4 *>(&S.sacc[(4 * warp + j) * 64 + 2 * lane]);
+                acc0[j].x |= s.x;
+                acc0[j].y |= s.y;
+                acc1[j].x |= s.z;
+                acc1[j].y |= s.w;
+            }
         }
 
         // ---- epilogue ----
@@ -169,30 +252,37 @@ __global__ void __launch_bounds__(kThreads, 4)
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             const uint32_t tj = tj0 + 4 * warp + j;
-            bool newbits = false;
+            uint32_t newcnt = 0;
             if (tj < T) {
 #pragma unroll
                 for (int rr = 0; rr < 2; ++rr) {
                     const uint2 a2 = rr ? acc1[j] : acc0[j];
                     const uint64_t a = ((uint64_t)a2.y << 32) | a2.x;
                     if (!a) continue;
+                    ++outw;
                     const size_t off = tile_offset(T, ti, tj) + 2 * lane + rr;
                     unsigned long long *cw = reinterpret_cast<unsigned long long *>(C.bits + off);
-                    const uint64_t seen = __ldcg(reinterpret_cast<const unsigned long long *>(cw));
+                    const uint64_t seen = __ldcg(cw);
                     if (!(a & ~seen)) continue;
                     const uint64_t prev = atomicOr(cw, (unsigned long long)a);
                     const uint64_t nw = a & ~prev;
                     if (nw) {
-                        newbits = true;
+                        ++neww;
+                        newcnt += __popcll(nw);
                         if (D.bits) atomicOr(reinterpret_cast<unsigned long long *>(D.bits + off), (unsigned long long)nw);
                     }
                 }
             }
-            if (__any_sync(kFull, newbits)) {
+            const uint32_t tile_new = __reduce_add_sync(kFull, newcnt);
+            if (tile_new) {
                 any_new = true;
                 if (lane == 0) {
+                    atomicAdd(C.nnz + (size_t)ti * T + tj, tile_new);
                     atomicOr(C.occ + (size_t)ti * C.ow + (tj >> 5), 1u << (tj & 31));
-                    if (D.bits) atomicOr(D.occ + (size_t)ti * D.ow + (tj >> 5), 1u << (tj & 31));
+                    if (D.bits) {
+                        atomicAdd(D.nnz + (size_t)ti * T + tj, tile_new);
+                        atomicOr(D.occ + (size_t)ti * D.ow + (tj >> 5), 1u << (tj & 31));
+                    }
                 }
             }
         }
@@ -202,7 +292,18 @@ __global__ void __launch_bounds__(kThreads, 4)
         }
         __syncthreads();  // S.item / k-list reuse
     }
-    if (triples) atomicAdd(&st->tile_triples, triples);
+    // per-CTA counters (warp-reduced) for statistics and the roofline report
+    for (int o = 16; o > 0; o >>= 1) {
+        triples += __shfl_down_sync(kFull, triples, o);
+        outw += __shfl_down_sync(kFull, outw, o);
+        neww += __shfl_down_sync(kFull, neww, o);
+    }
+    if (lane == 0) {
+        if (triples) atomicAdd(&st->tile_triples, triples);
+        if (outw) atomicAdd(&st->out_words, outw);
+        if (neww) atomicAdd(&st->new_words, neww);
+    }
+    if (tid == 0 && staged) atomicAdd(&st->bytes_staged, staged);
     if (timed_out && tid == 0) atomicExch(&st->error, 5u);
 }
 
@@ -210,6 +311,7 @@ __global__ void __launch_bounds__(kThreads, 4)
 
 int product_lop3_tiles_per_block() { return kBJ; }
 int product_lop3_max_tiles() { return kMaxTiles; }
+
 // Called once per context (before any stream capture): sets the kernel's
 // shared-memory attribute and returns the resident CTAs per SM.
 int product_lop3_blocks_per_sm() {

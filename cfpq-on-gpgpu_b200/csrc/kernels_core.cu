@@ -1,6 +1,6 @@
-// Core kernels: layout conversion, occupancy, bit scatter, result hash,
-// the plain dense product, and the plan / advance steps of the device-resident
-// closure iteration.
+// Core kernels: layout conversion, tile statistics (occupancy + population),
+// bit scatter, result hash, the plain dense product, and the plan / advance
+// steps of the device-resident closure iteration.
 #include "launch.h"
 
 namespace cfpq {
@@ -15,8 +15,34 @@ inline unsigned grid_for(size_t n, unsigned block) {
     return (unsigned)(g ? g : 1);
 }
 
+inline unsigned capped_grid(size_t n, unsigned block, unsigned cap) {
+    const unsigned g = grid_for(n, block);
+    return g > cap ? cap : g;
+}
+
 __device__ __forceinline__ void set_occ_bit(const DevMat &m, uint32_t ti, uint32_t tj) {
     atomicOr(m.occ + (size_t)ti * m.ow + (tj >> 5), 1u << (tj & 31));
+}
+
+// Set bit (r, c) given in vertex ids (mapped through the matrix's vertex
+// order); keep occupancy and population exact.
+__device__ __forceinline__ void set_one_bit(const DevMat &m, uint32_t r, uint32_t c) {
+    if (m.perm) {
+        r = m.perm[r];
+        c = m.perm[c];
+    }
+    unsigned long long *w =
+        reinterpret_cast<unsigned long long *>(m.bits + tile_offset(m.T, r >> 6, c >> 6) + (r & 63));
+    const unsigned long long bit = 1ULL << (c & 63);
+    const unsigned long long old = atomicOr(w, bit);
+    if (!(old & bit)) {
+        atomicAdd(m.nnz + (size_t)(r >> 6) * m.T + (c >> 6), 1u);
+        set_occ_bit(m, r >> 6, c >> 6);
+    }
+}
+
+__device__ __forceinline__ uint32_t warp_sum(uint32_t v) {
+    return __reduce_add_sync(kFull, v);
 }
 
 // ---- initialisation ---------------------------------------------------------
@@ -29,15 +55,12 @@ __global__ void k_set_bits(DevMat m, const uint32_t *__restrict__ rows, const ui
             atomicAdd(bad, 1u);
             continue;
         }
-        unsigned long long *w =
-            reinterpret_cast<unsigned long long *>(m.bits + tile_offset(m.T, r >> 6, c >> 6) + (r & 63));
-        atomicOr(w, 1ULL << (c & 63));
-        set_occ_bit(m, r >> 6, c >> 6);
+        set_one_bit(m, r, c);
     }
 }
 
 // Edge scatter: edge e sets (from, to) in every matrix its label derives
-// (cfpq-cpp/Grammar.h:41-45).  All matrices share n.
+// (cfpq-cpp/Grammar.h:41-45).
 __global__ void k_load_edges(const DevMat *__restrict__ mats, const uint32_t *__restrict__ from,
                              const uint32_t *__restrict__ label, const uint32_t *__restrict__ to, size_t ne,
                              const uint32_t *__restrict__ off, const uint32_t *__restrict__ lm, uint32_t nlabels,
@@ -52,25 +75,18 @@ __global__ void k_load_edges(const DevMat *__restrict__ mats, const uint32_t *__
                 atomicAdd(bad, 1u);
                 continue;
             }
-            unsigned long long *w =
-                reinterpret_cast<unsigned long long *>(m.bits + tile_offset(m.T, r >> 6, c >> 6) + (r & 63));
-            atomicOr(w, 1ULL << (c & 63));
-            set_occ_bit(m, r >> 6, c >> 6);
+            set_one_bit(m, r, c);
         }
     }
 }
 
 __global__ void k_set_diag(DevMat m) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m.n; i += gridDim.x * blockDim.x) {
-        unsigned long long *w =
-            reinterpret_cast<unsigned long long *>(m.bits + tile_offset(m.T, i >> 6, i >> 6) + (i & 63));
-        atomicOr(w, 1ULL << (i & 63));
-        set_occ_bit(m, i >> 6, i >> 6);
-    }
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m.n; i += gridDim.x * blockDim.x) set_one_bit(m, i, i);
 }
 
-// One warp per occupancy word (32 tiles of one tile-row).
-__global__ void k_occ_rebuild(DevMat m) {
+// Recompute occupancy and population from the bits.  One warp per occupancy
+// word (32 tiles of one tile-row).
+__global__ void k_tile_stats(DevMat m) {
     const size_t gw = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5;
     const uint32_t lane = threadIdx.x & 31;
     if (gw >= (size_t)m.T * m.ow) return;
@@ -80,13 +96,14 @@ __global__ void k_occ_rebuild(DevMat m) {
         const uint32_t tj = w * 32 + t;
         if (tj >= m.T) break;
         const uint64_t *tile = m.bits + tile_offset(m.T, ti, tj);
-        const uint64_t v = tile[lane] | tile[lane + 32];
-        if (__any_sync(kFull, v != 0)) word |= 1u << t;
+        const uint32_t cnt = warp_sum(__popcll(tile[lane]) + __popcll(tile[lane + 32]));
+        if (cnt) word |= 1u << t;
+        if (lane == 0) m.nnz[(size_t)ti * m.T + tj] = cnt;
     }
     if (lane == 0) m.occ[(size_t)ti * m.ow + w] = word;
 }
 
-// Row-major staging (n rows x T words) -> tiles.  Thread per (tile-row, word, row-in-tile).
+// Row-major staging (n rows x T words) -> tiles.
 __global__ void k_rows_to_tiles(DevMat m, const uint64_t *__restrict__ rows) {
     const size_t total = (size_t)m.T * m.T * 64;
     for (size_t x = blockIdx.x * (size_t)blockDim.x + threadIdx.x; x < total; x += (size_t)gridDim.x * blockDim.x) {
@@ -102,52 +119,92 @@ __global__ void k_tiles_to_rows(DevMat m, uint64_t *__restrict__ rows) {
     const size_t total = (size_t)m.n * m.T;
     for (size_t x = blockIdx.x * (size_t)blockDim.x + threadIdx.x; x < total; x += (size_t)gridDim.x * blockDim.x) {
         const uint32_t row = (uint32_t)(x / m.T), w = (uint32_t)(x % m.T);
-        rows[x] = m.bits[tile_offset(m.T, row >> 6, w) + (row & 63)];
+        if (!m.perm) {
+            rows[x] = m.bits[tile_offset(m.T, row >> 6, w) + (row & 63)];
+            continue;
+        }
+        // ordered matrix: gather the 64 bits of original columns 64w..64w+63
+        const uint32_t ir = m.perm[row];
+        const uint64_t *rbase = m.bits + tile_offset(m.T, ir >> 6, 0) + (ir & 63);
+        uint64_t out = 0;
+        const uint32_t cend = min(m.n, 64 * w + 64);
+        for (uint32_t c = 64 * w; c < cend; ++c) {
+            const uint32_t ic = m.perm[c];
+            out |= ((rbase[(size_t)(ic >> 6) * 64] >> (ic & 63)) & 1ULL) << (c & 63);
+        }
+        rows[x] = out;
+    }
+}
+
+// Ordered upload: scatter the set bits of row-major staging (original ids).
+__global__ void k_rows_scatter(DevMat m, const uint64_t *__restrict__ rows) {
+    const size_t total = (size_t)m.n * m.T;
+    for (size_t x = blockIdx.x * (size_t)blockDim.x + threadIdx.x; x < total; x += (size_t)gridDim.x * blockDim.x) {
+        uint64_t v = rows[x];
+        const uint32_t row = (uint32_t)(x / m.T), w = (uint32_t)(x % m.T);
+        while (v) {
+            const uint32_t c = 64 * w + (__ffsll((long long)v) - 1);
+            v &= v - 1;
+            if (c < m.n) set_one_bit(m, row, c);
+        }
     }
 }
 
 // ---- result hash ------------------------------------------------------------
-// line_hash(row) = sum over set columns c of 11^(n-1-c)   (mod p)
-// hash           = sum over rows r of line_hash(r) * 13^(n-1-r) (mod p)
-// which is the closed form of the reference's Horner loop
-// (cfpq-cpp/Grammar.cpp:86-97).  One block of 64 threads per tile-row; thread r
-// owns row ti*64 + r and walks its words tile by tile (coalesced across the
-// block).  d_out[0] accumulates the per-row terms (each < 2^30, so the 64-bit
-// sum cannot overflow for n < 2^33), d_out[1] the bit count.
-__global__ void k_hash_count(DevMat m, const uint32_t *__restrict__ pow11, const uint32_t *__restrict__ pow13,
-                             unsigned long long *out) {
-    const uint32_t ti = blockIdx.x;
-    const uint32_t r = threadIdx.x;
-    const uint32_t row = ti * 64 + r;
-    unsigned long long line = 0, cnt = 0;
-    for (uint32_t tj = 0; tj < m.T; ++tj) {
-        if (!((m.occ[(size_t)ti * m.ow + (tj >> 5)] >> (tj & 31)) & 1u)) continue;
-        uint64_t v = m.bits[tile_offset(m.T, ti, tj) + r];
-        cnt += __popcll(v);
-        const uint32_t base = tj * 64;
-        while (v) {
-            const int b = __ffsll((long long)v) - 1;
-            v &= v - 1;
-            line += pow11[base + b];
+// The reference's Horner loop (cfpq-cpp/Grammar.cpp:86-97) equals
+//   hash = sum over set bits (r, c) of 11^(n-1-c) * 13^(n-1-r)   (mod p),
+// a sum that is linear in the bits, so every word is reduced independently.
+// Block = 4 tiles x 64 rows; thread = one row word of one tile.  Unoccupied
+// tiles exit at once.  out[0] accumulates terms < 2^30 (no overflow below
+// 2^34 terms), out[1] the bit count.
+__global__ void __launch_bounds__(256) k_hash_count(DevMat m, const uint32_t *__restrict__ pow11,
+                                                    const uint32_t *__restrict__ pow13, unsigned long long *out) {
+    const size_t tile = (size_t)blockIdx.x * 4 + (threadIdx.x >> 6);
+    const uint32_t r = threadIdx.x & 63;
+    unsigned long long h = 0, cnt = 0;
+    if (tile < (size_t)m.T * m.T) {
+        const uint32_t ti = (uint32_t)(tile / m.T), tj = (uint32_t)(tile % m.T);
+        if ((m.occ[(size_t)ti * m.ow + (tj >> 5)] >> (tj & 31)) & 1u) {
+            uint64_t v = m.bits[tile * 64 + r];
+            if (v) {
+                cnt = __popcll(v);
+                const uint32_t *p = pow11 + tj * 64;
+                unsigned long long line = 0;
+                while (v) {
+                    const int b = __ffsll((long long)v) - 1;
+                    v &= v - 1;
+                    line += p[b];
+                }
+                h = ((line % kHashMod) * pow13[ti * 64 + r]) % kHashMod;
+            }
         }
     }
-    unsigned long long h = 0;
-    if (row < m.n) h = ((line % kHashMod) * pow13[row]) % kHashMod;
     for (int o = 16; o > 0; o >>= 1) {
         h += __shfl_down_sync(kFull, h, o);
         cnt += __shfl_down_sync(kFull, cnt, o);
     }
+    __shared__ unsigned long long sh[8], sc[8];
     if ((threadIdx.x & 31) == 0) {
-        atomicAdd(out, h);
-        atomicAdd(out + 1, cnt);
+        sh[threadIdx.x >> 5] = h;
+        sc[threadIdx.x >> 5] = cnt;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long H = 0, C = 0;
+        for (int i = 0; i < 8; ++i) {
+            H += sh[i];
+            C += sc[i];
+        }
+        if (H) atomicAdd(out, H);
+        if (C) atomicAdd(out + 1, C);
     }
 }
 
 // ---- plain dense product (variant PLAIN) ------------------------------------
 // The "plain single-variant" form: every output word walks the whole inner
-// dimension bit by bit, no shared memory, no tiles skipped -- the same work
-// shape as the reference's naive kernel (cuda/naive-gpu/Multiplication.cu:33-74)
-// on this library's layout.  Block = the 64 rows of output tile (ti, tj).
+// dimension bit by bit, no shared memory, no tiles skipped -- the work shape of
+// the reference's naive kernel (cuda/naive-gpu/Multiplication.cu:33-74) on this
+// library's layout.  Block = the 64 rows of output tile (ti, tj).
 __global__ void __launch_bounds__(64) k_plain_product(DevMat a, DevMat b, DevMat c, int mode, uint32_t *flag) {
     const uint32_t tj = blockIdx.x, ti = blockIdx.y, r = threadIdx.x;
     const uint32_t T = a.T;
@@ -159,20 +216,30 @@ __global__ void __launch_bounds__(64) k_plain_product(DevMat a, DevMat b, DevMat
             if ((av >> kk) & 1ULL) acc |= bt[kk];
     }
     uint64_t *cw = c.bits + tile_offset(T, ti, tj) + r;
+    __shared__ uint32_t s_cnt;
+    if (r == 0) s_cnt = 0;
+    __syncthreads();
     if (mode == 0) {
         const uint64_t old = *cw;
-        const int changed = (acc & ~old) != 0;
-        if (changed) *cw = old | acc;
-        if (__syncthreads_or(changed) && r == 0) {
+        const uint64_t nw = acc & ~old;
+        if (nw) {
+            *cw = old | acc;
+            atomicAdd(&s_cnt, (uint32_t)__popcll(nw));
+        }
+        __syncthreads();
+        if (r == 0 && s_cnt) {
+            atomicAdd(c.nnz + (size_t)ti * T + tj, s_cnt);
             set_occ_bit(c, ti, tj);
             *flag = 1;
         }
     } else {
         *cw = acc;
-        const int nz = __syncthreads_or(acc != 0);
+        if (acc) atomicAdd(&s_cnt, (uint32_t)__popcll(acc));
+        __syncthreads();
         if (r == 0) {
+            c.nnz[(size_t)ti * T + tj] = s_cnt;
             uint32_t *ow = c.occ + (size_t)ti * c.ow + (tj >> 5);
-            if (nz)
+            if (s_cnt)
                 atomicOr(ow, 1u << (tj & 31));
             else
                 atomicAnd(ow, ~(1u << (tj & 31)));
@@ -187,9 +254,15 @@ __global__ void __launch_bounds__(64) k_merge_or(DevMat dst, DevMat src, uint32_
     const uint64_t v = src.bits[tile_offset(src.T, ti, tj) + r];
     uint64_t *dw = dst.bits + tile_offset(dst.T, ti, tj) + r;
     const uint64_t old = *dw;
-    const int changed = (v & ~old) != 0;
-    if (changed) *dw = old | v;
-    if (__syncthreads_or(changed) && r == 0) {
+    const uint64_t nw = v & ~old;
+    if (nw) *dw = old | v;
+    __shared__ uint32_t s_cnt;
+    if (r == 0) s_cnt = 0;
+    __syncthreads();
+    if (nw) atomicAdd(&s_cnt, (uint32_t)__popcll(nw));
+    __syncthreads();
+    if (r == 0 && s_cnt) {
+        atomicAdd(dst.nnz + (size_t)ti * dst.T + tj, s_cnt);
         set_occ_bit(dst, ti, tj);
         *flag = 1;
     }
@@ -198,9 +271,8 @@ __global__ void __launch_bounds__(64) k_merge_or(DevMat dst, DevMat src, uint32_
 // ---- closure iteration: plan ---------------------------------------------------
 // One warp per (product, output tile-row ti).  The warp forms the coarse
 // (tile-level) product row  OR_{tk : occP(ti,tk)} occQ(tk, :)  and emits one
-// work item per block of `tpb` output tiles that can receive a bit.  The coarse
-// product is exact for skipping: a tile pair contributes only if both tiles are
-// occupied.
+// work item per block of `tpb` output tiles that can receive a bit.  Skipping
+// is exact: a tile pair contributes only if both tiles are occupied.
 __device__ __forceinline__ DevMat resolve_operand(const MatSlot &s, uint8_t use_delta, uint32_t iter) {
     if (!use_delta || iter == 0) return s.cur;
     return s.dlt[iter & 1];
@@ -212,15 +284,14 @@ __global__ void k_plan(const ProdDesc *__restrict__ prods, uint32_t nprods, uint
     const uint32_t gw = row_begin + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     const uint32_t lane = threadIdx.x & 31;
     if (gw >= total_rows || !st->active) return;
-    // product index: last p with row_start <= gw
-    uint32_t lo = 0, hi = nprods;
+    uint32_t lo = 0, hi = nprods;  // product: last p with row_start <= gw
     while (hi - lo > 1) {
         const uint32_t mid = (lo + hi) >> 1;
         if (prods[mid].row_start <= gw) lo = mid; else hi = mid;
     }
     const ProdDesc pd = prods[lo];
     const uint32_t iter = st->iter;
-    if (pd.term == 1 && iter == 0) return;  // first iteration: delta(A)*B with delta = A covers A*B
+    if (pd.term == 1 && iter == 0) return;  // first iteration: delta(A) = A, one term covers A*B
     const uint32_t ti = gw - pd.row_start;
     const DevMat P = resolve_operand(slots[pd.pslot], pd.p_delta, iter);
     const DevMat Q = resolve_operand(slots[pd.qslot], pd.q_delta, iter);
@@ -229,29 +300,31 @@ __global__ void k_plan(const ProdDesc *__restrict__ prods, uint32_t nprods, uint
     const uint32_t bpw = 32 / tpb;  // blocks per occupancy word
     const uint32_t bmask = tpb == 32 ? 0xffffffffu : ((1u << tpb) - 1);
     bool emitted = false;
-    for (uint32_t base = 0; base < ow; base += 32) {
-        const uint32_t w = base + lane;
-        uint32_t acc = 0;
-        for (uint32_t pw = 0; pw < ow; ++pw) {
-            uint32_t bits = prow[pw];
-            while (bits) {
-                const uint32_t tk = pw * 32 + (__ffs(bits) - 1);
-                bits &= bits - 1;
-                if (w < ow) acc |= Q.occ[(size_t)tk * ow + w];
+    const uint32_t G = kgroup_words(ow);
+    for (uint32_t kw = 0; kw * G < ow; ++kw) {  // inner-dimension group
+        const uint32_t pw_end = min(ow, kw * G + G);
+        for (uint32_t base = 0; base < ow; base += 32) {
+            const uint32_t w = base + lane;
+            uint32_t acc = 0;
+            for (uint32_t pw = kw * G; pw < pw_end; ++pw) {
+                uint32_t bits = prow[pw];
+                while (bits) {
+                    const uint32_t tk = pw * 32 + (__ffs(bits) - 1);
+                    bits &= bits - 1;
+                    if (w < ow) acc |= Q.occ[(size_t)tk * ow + w];
+                }
+                if (__all_sync(kFull, w >= ow || acc == 0xffffffffu)) break;
             }
-            if (__all_sync(kFull, w >= ow || acc == 0xffffffffu)) break;
-        }
-        for (uint32_t h = 0; h < bpw; ++h) {
-            const bool has = w < ow && ((acc >> (h * tpb)) & bmask) != 0;
-            const unsigned ball = __ballot_sync(kFull, has);
-            if (!ball) continue;
-            emitted = true;
-            uint32_t basepos = 0;
-            if (lane == 0) basepos = atomicAdd(&st->item_count, (uint32_t)__popc(ball));
-            basepos = __shfl_sync(kFull, basepos, 0);
-            if (has) {
-                const uint32_t pos = basepos + __popc(ball & ((1u << lane) - 1));
-                items[pos] = make_item(lo, ti, w * bpw + h);
+            for (uint32_t h = 0; h < bpw; ++h) {
+                const bool has = w < ow && ((acc >> (h * tpb)) & bmask) != 0;
+                const unsigned ball = __ballot_sync(kFull, has);
+                if (!ball) continue;
+                emitted = true;
+                uint32_t basepos = 0;
+                if (lane == 0) basepos = atomicAdd(&st->item_count, (uint32_t)__popc(ball));
+                basepos = __shfl_sync(kFull, basepos, 0);
+                if (has)
+                    items[basepos + __popc(ball & ((1u << lane) - 1))] = make_item(lo, ti, w * bpw + h, kw);
             }
         }
     }
@@ -264,9 +337,9 @@ __global__ void k_plan(const ProdDesc *__restrict__ prods, uint32_t nprods, uint
 }
 
 // ---- closure iteration: advance -------------------------------------------------
-// Clears the delta buffer that was read in this iteration (it receives next
-// iteration's new bits): zero every occupied tile, then the occupancy row.  One
-// warp per (slot, tile-row).
+// Clears the delta buffer that was read in this iteration (it receives the next
+// iteration's new bits): zero every occupied tile and its population, then the
+// occupancy row.  One warp per (slot, tile-row).
 __global__ void k_advance(const MatSlot *__restrict__ slots, uint32_t nslots, uint32_t total_rows, IterState *st) {
     const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t lane = threadIdx.x & 31;
@@ -286,6 +359,7 @@ __global__ void k_advance(const MatSlot *__restrict__ slots, uint32_t nslots, ui
             bits &= bits - 1;
             uint4 *tile = reinterpret_cast<uint4 *>(D.bits + tile_offset(D.T, ti, tj));
             tile[lane] = make_uint4(0, 0, 0, 0);
+            if (lane == 0) D.nnz[(size_t)ti * D.T + tj] = 0;
         }
     }
     __syncwarp();
@@ -337,8 +411,7 @@ __global__ void k_iter_end(IterState *st, QueryTrack qt, cudaGraphConditionalHan
 cudaError_t launch_set_bits(const DevMat &m, const uint32_t *d_rows, const uint32_t *d_cols, size_t count,
                             uint32_t *d_bad, cudaStream_t s) {
     if (count == 0) return cudaSuccess;
-    const unsigned g = grid_for(count, 256) > 65535u * 16 ? 65535u * 16 : grid_for(count, 256);
-    k_set_bits<<<g, 256, 0, s>>>(m, d_rows, d_cols, count, d_bad);
+    k_set_bits<<<capped_grid(count, 256, 65535u * 16), 256, 0, s>>>(m, d_rows, d_cols, count, d_bad);
     return cudaGetLastError();
 }
 
@@ -346,8 +419,8 @@ cudaError_t launch_load_edges(const DevMat *d_mats, const uint32_t *d_from, cons
                               const uint32_t *d_to, size_t ne, const uint32_t *d_off, const uint32_t *d_lm,
                               uint32_t nlabels, uint32_t *d_bad, cudaStream_t s) {
     if (ne == 0) return cudaSuccess;
-    const unsigned g = grid_for(ne, 256) > 65535u * 16 ? 65535u * 16 : grid_for(ne, 256);
-    k_load_edges<<<g, 256, 0, s>>>(d_mats, d_from, d_label, d_to, ne, d_off, d_lm, nlabels, d_bad);
+    k_load_edges<<<capped_grid(ne, 256, 65535u * 16), 256, 0, s>>>(d_mats, d_from, d_label, d_to, ne, d_off, d_lm,
+                                                                   nlabels, d_bad);
     return cudaGetLastError();
 }
 
@@ -360,15 +433,21 @@ cudaError_t launch_set_diag(const DevMat &m, cudaStream_t s) {
 cudaError_t launch_occ_rebuild(const DevMat &m, cudaStream_t s) {
     if (m.T == 0) return cudaSuccess;
     const size_t warps = (size_t)m.T * m.ow;
-    k_occ_rebuild<<<grid_for(warps * 32, 256), 256, 0, s>>>(m);
+    k_tile_stats<<<grid_for(warps * 32, 256), 256, 0, s>>>(m);
     return cudaGetLastError();
 }
 
 cudaError_t launch_rows_to_tiles(const DevMat &m, const uint64_t *d_rows, cudaStream_t s) {
     if (m.T == 0) return cudaSuccess;
+    if (m.perm) {
+        cudaError_t e = launch_clear_matrix(m, s);
+        if (e != cudaSuccess) return e;
+        const size_t words = (size_t)m.n * m.T;
+        k_rows_scatter<<<capped_grid(words, 256, 1u << 20), 256, 0, s>>>(m, d_rows);
+        return cudaGetLastError();
+    }
     const size_t total = (size_t)m.T * m.T * 64;
-    const unsigned g = grid_for(total, 256) > (1u << 20) ? (1u << 20) : grid_for(total, 256);
-    k_rows_to_tiles<<<g, 256, 0, s>>>(m, d_rows);
+    k_rows_to_tiles<<<capped_grid(total, 256, 1u << 20), 256, 0, s>>>(m, d_rows);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     return launch_occ_rebuild(m, s);
@@ -377,8 +456,7 @@ cudaError_t launch_rows_to_tiles(const DevMat &m, const uint64_t *d_rows, cudaSt
 cudaError_t launch_tiles_to_rows(const DevMat &m, uint64_t *d_rows, cudaStream_t s) {
     if (m.n == 0) return cudaSuccess;
     const size_t total = (size_t)m.n * m.T;
-    const unsigned g = grid_for(total, 256) > (1u << 20) ? (1u << 20) : grid_for(total, 256);
-    k_tiles_to_rows<<<g, 256, 0, s>>>(m, d_rows);
+    k_tiles_to_rows<<<capped_grid(total, 256, 1u << 20), 256, 0, s>>>(m, d_rows);
     return cudaGetLastError();
 }
 
@@ -387,12 +465,16 @@ cudaError_t launch_copy_matrix(const DevMat &dst, const DevMat &src, cudaStream_
     if (dst.T == 0) return cudaSuccess;
     cudaError_t e = cudaMemcpyAsync(dst.bits, src.bits, (size_t)src.T * src.T * 512, cudaMemcpyDeviceToDevice, s);
     if (e != cudaSuccess) return e;
+    e = cudaMemcpyAsync(dst.nnz, src.nnz, (size_t)src.T * src.T * 4, cudaMemcpyDeviceToDevice, s);
+    if (e != cudaSuccess) return e;
     return cudaMemcpyAsync(dst.occ, src.occ, (size_t)src.T * src.ow * 4, cudaMemcpyDeviceToDevice, s);
 }
 
 cudaError_t launch_clear_matrix(const DevMat &m, cudaStream_t s) {
     if (m.T == 0) return cudaSuccess;
     cudaError_t e = cudaMemsetAsync(m.bits, 0, (size_t)m.T * m.T * 512, s);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(m.nnz, 0, (size_t)m.T * m.T * 4, s);
     if (e != cudaSuccess) return e;
     return cudaMemsetAsync(m.occ, 0, (size_t)m.T * m.ow * 4, s);
 }
@@ -401,7 +483,8 @@ cudaError_t launch_hash_count(const DevMat &m, const uint32_t *d_pow11, const ui
                               unsigned long long *d_out, cudaStream_t s) {
     cudaError_t e = cudaMemsetAsync(d_out, 0, 2 * sizeof(unsigned long long), s);
     if (e != cudaSuccess || m.T == 0) return e;
-    k_hash_count<<<m.T, 64, 0, s>>>(m, d_pow11, d_pow13, d_out);
+    const size_t tiles = (size_t)m.T * m.T;
+    k_hash_count<<<(unsigned)((tiles + 3) / 4), 256, 0, s>>>(m, d_pow11, d_pow13, d_out);
     return cudaGetLastError();
 }
 

@@ -133,11 +133,22 @@ def label_map(grammar: CnfGrammar, graph: EdgeGraph) -> tuple[np.ndarray, np.nda
 
 
 class PreparedQuery:
-    """Matrices of one query allocated on the device (reusable across runs)."""
+    """Matrices of one query allocated on the device (reusable across runs).
 
-    def __init__(self, ctx: capi.Context, grammar: CnfGrammar, graph: EdgeGraph):
+    order: "auto" relabels vertices with the library's heuristic when it finds
+    one (results are reported in original vertex ids either way), None keeps
+    vertex v at index v, or an explicit permutation array."""
+
+    def __init__(self, ctx: capi.Context, grammar: CnfGrammar, graph: EdgeGraph, order="auto"):
         self.ctx, self.grammar, self.graph = ctx, grammar, graph
-        self.mats = [ctx.matrix(graph.n) for _ in grammar.nonterminals]
+        self.order = None
+        if isinstance(order, str) and order == "auto":
+            perm = capi.suggest_order(graph.n, graph.src, graph.label, graph.dst, ctx.lib)
+            if not np.array_equal(perm, np.arange(graph.n, dtype=np.uint32)):
+                self.order = ctx.order(perm)
+        elif order is not None:
+            self.order = ctx.order(np.asarray(order, dtype=np.uint32))
+        self.mats = [ctx.matrix(graph.n, self.order) for _ in grammar.nonterminals]
         self.off, self.lm = label_map(grammar, graph)
 
     def load(self) -> None:
@@ -153,6 +164,9 @@ class PreparedQuery:
         for m in self.mats:
             m.destroy()
         self.mats = []
+        if self.order is not None:
+            self.order.destroy()
+            self.order = None
 
     def run(self, driver="engine", variant="auto", use_graph=True) -> QueryResult:
         t0 = time.perf_counter()

@@ -92,7 +92,22 @@ typedef struct cfpq_closure_stats {
     double device_ms;           /* device time of the closure (CUDA events) */
     uint64_t kernel_launches;   /* kernels launched by this call */
     uint64_t variant_items[5];  /* work items per cfpq_variant */
+    uint64_t bytes_staged;      /* operand bytes staged global -> shared by product kernels */
+    uint64_t out_words;         /* non-zero 64-bit result words merged into heads */
+    uint64_t new_words;         /* result words that carried new bits */
 } cfpq_closure_stats;
+
+/* Per-kernel device times of the last closure run with
+ * opts->log_products & CFPQ_LOG_KERNELS (every launch bracketed by CUDA events
+ * on the context's stream; the iteration loop then runs from the host instead
+ * of a CUDA graph). */
+#define CFPQ_LOG_KERNELS 1
+#define CFPQ_LOG_PRODUCTS 2
+typedef struct cfpq_kernel_profile {
+    double plan_ms, product_ms, advance_ms, iter_end_ms;
+    uint64_t plan_launches, product_launches, advance_launches, iter_end_launches;
+} cfpq_kernel_profile;
+int cfpq_last_kernel_profile(cfpq_ctx *ctx, cfpq_kernel_profile *out);
 
 /* ---- context ------------------------------------------------------------ */
 
@@ -105,10 +120,35 @@ int cfpq_ctx_destroy(cfpq_ctx *ctx);
 int cfpq_ctx_synchronize(cfpq_ctx *ctx);
 /* Number of SMs of the context's device. */
 int cfpq_ctx_num_sms(const cfpq_ctx *ctx);
+/* The context's CUDA stream (a cudaStream_t), for callers that order their own
+ * work or timing events with the library's. */
+void *cfpq_ctx_stream(const cfpq_ctx *ctx);
 /* Description of the last error on this thread ("" if none). */
 const char *cfpq_last_error(void);
 /* Library ABI version (CFPQ_B200_ABI_VERSION). */
 int cfpq_abi_version(void);
+
+/* ---- vertex orders -------------------------------------------------------- */
+
+/* A relabeling of the n vertices of one query, shared by its matrices:
+ * perm[v] is the internal index of vertex v (perm is a permutation of 0..n-1).
+ * A matrix created with an order stores bit (perm[r], perm[c]) for (r, c);
+ * every entry point that takes or returns coordinates, row bits, hashes or
+ * counts still works in original vertex ids, so results are identical to an
+ * unordered matrix.  Products and closures need all operands to share one
+ * order.  The order exists so that the bits of sparse results cluster into
+ * few 64x64 tiles, which the engine skips when empty.  No reference
+ * counterpart (the reference stores vertex v at index v,
+ * cuda/naive-gpu/GpuMatrix.cpp:15-18). */
+typedef struct cfpq_order cfpq_order;
+int cfpq_order_create(cfpq_ctx *ctx, uint32_t n, const uint32_t *perm, cfpq_order **out);
+int cfpq_order_destroy(cfpq_ctx *ctx, cfpq_order *order);
+/* Host-side heuristic: suggests perm for a graph given as an edge list.  Keeps
+ * the identity when most edges already join nearby vertex ids; otherwise
+ * groups vertices by the set of labels on their incoming and outgoing edges
+ * and orders each group breadth-first (seeds by decreasing degree). */
+int cfpq_order_suggest(uint32_t n, const uint32_t *from, const uint32_t *label, const uint32_t *to,
+                       size_t nedges, uint32_t *perm_out);
 
 /* ---- matrices ----------------------------------------------------------- */
 
@@ -117,6 +157,8 @@ int cfpq_abi_version(void);
  * (cuda/naive-gpu/Multiplication.cu:103-119) and
  * gpu_m4ri::allocate_matrix_device (gpuMemoryManagement.cu:51-55). */
 int cfpq_matrix_create(cfpq_ctx *ctx, uint32_t n, cfpq_matrix **out);
+/* Same with a vertex order (order->n must equal n; order may be NULL). */
+int cfpq_matrix_create_ordered(cfpq_ctx *ctx, uint32_t n, cfpq_order *order, cfpq_matrix **out);
 int cfpq_matrix_destroy(cfpq_ctx *ctx, cfpq_matrix *m);
 uint32_t cfpq_matrix_size(const cfpq_matrix *m);
 
@@ -141,6 +183,13 @@ int cfpq_matrix_set_bits_device(cfpq_ctx *ctx, cfpq_matrix *m, const uint32_t *d
 int cfpq_load_edges(cfpq_ctx *ctx, cfpq_matrix *const *mats, size_t nmats, const uint32_t *from,
                     const uint32_t *label, const uint32_t *to, size_t nedges, const uint32_t *label_offsets,
                     const uint32_t *label_mats, uint32_t nlabels);
+/* Same as cfpq_load_edges with from / label / to already in device memory
+ * (label_offsets and label_mats stay host arrays).  Asynchronous on the
+ * context's stream; out-of-range coordinates are reported by the next
+ * synchronising call of the context. */
+int cfpq_load_edges_device(cfpq_ctx *ctx, cfpq_matrix *const *mats, size_t nmats, const uint32_t *d_from,
+                           const uint32_t *d_label, const uint32_t *d_to, size_t nedges,
+                           const uint32_t *label_offsets, const uint32_t *label_mats, uint32_t nlabels);
 /* Sets the diagonal (epsilon nonterminals, cfpq-cpp/Grammar.h:47-51). */
 int cfpq_matrix_set_diagonal(cfpq_ctx *ctx, cfpq_matrix *m);
 /* Clears all bits. */
@@ -163,6 +212,11 @@ int cfpq_matrix_hash_count(cfpq_ctx *ctx, const cfpq_matrix *m, uint64_t *hash,
                            uint64_t *count);
 /* Number of set bits only. */
 int cfpq_matrix_count(cfpq_ctx *ctx, const cfpq_matrix *m, uint64_t *count);
+/* Diagnostics: the matrix's 64x64-bit tile statistics as the engine keeps
+ * them.  occ_out: T*ceil(T/32) words (bit tj of row ti = tile occupied);
+ * nnz_out: T*T counts (set bits per tile), T = ceil(n/64).  Either may be NULL.
+ * No reference counterpart (tile statistics are this engine's own). */
+int cfpq_matrix_tile_stats(cfpq_ctx *ctx, const cfpq_matrix *m, uint32_t *occ_out, uint32_t *nnz_out);
 /* hash/count of several matrices with one synchronisation. */
 int cfpq_hash_count_many(cfpq_ctx *ctx, cfpq_matrix *const *mats, size_t nmats, uint64_t *hashes,
                          uint64_t *counts);

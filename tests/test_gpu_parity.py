@@ -26,6 +26,23 @@ def upload(ctx, n, rows):
     return m
 
 
+def tile_popcounts(rows, n):
+    T = (n + 63) // 64
+    padded = np.zeros((T * 64, T), dtype=np.uint64)
+    padded[:n] = rows
+    return np.bitwise_count(padded).reshape(T, 64, T).sum(axis=1).astype(np.uint32)
+
+
+def check_tile_stats(m, rows):
+    """The engine's tile populations are exact and occupancy covers every non-empty tile."""
+    occ, nnz = m.tile_stats()
+    exp = tile_popcounts(rows, m.n)
+    assert np.array_equal(nnz, exp)
+    T = exp.shape[0]
+    occ_bits = np.unpackbits(occ.view(np.uint8), axis=1, bitorder="little")[:, :T].astype(bool)
+    assert not np.any((exp > 0) & ~occ_bits)
+
+
 @pytest.mark.parametrize("variant", ["plain", "lop3"])
 @pytest.mark.parametrize("n", SIZES)
 def test_add_mul_random(ctx, oracle, variant, n):
@@ -39,6 +56,7 @@ def test_add_mul_random(ctx, oracle, variant, n):
         got = mc.download_rows()
         assert np.array_equal(got, exp), f"n={n} density={density}"
         assert ch == ch_exp
+        check_tile_stats(mc, exp)
         # a second identical product cannot change anything
         assert ctx.add_mul(mc, ma, mb, variant) is False
         for m in (ma, mb, mc):
@@ -103,6 +121,40 @@ def test_set_bits_and_diagonal(ctx, oracle):
     m.destroy()
 
 
+@pytest.mark.parametrize("n", [1, 63, 130, 700])
+def test_ordered_matrices(ctx, pkg, oracle, n):
+    """Matrices stored under a vertex relabeling behave exactly like unordered ones."""
+    rng = np.random.default_rng(n + 99)
+    order = ctx.order(rng.permutation(n).astype(np.uint32))
+    a, b, c = rand_rows(rng, n, 0.03), rand_rows(rng, n, 0.03), rand_rows(rng, n, 0.01)
+    ma, mb, mc = (ctx.matrix(n, order) for _ in range(3))
+    for m, rows in ((ma, a), (mb, b), (mc, c)):
+        m.upload_rows(rows)
+        assert np.array_equal(m.download_rows(), rows)
+        assert m.hash_count() == oracle.hash_count(rows, n)
+    exp = c.copy()
+    ch_exp = oracle.add_mul(exp, a, b, n)
+    for variant in ("lop3", "plain"):
+        mc.upload_rows(c)
+        assert ctx.add_mul(mc, ma, mb, variant) == ch_exp
+        assert np.array_equal(mc.download_rows(), exp)
+        assert mc.hash_count() == oracle.hash_count(exp, n)
+    r, cc = rng.integers(0, n, 50), rng.integers(0, n, 50)
+    md = ctx.matrix(n, order)
+    md.set_bits(r, cc)
+    md.set_diagonal()
+    expd = np.zeros((n, (n + 63) // 64), dtype=np.uint64)
+    for i, j in list(zip(r, cc)) + [(i, i) for i in range(n)]:
+        expd[i, j // 64] |= np.uint64(1) << np.uint64(j % 64)
+    assert np.array_equal(md.download_rows(), expd)
+    plain = ctx.matrix(n)
+    with pytest.raises(pkg.capi.CfpqError):
+        ctx.add_mul(plain, ma, mb)
+    for m in (ma, mb, mc, md, plain):
+        m.destroy()
+    order.destroy()
+
+
 def test_set_bits_out_of_range_is_an_error(ctx, pkg):
     m = ctx.matrix(10)
     with pytest.raises(pkg.capi.CfpqError) as e:
@@ -123,16 +175,18 @@ def _oracle_run(oracle, gp, rp):
         return p.results(), [p.matrix(i) for i in range(len(p.names))], p.names
 
 
-def _check_query(ctx, pkg, oracle, wl, tmp_path, **kw):
+def _check_query(ctx, pkg, oracle, wl, tmp_path, order="auto", **kw):
     gp, rp = _write(wl, tmp_path)
     exp_lines, exp_mats, names = _oracle_run(oracle, gp, rp)
-    q = pkg.query.PreparedQuery(ctx, wl.grammar, wl.graph)
+    q = pkg.query.PreparedQuery(ctx, wl.grammar, wl.graph, order=order)
     try:
         res = q.run(**kw)
         assert res.lines == exp_lines
         assert q.grammar.nonterminals == names
         for i, m in enumerate(q.mats):
             assert np.array_equal(m.download_rows(), exp_mats[i]), names[i]
+            if q.order is None:
+                check_tile_stats(m, exp_mats[i])
         return res
     finally:
         q.close()
@@ -148,10 +202,11 @@ def test_closure_brackets_full_size(ctx, pkg, oracle, tmp_path, kw):
         assert res.stats["iterations"] > 1
 
 
+@pytest.mark.parametrize("order", ["auto", None])
 @pytest.mark.parametrize("n,seed", [(512, 3), (2048, 4), (8192, 1)])
-def test_closure_same_generation(ctx, pkg, oracle, tmp_path, n, seed):
+def test_closure_same_generation(ctx, pkg, oracle, tmp_path, n, seed, order):
     wl = pkg.workloads.ontology_query(n, seed)
-    _check_query(ctx, pkg, oracle, wl, tmp_path)
+    _check_query(ctx, pkg, oracle, wl, tmp_path, order=order)
 
 
 @pytest.mark.parametrize("seed", [1, 2, 3])
