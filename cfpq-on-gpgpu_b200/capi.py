@@ -31,7 +31,7 @@ EXPORTED = (
     "cfpq_matrix_count", "cfpq_hash_count_many", "cfpq_add_mul", "cfpq_closure", "cfpq_closure_batch",
     "cfpq_product_log", "cfpq_last_kernel_profile", "cfpq_ctx_stream", "cfpq_load_edges_device",
     "cfpq_matrix_tile_stats", "cfpq_order_create", "cfpq_order_destroy", "cfpq_order_suggest",
-    "cfpq_matrix_create_ordered",
+    "cfpq_matrix_create_ordered", "cfpq_hash_count_rows_noalloc", "cfpq_noalloc_last_error",
 )
 
 

@@ -212,6 +212,25 @@ int cfpq_matrix_hash_count(cfpq_ctx *ctx, const cfpq_matrix *m, uint64_t *hash,
                            uint64_t *count);
 /* Number of set bits only. */
 int cfpq_matrix_count(cfpq_ctx *ctx, const cfpq_matrix *m, uint64_t *count);
+
+/* Result line (hash, count) of an n x n answer matrix that the caller keeps in
+ * its own device memory as row bits (n rows of ceil(n/64) words, column c at
+ * bit c % 64 of word c / 64), without allocating any memory.  No counterpart
+ * in the reference.  It is for callers that cannot call cudaMalloc: hosts
+ * whose own pool allocator owns the device memory, and latency-sensitive loops
+ * that cannot take the device synchronisation an allocation may cause.  The
+ * caller passes the input rows and d_out, a device buffer of two 64-bit words
+ * that receives (hash, count).  Asynchronous on `stream` (a cudaStream_t, NULL
+ * = the default stream) of `device`.  Scratch memory is a fixed device array
+ * in the library sized for n <= CFPQ_NOALLOC_MAX_N; larger n is rejected with
+ * CFPQ_ERR_UNSUPPORTED.  The first call on a device looks that array up, so
+ * make it before any stream capture.  All calls on a device share the array:
+ * calls that overlap on the GPU race and must be ordered by the caller.
+ * Errors are described by cfpq_noalloc_last_error(). */
+#define CFPQ_NOALLOC_MAX_N 65536u
+int cfpq_hash_count_rows_noalloc(int device, const uint64_t *d_rows, uint32_t n, unsigned long long *d_out,
+                                 void *stream);
+const char *cfpq_noalloc_last_error(void);
 /* Diagnostics: the matrix's 64x64-bit tile statistics as the engine keeps
  * them.  occ_out: T*ceil(T/32) words (bit tj of row ti = tile occupied);
  * nnz_out: T*T counts (set bits per tile), T = ceil(n/64).  Either may be NULL.
