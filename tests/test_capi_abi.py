@@ -1,0 +1,70 @@
+"""The C ABI library without a GPU: it loads, exports every entry point that
+include/*.h declares, and its host-only helpers behave; no compute calls."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "cfpq_b200.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(cfpq_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_function(pkg):
+    lib = pkg.capi.load_library()
+    names = declared_functions()
+    assert len(names) >= 30
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(names) == set(pkg.capi.EXPORTED)
+
+
+def test_abi_version(pkg):
+    lib = pkg.capi.load_library()
+    assert lib.cfpq_abi_version() == 1
+
+
+def test_null_arguments_are_errors_not_crashes(pkg):
+    lib = pkg.capi.load_library()
+    assert lib.cfpq_ctx_create(0, None) == pkg.capi.ERR_INVALID
+    assert lib.cfpq_last_error()
+    assert lib.cfpq_ctx_destroy(None) == pkg.capi.OK
+    assert lib.cfpq_product_log(None, None, 0) == 0
+
+
+def test_context_without_gpu_reports_an_error(pkg):
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(pkg.capi.CfpqError):
+        pkg.capi.Context(0)
+
+
+def test_order_suggest_identity_for_local_ids(pkg):
+    g = pkg.workloads.chain_graph(4096, 2.0, 0.9, 64, ["a", "b"], 3)
+    perm = pkg.capi.suggest_order(g.n, g.src, g.label, g.dst)
+    assert np.array_equal(perm, np.arange(g.n))
+
+
+def test_order_suggest_is_a_permutation_and_clusters(pkg):
+    g = pkg.workloads.ontology_graph(2048, 4)
+    perm = pkg.capi.suggest_order(g.n, g.src, g.label, g.dst)
+    assert np.array_equal(np.sort(perm), np.arange(g.n))
+    tiles = lambda p: len(set(zip((p[g.src] // 64).tolist(), (p[g.dst] // 64).tolist())))
+    assert tiles(perm.astype(np.int64)) < tiles(np.arange(g.n))
+
+
+def test_order_suggest_rejects_out_of_range(pkg):
+    lib = pkg.capi.load_library()
+    src = np.array([0, 5], dtype=np.uint32)
+    out = np.zeros(4, dtype=np.uint32)
+    rc = lib.cfpq_order_suggest(4, src.ctypes.data, src.ctypes.data, src.ctypes.data, 2, out.ctypes.data)
+    assert rc == pkg.capi.ERR_INVALID
