@@ -160,9 +160,8 @@ static inline uint32_t tiles_for(uint32_t n) { return (n + 63) / 64; }
 // Upper bound of the work items one product term can emit per iteration:
 // tile-rows x column blocks x inner-dimension groups.
 static inline size_t item_capacity(uint32_t T, int tpb) {
-    const uint32_t ow = (T + 31) / 32;
-    const uint32_t groups = (ow + kgroup_words(ow) - 1) / kgroup_words(ow);
-    return (size_t)T * ((T + tpb - 1) / tpb) * groups;
+    const uint32_t E = entries_per_item(T);
+    return (size_t)T * ((T + tpb - 1) / tpb) * ((T + E - 1) / E);
 }
 
 static int alloc_devmat(uint32_t n, DevMat *d) {

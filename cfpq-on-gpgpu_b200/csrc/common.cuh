@@ -101,10 +101,11 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
 }
 
 // Work item: (product, output tile-row ti, output tile-column block tjb,
-// inner-dimension word kw = k-tiles 32*kw .. 32*kw+31).  Items of the same
-// output block with different kw are independent: their partial products are
-// OR-ed into the head atomically.  Fields: p 21 bits, ti 15, tjb 12, kw 12
-// (n <= 2^21).
+// chunk kw).  The k-tiles tk that contribute to the block (occupied P tile
+// (ti, tk) and a non-empty Q block (tk, tjb)), taken in increasing tk order,
+// are cut into chunks of entries_per_item(T); the item processes chunk kw.
+// Items of the same output block are independent: their partial products are
+// OR-ed into the head atomically.  Fields: p 21 bits, ti 15, tjb 12, kw 12.
 __host__ __device__ inline uint64_t make_item(uint32_t p, uint32_t ti, uint32_t tjb, uint32_t kw) {
     return ((uint64_t)p << 39) | ((uint64_t)ti << 24) | ((uint64_t)tjb << 12) | (uint64_t)kw;
 }
@@ -113,12 +114,11 @@ __host__ __device__ inline uint32_t item_ti(uint64_t it) { return (uint32_t)((it
 __host__ __device__ inline uint32_t item_tjb(uint64_t it) { return (uint32_t)((it >> 12) & 0xFFF); }
 __host__ __device__ inline uint32_t item_kw(uint64_t it) { return (uint32_t)(it & 0xFFF); }
 
-// The inner dimension of an output block is split into at most kKSplit groups
-// of consecutive occupancy words; item kw = group index.
-constexpr uint32_t kKSplit = 4;
-__host__ __device__ inline uint32_t kgroup_words(uint32_t ow) {
-    const uint32_t g = (ow + kKSplit - 1) / kKSplit;
-    return g ? g : 1;
+// Contributing k-tiles per work item: short chains keep the per-item latency
+// low; at most 16 chunks per output block bound the item count.
+__host__ __device__ inline uint32_t entries_per_item(uint32_t T) {
+    const uint32_t e = T / 16;
+    return e > 8 ? e : 8;
 }
 
 __host__ __device__ inline size_t tile_offset(uint32_t T, uint32_t ti, uint32_t tj) {

@@ -54,6 +54,8 @@ struct __align__(128) Lop3Smem {
     uint16_t stile[kMaxTiles];   // sparse k-list
     uint16_t smask[kMaxTiles];
     uint16_t cand[kMaxTiles];    // occupied P tiles of the item's tile-row
+    uint16_t cmask[kMaxTiles];   // their Q block occupancy
+    uint32_t rball[kMaxTiles / 32], roff[kMaxTiles / 32];  // per-round ballots and rank offsets
     uint32_t nc, nd, ns;
     uint32_t item;
 };
@@ -113,10 +115,8 @@ __global__ void __launch_bounds__(kThreads, 4)
         if (warp == 0) {
             uint32_t nc = 0;
             const uint32_t *prow = P.occ + (size_t)ti * ow;
-            const uint32_t G = kgroup_words(ow);
-            const uint32_t w_begin = kw * G, w_end = min(ow, w_begin + G);
-            for (uint32_t base = w_begin; base < w_end; base += 32) {
-                uint32_t bits = (base + lane < w_end) ? prow[base + lane] : 0u;
+            for (uint32_t base = 0; base < ow; base += 32) {
+                uint32_t bits = (base + lane < ow) ? prow[base + lane] : 0u;
                 const uint32_t cnt = __popc(bits);
                 uint32_t pre = cnt;  // inclusive scan over lanes
 #pragma unroll
@@ -138,10 +138,41 @@ __global__ void __launch_bounds__(kThreads, 4)
             }
         }
         __syncthreads();
-        for (uint32_t c = tid; c < S.nc; c += kThreads) {
-            const uint32_t tk = S.cand[c];
-            const uint32_t mask = (Q.occ[(size_t)tk * ow + qword] >> qshift) & ((1u << kBJ) - 1);
+        // rank the candidates with a non-empty Q block in increasing tk order
+        // (ballot per round of 32) and keep ranks [kw*E, kw*E + E)
+        const uint32_t nc = S.nc, rounds = (nc + 31) / 32;
+        for (uint32_t r = warp; r < rounds; r += kThreads / 32) {
+            const uint32_t c = r * 32 + lane;
+            uint32_t mask = 0;
+            if (c < nc) mask = (Q.occ[(size_t)S.cand[c] * ow + qword] >> qshift) & ((1u << kBJ) - 1);
+            const unsigned ball = __ballot_sync(kFull, mask != 0);
+            if (c < nc) S.cmask[c] = (uint16_t)mask;
+            if (lane == 0) S.rball[r] = ball;
+        }
+        __syncthreads();
+        if (warp == 0) {  // exclusive prefix of the per-round counts
+            uint32_t carry = 0;
+            for (uint32_t base = 0; base < rounds; base += 32) {
+                const uint32_t r = base + lane;
+                const uint32_t cnt = r < rounds ? __popc(S.rball[r]) : 0;
+                uint32_t pre = cnt;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t v = __shfl_up_sync(kFull, pre, o);
+                    if (lane >= (uint32_t)o) pre += v;
+                }
+                if (r < rounds) S.roff[r] = carry + pre - cnt;
+                carry += __shfl_sync(kFull, pre, 31);
+            }
+        }
+        __syncthreads();
+        const uint32_t E = entries_per_item(T), rank_lo = kw * E, rank_hi = rank_lo + E;
+        for (uint32_t c = tid; c < nc; c += kThreads) {
+            const uint32_t mask = S.cmask[c];
             if (!mask) continue;
+            const uint32_t rank = S.roff[c >> 5] + __popc(S.rball[c >> 5] & ((1u << (c & 31)) - 1));
+            if (rank < rank_lo || rank >= rank_hi) continue;
+            const uint32_t tk = S.cand[c];
             triples += __popc(mask);
             if (P.nnz[(size_t)ti * T + tk] > kSparseMax) {
                 const uint32_t pos = atomicAdd(&S.nd, 1u);

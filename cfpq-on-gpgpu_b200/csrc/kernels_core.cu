@@ -300,32 +300,39 @@ __global__ void k_plan(const ProdDesc *__restrict__ prods, uint32_t nprods, uint
     const uint32_t bpw = 32 / tpb;  // blocks per occupancy word
     const uint32_t bmask = tpb == 32 ? 0xffffffffu : ((1u << tpb) - 1);
     bool emitted = false;
-    const uint32_t G = kgroup_words(ow);
-    for (uint32_t kw = 0; kw * G < ow; ++kw) {  // inner-dimension group
-        const uint32_t pw_end = min(ow, kw * G + G);
-        for (uint32_t base = 0; base < ow; base += 32) {
-            const uint32_t w = base + lane;
-            uint32_t acc = 0;
-            for (uint32_t pw = kw * G; pw < pw_end; ++pw) {
-                uint32_t bits = prow[pw];
-                while (bits) {
-                    const uint32_t tk = pw * 32 + (__ffs(bits) - 1);
-                    bits &= bits - 1;
-                    if (w < ow) acc |= Q.occ[(size_t)tk * ow + w];
+    const uint32_t E = entries_per_item(pd.T);
+    for (uint32_t base = 0; base < ow; base += 32) {
+        const uint32_t w = base + lane;
+        // contributing k-tiles per block of this lane's occupancy word (at most 4 blocks)
+        uint32_t cnt[4] = {0, 0, 0, 0};
+        for (uint32_t pw = 0; pw < ow; ++pw) {
+            uint32_t bits = prow[pw];
+            while (bits) {
+                const uint32_t tk = pw * 32 + (__ffs(bits) - 1);
+                bits &= bits - 1;
+                if (w < ow) {
+                    const uint32_t m = Q.occ[(size_t)tk * ow + w];
+#pragma unroll
+                    for (uint32_t h = 0; h < 4; ++h)
+                        if (h < bpw) cnt[h] += ((m >> (h * tpb)) & bmask) != 0;
                 }
-                if (__all_sync(kFull, w >= ow || acc == 0xffffffffu)) break;
             }
-            for (uint32_t h = 0; h < bpw; ++h) {
-                const bool has = w < ow && ((acc >> (h * tpb)) & bmask) != 0;
-                const unsigned ball = __ballot_sync(kFull, has);
-                if (!ball) continue;
-                emitted = true;
-                uint32_t basepos = 0;
-                if (lane == 0) basepos = atomicAdd(&st->item_count, (uint32_t)__popc(ball));
-                basepos = __shfl_sync(kFull, basepos, 0);
-                if (has)
-                    items[basepos + __popc(ball & ((1u << lane) - 1))] = make_item(lo, ti, w * bpw + h, kw);
+        }
+        for (uint32_t h = 0; h < bpw; ++h) {
+            const uint32_t nitem = w < ow ? (cnt[h] + E - 1) / E : 0;
+            uint32_t pre = nitem;  // inclusive scan over lanes
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t v = __shfl_up_sync(kFull, pre, o);
+                if (lane >= (uint32_t)o) pre += v;
             }
+            const uint32_t total = __shfl_sync(kFull, pre, 31);
+            if (!total) continue;
+            emitted = true;
+            uint32_t basepos = 0;
+            if (lane == 0) basepos = atomicAdd(&st->item_count, total);
+            basepos = __shfl_sync(kFull, basepos, 0) + pre - nitem;
+            for (uint32_t j = 0; j < nitem; ++j) items[basepos + j] = make_item(lo, ti, w * bpw + h, j);
         }
     }
     if (emitted && lane == 0 && prod_seen) {

@@ -146,7 +146,10 @@ def seeded_inputs():
     return cases
 
 
-def run_reference(exe: str, out_dir: str, prefix: str, source: str) -> None:
+def run_reference(exe: str, out_dir: str, prefix: str, source: str, check_against: str | None = None) -> None:
+    """Run a reference executable on the seeded inputs.  With check_against, an
+    answer that differs from the `check_against`_<case> answer in out_dir is a
+    reference defect: it goes to ../golden_defects instead of the fixtures."""
     for name, wl in seeded_inputs().items():
         with tempfile.TemporaryDirectory() as d:
             gp, rp, ap = (os.path.join(d, x) for x in ("g.txt", "r.txt", "a.txt"))
@@ -155,6 +158,12 @@ def run_reference(exe: str, out_dir: str, prefix: str, source: str) -> None:
             if p.returncode != 0 or p.stderr:
                 raise RuntimeError(f"{exe} failed: {p.stderr.decode()[:400]}")
             case = os.path.join(out_dir, f"{prefix}_{name}")
+            if check_against:
+                ref_answer = os.path.join(out_dir, f"{check_against}_{name}", "expected.txt")
+                if os.path.exists(ref_answer) and open(ref_answer).read() != open(ap).read():
+                    case = os.path.join(os.path.dirname(os.path.abspath(out_dir)), "golden_defects",
+                                        f"{prefix}_{name}")
+                    source += " -- DIFFERS from the least fixpoint (see golden_defects)"
             os.makedirs(case, exist_ok=True)
             shutil.copy(gp, os.path.join(case, "grammar.txt"))
             shutil.copy(rp, os.path.join(case, "graph.txt"))
@@ -176,7 +185,8 @@ def main():
                       "reference m4riCPU (m4ri/main.cpp + cfpq-cpp, restated libm4ri subset)")
     if args.ref_gpu:
         run_reference(os.path.join(ref, "naiveGPU"), args.out, "naivegpu",
-                      "reference naiveGPU (cuda/naive-gpu + cfpq-cpp) built for sm_100a, run on a B200")
+                      "reference naiveGPU (cuda/naive-gpu + cfpq-cpp) built for sm_100a, run on a B200",
+                      check_against="m4ricpu")
 
 
 if __name__ == "__main__":

@@ -260,6 +260,25 @@ def test_batch_matches_single_queries(ctx, pkg, oracle, tmp_path):
             q.close()
 
 
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+GOLDEN_CASES = sorted(d for d in os.listdir(GOLDEN) if os.path.isdir(os.path.join(GOLDEN, d)))
+
+
+@pytest.mark.parametrize("case", GOLDEN_CASES)
+def test_engine_matches_golden(ctx, pkg, oracle, case):
+    """The engine (through the C ABI) and the b200GPU drop-in executable
+    reproduce every committed golden answer."""
+    d = os.path.join(GOLDEN, case)
+    gp, rp = os.path.join(d, "grammar.txt"), os.path.join(d, "graph.txt")
+    expected = oracle.parse_answer(open(os.path.join(d, "expected.txt")).read())
+    grammar, graph = pkg.query.CnfGrammar.from_file(gp), pkg.query.EdgeGraph.from_file(rp)
+    res = pkg.query.run_query(ctx, grammar, graph)
+    assert res.lines == expected
+    exe = os.path.join(os.path.dirname(pkg.capi.LIB_PATH), "..", "bin", "b200GPU")
+    got, _ = oracle.run_executable(exe, gp, rp)
+    assert got == expected
+
+
 def test_b200gpu_executable(pkg, oracle, tmp_path):
     exe = os.path.join(os.path.dirname(pkg.capi.LIB_PATH), "..", "bin", "b200GPU")
     wl = pkg.workloads.brackets_query(n=512, nedges=2048, seed=3)
