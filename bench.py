@@ -208,6 +208,42 @@ def cpu_baseline(wl, budget_s=12.0) -> dict:
             "answer": answer}
 
 
+def dense_product_kernels(ctx, capi, torch, stream, n=8192, density=0.3, reps=3):
+    """One dense product C |= A*B (n=8192, every tile populated) per variant:
+    the word-level rooflines.  Dense-equivalent work n^3 bit-MACs; LOP3 bound
+    = 32 bit-MACs per logic instruction at the calibrated logic rate."""
+    import numpy as np
+
+    rng = np.random.default_rng(5)
+    wpr = n // 64
+    rows = [np.packbits(rng.random((n, n)) < density, axis=1, bitorder="little").view(np.uint64).reshape(n, wpr)
+            for _ in range(2)]
+    a, b, c = ctx.matrix(n), ctx.matrix(n), ctx.matrix(n)
+    a.upload_rows(rows[0])
+    b.upload_rows(rows[1])
+    cal = ctx.calibrate()
+    out = {"n": n, "density": density, "calibrated_logic_ops_per_s": cal["logic_ops_per_s"],
+           "calibrated_logic_ops_per_clk_sm": cal["logic_ops_per_clk_sm"], "variants": {}}
+    for variant in ("lop3", "m4r", "plain"):
+        ms = []
+        for _ in range(reps if variant != "plain" else 1):
+            c.clear()
+            ctx.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ctx.add_mul(c, a, b, variant)
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        t = min(ms)
+        rate = n ** 3 / (t / 1e3)
+        out["variants"][variant] = {"ms": t, "tbitmac_per_s": rate / 1e12,
+                                    "frac_of_lop3_bound": rate / cal["bitmac_per_s"]}
+    for m in (a, b, c):
+        m.destroy()
+    return out
+
+
 def ours_arm(args, world, rank, local):
     import numpy as np
     import torch
@@ -354,6 +390,8 @@ def ours_arm(args, world, rank, local):
                         "dense_equiv_gbitops": st["dense_bitops"] / (total_ms / args.steps / 1e3) / 1e9,
                         "result": {k: list(v) for k, v in zip(grammar.nonterminals, lines)}},
         }
+        if not args.no_profile:
+            out["dense_product_kernels"] = dense_product_kernels(ctx, capi, torch, stream)
         if world == 1 and not args.no_cpu_baseline:
             cb = cpu_baseline(wl)
             answer = cb.pop("answer")

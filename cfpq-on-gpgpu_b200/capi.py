@@ -31,8 +31,13 @@ EXPORTED = (
     "cfpq_matrix_count", "cfpq_hash_count_many", "cfpq_add_mul", "cfpq_closure", "cfpq_closure_batch",
     "cfpq_product_log", "cfpq_last_kernel_profile", "cfpq_ctx_stream", "cfpq_load_edges_device",
     "cfpq_matrix_tile_stats", "cfpq_order_create", "cfpq_order_destroy", "cfpq_order_suggest",
-    "cfpq_matrix_create_ordered", "cfpq_hash_count_rows_noalloc", "cfpq_noalloc_last_error",
+    "cfpq_matrix_create_ordered", "cfpq_hash_count_rows_noalloc", "cfpq_noalloc_last_error", "cfpq_calibrate",
 )
+
+
+class Calibration(ctypes.Structure):
+    _fields_ = [("logic_ops_per_s", ctypes.c_double), ("logic_ops_per_clk_sm", ctypes.c_double),
+                ("bitmac_per_s", ctypes.c_double), ("ms", ctypes.c_double)]
 
 
 class CfpqError(RuntimeError):
@@ -135,6 +140,7 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "cfpq_order_destroy": ([vp, vp], i32),
         "cfpq_order_suggest": ([u32, vp, vp, vp, sz, vp], i32),
         "cfpq_matrix_create_ordered": ([vp, u32, vp, P(vp)], i32),
+        "cfpq_calibrate": ([vp, P(Calibration)], i32),
         "cfpq_load_edges_device": ([vp, P(vp), sz, vp, vp, vp, sz, vp, vp, u32], i32),
     }
     for name, (args, res) in sigs.items():
@@ -358,6 +364,11 @@ class Context:
         _check(self.lib, self.lib.cfpq_load_edges_device(self.handle, hs, len(mats), ctypes.c_void_p(d_src),
                                                          ctypes.c_void_p(d_label), ctypes.c_void_p(d_dst),
                                                          int(nedges), _ptr(off), _ptr(lm), off.size - 1))
+
+    def calibrate(self) -> dict:
+        c = Calibration()
+        _check(self.lib, self.lib.cfpq_calibrate(self.handle, ctypes.byref(c)))
+        return {k: getattr(c, k) for k, _ in c._fields_}
 
     def kernel_profile(self) -> dict:
         p = KernelProfile()

@@ -144,7 +144,7 @@ struct cfpq_ctx {
     std::unordered_map<uint32_t, PowTables> pow;
     std::vector<cfpq_matrix *> pool;  // zeroed spare matrices (deltas, alias copies)
     GraphCache gcache;
-    int lop3_grid = 0;
+    int lop3_grid = 0, m4r_grid = 0;
     std::vector<cfpq_product_record> log;
     cudaEvent_t kev[5] = {};
     cfpq_kernel_profile prof = {};
@@ -355,7 +355,8 @@ extern "C" int cfpq_ctx_create(int device, cfpq_ctx **out) {
     CUDA_TRY(cudaMalloc(&c->d_bad, 64));
     CUDA_TRY(cudaMallocHost(&c->h_st, sizeof(IterState)));
     CUDA_TRY(cudaMallocHost(&c->h_flag, 64));
-    c->lop3_grid = c->num_sms * product_lop3_blocks_per_sm();
+    c->lop3_grid = c->num_sms * product_tiled_blocks_per_sm(0);
+    c->m4r_grid = c->num_sms * product_tiled_blocks_per_sm(1);
     *out = c;
     return CFPQ_OK;
 }
@@ -674,7 +675,7 @@ static int read_flag(cfpq_ctx *ctx, uint32_t *dflag, int *changed) {
 }
 
 // Enqueue c |= a * b with the tiled LOP3 kernel (operands must not alias c).
-static int enqueue_tiled_product(cfpq_ctx *ctx, const DevMat &a, const DevMat &b, const DevMat &c) {
+static int enqueue_tiled_product(cfpq_ctx *ctx, const DevMat &a, const DevMat &b, const DevMat &c, int variant) {
     const uint32_t T = a.T;
     const int tpb = product_lop3_tiles_per_block();
     MatSlot hs[3];
@@ -689,10 +690,11 @@ static int enqueue_tiled_product(cfpq_ctx *ctx, const DevMat &a, const DevMat &b
     pd.qslot = 1;
     pd.T = T;
     pd.n = a.n;
-    const size_t cap = item_capacity(T, tpb);
+    pd.variant = (uint8_t)variant;
+    const size_t cap = std::max<size_t>(item_capacity(T, tpb), 1);
     TRY(ctx->slots.ensure(sizeof(hs)));
     TRY(ctx->prods.ensure(sizeof(pd)));
-    TRY(ctx->items.ensure(std::max<size_t>(cap, 1) * 8));
+    TRY(ctx->items.ensure(2 * cap * 8));
     IterState st;
     memset(&st, 0, sizeof(st));
     st.iter = 1;
@@ -702,9 +704,22 @@ static int enqueue_tiled_product(cfpq_ctx *ctx, const DevMat &a, const DevMat &b
     CUDA_TRY(cudaMemcpyAsync(ctx->prods.p, &pd, sizeof(pd), cudaMemcpyHostToDevice, ctx->stream));
     CUDA_TRY(cudaMemcpyAsync(ctx->d_st, ctx->h_st, sizeof(IterState), cudaMemcpyHostToDevice, ctx->stream));
     CUDA_TRY(launch_plan(ctx->prods.as<ProdDesc>(), 1, 0, T, ctx->slots.as<MatSlot>(), ctx->d_st,
-                         ctx->items.as<uint64_t>(), tpb, nullptr, ctx->stream));
-    CUDA_TRY(launch_product_lop3(ctx->prods.as<ProdDesc>(), ctx->slots.as<MatSlot>(), ctx->d_st,
-                                 ctx->items.as<uint64_t>(), nullptr, ctx->lop3_grid, ctx->stream));
+                         ctx->items.as<uint64_t>(), cap, tpb, nullptr, ctx->stream));
+    const int m4r = variant == CFPQ_VARIANT_M4R;
+    CUDA_TRY(launch_product_tiled(m4r, ctx->prods.as<ProdDesc>(), ctx->slots.as<MatSlot>(), ctx->d_st,
+                                  ctx->items.as<uint64_t>(), cap, nullptr, m4r ? ctx->m4r_grid : ctx->lop3_grid,
+                                  ctx->stream));
+    return CFPQ_OK;
+}
+
+// Product kernels of one closure iteration: one launch per item list in use.
+static int launch_products(cfpq_ctx *ctx, size_t list_cap, bool lop3, bool m4r, uint32_t *qchanged, cudaStream_t s) {
+    if (lop3)
+        CUDA_TRY(launch_product_tiled(0, ctx->prods.as<ProdDesc>(), ctx->slots.as<MatSlot>(), ctx->d_st,
+                                      ctx->items.as<uint64_t>(), list_cap, qchanged, ctx->lop3_grid, s));
+    if (m4r)
+        CUDA_TRY(launch_product_tiled(1, ctx->prods.as<ProdDesc>(), ctx->slots.as<MatSlot>(), ctx->d_st,
+                                      ctx->items.as<uint64_t>(), list_cap, qchanged, ctx->m4r_grid, s));
     return CFPQ_OK;
 }
 
@@ -733,7 +748,7 @@ extern "C" int cfpq_add_mul(cfpq_ctx *ctx, cfpq_matrix *c, const cfpq_matrix *a,
         }
         return read_flag(ctx, ctx->d_flag, changed);
     }
-    if (variant != CFPQ_VARIANT_LOP3)
+    if (variant != CFPQ_VARIANT_LOP3 && variant != CFPQ_VARIANT_M4R)
         return set_error(CFPQ_ERR_UNSUPPORTED, "variant %d is not available for add_mul", variant);
     // Snapshot semantics: operands that alias c are read from a copy.
     cfpq_matrix *ca = nullptr, *cb = nullptr;
@@ -752,7 +767,7 @@ extern "C" int cfpq_add_mul(cfpq_ctx *ctx, cfpq_matrix *c, const cfpq_matrix *a,
             db = cb->d;
         }
     }
-    TRY(enqueue_tiled_product(ctx, da, db, c->d));
+    TRY(enqueue_tiled_product(ctx, da, db, c->d, variant));
     CUDA_TRY(cudaMemcpyAsync(ctx->h_st, ctx->d_st, sizeof(IterState), cudaMemcpyDeviceToHost, ctx->stream));
     CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     if (ca) TRY(pool_give(ctx, ca, true));
@@ -779,7 +794,8 @@ struct ClosurePlan {
     std::vector<ProdDesc> prods;
     std::vector<cfpq_matrix *> deltas;
     uint32_t slot_rows = 0, prod_rows = 0;
-    size_t item_cap = 0;
+    size_t item_cap = 0;  // per item list
+    bool uses_lop3 = false, uses_m4r = false;
 };
 
 }  // namespace
@@ -841,7 +857,8 @@ static int build_plan(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, int variant
                 pd.p_delta = term == 0;
                 pd.q_delta = term == 1;
                 pd.term = term;
-                pd.variant = (uint8_t)variant;
+                pd.variant = (uint8_t)(variant == CFPQ_VARIANT_M4R ? CFPQ_VARIANT_M4R : CFPQ_VARIANT_LOP3);
+                (pd.variant == CFPQ_VARIANT_M4R ? pl->uses_m4r : pl->uses_lop3) = true;
                 pd.query = (uint32_t)qi;
                 pd.rule = (uint32_t)r;
                 pd.T = T;
@@ -853,6 +870,7 @@ static int build_plan(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, int variant
             }
         }
     }
+    pl->item_cap = std::max<size_t>(pl->item_cap, 1);
     return CFPQ_OK;
 }
 
@@ -860,10 +878,9 @@ static int enqueue_iteration(cfpq_ctx *ctx, const ClosurePlan &pl, const QueryTr
                              cudaGraphConditionalHandle handle, int use_handle) {
     const int tpb = product_lop3_tiles_per_block();
     CUDA_TRY(launch_plan(ctx->prods.as<ProdDesc>(), (uint32_t)pl.prods.size(), 0, pl.prod_rows,
-                         ctx->slots.as<MatSlot>(), ctx->d_st, ctx->items.as<uint64_t>(), tpb,
+                         ctx->slots.as<MatSlot>(), ctx->d_st, ctx->items.as<uint64_t>(), pl.item_cap, tpb,
                          ctx->prod_seen.as<uint32_t>(), ctx->stream));
-    CUDA_TRY(launch_product_lop3(ctx->prods.as<ProdDesc>(), ctx->slots.as<MatSlot>(), ctx->d_st,
-                                 ctx->items.as<uint64_t>(), qt.changed, ctx->lop3_grid, ctx->stream));
+    TRY(launch_products(ctx, pl.item_cap, pl.uses_lop3, pl.uses_m4r, qt.changed, ctx->stream));
     CUDA_TRY(launch_advance(ctx->slots.as<MatSlot>(), (uint32_t)pl.slots.size(), pl.slot_rows, ctx->d_st,
                             ctx->stream));
     CUDA_TRY(launch_iter_end(ctx->d_st, qt, handle, use_handle, ctx->stream));
@@ -876,11 +893,10 @@ static int enqueue_iteration_timed(cfpq_ctx *ctx, const ClosurePlan &pl, const Q
     cudaStream_t s = ctx->stream;
     CUDA_TRY(cudaEventRecord(ctx->kev[0], s));
     CUDA_TRY(launch_plan(ctx->prods.as<ProdDesc>(), (uint32_t)pl.prods.size(), 0, pl.prod_rows,
-                         ctx->slots.as<MatSlot>(), ctx->d_st, ctx->items.as<uint64_t>(), tpb,
+                         ctx->slots.as<MatSlot>(), ctx->d_st, ctx->items.as<uint64_t>(), pl.item_cap, tpb,
                          ctx->prod_seen.as<uint32_t>(), s));
     CUDA_TRY(cudaEventRecord(ctx->kev[1], s));
-    CUDA_TRY(launch_product_lop3(ctx->prods.as<ProdDesc>(), ctx->slots.as<MatSlot>(), ctx->d_st,
-                                 ctx->items.as<uint64_t>(), qt.changed, ctx->lop3_grid, s));
+    TRY(launch_products(ctx, pl.item_cap, pl.uses_lop3, pl.uses_m4r, qt.changed, s));
     CUDA_TRY(cudaEventRecord(ctx->kev[2], s));
     CUDA_TRY(launch_advance(ctx->slots.as<MatSlot>(), (uint32_t)pl.slots.size(), pl.slot_rows, ctx->d_st, s));
     CUDA_TRY(cudaEventRecord(ctx->kev[3], s));
@@ -903,6 +919,22 @@ static int accumulate_kernel_times(cfpq_ctx *ctx) {
     return CFPQ_OK;
 }
 
+extern "C" int cfpq_calibrate(cfpq_ctx *ctx, cfpq_calibration *out) {
+    TRY(use_device(ctx));
+    if (!out) return set_error(CFPQ_ERR_INVALID, "null argument");
+    memset(out, 0, sizeof(*out));
+    TRY(ctx->stage.ensure((size_t)ctx->num_sms * 8 * 256 * 4));
+    double ops = 0, ms = 0;
+    CUDA_TRY(measure_logic_rate(ctx->num_sms, ctx->stage.as<uint32_t>(), ctx->stream, ctx->ev0, ctx->ev1, &ops, &ms));
+    int clk_khz = 0;
+    CUDA_TRY(cudaDeviceGetAttribute(&clk_khz, cudaDevAttrClockRate, ctx->device));
+    out->logic_ops_per_s = ops;
+    out->logic_ops_per_clk_sm = clk_khz ? ops / ctx->num_sms / (clk_khz * 1e3) : 0;
+    out->bitmac_per_s = 32.0 * ops;
+    out->ms = ms;
+    return CFPQ_OK;
+}
+
 extern "C" int cfpq_last_kernel_profile(cfpq_ctx *ctx, cfpq_kernel_profile *out) {
     if (!ctx || !out) return set_error(CFPQ_ERR_INVALID, "null argument");
     *out = ctx->prof;
@@ -916,7 +948,8 @@ static int get_loop_graph(cfpq_ctx *ctx, const ClosurePlan &pl, const QueryTrack
                                  (uint64_t)pl.slots.size(),           (uint64_t)pl.slot_rows,
                                  (uint64_t)(uintptr_t)ctx->items.p,   (uint64_t)(uintptr_t)ctx->prod_seen.p,
                                  (uint64_t)(uintptr_t)qt.changed,     (uint64_t)(uintptr_t)qt.last_iter,
-                                 (uint64_t)(uintptr_t)qt.done_ns,     (uint64_t)ctx->lop3_grid};
+                                 (uint64_t)(uintptr_t)qt.done_ns,     (uint64_t)ctx->lop3_grid,
+                                 (uint64_t)pl.item_cap,               (uint64_t)(pl.uses_lop3 + 2 * pl.uses_m4r)};
     if (ctx->gcache.exec && ctx->gcache.key == key) {
         *out = ctx->gcache.exec;
         return CFPQ_OK;
@@ -985,7 +1018,7 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
     // device tables
     TRY(ctx->slots.ensure(pl.slots.size() * sizeof(MatSlot)));
     TRY(ctx->prods.ensure(pl.prods.size() * sizeof(ProdDesc)));
-    TRY(ctx->items.ensure(std::max<size_t>(pl.item_cap, 1) * 8));
+    TRY(ctx->items.ensure(2 * pl.item_cap * 8));
     TRY(ctx->prod_seen.ensure(pl.prods.size() * 4));
     const size_t qbytes = nq * (4 + 4 + 8) + 64;
     TRY(ctx->qtrack.ensure(qbytes));
@@ -1135,7 +1168,7 @@ extern "C" int cfpq_closure(cfpq_ctx *ctx, const cfpq_rule *rules, size_t nrules
     QueryIn q{rules, nrules, mats, nmats};
     if (o.driver == CFPQ_DRIVER_WORKLIST) return run_worklist(ctx, q, o, stats);
     if (o.driver != CFPQ_DRIVER_ENGINE) return set_error(CFPQ_ERR_INVALID, "unknown driver %d", o.driver);
-    if (o.variant != CFPQ_VARIANT_AUTO && o.variant != CFPQ_VARIANT_LOP3)
+    if (o.variant != CFPQ_VARIANT_AUTO && o.variant != CFPQ_VARIANT_LOP3 && o.variant != CFPQ_VARIANT_M4R)
         return set_error(CFPQ_ERR_UNSUPPORTED, "variant %d is not available in the engine driver", o.variant);
     std::vector<QueryIn> qs{q};
     return run_engine(ctx, qs, o, stats, nullptr, nullptr);
@@ -1148,7 +1181,7 @@ extern "C" int cfpq_closure_batch(cfpq_ctx *ctx, const cfpq_query *queries, size
     if (nqueries && !queries) return set_error(CFPQ_ERR_INVALID, "null query array");
     const cfpq_closure_opts o = opts ? *opts : default_opts();
     if (o.driver != CFPQ_DRIVER_ENGINE) return set_error(CFPQ_ERR_INVALID, "batched closure needs the engine driver");
-    if (o.variant != CFPQ_VARIANT_AUTO && o.variant != CFPQ_VARIANT_LOP3)
+    if (o.variant != CFPQ_VARIANT_AUTO && o.variant != CFPQ_VARIANT_LOP3 && o.variant != CFPQ_VARIANT_M4R)
         return set_error(CFPQ_ERR_UNSUPPORTED, "variant %d is not available in the engine driver", o.variant);
     std::vector<QueryIn> qs;
     qs.reserve(nqueries);

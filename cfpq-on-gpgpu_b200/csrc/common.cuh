@@ -63,8 +63,9 @@ struct ProdDesc {
 // Device-resident iteration state of a closure (one per context).
 struct IterState {
     uint32_t iter;          // iteration index (parity selects delta buffers)
-    uint32_t item_count;    // work items written by the plan kernel
-    uint32_t item_next;     // work-stealing counter of the product kernel
+    uint32_t item_count[2]; // work items written by the plan kernel, per list
+                            // (list 0: LOP3 inner loop, list 1: Four Russians)
+    uint32_t item_next[2];  // work-stealing counters of the product kernels
     uint32_t changed;       // set when any new bit appeared in this iteration
     uint32_t last_changed;  // copy of `changed` at the end of the iteration
     uint32_t error;         // nonzero: a bounded wait gave up (cfpq_status)

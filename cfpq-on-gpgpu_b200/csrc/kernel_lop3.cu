@@ -1,30 +1,37 @@
-// Variant LOP3: tiled word-level Boolean product C |= P * Q over the work items
-// of one closure iteration (or one add_mul).
+// Tiled Boolean product C |= P * Q over the work items of one closure
+// iteration (or one add_mul), with two dense inner loops:
+//   variant LOP3  (item list 0): word-level AND/OR with LOP3
+//   variant M4R   (item list 1): Four Russians with 4-bit tables in shared memory
 //
-// Work item = (product, output tile-row ti, block of kBJ output tiles).  A CTA
-// of 4 warps owns the 64 x (64*kBJ) output block in registers: warp w owns
-// tiles 4w..4w+3 of the block, lane l owns rows 2l and 2l+1, so every thread
-// keeps 2 rows x 4 tiles x 64 bits = 16 uint32 accumulators.
+// Work item = (product, output tile-row ti, block of kBJ output tiles, chunk of
+// contributing k-tiles).  A CTA of 4 warps owns the 64 x (64*kBJ) output block
+// in registers: warp w owns tiles 4w..4w+3 of the block, lane l owns rows 2l
+// and 2l+1, so every thread keeps 2 rows x 4 tiles x 64 bits = 16 uint32
+// accumulators.
 //
-// Inner dimension: warp 0 lists the k-tiles tk whose P tile (ti, tk) is
-// occupied and whose Q tiles (tk, block) are not all empty, and sorts them by
-// the population of the P tile:
+// Inner dimension: the contributing k-tiles tk (occupied P tile (ti, tk) and a
+// non-empty Q block (tk, block)) in increasing tk order, cut into chunks of
+// entries_per_item(T); the item keeps its chunk and sorts it by the
+// population of the P tile:
 //   dense  (population > kSparseMax): one elected thread stages the P tile
 //          (512 B) and the kBJ Q tiles (kBJ*512 B, one contiguous range of the
 //          tiled layout) into shared memory with bulk copies (cp.async.bulk,
-//          the TMA engine) completing on an mbarrier, double-buffered.  Per row
-//          and inner index k: mask = -(P[row] bit k) (2 ALU ops), then
-//          acc |= mask & Q[k] on 8 uint32 words (one LOP3 each); Q rows k, k+1
-//          of a tile come in one 16-byte shared load that all lanes of the
-//          warp read at the same address (broadcast).
+//          the TMA engine) completing on an mbarrier, double-buffered.
+//          LOP3: per row and inner index k, mask = -(P[row] bit k) (2 ALU
+//          ops), then acc |= mask & Q[k] on 8 uint32 words (one LOP3 each); Q
+//          rows k, k+1 of a tile come in one 16-byte shared load read by all
+//          lanes of the warp at the same address (broadcast).
+//          M4R: the CTA first builds, for each of the 16 four-bit slabs of the
+//          k-tile and each of the kBJ Q tiles, the 16 ORs of the slab's Q rows
+//          (a table row per key, padded to 17 words so that lanes reading
+//          different keys hit different banks); each row then ORs one table
+//          word per slab and tile: 16 loads instead of 64 masked LOP3s.
 //   sparse (population <= kSparseMax): nothing is staged.  The (k-tile, row)
 //          pairs of all sparse k-tiles are spread over the CTA's 128 threads
 //          (4 pairs in flight per thread); a thread walks the set bits k of
 //          its P row word and ORs the Q words of row k of the occupied tiles,
-//          read straight from L2, into a shared-memory accumulator with shared
-//          atomics.  Latency is hidden by the number of independent pairs, not
-//          by a per-warp chain over k-tiles.
-// A warp whose 4 Q tiles are all empty skips a dense k-tile.
+//          read straight from L2, into a shared-memory accumulator.
+// A warp whose 4 Q tiles are all empty skips the LOP3 loop / the lookups.
 //
 // Epilogue: for each non-zero accumulator word, new = acc & ~old via a 64-bit
 // atomicOr (several products of one iteration may write the same head); new
@@ -38,16 +45,19 @@ namespace cfpq {
 
 namespace {
 
-constexpr int kBJ = 16;            // output tiles per work item (1024 columns)
-constexpr int kThreads = 128;      // 4 warps
-constexpr int kMaxTiles = 2048;    // k-list capacity (n <= 131072)
+constexpr int kBJ = 16;              // output tiles per work item (1024 columns)
+constexpr int kThreads = 128;        // 4 warps
+constexpr int kMaxTiles = 2048;      // k-list capacity (n <= 131072)
 constexpr uint32_t kSparseMax = 96;  // P-tile population up to which the sparse loop runs
+constexpr int kTabRow = kBJ + 1;     // padded table row (uint64 words)
 constexpr unsigned kFull = 0xffffffffu;
 
-struct __align__(128) Lop3Smem {
+template <bool kM4R>
+struct __align__(128) TiledSmem {
     uint64_t q[2][kBJ * 64];     // 2 x 8 KiB
     uint64_t p[2][64];           // 2 x 512 B
     unsigned long long sacc[kBJ * 64];  // sparse-phase accumulator [tile][row], 8 KiB
+    uint64_t tab[kM4R ? 16 * 16 * kTabRow : 1];  // M4R tables [slab][key][tile], 34 KiB
     uint64_t bar[2];
     uint16_t dtile[kMaxTiles];   // dense k-list: tile index
     uint16_t dmask[kMaxTiles];   //               occupancy of the kBJ Q tiles
@@ -74,12 +84,20 @@ __device__ __forceinline__ uint64_t ld_cg(const uint64_t *p) {
     return __ldcg(reinterpret_cast<const unsigned long long *>(p));
 }
 
+__device__ __forceinline__ void or64(uint2 &a, uint64_t v) {
+    a.x |= (uint32_t)v;
+    a.y |= (uint32_t)(v >> 32);
+}
+
+template <bool kM4R>
 __global__ void __launch_bounds__(kThreads, 4)
-    k_product_lop3(const ProdDesc *__restrict__ prods, const MatSlot *__restrict__ slots, IterState *st,
-                   const uint64_t *__restrict__ items, uint32_t *qchanged) {
+    k_product_tiled(const ProdDesc *__restrict__ prods, const MatSlot *__restrict__ slots, IterState *st,
+                    const uint64_t *__restrict__ items_all, size_t list_cap, uint32_t *qchanged) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    Lop3Smem &S = *reinterpret_cast<Lop3Smem *>(smem_raw);
+    TiledSmem<kM4R> &S = *reinterpret_cast<TiledSmem<kM4R> *>(smem_raw);
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t list = kM4R ? 1u : 0u;
+    const uint64_t *items = items_all + list * list_cap;
 
     if (tid == 0) {
         mbar_init(&S.bar[0], 1);
@@ -89,12 +107,12 @@ __global__ void __launch_bounds__(kThreads, 4)
     __syncthreads();
     uint32_t phase = 0;  // bit s = next parity to wait for on stage s
     const uint32_t iter = st->iter;
-    const uint32_t nitems = st->item_count;
+    const uint32_t nitems = st->item_count[list];
     unsigned long long triples = 0, staged = 0, outw = 0, neww = 0;
     bool timed_out = false;
 
     for (;;) {
-        if (tid == 0) S.item = atomicAdd(&st->item_next, 1u);
+        if (tid == 0) S.item = atomicAdd(&st->item_next[list], 1u);
         __syncthreads();
         const uint32_t idx = S.item;
         if (idx >= nitems) break;
@@ -191,7 +209,7 @@ __global__ void __launch_bounds__(kThreads, 4)
 #pragma unroll
         for (int j = 0; j < 4; ++j) acc0[j] = acc1[j] = make_uint2(0, 0);
 
-        // ---- dense k-tiles: staged panels, LOP3 inner loop ----
+        // ---- dense k-tiles: staged panels ----
         auto issue = [&](uint32_t e, uint32_t stage) {
             const uint32_t tk = S.dtile[e];
             fence_proxy_async_smem();
@@ -209,28 +227,70 @@ __global__ void __launch_bounds__(kThreads, 4)
             if (!timed_out && !mbar_wait_bounded(&S.bar[stage], (phase >> stage) & 1u)) timed_out = true;
             phase ^= 1u << stage;
             const uint32_t wmask = ((uint32_t)S.dmask[e] >> (4 * warp)) & 0xFu;
-            if (wmask && !timed_out) {
-                const uint4 pp = *reinterpret_cast<const uint4 *>(&S.p[stage][2 * lane]);
-                const uint64_t *q = &S.q[stage][(4 * warp) * 64];
+            const uint4 pp = *reinterpret_cast<const uint4 *>(&S.p[stage][2 * lane]);
+            if constexpr (kM4R) {
+                // build: (slab s, tile j) pairs over the CTA; 16 keys each
+                for (uint32_t pr = tid; pr < 16 * kBJ; pr += kThreads) {
+                    const uint32_t s = pr / kBJ, j = pr % kBJ;
+                    const uint64_t *qr = &S.q[stage][j * 64 + 4 * s];
+                    const uint64_t q0 = qr[0], q1 = qr[1], q2 = qr[2], q3 = qr[3];
+                    uint64_t *t = &S.tab[(s * 16) * kTabRow + j];
+                    const uint64_t a01 = q0 | q1, a23 = q2 | q3;
+                    t[0 * kTabRow] = 0;
+                    t[1 * kTabRow] = q0;
+                    t[2 * kTabRow] = q1;
+                    t[3 * kTabRow] = a01;
+                    t[4 * kTabRow] = q2;
+                    t[5 * kTabRow] = q0 | q2;
+                    t[6 * kTabRow] = q1 | q2;
+                    t[7 * kTabRow] = a01 | q2;
+                    t[8 * kTabRow] = q3;
+                    t[9 * kTabRow] = q0 | q3;
+                    t[10 * kTabRow] = q1 | q3;
+                    t[11 * kTabRow] = a01 | q3;
+                    t[12 * kTabRow] = a23;
+                    t[13 * kTabRow] = q0 | a23;
+                    t[14 * kTabRow] = q1 | a23;
+                    t[15 * kTabRow] = a01 | a23;
+                }
+                __syncthreads();
+                if (wmask && !timed_out) {
+                    const uint64_t pa = ((uint64_t)pp.y << 32) | pp.x;  // row 2l
+                    const uint64_t pb = ((uint64_t)pp.w << 32) | pp.z;  // row 2l+1
 #pragma unroll
-                for (int kk = 0; kk < 64; kk += 2) {
-                    const uint32_t pa = kk < 32 ? pp.x : pp.y;  // row 2l
-                    const uint32_t pb = kk < 32 ? pp.z : pp.w;  // row 2l+1
-                    const int b = kk & 31;
-                    const uint32_t ma0 = bitmask(pa, b), ma1 = bitmask(pa, b + 1);
-                    const uint32_t mb0 = bitmask(pb, b), mb1 = bitmask(pb, b + 1);
+                    for (int s = 0; s < 16; ++s) {
+                        const uint64_t *ta = &S.tab[(s * 16 + (uint32_t)((pa >> (4 * s)) & 15u)) * kTabRow + 4 * warp];
+                        const uint64_t *tb = &S.tab[(s * 16 + (uint32_t)((pb >> (4 * s)) & 15u)) * kTabRow + 4 * warp];
 #pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        const uint4 qv = *reinterpret_cast<const uint4 *>(q + j * 64 + kk);
-                        acc0[j].x |= (qv.x & ma0) | (qv.z & ma1);
-                        acc0[j].y |= (qv.y & ma0) | (qv.w & ma1);
-                        acc1[j].x |= (qv.x & mb0) | (qv.z & mb1);
-                        acc1[j].y |= (qv.y & mb0) | (qv.w & mb1);
+                        for (int j = 0; j < 4; ++j) {
+                            or64(acc0[j], ta[j]);
+                            or64(acc1[j], tb[j]);
+                        }
+                    }
+                }
+            } else {
+                if (wmask && !timed_out) {
+                    const uint64_t *q = &S.q[stage][(4 * warp) * 64];
+#pragma unroll
+                    for (int kk = 0; kk < 64; kk += 2) {
+                        const uint32_t pa = kk < 32 ? pp.x : pp.y;  // row 2l
+                        const uint32_t pb = kk < 32 ? pp.z : pp.w;  // row 2l+1
+                        const int b = kk & 31;
+                        const uint32_t ma0 = bitmask(pa, b), ma1 = bitmask(pa, b + 1);
+                        const uint32_t mb0 = bitmask(pb, b), mb1 = bitmask(pb, b + 1);
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) {
+                            const uint4 qv = *reinterpret_cast<const uint4 *>(q + j * 64 + kk);
+                            acc0[j].x |= (qv.x & ma0) | (qv.z & ma1);
+                            acc0[j].y |= (qv.y & ma0) | (qv.w & ma1);
+                            acc1[j].x |= (qv.x & mb0) | (qv.z & mb1);
+                            acc1[j].y |= (qv.y & mb0) | (qv.w & mb1);
+                        }
                     }
                 }
             }
-            // all threads are done with this stage before it is refilled; a
-            // timeout anywhere in the CTA stops every later wait
+            // all threads are done with this stage (and the tables) before they
+            // are refilled; a timeout anywhere in the CTA stops every later wait
             timed_out = __syncthreads_or(timed_out) != 0;
             stage ^= 1;
         }
@@ -343,18 +403,30 @@ __global__ void __launch_bounds__(kThreads, 4)
 int product_lop3_tiles_per_block() { return kBJ; }
 int product_lop3_max_tiles() { return kMaxTiles; }
 
-// Called once per context (before any stream capture): sets the kernel's
-// shared-memory attribute and returns the resident CTAs per SM.
-int product_lop3_blocks_per_sm() {
-    cudaFuncSetAttribute(k_product_lop3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Lop3Smem));
+int product_tiled_blocks_per_sm(int m4r) {
     int nb = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_product_lop3, kThreads, sizeof(Lop3Smem));
+    if (m4r) {
+        cudaFuncSetAttribute(k_product_tiled<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(TiledSmem<true>));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_product_tiled<true>, kThreads, sizeof(TiledSmem<true>));
+    } else {
+        cudaFuncSetAttribute(k_product_tiled<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(TiledSmem<false>));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_product_tiled<false>, kThreads,
+                                                      sizeof(TiledSmem<false>));
+    }
     return nb > 0 ? nb : 1;
 }
 
-cudaError_t launch_product_lop3(const ProdDesc *d_prods, const MatSlot *d_slots, IterState *d_st,
-                                const uint64_t *d_items, uint32_t *d_qchanged, int grid, cudaStream_t s) {
-    k_product_lop3<<<grid, kThreads, sizeof(Lop3Smem), s>>>(d_prods, d_slots, d_st, d_items, d_qchanged);
+cudaError_t launch_product_tiled(int m4r, const ProdDesc *d_prods, const MatSlot *d_slots, IterState *d_st,
+                                 const uint64_t *d_items, size_t list_cap, uint32_t *d_qchanged, int grid,
+                                 cudaStream_t s) {
+    if (m4r)
+        k_product_tiled<true><<<grid, kThreads, sizeof(TiledSmem<true>), s>>>(d_prods, d_slots, d_st, d_items, list_cap,
+                                                                              d_qchanged);
+    else
+        k_product_tiled<false><<<grid, kThreads, sizeof(TiledSmem<false>), s>>>(d_prods, d_slots, d_st, d_items,
+                                                                                list_cap, d_qchanged);
     return cudaGetLastError();
 }
 

@@ -278,9 +278,11 @@ __device__ __forceinline__ DevMat resolve_operand(const MatSlot &s, uint8_t use_
     return s.dlt[iter & 1];
 }
 
+// Items go to list 0 (LOP3 inner loop) or list 1 (Four Russians) by the
+// product's variant; list l starts at items + l * list_cap.
 __global__ void k_plan(const ProdDesc *__restrict__ prods, uint32_t nprods, uint32_t row_begin, uint32_t total_rows,
-                       const MatSlot *__restrict__ slots, IterState *st, uint64_t *__restrict__ items, int tpb,
-                       uint32_t *prod_seen) {
+                       const MatSlot *__restrict__ slots, IterState *st, uint64_t *__restrict__ items_all,
+                       size_t list_cap, int tpb, uint32_t *prod_seen) {
     const uint32_t gw = row_begin + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     const uint32_t lane = threadIdx.x & 31;
     if (gw >= total_rows || !st->active) return;
@@ -292,6 +294,8 @@ __global__ void k_plan(const ProdDesc *__restrict__ prods, uint32_t nprods, uint
     const ProdDesc pd = prods[lo];
     const uint32_t iter = st->iter;
     if (pd.term == 1 && iter == 0) return;  // first iteration: delta(A) = A, one term covers A*B
+    const uint32_t list = pd.variant == 3 ? 1u : 0u;  // CFPQ_VARIANT_M4R
+    uint64_t *items = items_all + list * list_cap;
     const uint32_t ti = gw - pd.row_start;
     const DevMat P = resolve_operand(slots[pd.pslot], pd.p_delta, iter);
     const DevMat Q = resolve_operand(slots[pd.qslot], pd.q_delta, iter);
@@ -330,7 +334,7 @@ __global__ void k_plan(const ProdDesc *__restrict__ prods, uint32_t nprods, uint
             if (!total) continue;
             emitted = true;
             uint32_t basepos = 0;
-            if (lane == 0) basepos = atomicAdd(&st->item_count, total);
+            if (lane == 0) basepos = atomicAdd(&st->item_count[list], total);
             basepos = __shfl_sync(kFull, basepos, 0) + pre - nitem;
             for (uint32_t j = 0; j < nitem; ++j) items[basepos + j] = make_item(lo, ti, w * bpw + h, j);
         }
@@ -388,9 +392,11 @@ __global__ void k_iter_end(IterState *st, QueryTrack qt, cudaGraphConditionalHan
             const uint32_t changed = st->changed;
             st->last_changed = changed;
             st->changed = 0;
-            st->items_total += st->item_count;
-            st->item_count = 0;
-            st->item_next = 0;
+            st->items_total += st->item_count[0] + st->item_count[1];
+            st->items_by_variant[2] += st->item_count[0];
+            st->items_by_variant[3] += st->item_count[1];
+            st->item_count[0] = st->item_count[1] = 0;
+            st->item_next[0] = st->item_next[1] = 0;
             const uint32_t it = ++st->iter;
             s_iter = it;
             s_go = changed && st->error == 0 && (st->max_iter == 0 || it < st->max_iter);
@@ -509,11 +515,11 @@ cudaError_t launch_merge_or(const DevMat &dst, const DevMat &src, uint32_t *d_fl
 }
 
 cudaError_t launch_plan(const ProdDesc *d_prods, uint32_t nprods, uint32_t row_begin, uint32_t row_end,
-                        const MatSlot *d_slots, IterState *d_st, uint64_t *d_items, int tiles_per_block,
-                        uint32_t *d_prod_seen, cudaStream_t s) {
+                        const MatSlot *d_slots, IterState *d_st, uint64_t *d_items, size_t list_cap,
+                        int tiles_per_block, uint32_t *d_prod_seen, cudaStream_t s) {
     if (row_end <= row_begin || nprods == 0) return cudaSuccess;
     k_plan<<<grid_for((size_t)(row_end - row_begin) * 32, 256), 256, 0, s>>>(
-        d_prods, nprods, row_begin, row_end, d_slots, d_st, d_items, tiles_per_block, d_prod_seen);
+        d_prods, nprods, row_begin, row_end, d_slots, d_st, d_items, list_cap, tiles_per_block, d_prod_seen);
     return cudaGetLastError();
 }
 

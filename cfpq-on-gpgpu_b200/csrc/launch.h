@@ -34,16 +34,24 @@ cudaError_t launch_merge_or(const DevMat &dst, const DevMat &src, uint32_t *d_fl
 
 // Closure iteration
 cudaError_t launch_plan(const ProdDesc *d_prods, uint32_t nprods, uint32_t row_begin, uint32_t row_end,
-                        const MatSlot *d_slots, IterState *d_st, uint64_t *d_items, int tiles_per_block,
-                        uint32_t *d_prod_seen, cudaStream_t s);
-cudaError_t launch_product_lop3(const ProdDesc *d_prods, const MatSlot *d_slots, IterState *d_st,
-                                const uint64_t *d_items, uint32_t *d_qchanged, int grid, cudaStream_t s);
+                        const MatSlot *d_slots, IterState *d_st, uint64_t *d_items, size_t list_cap,
+                        int tiles_per_block, uint32_t *d_prod_seen, cudaStream_t s);
+// Tiled product over item list `m4r` (0: LOP3 inner loop, 1: Four Russians
+// inner loop); items of list l start at d_items + l * list_cap.
+cudaError_t launch_product_tiled(int m4r, const ProdDesc *d_prods, const MatSlot *d_slots, IterState *d_st,
+                                 const uint64_t *d_items, size_t list_cap, uint32_t *d_qchanged, int grid,
+                                 cudaStream_t s);
 int product_lop3_tiles_per_block();
 int product_lop3_max_tiles();
-int product_lop3_blocks_per_sm();
+// Called once per context before any capture: sets kernel attributes, returns
+// resident CTAs per SM of the given inner loop.
+int product_tiled_blocks_per_sm(int m4r);
 cudaError_t launch_advance(const MatSlot *d_slots, uint32_t nslots, uint32_t total_rows, IterState *d_st,
                            cudaStream_t s);
 cudaError_t launch_mark_start(IterState *d_st, cudaStream_t s);
+// Calibration: logic instructions per second of the whole GPU (d_out: 8*256*num_sms words).
+cudaError_t measure_logic_rate(int num_sms, uint32_t *d_out, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1,
+                               double *ops_per_s, double *ms_out);
 cudaError_t launch_iter_end(IterState *d_st, const QueryTrack &qt, cudaGraphConditionalHandle handle, int use_handle,
                             cudaStream_t s);
 

@@ -97,6 +97,17 @@ typedef struct cfpq_closure_stats {
     uint64_t new_words;         /* result words that carried new bits */
 } cfpq_closure_stats;
 
+/* Measured device rates, the denominators of the word-level rooflines: a
+ * register-only kernel of independent 3-input logic chains (the LOP3 pipe)
+ * timed with CUDA events on the context's stream.  No reference counterpart. */
+typedef struct cfpq_calibration {
+    double logic_ops_per_s;       /* 32-bit logic instructions per second, whole GPU */
+    double logic_ops_per_clk_sm;  /* the same per SM per clock at the nominal clock */
+    double bitmac_per_s;          /* Boolean AND-OR pairs per second = 32 x logic_ops_per_s */
+    double ms;                    /* duration of the timed kernel */
+} cfpq_calibration;
+int cfpq_calibrate(cfpq_ctx *ctx, cfpq_calibration *out);
+
 /* Per-kernel device times of the last closure run with
  * opts->log_products & CFPQ_LOG_KERNELS (every launch bracketed by CUDA events
  * on the context's stream; the iteration loop then runs from the host instead

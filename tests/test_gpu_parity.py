@@ -43,7 +43,7 @@ def check_tile_stats(m, rows):
     assert not np.any((exp > 0) & ~occ_bits)
 
 
-@pytest.mark.parametrize("variant", ["plain", "lop3"])
+@pytest.mark.parametrize("variant", ["plain", "lop3", "m4r"])
 @pytest.mark.parametrize("n", SIZES)
 def test_add_mul_random(ctx, oracle, variant, n):
     rng = np.random.default_rng(n * 7 + len(variant))
@@ -63,7 +63,7 @@ def test_add_mul_random(ctx, oracle, variant, n):
             m.destroy()
 
 
-@pytest.mark.parametrize("variant", ["plain", "lop3"])
+@pytest.mark.parametrize("variant", ["plain", "lop3", "m4r"])
 @pytest.mark.parametrize("alias", ["a", "b", "ab"])
 def test_add_mul_aliasing(ctx, oracle, variant, alias):
     n = 200
@@ -134,7 +134,7 @@ def test_ordered_matrices(ctx, pkg, oracle, n):
         assert m.hash_count() == oracle.hash_count(rows, n)
     exp = c.copy()
     ch_exp = oracle.add_mul(exp, a, b, n)
-    for variant in ("lop3", "plain"):
+    for variant in ("lop3", "plain", "m4r"):
         mc.upload_rows(c)
         assert ctx.add_mul(mc, ma, mb, variant) == ch_exp
         assert np.array_equal(mc.download_rows(), exp)
@@ -194,7 +194,9 @@ def _check_query(ctx, pkg, oracle, wl, tmp_path, order="auto", **kw):
 
 @pytest.mark.parametrize("kw", [dict(driver="engine", use_graph=True), dict(driver="engine", use_graph=False),
                                 dict(driver="worklist", variant="plain"),
-                                dict(driver="worklist", variant="lop3")])
+                                dict(driver="worklist", variant="lop3"),
+                                dict(driver="engine", variant="m4r"),
+                                dict(driver="worklist", variant="m4r")])
 def test_closure_brackets_full_size(ctx, pkg, oracle, tmp_path, kw):
     wl = pkg.workloads.brackets_query()  # N=1024, 4096 edges
     res = _check_query(ctx, pkg, oracle, wl, tmp_path, **kw)
@@ -209,13 +211,14 @@ def test_closure_same_generation(ctx, pkg, oracle, tmp_path, n, seed, order):
     _check_query(ctx, pkg, oracle, wl, tmp_path, order=order)
 
 
+@pytest.mark.parametrize("variant", ["lop3", "m4r"])
 @pytest.mark.parametrize("seed", [1, 2, 3])
-def test_closure_random_cnf(ctx, pkg, oracle, tmp_path, seed):
+def test_closure_random_cnf(ctx, pkg, oracle, tmp_path, seed, variant):
     labels = ["x", "y", "z"]
     g = pkg.workloads.uniform_graph(700, 1400, labels, seed)
     gram = pkg.workloads.random_cnf(8, 20, labels, seed)
     wl = pkg.workloads.Workload("random_cnf", gram, g, {})
-    _check_query(ctx, pkg, oracle, wl, tmp_path)
+    _check_query(ctx, pkg, oracle, wl, tmp_path, variant=variant)
 
 
 def test_closure_epsilon_and_self_loops(ctx, pkg, oracle, tmp_path):
