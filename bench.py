@@ -224,7 +224,7 @@ def dense_product_kernels(ctx, capi, torch, stream, n=8192, density=0.3, reps=3)
     cal = ctx.calibrate()
     out = {"n": n, "density": density, "calibrated_logic_ops_per_s": cal["logic_ops_per_s"],
            "calibrated_logic_ops_per_clk_sm": cal["logic_ops_per_clk_sm"], "variants": {}}
-    for variant in ("lop3", "m4r", "plain"):
+    for variant in ("tc", "lop3", "m4r", "plain"):
         ms = []
         for _ in range(reps if variant != "plain" else 1):
             c.clear()

@@ -140,11 +140,11 @@ struct cfpq_ctx {
     unsigned long long *h_hash = nullptr;
     size_t h_hash_cap = 0;
     // growable device scratch
-    DevBuf stage, items, prods, slots, qtrack, prod_seen, mats_desc, edge_buf;
+    DevBuf stage, items, prods, slots, qtrack, prod_seen, mats_desc, edge_buf, xbuf;
     std::unordered_map<uint32_t, PowTables> pow;
     std::vector<cfpq_matrix *> pool;  // zeroed spare matrices (deltas, alias copies)
     GraphCache gcache;
-    int lop3_grid = 0, m4r_grid = 0;
+    int lop3_grid = 0, m4r_grid = 0, tc_grid = 0;  // tc_grid 0: tensor-core variant unavailable
     std::vector<cfpq_product_record> log;
     cudaEvent_t kev[5] = {};
     cfpq_kernel_profile prof = {};
@@ -357,6 +357,9 @@ extern "C" int cfpq_ctx_create(int device, cfpq_ctx **out) {
     CUDA_TRY(cudaMallocHost(&c->h_flag, 64));
     c->lop3_grid = c->num_sms * product_tiled_blocks_per_sm(0);
     c->m4r_grid = c->num_sms * product_tiled_blocks_per_sm(1);
+    // The tensor-core kernel allocates all 512 TMEM columns of its SM, so it
+    // must run one CTA per SM; it is only enabled when that is guaranteed.
+    c->tc_grid = product_tc_blocks_per_sm() == 1 ? c->num_sms : 0;
     *out = c;
     return CFPQ_OK;
 }
@@ -375,7 +378,7 @@ extern "C" int cfpq_ctx_destroy(cfpq_ctx *ctx) {
         cudaFree(kv.second.d_pow13);
     }
     for (DevBuf *b : {&ctx->stage, &ctx->items, &ctx->prods, &ctx->slots, &ctx->qtrack, &ctx->prod_seen,
-                      &ctx->mats_desc, &ctx->edge_buf})
+                      &ctx->mats_desc, &ctx->edge_buf, &ctx->xbuf})
         b->release();
     cudaFree(ctx->d_st);
     cudaFree(ctx->d_flag);
@@ -674,7 +677,39 @@ static int read_flag(cfpq_ctx *ctx, uint32_t *dflag, int *changed) {
     return CFPQ_OK;
 }
 
-// Enqueue c |= a * b with the tiled LOP3 kernel (operands must not alias c).
+static int launch_products(cfpq_ctx *ctx, size_t list_cap, bool lop3, bool m4r, uint32_t *qchanged, cudaStream_t s);
+
+// A tensor-core product term of a closure plan.
+struct TcProduct {
+    uint32_t index, T, row_start, rows;
+};
+
+// Expanded-operand scratch for tensor-core products of up to T tiles per side
+// (P by rows and Q transposed, 4 KiB per tile each).  Allocated before any
+// graph capture.
+static int ensure_expand_scratch(cfpq_ctx *ctx, uint32_t T) {
+    return ctx->xbuf.ensure(2 * (size_t)T * T * 4096);
+}
+
+// One tensor-core product: expand its operands, plan its items, run the
+// tensor-core kernel, close the item list.
+static int launch_tc_product(cfpq_ctx *ctx, const TcProduct &tp, uint32_t nprods, size_t list_cap,
+                             uint32_t *prod_seen, uint32_t *qchanged, cudaStream_t s) {
+    uint8_t *xp = ctx->xbuf.as<uint8_t>();
+    uint8_t *xq = xp + (size_t)tp.T * tp.T * 4096;
+    const ProdDesc *pr = ctx->prods.as<ProdDesc>();
+    const MatSlot *sl = ctx->slots.as<MatSlot>();
+    CUDA_TRY(launch_expand_operand(pr, tp.index, tp.T, sl, ctx->d_st, 0, xp, ctx->num_sms, s));
+    CUDA_TRY(launch_expand_operand(pr, tp.index, tp.T, sl, ctx->d_st, 1, xq, ctx->num_sms, s));
+    CUDA_TRY(launch_plan(pr, nprods, tp.row_start, tp.row_start + tp.rows, sl, ctx->d_st, ctx->items.as<uint64_t>(),
+                         list_cap, product_lop3_tiles_per_block(), prod_seen, 1, s));
+    CUDA_TRY(launch_product_tc(pr, sl, ctx->d_st, ctx->items.as<uint64_t>(), list_cap, qchanged, ctx->tc_grid, xp, xq,
+                               s));
+    CUDA_TRY(launch_reset_list(ctx->d_st, 2, s));
+    return CFPQ_OK;
+}
+
+// Enqueue c |= a * b with a tiled variant (operands must not alias c).
 static int enqueue_tiled_product(cfpq_ctx *ctx, const DevMat &a, const DevMat &b, const DevMat &c, int variant) {
     const uint32_t T = a.T;
     const int tpb = product_lop3_tiles_per_block();
@@ -694,7 +729,7 @@ static int enqueue_tiled_product(cfpq_ctx *ctx, const DevMat &a, const DevMat &b
     const size_t cap = std::max<size_t>(item_capacity(T, tpb), 1);
     TRY(ctx->slots.ensure(sizeof(hs)));
     TRY(ctx->prods.ensure(sizeof(pd)));
-    TRY(ctx->items.ensure(2 * cap * 8));
+    TRY(ctx->items.ensure(3 * cap * 8));
     IterState st;
     memset(&st, 0, sizeof(st));
     st.iter = 1;
@@ -703,16 +738,18 @@ static int enqueue_tiled_product(cfpq_ctx *ctx, const DevMat &a, const DevMat &b
     CUDA_TRY(cudaMemcpyAsync(ctx->slots.p, hs, sizeof(hs), cudaMemcpyHostToDevice, ctx->stream));
     CUDA_TRY(cudaMemcpyAsync(ctx->prods.p, &pd, sizeof(pd), cudaMemcpyHostToDevice, ctx->stream));
     CUDA_TRY(cudaMemcpyAsync(ctx->d_st, ctx->h_st, sizeof(IterState), cudaMemcpyHostToDevice, ctx->stream));
+    if (variant == CFPQ_VARIANT_TC) {
+        TRY(ensure_expand_scratch(ctx, T));
+        return launch_tc_product(ctx, TcProduct{0, T, 0, (T + 3) / 4}, 1, cap, nullptr, nullptr, ctx->stream);
+    }
     CUDA_TRY(launch_plan(ctx->prods.as<ProdDesc>(), 1, 0, T, ctx->slots.as<MatSlot>(), ctx->d_st,
-                         ctx->items.as<uint64_t>(), cap, tpb, nullptr, ctx->stream));
-    const int m4r = variant == CFPQ_VARIANT_M4R;
-    CUDA_TRY(launch_product_tiled(m4r, ctx->prods.as<ProdDesc>(), ctx->slots.as<MatSlot>(), ctx->d_st,
-                                  ctx->items.as<uint64_t>(), cap, nullptr, m4r ? ctx->m4r_grid : ctx->lop3_grid,
-                                  ctx->stream));
+                         ctx->items.as<uint64_t>(), cap, tpb, nullptr, 0, ctx->stream));
+    TRY(launch_products(ctx, cap, variant == CFPQ_VARIANT_LOP3, variant == CFPQ_VARIANT_M4R, nullptr, ctx->stream));
     return CFPQ_OK;
 }
 
-// Product kernels of one closure iteration: one launch per item list in use.
+// Word-level product kernels of one closure iteration: one launch per item
+// list in use.
 static int launch_products(cfpq_ctx *ctx, size_t list_cap, bool lop3, bool m4r, uint32_t *qchanged, cudaStream_t s) {
     if (lop3)
         CUDA_TRY(launch_product_tiled(0, ctx->prods.as<ProdDesc>(), ctx->slots.as<MatSlot>(), ctx->d_st,
@@ -748,8 +785,10 @@ extern "C" int cfpq_add_mul(cfpq_ctx *ctx, cfpq_matrix *c, const cfpq_matrix *a,
         }
         return read_flag(ctx, ctx->d_flag, changed);
     }
-    if (variant != CFPQ_VARIANT_LOP3 && variant != CFPQ_VARIANT_M4R)
+    if (variant != CFPQ_VARIANT_LOP3 && variant != CFPQ_VARIANT_M4R && variant != CFPQ_VARIANT_TC)
         return set_error(CFPQ_ERR_UNSUPPORTED, "variant %d is not available for add_mul", variant);
+    if (variant == CFPQ_VARIANT_TC && !ctx->tc_grid)
+        return set_error(CFPQ_ERR_UNSUPPORTED, "tensor-core variant unavailable (needs one CTA per SM)");
     // Snapshot semantics: operands that alias c are read from a copy.
     cfpq_matrix *ca = nullptr, *cb = nullptr;
     DevMat da = a->d, db = b->d;
@@ -795,7 +834,9 @@ struct ClosurePlan {
     std::vector<cfpq_matrix *> deltas;
     uint32_t slot_rows = 0, prod_rows = 0;
     size_t item_cap = 0;  // per item list
-    bool uses_lop3 = false, uses_m4r = false;
+    bool uses_lop3 = false, uses_m4r = false, uses_tc = false;
+    std::vector<TcProduct> tc_prods;
+    uint32_t tc_max_T = 0;
 };
 
 }  // namespace
@@ -857,14 +898,20 @@ static int build_plan(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, int variant
                 pd.p_delta = term == 0;
                 pd.q_delta = term == 1;
                 pd.term = term;
-                pd.variant = (uint8_t)(variant == CFPQ_VARIANT_M4R ? CFPQ_VARIANT_M4R : CFPQ_VARIANT_LOP3);
-                (pd.variant == CFPQ_VARIANT_M4R ? pl->uses_m4r : pl->uses_lop3) = true;
+                pd.variant = (uint8_t)(variant == CFPQ_VARIANT_M4R || variant == CFPQ_VARIANT_TC ? variant
+                                                                                                    : CFPQ_VARIANT_LOP3);
+                (pd.variant == CFPQ_VARIANT_M4R ? pl->uses_m4r
+                                                : pd.variant == CFPQ_VARIANT_TC ? pl->uses_tc : pl->uses_lop3) = true;
                 pd.query = (uint32_t)qi;
                 pd.rule = (uint32_t)r;
                 pd.T = T;
                 pd.n = n;
                 pd.row_start = pl->prod_rows;
-                pl->prod_rows += T;
+                if (pd.variant == CFPQ_VARIANT_TC) {  // plan rows: tile-row groups of 4 for tc
+                    pl->tc_prods.push_back(TcProduct{(uint32_t)pl->prods.size(), T, pl->prod_rows, (T + 3) / 4});
+                    pl->tc_max_T = std::max(pl->tc_max_T, T);
+                }
+                pl->prod_rows += pd.variant == CFPQ_VARIANT_TC ? (T + 3) / 4 : T;
                 pl->item_cap += item_capacity(T, tpb);
                 pl->prods.push_back(pd);
             }
@@ -879,8 +926,11 @@ static int enqueue_iteration(cfpq_ctx *ctx, const ClosurePlan &pl, const QueryTr
     const int tpb = product_lop3_tiles_per_block();
     CUDA_TRY(launch_plan(ctx->prods.as<ProdDesc>(), (uint32_t)pl.prods.size(), 0, pl.prod_rows,
                          ctx->slots.as<MatSlot>(), ctx->d_st, ctx->items.as<uint64_t>(), pl.item_cap, tpb,
-                         ctx->prod_seen.as<uint32_t>(), ctx->stream));
+                         ctx->prod_seen.as<uint32_t>(), 0, ctx->stream));
     TRY(launch_products(ctx, pl.item_cap, pl.uses_lop3, pl.uses_m4r, qt.changed, ctx->stream));
+    for (const TcProduct &tp : pl.tc_prods)
+        TRY(launch_tc_product(ctx, tp, (uint32_t)pl.prods.size(), pl.item_cap, ctx->prod_seen.as<uint32_t>(),
+                              qt.changed, ctx->stream));
     CUDA_TRY(launch_advance(ctx->slots.as<MatSlot>(), (uint32_t)pl.slots.size(), pl.slot_rows, ctx->d_st,
                             ctx->stream));
     CUDA_TRY(launch_iter_end(ctx->d_st, qt, handle, use_handle, ctx->stream));
@@ -894,9 +944,12 @@ static int enqueue_iteration_timed(cfpq_ctx *ctx, const ClosurePlan &pl, const Q
     CUDA_TRY(cudaEventRecord(ctx->kev[0], s));
     CUDA_TRY(launch_plan(ctx->prods.as<ProdDesc>(), (uint32_t)pl.prods.size(), 0, pl.prod_rows,
                          ctx->slots.as<MatSlot>(), ctx->d_st, ctx->items.as<uint64_t>(), pl.item_cap, tpb,
-                         ctx->prod_seen.as<uint32_t>(), s));
+                         ctx->prod_seen.as<uint32_t>(), 0, s));
     CUDA_TRY(cudaEventRecord(ctx->kev[1], s));
     TRY(launch_products(ctx, pl.item_cap, pl.uses_lop3, pl.uses_m4r, qt.changed, s));
+    for (const TcProduct &tp : pl.tc_prods)
+        TRY(launch_tc_product(ctx, tp, (uint32_t)pl.prods.size(), pl.item_cap, ctx->prod_seen.as<uint32_t>(),
+                              qt.changed, s));
     CUDA_TRY(cudaEventRecord(ctx->kev[2], s));
     CUDA_TRY(launch_advance(ctx->slots.as<MatSlot>(), (uint32_t)pl.slots.size(), pl.slot_rows, ctx->d_st, s));
     CUDA_TRY(cudaEventRecord(ctx->kev[3], s));
@@ -949,7 +1002,12 @@ static int get_loop_graph(cfpq_ctx *ctx, const ClosurePlan &pl, const QueryTrack
                                  (uint64_t)(uintptr_t)ctx->items.p,   (uint64_t)(uintptr_t)ctx->prod_seen.p,
                                  (uint64_t)(uintptr_t)qt.changed,     (uint64_t)(uintptr_t)qt.last_iter,
                                  (uint64_t)(uintptr_t)qt.done_ns,     (uint64_t)ctx->lop3_grid,
-                                 (uint64_t)pl.item_cap,               (uint64_t)(pl.uses_lop3 + 2 * pl.uses_m4r)};
+                                 (uint64_t)pl.item_cap,               (uint64_t)(pl.uses_lop3 + 2 * pl.uses_m4r + 4 * pl.uses_tc),
+                                 (uint64_t)(uintptr_t)ctx->xbuf.p};
+    for (const TcProduct &tp : pl.tc_prods) {  // kernel arguments of the tensor-core launches
+        key.push_back(((uint64_t)tp.index << 32) | tp.T);
+        key.push_back(((uint64_t)tp.row_start << 32) | tp.rows);
+    }
     if (ctx->gcache.exec && ctx->gcache.key == key) {
         *out = ctx->gcache.exec;
         return CFPQ_OK;
@@ -1018,8 +1076,9 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
     // device tables
     TRY(ctx->slots.ensure(pl.slots.size() * sizeof(MatSlot)));
     TRY(ctx->prods.ensure(pl.prods.size() * sizeof(ProdDesc)));
-    TRY(ctx->items.ensure(2 * pl.item_cap * 8));
+    TRY(ctx->items.ensure(3 * pl.item_cap * 8));
     TRY(ctx->prod_seen.ensure(pl.prods.size() * 4));
+    if (pl.tc_max_T) TRY(ensure_expand_scratch(ctx, pl.tc_max_T));
     const size_t qbytes = nq * (4 + 4 + 8) + 64;
     TRY(ctx->qtrack.ensure(qbytes));
     QueryTrack qt;
@@ -1168,7 +1227,10 @@ extern "C" int cfpq_closure(cfpq_ctx *ctx, const cfpq_rule *rules, size_t nrules
     QueryIn q{rules, nrules, mats, nmats};
     if (o.driver == CFPQ_DRIVER_WORKLIST) return run_worklist(ctx, q, o, stats);
     if (o.driver != CFPQ_DRIVER_ENGINE) return set_error(CFPQ_ERR_INVALID, "unknown driver %d", o.driver);
-    if (o.variant != CFPQ_VARIANT_AUTO && o.variant != CFPQ_VARIANT_LOP3 && o.variant != CFPQ_VARIANT_M4R)
+    if (o.variant == CFPQ_VARIANT_TC && !ctx->tc_grid)
+        return set_error(CFPQ_ERR_UNSUPPORTED, "tensor-core variant unavailable (needs one CTA per SM)");
+    if (o.variant != CFPQ_VARIANT_AUTO && o.variant != CFPQ_VARIANT_LOP3 && o.variant != CFPQ_VARIANT_M4R &&
+        o.variant != CFPQ_VARIANT_TC)
         return set_error(CFPQ_ERR_UNSUPPORTED, "variant %d is not available in the engine driver", o.variant);
     std::vector<QueryIn> qs{q};
     return run_engine(ctx, qs, o, stats, nullptr, nullptr);
@@ -1181,7 +1243,10 @@ extern "C" int cfpq_closure_batch(cfpq_ctx *ctx, const cfpq_query *queries, size
     if (nqueries && !queries) return set_error(CFPQ_ERR_INVALID, "null query array");
     const cfpq_closure_opts o = opts ? *opts : default_opts();
     if (o.driver != CFPQ_DRIVER_ENGINE) return set_error(CFPQ_ERR_INVALID, "batched closure needs the engine driver");
-    if (o.variant != CFPQ_VARIANT_AUTO && o.variant != CFPQ_VARIANT_LOP3 && o.variant != CFPQ_VARIANT_M4R)
+    if (o.variant == CFPQ_VARIANT_TC && !ctx->tc_grid)
+        return set_error(CFPQ_ERR_UNSUPPORTED, "tensor-core variant unavailable (needs one CTA per SM)");
+    if (o.variant != CFPQ_VARIANT_AUTO && o.variant != CFPQ_VARIANT_LOP3 && o.variant != CFPQ_VARIANT_M4R &&
+        o.variant != CFPQ_VARIANT_TC)
         return set_error(CFPQ_ERR_UNSUPPORTED, "variant %d is not available in the engine driver", o.variant);
     std::vector<QueryIn> qs;
     qs.reserve(nqueries);

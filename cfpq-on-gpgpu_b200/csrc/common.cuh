@@ -63,9 +63,9 @@ struct ProdDesc {
 // Device-resident iteration state of a closure (one per context).
 struct IterState {
     uint32_t iter;          // iteration index (parity selects delta buffers)
-    uint32_t item_count[2]; // work items written by the plan kernel, per list
-                            // (list 0: LOP3 inner loop, list 1: Four Russians)
-    uint32_t item_next[2];  // work-stealing counters of the product kernels
+    uint32_t item_count[3]; // work items written by the plan kernel, per list
+                            // (list 0: LOP3 inner loop, 1: Four Russians, 2: tensor cores)
+    uint32_t item_next[3];  // work-stealing counters of the product kernels
     uint32_t changed;       // set when any new bit appeared in this iteration
     uint32_t last_changed;  // copy of `changed` at the end of the iteration
     uint32_t error;         // nonzero: a bounded wait gave up (cfpq_status)
@@ -121,6 +121,9 @@ __host__ __device__ inline uint32_t entries_per_item(uint32_t T) {
     const uint32_t e = T / 16;
     return e > 8 ? e : 8;
 }
+// Tensor-core items keep the whole inner dimension: their TMEM epilogue is
+// amortised over every k-tile of the 256 x 256 block.
+__host__ __device__ inline uint32_t entries_per_item_tc(uint32_t T) { return T > 0 ? T : 1; }
 
 __host__ __device__ inline size_t tile_offset(uint32_t T, uint32_t ti, uint32_t tj) {
     return ((size_t)ti * T + tj) * kTileWords;

@@ -1,0 +1,355 @@
+// Variant TC: exact Boolean product C |= P * Q on the 5th-generation tensor
+// cores (tcgen05.mma kind::i8, 0/1 operands, int32 accumulators in TMEM,
+// result bit = accumulator > 0).
+//
+// Operands come pre-expanded (kernel_expand.cu): P as 0/1 bytes by rows and Q
+// transposed, both in the canonical no-swizzle K-major layout (8-row x 16-byte
+// core matrices, K-adjacent core matrices 128 B apart, M/N-adjacent 512 B
+// apart), one 4 KiB block per 64 x 64 tile.  The main loop does no ALU work on
+// operands: a single thread drives
+//   bulk copies (TMA engine) of the 4 P blocks (ti0..ti0+3, tk) and the 4 Q
+//   blocks (tk, tj0..tj0+3) of k-tile tk into one of kStages operand stages
+//   (32 KiB each, completion on the stage's mbarrier), and
+//   4 tcgen05.mma per k-tile (2 accumulators of M=128 x N=256, 2 K-halves of
+//   32), committed to the stage's mbarrier; a stage is refilled once its MMAs
+//   completed.
+// Work item (item list 2) = (product, group of 4 output tile-rows, block of 4
+// output tiles): a 256 x 256-bit output block over the whole inner dimension,
+// accumulated in TMEM as two 128 x 256 int32 matrices (all 512 TMEM columns;
+// one CTA per SM).
+// Epilogue (all 8 warps): tcgen05.ld 32x32b.x64 (warp w reads accumulator
+// w/4, TMEM lanes 32*(w%4)..), threshold > 0, pack 64 columns into a word,
+// then the atomic-OR epilogue of the word-level kernels (C, next delta D,
+// occupancy, populations).
+//
+// Arithmetic: 256*256*64 MACs per k-tile; bound = the tensor pipe's dense int8
+// rate.  All waits are bounded and report CFPQ_ERR_TIMEOUT.
+#include "launch.h"
+
+namespace cfpq {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kMaxTiles = 2048;
+constexpr uint32_t kTmemCols = 512;
+constexpr unsigned kFull = 0xffffffffu;
+constexpr uint32_t kOperandBytes = 256 * 64;  // one operand, one stage: 256 rows x 64 bytes
+constexpr uint32_t kStages = 4;               // operand stages in flight
+
+// Instruction descriptor, kind::i8: D = S32 (bits 4-5 = 2), A = B = U8 (0),
+// both K-major, N = 256 (bits 17-22 = N/8), M = 128 (bits 24-28 = M/16).
+constexpr uint32_t kIdesc = (2u << 4) | ((256u / 8) << 17) | ((128u / 16) << 24);
+
+struct __align__(1024) TcSmem {
+    uint8_t a[kStages][kOperandBytes];  // P blocks of 4 tile-rows, 4 x 4 KiB per stage
+    uint8_t b[kStages][kOperandBytes];  // Q^T blocks of 4 tiles, 4 x 4 KiB per stage
+    uint64_t ready_bar[kStages];
+    uint64_t mma_bar[kStages];
+    uint32_t tmem_base;
+    uint32_t item;
+    uint16_t cand[kMaxTiles];
+    uint16_t cmask[kMaxTiles];
+    uint16_t ktile[kMaxTiles];
+    uint32_t rball[kMaxTiles / 32], roff[kMaxTiles / 32];
+    uint32_t nc, nk;
+};
+
+__device__ __forceinline__ DevMat resolve_operand(const MatSlot &s, uint8_t use_delta, uint32_t iter) {
+    if (!use_delta || iter == 0) return s.cur;
+    return s.dlt[iter & 1];
+}
+
+// 64-bit shared-memory matrix descriptor, no swizzle, sm_100 version bit 46.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((addr & 0x3FFFFu) >> 4) | ((uint64_t)(lbo >> 4) << 16) | ((uint64_t)(sbo >> 4) << 32) |
+           (1ULL << 46);
+}
+
+__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_addr(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// 32 lanes x 64 consecutive 32-bit TMEM columns -> 64 registers.
+__device__ __forceinline__ void tmem_ld64(uint32_t taddr, uint32_t (&r)[64]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x64.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,"
+        "%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47,"
+        "%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, [%64];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]),
+          "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]),
+          "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]),
+          "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]),
+          "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+    k_product_tc(const ProdDesc *__restrict__ prods, const MatSlot *__restrict__ slots, IterState *st,
+                 const uint64_t *__restrict__ items_all, size_t list_cap, uint32_t *qchanged,
+                 const uint8_t *__restrict__ xp, const uint8_t *__restrict__ xq) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    TcSmem &S = *reinterpret_cast<TcSmem *>(smem_raw);
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint64_t *items = items_all + 2 * list_cap;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&S.tmem_base)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        for (uint32_t s = 0; s < kStages; ++s) {
+            mbar_init(&S.ready_bar[s], 1);
+            mbar_init(&S.mma_bar[s], 1);
+        }
+        fence_mbar_init();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = S.tmem_base;
+    uint32_t ready_phase = 0, mma_phase = 0;  // thread 0's per-stage parities
+    const uint32_t iter = st->iter;
+    const uint32_t nitems = st->item_count[2];
+    unsigned long long triples = 0, outw = 0, neww = 0;
+    bool timed_out = false;
+
+    for (;;) {
+        if (tid == 0) S.item = atomicAdd(&st->item_next[2], 1u);
+        __syncthreads();
+        const uint32_t idx = S.item;
+        if (idx >= nitems) break;
+        const uint64_t it = items[idx];
+        const ProdDesc pd = prods[item_prod(it)];
+        const uint32_t tig = item_ti(it), tjb = item_tjb(it), kw = item_kw(it);
+        const DevMat P = resolve_operand(slots[pd.pslot], pd.p_delta, iter);
+        const DevMat Q = resolve_operand(slots[pd.qslot], pd.q_delta, iter);
+        const DevMat C = slots[pd.head].cur;
+        const DevMat D = slots[pd.head].dlt[(iter & 1) ^ 1];
+        const uint32_t T = pd.T, ow = P.ow;
+        const uint32_t ti0 = tig * 4, tj0 = tjb * 4;
+        const uint32_t qword = tj0 >> 5, qshift = tj0 & 31;
+
+        // ---- k-list: tk with an occupied P tile in the 4 tile-rows and a
+        // non-empty Q block, increasing tk, chunk kw ----
+        if (warp == 0) {
+            uint32_t nc = 0;
+            for (uint32_t base = 0; base < ow; base += 32) {
+                uint32_t bits = 0;
+                if (base + lane < ow)
+                    for (uint32_t g = 0; g < 4 && ti0 + g < T; ++g) bits |= P.occ[(size_t)(ti0 + g) * ow + base + lane];
+                const uint32_t cnt = __popc(bits);
+                uint32_t pre = cnt;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t v = __shfl_up_sync(kFull, pre, o);
+                    if (lane >= (uint32_t)o) pre += v;
+                }
+                uint32_t pos = nc + pre - cnt;
+                while (bits) {
+                    S.cand[pos++] = (uint16_t)((base + lane) * 32 + (__ffs(bits) - 1));
+                    bits &= bits - 1;
+                }
+                nc += __shfl_sync(kFull, pre, 31);
+            }
+            if (lane == 0) S.nc = nc;
+        }
+        __syncthreads();
+        const uint32_t nc = S.nc, rounds = (nc + 31) / 32;
+        for (uint32_t r = warp; r < rounds; r += kThreads / 32) {
+            const uint32_t c = r * 32 + lane;
+            uint32_t mask = 0;
+            if (c < nc) mask = (Q.occ[(size_t)S.cand[c] * ow + qword] >> qshift) & 0xFu;
+            const unsigned ball = __ballot_sync(kFull, mask != 0);
+            if (c < nc) S.cmask[c] = (uint16_t)mask;
+            if (lane == 0) S.rball[r] = ball;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            uint32_t carry = 0;
+            for (uint32_t base = 0; base < rounds; base += 32) {
+                const uint32_t r = base + lane;
+                const uint32_t cnt = r < rounds ? __popc(S.rball[r]) : 0;
+                uint32_t pre = cnt;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t v = __shfl_up_sync(kFull, pre, o);
+                    if (lane >= (uint32_t)o) pre += v;
+                }
+                if (r < rounds) S.roff[r] = carry + pre - cnt;
+                carry += __shfl_sync(kFull, pre, 31);
+            }
+        }
+        __syncthreads();
+        const uint32_t E = entries_per_item_tc(T), rank_lo = kw * E, rank_hi = rank_lo + E;
+        for (uint32_t c = tid; c < nc; c += kThreads) {
+            if (!S.cmask[c]) continue;
+            const uint32_t rank = S.roff[c >> 5] + __popc(S.rball[c >> 5] & ((1u << (c & 31)) - 1));
+            if (rank < rank_lo || rank >= rank_hi) continue;
+            S.ktile[rank - rank_lo] = S.cand[c];  // keeps increasing tk order
+            triples += 16;
+        }
+        if (tid == 0) {
+            const uint32_t total = rounds ? S.roff[rounds - 1] + __popc(S.rball[rounds - 1]) : 0u;
+            S.nk = total > rank_lo ? min(E, total - rank_lo) : 0u;
+        }
+        __syncthreads();
+        const uint32_t nk = S.nk;
+
+        // ---- main loop: one thread drives copies and MMAs ----
+        if (tid == 0 && nk > 0) {
+            const uint32_t np = min(4u, T - ti0), nq = min(4u, T - tj0);  // existing P tile-rows / Q tiles
+            auto issue_copies = [&](uint32_t e) {
+                const uint32_t s = e % kStages, tk = S.ktile[e];
+                mbar_arrive_expect_tx(&S.ready_bar[s], (np + nq) * 4096u);
+                for (uint32_t g = 0; g < np; ++g)
+                    bulk_g2s(S.a[s] + g * 4096, xp + tile_offset(T, ti0 + g, tk) * 64, 4096u, &S.ready_bar[s]);
+                bulk_g2s(S.b[s], xq + tile_offset(T, tk, tj0) * 64, nq * 4096u, &S.ready_bar[s]);
+            };
+            auto wait_phase = [&](uint64_t *bars, uint32_t &phases, uint32_t s) {
+                if (!timed_out && !mbar_wait_bounded(&bars[s], (phases >> s) & 1u)) timed_out = true;
+                phases ^= 1u << s;
+            };
+            for (uint32_t e = 0; e < nk && e < kStages; ++e) issue_copies(e);
+            for (uint32_t e = 0; e < nk; ++e) {
+                const uint32_t s = e % kStages;
+                wait_phase(S.ready_bar, ready_phase, s);
+                if (timed_out) break;
+                tc_fence_after();
+                const uint32_t abase = smem_addr(S.a[s]), bbase = smem_addr(S.b[s]);
+#pragma unroll
+                for (uint32_t h = 0; h < 2; ++h) {      // accumulator h: operand rows 128h .. 128h+127
+#pragma unroll
+                    for (uint32_t kh = 0; kh < 2; ++kh) {  // K halves of 32 bytes
+                        const uint64_t ad = smem_desc(abase + h * 8192 + kh * 256, 128, 512);
+                        const uint64_t bd = smem_desc(bbase + kh * 256, 128, 512);
+                        mma_i8(tmem + h * 256, ad, bd, (e > 0 || kh > 0) ? 1u : 0u);
+                    }
+                }
+                mma_commit(&S.mma_bar[s]);
+                // refill the stage of k-tile e-1 once its MMAs completed (the
+                // tensor pipe keeps working on k-tile e meanwhile)
+                if (e >= 1 && e - 1 + kStages < nk) {
+                    const uint32_t s1 = (e - 1) % kStages;
+                    wait_phase(S.mma_bar, mma_phase, s1);
+                    if (timed_out) break;
+                    issue_copies(e - 1 + kStages);
+                }
+            }
+            // drain: every commit not waited for above (the last kStages k-tiles)
+            const uint32_t first_unwaited = nk > kStages ? nk - kStages : 0;
+            for (uint32_t e = first_unwaited; e < nk; ++e) wait_phase(S.mma_bar, mma_phase, e % kStages);
+        }
+        tc_fence_before();
+        timed_out = __syncthreads_or(timed_out) != 0;
+        tc_fence_after();
+        if (timed_out) break;  // uniform: the error status is set below
+
+        // ---- epilogue ----
+        bool any_new = false;
+        if (nk > 0) {
+            const uint32_t h = warp >> 2, q = warp & 3;
+            const uint32_t m = 128 * h + 32 * q + lane;  // output row within the 256-row block
+            const uint32_t ti = ti0 + (m >> 6), r = m & 63;
+#pragma unroll 1
+            for (uint32_t jt = 0; jt < 4; ++jt) {
+                uint32_t v[64];
+                tmem_ld64(tmem + ((32 * q) << 16) + h * 256 + jt * 64, v);
+                uint64_t a = 0;
+#pragma unroll
+                for (int c = 0; c < 64; ++c) a |= (uint64_t)(v[c] != 0) << c;
+                const uint32_t tj = tj0 + jt;
+                uint32_t newcnt = 0;
+                if (a && ti < T && tj < T) {
+                    ++outw;
+                    const size_t off = tile_offset(T, ti, tj) + r;
+                    unsigned long long *cw = reinterpret_cast<unsigned long long *>(C.bits + off);
+                    const uint64_t seen = __ldcg(cw);
+                    if (a & ~seen) {
+                        const uint64_t prev = atomicOr(cw, (unsigned long long)a);
+                        const uint64_t nw = a & ~prev;
+                        if (nw) {
+                            ++neww;
+                            newcnt = __popcll(nw);
+                            if (D.bits)
+                                atomicOr(reinterpret_cast<unsigned long long *>(D.bits + off), (unsigned long long)nw);
+                        }
+                    }
+                }
+                const uint32_t tile_new = __reduce_add_sync(kFull, newcnt);  // the warp's 32 rows share (ti, tj)
+                if (tile_new) {
+                    any_new = true;
+                    if (lane == 0) {
+                        atomicAdd(C.nnz + (size_t)ti * T + tj, tile_new);
+                        atomicOr(C.occ + (size_t)ti * C.ow + (tj >> 5), 1u << (tj & 31));
+                        if (D.bits) {
+                            atomicAdd(D.nnz + (size_t)ti * T + tj, tile_new);
+                            atomicOr(D.occ + (size_t)ti * D.ow + (tj >> 5), 1u << (tj & 31));
+                        }
+                    }
+                }
+            }
+        }
+        if (any_new && lane == 0) {
+            st->changed = 1u;
+            if (qchanged) qchanged[pd.query] = 1u;
+        }
+        tc_fence_before();
+        __syncthreads();  // TMEM reads done before the next item's first MMA overwrites it
+        tc_fence_after();
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        triples += __shfl_down_sync(kFull, triples, o);
+        outw += __shfl_down_sync(kFull, outw, o);
+        neww += __shfl_down_sync(kFull, neww, o);
+    }
+    if (lane == 0) {
+        if (triples) atomicAdd(&st->tile_triples, triples);
+        if (outw) atomicAdd(&st->out_words, outw);
+        if (neww) atomicAdd(&st->new_words, neww);
+    }
+    if (timed_out && tid == 0) atomicExch(&st->error, 5u);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+}
+
+}  // namespace
+
+int product_tc_blocks_per_sm() {
+    cudaFuncSetAttribute(k_product_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TcSmem));
+    int nb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_product_tc, kThreads, sizeof(TcSmem));
+    return nb;
+}
+
+cudaError_t launch_product_tc(const ProdDesc *d_prods, const MatSlot *d_slots, IterState *d_st,
+                              const uint64_t *d_items, size_t list_cap, uint32_t *d_qchanged, int grid,
+                              const uint8_t *xp, const uint8_t *xq, cudaStream_t s) {
+    k_product_tc<<<grid, kThreads, sizeof(TcSmem), s>>>(d_prods, d_slots, d_st, d_items, list_cap, d_qchanged, xp,
+                                                        xq);
+    return cudaGetLastError();
+}
+
+}  // namespace cfpq

@@ -282,7 +282,7 @@ __device__ __forceinline__ DevMat resolve_operand(const MatSlot &s, uint8_t use_
 // product's variant; list l starts at items + l * list_cap.
 __global__ void k_plan(const ProdDesc *__restrict__ prods, uint32_t nprods, uint32_t row_begin, uint32_t total_rows,
                        const MatSlot *__restrict__ slots, IterState *st, uint64_t *__restrict__ items_all,
-                       size_t list_cap, int tpb, uint32_t *prod_seen) {
+                       size_t list_cap, int tpb, uint32_t *prod_seen, int tc_mode) {
     const uint32_t gw = row_begin + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     const uint32_t lane = threadIdx.x & 31;
     if (gw >= total_rows || !st->active) return;
@@ -294,30 +294,37 @@ __global__ void k_plan(const ProdDesc *__restrict__ prods, uint32_t nprods, uint
     const ProdDesc pd = prods[lo];
     const uint32_t iter = st->iter;
     if (pd.term == 1 && iter == 0) return;  // first iteration: delta(A) = A, one term covers A*B
-    const uint32_t list = pd.variant == 3 ? 1u : 0u;  // CFPQ_VARIANT_M4R
+    // list 0: LOP3 items, list 1: Four Russians items (both 1 tile-row x tpb
+    // tiles); list 2: tensor-core items (4 tile-rows x 4 tiles)
+    const bool tc = pd.variant == 4;                         // CFPQ_VARIANT_TC
+    if (tc != (tc_mode != 0)) return;  // word-level and tensor-core products are planned by separate launches
+    const uint32_t list = tc ? 2u : (pd.variant == 3 ? 1u : 0u);  // CFPQ_VARIANT_M4R
+    if (tc) tpb = 4;
+    const uint32_t rows_per_item = tc ? 4u : 1u;
     uint64_t *items = items_all + list * list_cap;
-    const uint32_t ti = gw - pd.row_start;
+    const uint32_t ti = gw - pd.row_start;  // tile-row, or group of 4 tile-rows for tc
     const DevMat P = resolve_operand(slots[pd.pslot], pd.p_delta, iter);
     const DevMat Q = resolve_operand(slots[pd.qslot], pd.q_delta, iter);
     const uint32_t ow = P.ow;
-    const uint32_t *prow = P.occ + (size_t)ti * ow;
     const uint32_t bpw = 32 / tpb;  // blocks per occupancy word
     const uint32_t bmask = tpb == 32 ? 0xffffffffu : ((1u << tpb) - 1);
     bool emitted = false;
-    const uint32_t E = entries_per_item(pd.T);
+    const uint32_t E = tc ? entries_per_item_tc(pd.T) : entries_per_item(pd.T);
     for (uint32_t base = 0; base < ow; base += 32) {
         const uint32_t w = base + lane;
-        // contributing k-tiles per block of this lane's occupancy word (at most 4 blocks)
-        uint32_t cnt[4] = {0, 0, 0, 0};
+        // contributing k-tiles per block of this lane's occupancy word (at most 8 blocks)
+        uint32_t cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
         for (uint32_t pw = 0; pw < ow; ++pw) {
-            uint32_t bits = prow[pw];
+            uint32_t bits = 0;
+            for (uint32_t g = 0; g < rows_per_item && ti * rows_per_item + g < pd.T; ++g)
+                bits |= P.occ[(size_t)(ti * rows_per_item + g) * ow + pw];
             while (bits) {
                 const uint32_t tk = pw * 32 + (__ffs(bits) - 1);
                 bits &= bits - 1;
                 if (w < ow) {
                     const uint32_t m = Q.occ[(size_t)tk * ow + w];
 #pragma unroll
-                    for (uint32_t h = 0; h < 4; ++h)
+                    for (uint32_t h = 0; h < 8; ++h)
                         if (h < bpw) cnt[h] += ((m >> (h * tpb)) & bmask) != 0;
                 }
             }
@@ -392,11 +399,12 @@ __global__ void k_iter_end(IterState *st, QueryTrack qt, cudaGraphConditionalHan
             const uint32_t changed = st->changed;
             st->last_changed = changed;
             st->changed = 0;
-            st->items_total += st->item_count[0] + st->item_count[1];
+            st->items_total += st->item_count[0] + st->item_count[1] + st->item_count[2];
             st->items_by_variant[2] += st->item_count[0];
             st->items_by_variant[3] += st->item_count[1];
-            st->item_count[0] = st->item_count[1] = 0;
-            st->item_next[0] = st->item_next[1] = 0;
+            st->items_by_variant[4] += st->item_count[2];
+            st->item_count[0] = st->item_count[1] = st->item_count[2] = 0;
+            st->item_next[0] = st->item_next[1] = st->item_next[2] = 0;
             const uint32_t it = ++st->iter;
             s_iter = it;
             s_go = changed && st->error == 0 && (st->max_iter == 0 || it < st->max_iter);
@@ -516,10 +524,10 @@ cudaError_t launch_merge_or(const DevMat &dst, const DevMat &src, uint32_t *d_fl
 
 cudaError_t launch_plan(const ProdDesc *d_prods, uint32_t nprods, uint32_t row_begin, uint32_t row_end,
                         const MatSlot *d_slots, IterState *d_st, uint64_t *d_items, size_t list_cap,
-                        int tiles_per_block, uint32_t *d_prod_seen, cudaStream_t s) {
+                        int tiles_per_block, uint32_t *d_prod_seen, int tc_mode, cudaStream_t s) {
     if (row_end <= row_begin || nprods == 0) return cudaSuccess;
     k_plan<<<grid_for((size_t)(row_end - row_begin) * 32, 256), 256, 0, s>>>(
-        d_prods, nprods, row_begin, row_end, d_slots, d_st, d_items, list_cap, tiles_per_block, d_prod_seen);
+        d_prods, nprods, row_begin, row_end, d_slots, d_st, d_items, list_cap, tiles_per_block, d_prod_seen, tc_mode);
     return cudaGetLastError();
 }
 

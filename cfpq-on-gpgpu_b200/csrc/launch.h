@@ -35,12 +35,26 @@ cudaError_t launch_merge_or(const DevMat &dst, const DevMat &src, uint32_t *d_fl
 // Closure iteration
 cudaError_t launch_plan(const ProdDesc *d_prods, uint32_t nprods, uint32_t row_begin, uint32_t row_end,
                         const MatSlot *d_slots, IterState *d_st, uint64_t *d_items, size_t list_cap,
-                        int tiles_per_block, uint32_t *d_prod_seen, cudaStream_t s);
+                        int tiles_per_block, uint32_t *d_prod_seen, int tc_mode, cudaStream_t s);
+// (tc_mode 0 plans the word-level products of the row range, 1 the tensor-core ones.)
 // Tiled product over item list `m4r` (0: LOP3 inner loop, 1: Four Russians
 // inner loop); items of list l start at d_items + l * list_cap.
 cudaError_t launch_product_tiled(int m4r, const ProdDesc *d_prods, const MatSlot *d_slots, IterState *d_st,
                                  const uint64_t *d_items, size_t list_cap, uint32_t *d_qchanged, int grid,
                                  cudaStream_t s);
+// Tensor-core product over item list 2 (d_items + 2 * list_cap) of one
+// product whose operands were expanded into xp (P by rows) and xq (Q
+// transposed); one CTA per SM (it owns all 512 TMEM columns).
+cudaError_t launch_product_tc(const ProdDesc *d_prods, const MatSlot *d_slots, IterState *d_st,
+                              const uint64_t *d_items, size_t list_cap, uint32_t *d_qchanged, int grid,
+                              const uint8_t *xp, const uint8_t *xq, cudaStream_t s);
+int product_tc_blocks_per_sm();
+// Operand expansion for the tensor-core product (4 KiB of 0/1 bytes per tile,
+// canonical layout): side 0 = P of product p by rows, side 1 = Q transposed.
+cudaError_t launch_expand_operand(const ProdDesc *d_prods, uint32_t p, uint32_t T, const MatSlot *d_slots,
+                                  const IterState *d_st, int side, uint8_t *out, int num_sms, cudaStream_t s);
+// Closes a tensor-core product's item list (counts it, resets the counters).
+cudaError_t launch_reset_list(IterState *st, int list, cudaStream_t s);
 int product_lop3_tiles_per_block();
 int product_lop3_max_tiles();
 // Called once per context before any capture: sets kernel attributes, returns
