@@ -158,10 +158,9 @@ struct cfpq_ctx {
 static inline uint32_t tiles_for(uint32_t n) { return (n + 63) / 64; }
 
 // Upper bound of the work items one product term can emit per iteration:
-// tile-rows x column blocks x inner-dimension groups.
+// tile-rows x column blocks x chunks per block (tensor-core items: fewer).
 static inline size_t item_capacity(uint32_t T, int tpb) {
-    const uint32_t E = entries_per_item(T);
-    return (size_t)T * ((T + tpb - 1) / tpb) * ((T + E - 1) / E);
+    return (size_t)T * ((T + tpb - 1) / tpb) * kMaxChunksPerBlock;
 }
 
 static int alloc_devmat(uint32_t n, DevMat *d) {
@@ -918,6 +917,9 @@ static int build_plan(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, int variant
         }
     }
     pl->item_cap = std::max<size_t>(pl->item_cap, 1);
+    if (pl->prods.size() > kMaxItemProducts)
+        return set_error(CFPQ_ERR_INVALID, "%zu rule products in one closure (at most %u)", pl->prods.size(),
+                         kMaxItemProducts);
     return CFPQ_OK;
 }
 

@@ -102,28 +102,45 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
 }
 
 // Work item: (product, output tile-row ti, output tile-column block tjb,
-// chunk kw).  The k-tiles tk that contribute to the block (occupied P tile
-// (ti, tk) and a non-empty Q block (tk, tjb)), taken in increasing tk order,
-// are cut into chunks of entries_per_item(T); the item processes chunk kw.
-// Items of the same output block are independent: their partial products are
-// OR-ed into the head atomically.  Fields: p 21 bits, ti 15, tjb 12, kw 12.
-__host__ __device__ inline uint64_t make_item(uint32_t p, uint32_t ti, uint32_t tjb, uint32_t kw) {
-    return ((uint64_t)p << 39) | ((uint64_t)ti << 24) | ((uint64_t)tjb << 12) | (uint64_t)kw;
+// inner-dimension range [klo, khi)).  The item processes the k-tiles tk in its
+// range that contribute to the block (occupied P tile (ti, tk) and a non-empty
+// Q block (tk, tjb)).  The ranges of one block partition [0, T), so every
+// k-tile present when the iteration started is processed exactly once (a
+// k-tile that appears during the iteration may be processed or not: its bits
+// are also in the next delta).  Items of the same output block are
+// independent: their partial products are OR-ed into the head atomically.
+// Fields: p 16 bits, ti 11, tjb 9, klo 12, khi 12 (T <= 2048).
+constexpr uint32_t kMaxItemProducts = 1u << 16;
+__host__ __device__ inline uint64_t make_item(uint32_t p, uint32_t ti, uint32_t tjb, uint32_t klo, uint32_t khi) {
+    return ((uint64_t)p << 48) | ((uint64_t)ti << 37) | ((uint64_t)tjb << 28) | ((uint64_t)klo << 16) |
+           ((uint64_t)khi << 4);
 }
-__host__ __device__ inline uint32_t item_prod(uint64_t it) { return (uint32_t)(it >> 39); }
-__host__ __device__ inline uint32_t item_ti(uint64_t it) { return (uint32_t)((it >> 24) & 0x7FFF); }
-__host__ __device__ inline uint32_t item_tjb(uint64_t it) { return (uint32_t)((it >> 12) & 0xFFF); }
-__host__ __device__ inline uint32_t item_kw(uint64_t it) { return (uint32_t)(it & 0xFFF); }
+__host__ __device__ inline uint32_t item_prod(uint64_t it) { return (uint32_t)(it >> 48); }
+__host__ __device__ inline uint32_t item_ti(uint64_t it) { return (uint32_t)((it >> 37) & 0x7FF); }
+__host__ __device__ inline uint32_t item_tjb(uint64_t it) { return (uint32_t)((it >> 28) & 0x1FF); }
+__host__ __device__ inline uint32_t item_klo(uint64_t it) { return (uint32_t)((it >> 16) & 0xFFF); }
+__host__ __device__ inline uint32_t item_khi(uint64_t it) { return (uint32_t)((it >> 4) & 0xFFF); }
 
-// Contributing k-tiles per work item: short chains keep the per-item latency
-// low; at most 16 chunks per output block bound the item count.
-__host__ __device__ inline uint32_t entries_per_item(uint32_t T) {
-    const uint32_t e = T / 16;
-    return e > 8 ? e : 8;
+// Chunk length of the word-level items of a tile-row whose P operand has `np`
+// occupied tiles: at most kMaxChunksPerBlock chunks per output block (short
+// chains keep the per-item latency low when an iteration has few blocks; each
+// chunk re-does the block's epilogue).
+constexpr uint32_t kMaxChunksPerBlock = 8;
+
+// Bits of occupancy word w (tiles 32w .. 32w+31) that lie in [lo, hi).
+__host__ __device__ inline uint32_t range_word_mask(uint32_t w, uint32_t lo, uint32_t hi) {
+    const int a = (int)lo - (int)(w * 32), z = (int)hi - (int)(w * 32);
+    uint32_t m = 0xffffffffu;
+    if (a > 0) m = a >= 32 ? 0u : (m & (0xffffffffu << a));
+    if (z < 32) m = z <= 0 ? 0u : (m & (0xffffffffu >> (32 - z)));
+    return m;
 }
-// Tensor-core items keep the whole inner dimension: their TMEM epilogue is
-// amortised over every k-tile of the 256 x 256 block.
-__host__ __device__ inline uint32_t entries_per_item_tc(uint32_t T) { return T > 0 ? T : 1; }
+__host__ __device__ inline uint32_t item_entries(uint32_t np) {
+    const uint32_t e = (np + kMaxChunksPerBlock - 1) / kMaxChunksPerBlock;
+    return e < 1 ? 1 : e;
+}
+// Tensor-core items keep the whole inner dimension ([0, T), one chunk): their
+// TMEM epilogue is amortised over every k-tile of the 256 x 256 block.
 
 __host__ __device__ inline size_t tile_offset(uint32_t T, uint32_t ti, uint32_t tj) {
     return ((size_t)ti * T + tj) * kTileWords;

@@ -10,13 +10,14 @@
 // accumulators.
 //
 // Inner dimension: the contributing k-tiles tk (occupied P tile (ti, tk) and a
-// non-empty Q block (tk, block)) in increasing tk order, cut into chunks of
-// entries_per_item(T); the item keeps its chunk and sorts it by the
+// non-empty Q block (tk, block)) of the item's k-tile range, in increasing tk
+// order.  One elected thread stages,
+// per k-tile, the P tile (512 B) and the Q tiles with bulk copies
+// (cp.async.bulk, the TMA engine) completing on an mbarrier, double-buffered,
+// and the CTA runs one of three inner loops on the staged tiles, chosen by the
 // population of the P tile:
-//   dense  (population > kSparseMax): one elected thread stages the P tile
-//          (512 B) and the kBJ Q tiles (kBJ*512 B, one contiguous range of the
-//          tiled layout) into shared memory with bulk copies (cp.async.bulk,
-//          the TMA engine) completing on an mbarrier, double-buffered.
+//   dense  (population > kSparseMax), all kBJ Q tiles staged (one contiguous
+//          range of the tiled layout, empty tiles are zeros):
 //          LOP3: per row and inner index k, mask = -(P[row] bit k) (2 ALU
 //          ops), then acc |= mask & Q[k] on 8 uint32 words (one LOP3 each); Q
 //          rows k, k+1 of a tile come in one 16-byte shared load read by all
@@ -26,12 +27,10 @@
 //          (a table row per key, padded to 17 words so that lanes reading
 //          different keys hit different banks); each row then ORs one table
 //          word per slab and tile: 16 loads instead of 64 masked LOP3s.
-//   sparse (population <= kSparseMax): nothing is staged.  The (k-tile, row)
-//          pairs of all sparse k-tiles are spread over the CTA's 128 threads
-//          (4 pairs in flight per thread); a thread walks the set bits k of
-//          its P row word and ORs the Q words of row k of the occupied tiles,
-//          read straight from L2, into a shared-memory accumulator.
-// A warp whose 4 Q tiles are all empty skips the LOP3 loop / the lookups.
+//   sparse (population <= kSparseMax), only the range of occupied Q tiles
+//          staged: a thread walks the set bits k of its two P rows and ORs
+//          row k of each occupied Q tile of its warp from shared memory.
+// A warp whose 4 Q tiles are all empty skips the inner loop.
 //
 // Epilogue: for each non-zero accumulator word, new = acc & ~old via a 64-bit
 // atomicOr (several products of one iteration may write the same head); new
@@ -56,17 +55,14 @@ template <bool kM4R>
 struct __align__(128) TiledSmem {
     uint64_t q[2][kBJ * 64];     // 2 x 8 KiB
     uint64_t p[2][64];           // 2 x 512 B
-    unsigned long long sacc[kBJ * 64];  // sparse-phase accumulator [tile][row], 8 KiB
     uint64_t tab[kM4R ? 16 * 16 * kTabRow : 1];  // M4R tables [slab][key][tile], 34 KiB
     uint64_t bar[2];
-    uint16_t dtile[kMaxTiles];   // dense k-list: tile index
-    uint16_t dmask[kMaxTiles];   //               occupancy of the kBJ Q tiles
-    uint16_t stile[kMaxTiles];   // sparse k-list
-    uint16_t smask[kMaxTiles];
     uint16_t cand[kMaxTiles];    // occupied P tiles of the item's tile-row
     uint16_t cmask[kMaxTiles];   // their Q block occupancy
     uint32_t rball[kMaxTiles / 32], roff[kMaxTiles / 32];  // per-round ballots and rank offsets
-    uint32_t nc, nd, ns;
+    uint16_t ktile[kMaxTiles];   // the item's k-tiles, increasing; bit 15: dense P tile
+    uint16_t kmask[kMaxTiles];   // their Q block occupancy
+    uint32_t nc, nk;
     uint32_t item;
 };
 
@@ -78,10 +74,6 @@ __device__ __forceinline__ DevMat resolve_operand(const MatSlot &s, uint8_t use_
 __device__ __forceinline__ uint32_t bitmask(uint32_t word, int b) {
     // all-ones if bit b of word is set, else zero
     return (uint32_t)((int32_t)(word << (31 - b)) >> 31);
-}
-
-__device__ __forceinline__ uint64_t ld_cg(const uint64_t *p) {
-    return __ldcg(reinterpret_cast<const unsigned long long *>(p));
 }
 
 __device__ __forceinline__ void or64(uint2 &a, uint64_t v) {
@@ -118,7 +110,7 @@ __global__ void __launch_bounds__(kThreads, 4)
         if (idx >= nitems) break;
         const uint64_t it = items[idx];
         const ProdDesc pd = prods[item_prod(it)];
-        const uint32_t ti = item_ti(it), tjb = item_tjb(it), kw = item_kw(it);
+        const uint32_t ti = item_ti(it), tjb = item_tjb(it), klo = item_klo(it), khi = item_khi(it);
         const DevMat P = resolve_operand(slots[pd.pslot], pd.p_delta, iter);
         const DevMat Q = resolve_operand(slots[pd.qslot], pd.q_delta, iter);
         const DevMat C = slots[pd.head].cur;
@@ -128,13 +120,14 @@ __global__ void __launch_bounds__(kThreads, 4)
         const uint32_t nblk = min((uint32_t)kBJ, T - tj0);
         const uint32_t qword = tj0 >> 5, qshift = tj0 & 31;
 
-        // ---- k-lists: warp 0 compacts the occupied P tiles of row ti into a
-        // candidate list, then all threads classify candidates in parallel ----
+        // ---- k-list: warp 0 compacts the occupied P tiles of row ti in
+        // [klo, khi) into a candidate list, then all threads classify the
+        // candidates in parallel ----
         if (warp == 0) {
             uint32_t nc = 0;
             const uint32_t *prow = P.occ + (size_t)ti * ow;
             for (uint32_t base = 0; base < ow; base += 32) {
-                uint32_t bits = (base + lane < ow) ? prow[base + lane] : 0u;
+                uint32_t bits = (base + lane < ow) ? prow[base + lane] & range_word_mask(base + lane, klo, khi) : 0u;
                 const uint32_t cnt = __popc(bits);
                 uint32_t pre = cnt;  // inclusive scan over lanes
 #pragma unroll
@@ -149,15 +142,11 @@ __global__ void __launch_bounds__(kThreads, 4)
                 }
                 nc += __shfl_sync(kFull, pre, 31);
             }
-            if (lane == 0) {
-                S.nc = nc;
-                S.nd = 0;
-                S.ns = 0;
-            }
+            if (lane == 0) S.nc = nc;
         }
         __syncthreads();
         // rank the candidates with a non-empty Q block in increasing tk order
-        // (ballot per round of 32) and keep ranks [kw*E, kw*E + E)
+        // (ballot per round of 32)
         const uint32_t nc = S.nc, rounds = (nc + 31) / 32;
         for (uint32_t r = warp; r < rounds; r += kThreads / 32) {
             const uint32_t c = r * 32 + lane;
@@ -184,51 +173,72 @@ __global__ void __launch_bounds__(kThreads, 4)
             }
         }
         __syncthreads();
-        const uint32_t E = entries_per_item(T), rank_lo = kw * E, rank_hi = rank_lo + E;
         for (uint32_t c = tid; c < nc; c += kThreads) {
             const uint32_t mask = S.cmask[c];
             if (!mask) continue;
             const uint32_t rank = S.roff[c >> 5] + __popc(S.rball[c >> 5] & ((1u << (c & 31)) - 1));
-            if (rank < rank_lo || rank >= rank_hi) continue;
             const uint32_t tk = S.cand[c];
             triples += __popc(mask);
-            if (P.nnz[(size_t)ti * T + tk] > kSparseMax) {
-                const uint32_t pos = atomicAdd(&S.nd, 1u);
-                S.dtile[pos] = (uint16_t)tk;
-                S.dmask[pos] = (uint16_t)mask;
-            } else {
-                const uint32_t pos = atomicAdd(&S.ns, 1u);
-                S.stile[pos] = (uint16_t)tk;
-                S.smask[pos] = (uint16_t)mask;
-            }
+            const bool dense = P.nnz[(size_t)ti * T + tk] > kSparseMax;
+            S.ktile[rank] = (uint16_t)(tk | (dense ? 0x8000u : 0u));
+            S.kmask[rank] = (uint16_t)mask;
         }
+        if (tid == 0) S.nk = rounds ? S.roff[rounds - 1] + __popc(S.rball[rounds - 1]) : 0u;
         __syncthreads();
-        const uint32_t nd = S.nd, ns = S.ns;
+        const uint32_t nk = S.nk;
 
         uint2 acc0[4], acc1[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) acc0[j] = acc1[j] = make_uint2(0, 0);
 
-        // ---- dense k-tiles: staged panels ----
-        auto issue = [&](uint32_t e, uint32_t stage) {
-            const uint32_t tk = S.dtile[e];
+        // ---- staged k-tiles ----
+        auto issue = [&](uint32_t e, uint32_t stage) -> uint32_t {
+            const uint32_t kt = S.ktile[e], tk = kt & 0x7FFFu, mask = S.kmask[e];
+            // dense: the whole block (its empty tiles read as zeros); sparse:
+            // the range of occupied tiles only
+            const uint32_t lo = (kt & 0x8000u) ? 0u : (uint32_t)(__ffs(mask) - 1);
+            const uint32_t hi = (kt & 0x8000u) ? nblk - 1 : 31u - __clz(mask);
+            const uint32_t qbytes = (hi - lo + 1) * 512u;
             fence_proxy_async_smem();
-            mbar_arrive_expect_tx(&S.bar[stage], 512u + nblk * 512u);
+            mbar_arrive_expect_tx(&S.bar[stage], 512u + qbytes);
             bulk_g2s(S.p[stage], P.bits + tile_offset(T, ti, tk), 512u, &S.bar[stage]);
-            bulk_g2s(S.q[stage], Q.bits + tile_offset(T, tk, tj0), nblk * 512u, &S.bar[stage]);
+            bulk_g2s(&S.q[stage][lo * 64], Q.bits + tile_offset(T, tk, tj0 + lo), qbytes, &S.bar[stage]);
+            return 512u + qbytes;
         };
-        if (tid == 0 && nd > 0) {
-            issue(0, 0);
-            staged += (unsigned long long)nd * (512u + nblk * 512u);
-        }
+        if (tid == 0 && nk > 0) staged += issue(0, 0);
         uint32_t stage = 0;
-        for (uint32_t e = 0; e < nd; ++e) {
-            if (tid == 0 && e + 1 < nd) issue(e + 1, stage ^ 1);
+        for (uint32_t e = 0; e < nk; ++e) {
+            if (tid == 0 && e + 1 < nk) staged += issue(e + 1, stage ^ 1);
             if (!timed_out && !mbar_wait_bounded(&S.bar[stage], (phase >> stage) & 1u)) timed_out = true;
             phase ^= 1u << stage;
-            const uint32_t wmask = ((uint32_t)S.dmask[e] >> (4 * warp)) & 0xFu;
+            const bool dense = (S.ktile[e] & 0x8000u) != 0;
+            const uint32_t wmask = ((uint32_t)S.kmask[e] >> (4 * warp)) & 0xFu;
             const uint4 pp = *reinterpret_cast<const uint4 *>(&S.p[stage][2 * lane]);
-            if constexpr (kM4R) {
+            if (!dense) {
+                // sparse P tile: walk the set bits of rows 2l and 2l+1; only
+                // the occupied Q tiles of this warp were staged and are read
+                if (wmask && !timed_out) {
+                    const uint64_t *q = &S.q[stage][(4 * warp) * 64];
+                    uint64_t xa = ((uint64_t)pp.y << 32) | pp.x;
+                    uint64_t xb = ((uint64_t)pp.w << 32) | pp.z;
+                    while (xa | xb) {
+                        if (xa) {
+                            const int k = __ffsll((long long)xa) - 1;
+                            xa &= xa - 1;
+#pragma unroll
+                            for (int j = 0; j < 4; ++j)
+                                if ((wmask >> j) & 1u) or64(acc0[j], q[j * 64 + k]);
+                        }
+                        if (xb) {
+                            const int k = __ffsll((long long)xb) - 1;
+                            xb &= xb - 1;
+#pragma unroll
+                            for (int j = 0; j < 4; ++j)
+                                if ((wmask >> j) & 1u) or64(acc1[j], q[j * 64 + k]);
+                        }
+                    }
+                }
+            } else if constexpr (kM4R) {
                 // build: (slab s, tile j) pairs over the CTA; 16 keys each
                 for (uint32_t pr = tid; pr < 16 * kBJ; pr += kThreads) {
                     const uint32_t s = pr / kBJ, j = pr % kBJ;
@@ -294,50 +304,6 @@ __global__ void __launch_bounds__(kThreads, 4)
             timed_out = __syncthreads_or(timed_out) != 0;
             stage ^= 1;
         }
-
-        // ---- sparse k-tiles: (k-tile, row) pairs over all threads ----
-        if (ns > 0) {
-            for (uint32_t i = tid; i < kBJ * 64; i += kThreads) S.sacc[i] = 0ULL;
-            __syncthreads();
-            const uint32_t units = ns * 64;
-            for (uint32_t u0 = tid; u0 < units; u0 += 4 * kThreads) {
-                uint64_t pw[4];
-#pragma unroll
-                for (int g = 0; g < 4; ++g) {
-                    const uint32_t u = u0 + g * kThreads;
-                    pw[g] = u < units ? ld_cg(P.bits + tile_offset(T, ti, S.stile[u >> 6]) + (u & 63)) : 0ULL;
-                }
-#pragma unroll
-                for (int g = 0; g < 4; ++g) {
-                    uint64_t x = pw[g];
-                    if (!x) continue;
-                    const uint32_t u = u0 + g * kThreads;
-                    const uint32_t e = u >> 6, r = u & 63;
-                    const uint32_t mask = S.smask[e];
-                    const uint64_t *qb = Q.bits + tile_offset(T, S.stile[e], tj0);
-                    while (x) {
-                        const int k = __ffsll((long long)x) - 1;
-                        x &= x - 1;
-                        uint64_t qv[kBJ];
-#pragma unroll
-                        for (int j = 0; j < kBJ; ++j) qv[j] = ((mask >> j) & 1u) ? ld_cg(qb + j * 64 + k) : 0ULL;
-#pragma unroll
-                        for (int j = 0; j < kBJ; ++j)
-                            if (qv[j]) atomicOr(&S.sacc[j * 64 + r], (unsigned long long)qv[j]);
-                    }
-                }
-            }
-            __syncthreads();
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const uint4 s = *reinterpret_cast<const uint4 *>(&S.sacc[(4 * warp + j) * 64 + 2 * lane]);
-                acc0[j].x |= s.x;
-                acc0[j].y |= s.y;
-                acc1[j].x |= s.z;
-                acc1[j].y |= s.w;
-            }
-        }
-
         // ---- epilogue ----
         bool any_new = false;
 #pragma unroll

@@ -35,7 +35,7 @@ constexpr int kMaxTiles = 2048;
 constexpr uint32_t kTmemCols = 512;
 constexpr unsigned kFull = 0xffffffffu;
 constexpr uint32_t kOperandBytes = 256 * 64;  // one operand, one stage: 256 rows x 64 bytes
-constexpr uint32_t kStages = 4;               // operand stages in flight
+constexpr uint32_t kStages = 6;               // operand stages in flight
 
 // Instruction descriptor, kind::i8: D = S32 (bits 4-5 = 2), A = B = U8 (0),
 // both K-major, N = 256 (bits 17-22 = N/8), M = 128 (bits 24-28 = M/16).
@@ -141,7 +141,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (idx >= nitems) break;
         const uint64_t it = items[idx];
         const ProdDesc pd = prods[item_prod(it)];
-        const uint32_t tig = item_ti(it), tjb = item_tjb(it), kw = item_kw(it);
+        const uint32_t tig = item_ti(it), tjb = item_tjb(it), klo = item_klo(it), khi = item_khi(it);
         const DevMat P = resolve_operand(slots[pd.pslot], pd.p_delta, iter);
         const DevMat Q = resolve_operand(slots[pd.qslot], pd.q_delta, iter);
         const DevMat C = slots[pd.head].cur;
@@ -151,13 +151,15 @@ __global__ void __launch_bounds__(kThreads, 1)
         const uint32_t qword = tj0 >> 5, qshift = tj0 & 31;
 
         // ---- k-list: tk with an occupied P tile in the 4 tile-rows and a
-        // non-empty Q block, increasing tk, chunk kw ----
+        // non-empty Q block, increasing tk, within the item's range ----
         if (warp == 0) {
             uint32_t nc = 0;
             for (uint32_t base = 0; base < ow; base += 32) {
                 uint32_t bits = 0;
-                if (base + lane < ow)
+                if (base + lane < ow) {
                     for (uint32_t g = 0; g < 4 && ti0 + g < T; ++g) bits |= P.occ[(size_t)(ti0 + g) * ow + base + lane];
+                    bits &= range_word_mask(base + lane, klo, khi);
+                }
                 const uint32_t cnt = __popc(bits);
                 uint32_t pre = cnt;
 #pragma unroll
@@ -201,18 +203,13 @@ __global__ void __launch_bounds__(kThreads, 1)
             }
         }
         __syncthreads();
-        const uint32_t E = entries_per_item_tc(T), rank_lo = kw * E, rank_hi = rank_lo + E;
         for (uint32_t c = tid; c < nc; c += kThreads) {
             if (!S.cmask[c]) continue;
             const uint32_t rank = S.roff[c >> 5] + __popc(S.rball[c >> 5] & ((1u << (c & 31)) - 1));
-            if (rank < rank_lo || rank >= rank_hi) continue;
-            S.ktile[rank - rank_lo] = S.cand[c];  // keeps increasing tk order
+            S.ktile[rank] = S.cand[c];  // keeps increasing tk order
             triples += 16;
         }
-        if (tid == 0) {
-            const uint32_t total = rounds ? S.roff[rounds - 1] + __popc(S.rball[rounds - 1]) : 0u;
-            S.nk = total > rank_lo ? min(E, total - rank_lo) : 0u;
-        }
+        if (tid == 0) S.nk = rounds ? S.roff[rounds - 1] + __popc(S.rball[rounds - 1]) : 0u;
         __syncthreads();
         const uint32_t nk = S.nk;
 
