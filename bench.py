@@ -278,8 +278,7 @@ def ours_arm(args, world, rank, local):
     launches = {"n": 0}
 
     def step_value():
-        for m in q.mats:
-            m.clear()
+        ctx.clear_many(q.mats)
         ctx.load_edges_device(q.mats, d_src.data_ptr(), d_lab.data_ptr(), d_dst.data_ptr(), graph.nedges,
                               q.off, q.lm)
         for e in grammar.epsilon:
@@ -289,8 +288,7 @@ def ours_arm(args, world, rank, local):
         return st
 
     def step_e2e():
-        for m in q.mats:
-            m.clear()
+        ctx.clear_many(q.mats)
         ctx.load_edges(q.mats, h_src, h_lab, h_dst, q.off, q.lm)
         for e in grammar.epsilon:
             q.mats[e].set_diagonal()
@@ -335,6 +333,7 @@ def ours_arm(args, world, rank, local):
     barrier()
     total_ms = max_over_ranks(sum(times))
     gpu_launches = launches["n"]
+    phases = ctx.phase_log()  # per-iteration (plan, products) us of the last persistent closure
     value = world * args.steps / (total_ms / 1e3)
 
     # end to end through the C ABI with host buffers
@@ -351,15 +350,13 @@ def ours_arm(args, world, rank, local):
     # per-kernel device times (instrumented pass: every launch bracketed by events)
     roofline, prof = None, None
     if not args.no_profile:
-        for m in q.mats:
-            m.clear()
+        ctx.clear_many(q.mats)
         ctx.load_edges_device(q.mats, d_src.data_ptr(), d_lab.data_ptr(), d_dst.data_ptr(), graph.nedges,
                               q.off, q.lm)
         pst = ctx.closure(grammar.rules, q.mats, use_graph=False, log_products=capi.LOG_KERNELS)
         prof = ctx.kernel_profile()
         peaks = measured_peaks()
-        kern = {"product": prof["product_ms"], "plan": prof["plan_ms"], "advance": prof["advance_ms"],
-                "iter_end": prof["iter_end_ms"]}
+        kern = {"product": prof["product_ms"], "plan": prof["plan_ms"], "advance_end": prof["advance_ms"]}
         launches_p = max(1, prof["product_launches"])
         avg_ms = prof["product_ms"] / launches_p
         alg_bytes = (pst["bytes_staged"] + 16 * pst["out_words"] + 8 * pst["new_words"]) / launches_p
@@ -392,6 +389,9 @@ def ours_arm(args, world, rank, local):
             "closure": {"iterations": st["iterations"], "products": st["products"], "work_items": st["work_items"],
                         "tile_triples": st["tile_triples"], "device_ms_last": st["device_ms"],
                         "dense_equiv_gbitops": st["dense_bitops"] / (total_ms / args.steps / 1e3) / 1e9,
+                        "loop": "persistent kernel" if len(phases) else "CUDA graph",
+                        "phase_us_per_iteration": {"plan": float(phases[:, 0].mean()),
+                                                   "products": float(phases[:, 1].mean())} if len(phases) else None,
                         "result": {k: list(v) for k, v in zip(grammar.nonterminals, lines)}},
         }
         if not args.no_profile:

@@ -20,6 +20,7 @@ ERR_INVALID, ERR_CUDA, ERR_OOM, ERR_UNSUPPORTED, ERR_TIMEOUT, ERR_IO = 1, 2, 3, 
 
 VARIANT_AUTO, VARIANT_PLAIN, VARIANT_LOP3, VARIANT_M4R, VARIANT_TC = 0, 1, 2, 3, 4
 VARIANTS = {"auto": 0, "plain": 1, "lop3": 2, "m4r": 3, "tc": 4}
+LOOPS = {"host": 0, "device": 1, "graph": 2}
 DRIVER_ENGINE, DRIVER_WORKLIST = 0, 1
 
 # Every entry point declared in include/cfpq_b200.h.
@@ -32,6 +33,7 @@ EXPORTED = (
     "cfpq_product_log", "cfpq_last_kernel_profile", "cfpq_ctx_stream", "cfpq_load_edges_device",
     "cfpq_matrix_tile_stats", "cfpq_order_create", "cfpq_order_destroy", "cfpq_order_suggest",
     "cfpq_matrix_create_ordered", "cfpq_hash_count_rows_noalloc", "cfpq_noalloc_last_error", "cfpq_calibrate",
+    "cfpq_last_phase_log", "cfpq_matrices_clear",
 )
 
 
@@ -142,6 +144,8 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "cfpq_matrix_create_ordered": ([vp, u32, vp, P(vp)], i32),
         "cfpq_calibrate": ([vp, P(Calibration)], i32),
         "cfpq_load_edges_device": ([vp, P(vp), sz, vp, vp, vp, sz, vp, vp, u32], i32),
+        "cfpq_last_phase_log": ([vp, P(u64), sz], sz),
+        "cfpq_matrices_clear": ([vp, P(vp), sz], i32),
     }
     for name, (args, res) in sigs.items():
         f = getattr(lib, name)
@@ -298,7 +302,9 @@ class Context:
         o = ClosureOpts()
         o.driver = {"engine": DRIVER_ENGINE, "worklist": DRIVER_WORKLIST}.get(driver, driver)
         o.variant = VARIANTS[variant] if isinstance(variant, str) else int(variant)
-        o.use_graph = int(use_graph)
+        # loop sequencing: True / "device" (persistent kernel when possible),
+        # "graph" (CUDA-graph loop), False / "host" (host loop)
+        o.use_graph = LOOPS[use_graph] if isinstance(use_graph, str) else int(bool(use_graph))
         o.max_iterations = int(max_iterations)
         o.log_products = int(log_products)
         return o
@@ -370,10 +376,28 @@ class Context:
         _check(self.lib, self.lib.cfpq_calibrate(self.handle, ctypes.byref(c)))
         return {k: getattr(c, k) for k, _ in c._fields_}
 
+    def phase_log(self) -> np.ndarray:
+        """Per-iteration phase durations (plan, products) in microseconds of the
+        last persistent closure, shape (iterations, 2); empty if none."""
+        n = self.lib.cfpq_last_phase_log(self.handle, None, 0)
+        if n == 0:
+            return np.zeros((0, 2))
+        buf = np.zeros(3 * n, dtype=np.uint64)
+        self.lib.cfpq_last_phase_log(self.handle, buf.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), buf.size)
+        t = buf.reshape(n, 3).astype(np.float64)
+        return np.stack([t[:, 1] - t[:, 0], t[:, 2] - t[:, 1]], axis=1) / 1e3
+
     def kernel_profile(self) -> dict:
         p = KernelProfile()
         _check(self.lib, self.lib.cfpq_last_kernel_profile(self.handle, ctypes.byref(p)))
         return p.as_dict()
+
+    def clear_many(self, mats: Sequence[Matrix]) -> None:
+        """Clear several matrices with one kernel (occupied tiles only)."""
+        if not mats:
+            return
+        hs = (ctypes.c_void_p * len(mats))(*[m.handle for m in mats])
+        _check(self.lib, self.lib.cfpq_matrices_clear(self.handle, hs, len(mats)))
 
     def hash_count_many(self, mats: Sequence[Matrix]) -> list[tuple[int, int]]:
         if not mats:

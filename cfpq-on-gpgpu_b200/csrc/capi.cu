@@ -11,10 +11,11 @@
 //               after an iteration without new bits.  Every bit of the least
 //               fixpoint is produced because each pair (A bit, B bit) meets in
 //               the iteration after the later of the two appeared.  Iterations
-//               are plan -> product -> advance -> iter_end kernels, either
+//               are plan -> product -> advance+end kernels, either
 //               launched from a host loop that checks the flag every few
 //               iterations or captured once as the body of a CUDA-graph while
-//               node whose condition the iter_end kernel sets on the device.
+//               node whose condition the last block of the advance+end kernel
+//               sets on the device.
 //   WORKLIST -- the reference loop (cfpq-cpp/Grammar.h:58-69): one add_mul at
 //               a time with the changed flag read back after each product.
 #include <algorithm>
@@ -123,6 +124,9 @@ struct cfpq_matrix {
     cfpq_order *order = nullptr;
 };
 
+struct PlanCache;
+static void free_plan_cache(cfpq_ctx *ctx);
+
 struct cfpq_ctx {
     int device = 0;
     int num_sms = 0;
@@ -140,11 +144,17 @@ struct cfpq_ctx {
     unsigned long long *h_hash = nullptr;
     size_t h_hash_cap = 0;
     // growable device scratch
-    DevBuf stage, items, prods, slots, qtrack, prod_seen, mats_desc, edge_buf, xbuf;
+    DevBuf stage, items, prods, slots, qtrack, prod_seen, mats_desc, edge_buf, xbuf, clear_desc;
     std::unordered_map<uint32_t, PowTables> pow;
     std::vector<cfpq_matrix *> pool;  // zeroed spare matrices (deltas, alias copies)
     GraphCache gcache;
+    PlanCache *pcache = nullptr;  // created by the first closure
+    uint64_t plan_ids = 0;
+    uint64_t tables_owner = 0;  // plan id whose slot / product tables are in `slots` / `prods`
     int lop3_grid = 0, m4r_grid = 0, tc_grid = 0;  // tc_grid 0: tensor-core variant unavailable
+    int persist_grid[2] = {0, 0};  // persistent closure CTAs [with M4R items]; 0: unavailable
+    DevBuf phase_log;              // persistent closure: 3 timestamps per iteration
+    uint32_t phase_log_iters = 0;  // iterations logged by the last closure
     std::vector<cfpq_product_record> log;
     cudaEvent_t kev[5] = {};
     cfpq_kernel_profile prof = {};
@@ -156,6 +166,9 @@ struct cfpq_ctx {
 // helpers
 
 static inline uint32_t tiles_for(uint32_t n) { return (n + 63) / 64; }
+
+// Iterations of a persistent closure whose phase timestamps are kept.
+constexpr uint32_t kPhaseLogIters = 4096;
 
 // Upper bound of the work items one product term can emit per iteration:
 // tile-rows x column blocks x chunks per block (tensor-core items: fewer).
@@ -359,6 +372,9 @@ extern "C" int cfpq_ctx_create(int device, cfpq_ctx **out) {
     // The tensor-core kernel allocates all 512 TMEM columns of its SM, so it
     // must run one CTA per SM; it is only enabled when that is guaranteed.
     c->tc_grid = product_tc_blocks_per_sm() == 1 ? c->num_sms : 0;
+    int coop = 0;
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
+    for (int m = 0; m < 2; ++m) c->persist_grid[m] = coop ? persistent_blocks_per_sm(m) * c->num_sms : 0;
     *out = c;
     return CFPQ_OK;
 }
@@ -368,6 +384,7 @@ extern "C" int cfpq_ctx_destroy(cfpq_ctx *ctx) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     ctx->gcache.release();
+    free_plan_cache(ctx);
     for (auto *m : ctx->pool) {
         free_devmat(&m->d);
         delete m;
@@ -377,7 +394,7 @@ extern "C" int cfpq_ctx_destroy(cfpq_ctx *ctx) {
         cudaFree(kv.second.d_pow13);
     }
     for (DevBuf *b : {&ctx->stage, &ctx->items, &ctx->prods, &ctx->slots, &ctx->qtrack, &ctx->prod_seen,
-                      &ctx->mats_desc, &ctx->edge_buf, &ctx->xbuf})
+                      &ctx->mats_desc, &ctx->edge_buf, &ctx->xbuf, &ctx->phase_log, &ctx->clear_desc})
         b->release();
     cudaFree(ctx->d_st);
     cudaFree(ctx->d_flag);
@@ -576,6 +593,26 @@ extern "C" int cfpq_matrix_clear(cfpq_ctx *ctx, cfpq_matrix *m) {
     return CFPQ_OK;
 }
 
+extern "C" int cfpq_matrices_clear(cfpq_ctx *ctx, cfpq_matrix *const *mats, size_t count) {
+    TRY(use_device(ctx));
+    if (count == 0) return CFPQ_OK;
+    if (!mats) return set_error(CFPQ_ERR_INVALID, "null matrix list");
+    std::vector<MatRows> tab(count);
+    uint32_t rows = 0;
+    for (size_t i = 0; i < count; ++i) {
+        if (!mats[i]) return set_error(CFPQ_ERR_INVALID, "matrix %zu is null", i);
+        tab[i].m = mats[i]->d;
+        tab[i].row_start = rows;
+        tab[i].pad = 0;
+        rows += mats[i]->d.T;
+    }
+    TRY(ctx->clear_desc.ensure(count * sizeof(MatRows)));
+    CUDA_TRY(cudaMemcpyAsync(ctx->clear_desc.p, tab.data(), count * sizeof(MatRows), cudaMemcpyHostToDevice,
+                             ctx->stream));
+    CUDA_TRY(launch_clear_rows(ctx->clear_desc.as<MatRows>(), (uint32_t)count, rows, ctx->stream));
+    return CFPQ_OK;
+}
+
 extern "C" int cfpq_matrix_copy(cfpq_ctx *ctx, cfpq_matrix *dst, const cfpq_matrix *src) {
     TRY(use_device(ctx));
     if (!dst || !src) return set_error(CFPQ_ERR_INVALID, "null matrix");
@@ -726,6 +763,7 @@ static int enqueue_tiled_product(cfpq_ctx *ctx, const DevMat &a, const DevMat &b
     pd.n = a.n;
     pd.variant = (uint8_t)variant;
     const size_t cap = std::max<size_t>(item_capacity(T, tpb), 1);
+    ctx->tables_owner = 0;
     TRY(ctx->slots.ensure(sizeof(hs)));
     TRY(ctx->prods.ensure(sizeof(pd)));
     TRY(ctx->items.ensure(3 * cap * 8));
@@ -838,7 +876,27 @@ struct ClosurePlan {
     uint32_t tc_max_T = 0;
 };
 
+
 }  // namespace
+
+// The plan of the last closure, reused while the next closure has the same
+// rules, matrices and variant (a prepared query run again): its delta buffers
+// stay attached, and its device tables are re-sent only if something else
+// used the table buffers in between.
+struct PlanCache {
+    bool valid = false;
+    uint64_t id = 0;
+    std::vector<uint64_t> key;
+    ClosurePlan pl;
+};
+
+// Frees the cached plan at context destruction (deltas go to the pool first).
+static void free_plan_cache(cfpq_ctx *ctx) {
+    if (!ctx->pcache) return;
+    for (auto *m : ctx->pcache->pl.deltas) ctx->pool.push_back(m);
+    delete ctx->pcache;
+    ctx->pcache = nullptr;
+}
 
 static int validate_query(const QueryIn &q, size_t qi) {
     if (q.nmats && !q.mats) return set_error(CFPQ_ERR_INVALID, "query %zu: null matrix array", qi);
@@ -923,6 +981,35 @@ static int build_plan(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, int variant
     return CFPQ_OK;
 }
 
+// Cache key of a closure: variant, and per query its rules and the device
+// layout of its matrices.
+static void plan_key(const std::vector<QueryIn> &qs, int variant, std::vector<uint64_t> *key) {
+    key->clear();
+    key->push_back(((uint64_t)(uint32_t)variant << 32) | (uint64_t)qs.size());
+    for (const QueryIn &q : qs) {
+        key->push_back(((uint64_t)q.nrules << 32) | (uint64_t)q.nmats);
+        for (size_t r = 0; r < q.nrules; ++r)
+            key->push_back(((uint64_t)q.rules[r].head << 42) ^ ((uint64_t)q.rules[r].body1 << 21) ^
+                           (uint64_t)q.rules[r].body2);
+        for (size_t i = 0; i < q.nmats; ++i) {
+            const DevMat &d = q.mats[i]->d;
+            key->push_back((uint64_t)(uintptr_t)d.bits);
+            key->push_back((uint64_t)(uintptr_t)d.occ ^ ((uint64_t)(uintptr_t)d.nnz << 1));
+            key->push_back((uint64_t)(uintptr_t)d.perm ^ ((uint64_t)d.n << 40));
+        }
+    }
+}
+
+// Forget the cached plan; its deltas go back to the pool (cleared if dirty).
+static void drop_plan_cache(cfpq_ctx *ctx, bool dirty) {
+    if (!ctx->pcache) return;
+    PlanCache &pc = *ctx->pcache;
+    for (auto *m : pc.pl.deltas) pool_give(ctx, m, dirty);
+    pc.pl = ClosurePlan();
+    pc.key.clear();
+    pc.valid = false;
+}
+
 static int enqueue_iteration(cfpq_ctx *ctx, const ClosurePlan &pl, const QueryTrack &qt,
                              cudaGraphConditionalHandle handle, int use_handle) {
     const int tpb = product_lop3_tiles_per_block();
@@ -933,9 +1020,8 @@ static int enqueue_iteration(cfpq_ctx *ctx, const ClosurePlan &pl, const QueryTr
     for (const TcProduct &tp : pl.tc_prods)
         TRY(launch_tc_product(ctx, tp, (uint32_t)pl.prods.size(), pl.item_cap, ctx->prod_seen.as<uint32_t>(),
                               qt.changed, ctx->stream));
-    CUDA_TRY(launch_advance(ctx->slots.as<MatSlot>(), (uint32_t)pl.slots.size(), pl.slot_rows, ctx->d_st,
-                            ctx->stream));
-    CUDA_TRY(launch_iter_end(ctx->d_st, qt, handle, use_handle, ctx->stream));
+    CUDA_TRY(launch_advance_end(ctx->slots.as<MatSlot>(), (uint32_t)pl.slots.size(), pl.slot_rows, ctx->d_st, qt,
+                                handle, use_handle, ctx->stream));
     return CFPQ_OK;
 }
 
@@ -953,24 +1039,21 @@ static int enqueue_iteration_timed(cfpq_ctx *ctx, const ClosurePlan &pl, const Q
         TRY(launch_tc_product(ctx, tp, (uint32_t)pl.prods.size(), pl.item_cap, ctx->prod_seen.as<uint32_t>(),
                               qt.changed, s));
     CUDA_TRY(cudaEventRecord(ctx->kev[2], s));
-    CUDA_TRY(launch_advance(ctx->slots.as<MatSlot>(), (uint32_t)pl.slots.size(), pl.slot_rows, ctx->d_st, s));
+    CUDA_TRY(launch_advance_end(ctx->slots.as<MatSlot>(), (uint32_t)pl.slots.size(), pl.slot_rows, ctx->d_st, qt, 0, 0,
+                                s));
     CUDA_TRY(cudaEventRecord(ctx->kev[3], s));
-    CUDA_TRY(launch_iter_end(ctx->d_st, qt, 0, 0, s));
-    CUDA_TRY(cudaEventRecord(ctx->kev[4], s));
     return CFPQ_OK;
 }
 
 static int accumulate_kernel_times(cfpq_ctx *ctx) {
-    float t[4];
-    for (int i = 0; i < 4; ++i) CUDA_TRY(cudaEventElapsedTime(&t[i], ctx->kev[i], ctx->kev[i + 1]));
+    float t[3];
+    for (int i = 0; i < 3; ++i) CUDA_TRY(cudaEventElapsedTime(&t[i], ctx->kev[i], ctx->kev[i + 1]));
     ctx->prof.plan_ms += t[0];
     ctx->prof.product_ms += t[1];
-    ctx->prof.advance_ms += t[2];
-    ctx->prof.iter_end_ms += t[3];
+    ctx->prof.advance_ms += t[2];  // advance and iteration end are one kernel
     ctx->prof.plan_launches++;
     ctx->prof.product_launches++;
     ctx->prof.advance_launches++;
-    ctx->prof.iter_end_launches++;
     return CFPQ_OK;
 }
 
@@ -1055,19 +1138,24 @@ static int get_loop_graph(cfpq_ctx *ctx, const ClosurePlan &pl, const QueryTrack
 static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_closure_opts &o,
                       cfpq_closure_stats *stats, uint32_t *iters_out, double *done_ms_out) {
     for (size_t qi = 0; qi < qs.size(); ++qi) TRY(validate_query(qs[qi], qi));
-    ClosurePlan pl;
-    int rc = build_plan(ctx, qs, o.variant, &pl);
-    auto give_back = [&](bool dirty) {
-        for (auto *m : pl.deltas) pool_give(ctx, m, dirty);
-        pl.deltas.clear();
-    };
-    if (rc != CFPQ_OK) {
-        give_back(false);
-        return rc;
+    std::vector<uint64_t> key;
+    plan_key(qs, o.variant, &key);
+    if (!ctx->pcache) ctx->pcache = new PlanCache();
+    PlanCache &pc = *ctx->pcache;
+    if (!pc.valid || pc.key != key) {
+        drop_plan_cache(ctx, false);
+        int rc = build_plan(ctx, qs, o.variant, &pc.pl);
+        if (rc != CFPQ_OK) {
+            drop_plan_cache(ctx, false);
+            return rc;
+        }
+        pc.valid = true;
+        pc.key = std::move(key);
+        pc.id = ++ctx->plan_ids;
     }
+    ClosurePlan &pl = pc.pl;
     const size_t nq = qs.size();
     if (pl.prods.empty()) {
-        give_back(false);
         if (stats) memset(stats, 0, sizeof(*stats));
         for (size_t q = 0; q < nq; ++q) {
             if (iters_out) iters_out[q] = 0;
@@ -1076,21 +1164,31 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
         return CFPQ_OK;
     }
     // device tables
+    void *const slots_before = ctx->slots.p, *const prods_before = ctx->prods.p;
     TRY(ctx->slots.ensure(pl.slots.size() * sizeof(MatSlot)));
     TRY(ctx->prods.ensure(pl.prods.size() * sizeof(ProdDesc)));
-    TRY(ctx->items.ensure(3 * pl.item_cap * 8));
+    const bool tables_current =
+        ctx->tables_owner == pc.id && ctx->slots.p == slots_before && ctx->prods.p == prods_before;
+    const bool timed = (o.log_products & CFPQ_LOG_KERNELS) != 0;
+    const int persist_grid = ctx->persist_grid[pl.uses_m4r ? 1 : 0];
+    const bool persistent = o.use_graph == CFPQ_LOOP_DEVICE && !timed && !pl.uses_tc && persist_grid > 0;
+    TRY(ctx->items.ensure((persistent ? 4 : 3) * pl.item_cap * 8));
     TRY(ctx->prod_seen.ensure(pl.prods.size() * 4));
     if (pl.tc_max_T) TRY(ensure_expand_scratch(ctx, pl.tc_max_T));
+    if (persistent) TRY(ctx->phase_log.ensure(kPhaseLogIters * 3 * 8));
     const size_t qbytes = nq * (4 + 4 + 8) + 64;
     TRY(ctx->qtrack.ensure(qbytes));
     QueryTrack qt;
     qt.done_ns = ctx->qtrack.as<unsigned long long>();
     qt.changed = reinterpret_cast<uint32_t *>(qt.done_ns + nq);
     qt.last_iter = qt.changed + nq;
-    CUDA_TRY(cudaMemcpyAsync(ctx->slots.p, pl.slots.data(), pl.slots.size() * sizeof(MatSlot),
-                             cudaMemcpyHostToDevice, ctx->stream));
-    CUDA_TRY(cudaMemcpyAsync(ctx->prods.p, pl.prods.data(), pl.prods.size() * sizeof(ProdDesc),
-                             cudaMemcpyHostToDevice, ctx->stream));
+    if (!tables_current) {
+        CUDA_TRY(cudaMemcpyAsync(ctx->slots.p, pl.slots.data(), pl.slots.size() * sizeof(MatSlot),
+                                 cudaMemcpyHostToDevice, ctx->stream));
+        CUDA_TRY(cudaMemcpyAsync(ctx->prods.p, pl.prods.data(), pl.prods.size() * sizeof(ProdDesc),
+                                 cudaMemcpyHostToDevice, ctx->stream));
+        ctx->tables_owner = pc.id;
+    }
     CUDA_TRY(cudaMemsetAsync(ctx->prod_seen.p, 0, pl.prods.size() * 4, ctx->stream));
     CUDA_TRY(cudaMemsetAsync(ctx->qtrack.p, 0, qbytes, ctx->stream));
     IterState st;
@@ -1101,9 +1199,8 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
     *ctx->h_st = st;
     CUDA_TRY(cudaMemcpyAsync(ctx->d_st, ctx->h_st, sizeof(IterState), cudaMemcpyHostToDevice, ctx->stream));
 
-    const bool timed = (o.log_products & CFPQ_LOG_KERNELS) != 0;
     cudaGraphExec_t exec = nullptr;
-    if (o.use_graph && !timed) TRY(get_loop_graph(ctx, pl, qt, &exec));
+    if (o.use_graph && !timed && !persistent) TRY(get_loop_graph(ctx, pl, qt, &exec));
     if (timed) memset(&ctx->prof, 0, sizeof(ctx->prof));
 
     CUDA_TRY(launch_mark_start(ctx->d_st, ctx->stream));
@@ -1117,6 +1214,13 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
             if (!ctx->h_st->active) break;
             if (it > (1u << 24)) return set_error(CFPQ_ERR_CUDA, "closure did not converge");
         }
+    } else if (persistent) {
+        CUDA_TRY(launch_closure_persistent(pl.uses_m4r ? 1 : 0, persist_grid, ctx->prods.as<ProdDesc>(),
+                                           (uint32_t)pl.prods.size(), pl.prod_rows, ctx->slots.as<MatSlot>(),
+                                           (uint32_t)pl.slots.size(), pl.slot_rows, ctx->d_st,
+                                           ctx->items.as<uint64_t>(), pl.item_cap, ctx->prod_seen.as<uint32_t>(), qt,
+                                           product_lop3_tiles_per_block(),
+                                           ctx->phase_log.as<unsigned long long>(), kPhaseLogIters, ctx->stream));
     } else if (exec) {
         CUDA_TRY(cudaGraphLaunch(exec, ctx->stream));
     } else {
@@ -1144,8 +1248,13 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
     CUDA_TRY(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
     const IterState &hs = *ctx->h_st;
     const bool converged = hs.last_changed == 0;
-    give_back(!converged);
-    if (hs.error) return set_error(CFPQ_ERR_TIMEOUT, "a bounded device wait gave up during the closure");
+    ctx->phase_log_iters = persistent ? std::min<uint32_t>(hs.iter, kPhaseLogIters) : 0;
+    if (hs.error) {
+        drop_plan_cache(ctx, true);
+        return set_error(CFPQ_ERR_TIMEOUT, "a bounded device wait gave up during the closure");
+    }
+    if (!converged)  // stopped by the iteration limit: the deltas still hold bits
+        for (auto *m : pl.deltas) CUDA_TRY(launch_clear_matrix(m->d, ctx->stream));
     if (stats) {
         memset(stats, 0, sizeof(*stats));
         stats->iterations = hs.iter;
@@ -1154,8 +1263,10 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
         stats->work_items = hs.items_total;
         stats->dense_bitops = hs.dense_bitops;
         stats->device_ms = ms;
-        stats->kernel_launches = (uint64_t)hs.iter * 4 + 1;
-        stats->variant_items[CFPQ_VARIANT_LOP3] = hs.items_total;
+        stats->kernel_launches = persistent ? 2 : (uint64_t)hs.iter * 3 + 1;
+        stats->variant_items[CFPQ_VARIANT_LOP3] = hs.items_by_variant[2];
+        stats->variant_items[CFPQ_VARIANT_M4R] = hs.items_by_variant[3];
+        stats->variant_items[CFPQ_VARIANT_TC] = hs.items_by_variant[4];
         stats->bytes_staged = hs.bytes_staged;
         stats->out_words = hs.out_words;
         stats->new_words = hs.new_words;
@@ -1254,6 +1365,16 @@ extern "C" int cfpq_closure_batch(cfpq_ctx *ctx, const cfpq_query *queries, size
     qs.reserve(nqueries);
     for (size_t i = 0; i < nqueries; ++i) qs.push_back({queries[i].rules, queries[i].nrules, queries[i].mats, queries[i].nmats});
     return run_engine(ctx, qs, o, stats, iterations_out, done_ms_out);
+}
+
+extern "C" size_t cfpq_last_phase_log(cfpq_ctx *ctx, uint64_t *out, size_t cap) {
+    if (!ctx) return 0;
+    const size_t n = ctx->phase_log_iters;
+    const size_t k = std::min(cap, 3 * n);
+    if (out && k) {
+        if (cudaMemcpy(out, ctx->phase_log.p, k * 8, cudaMemcpyDeviceToHost) != cudaSuccess) return 0;
+    }
+    return n;
 }
 
 extern "C" size_t cfpq_product_log(cfpq_ctx *ctx, cfpq_product_record *out, size_t cap) {

@@ -72,7 +72,11 @@ struct IterState {
     uint32_t max_iter;      // 0 = unbounded
     uint32_t active;        // loop condition mirror (1 while iterating)
     uint32_t nqueries;
-    uint32_t pad;
+    uint32_t blocks_done;   // blocks of the advance kernel that finished (the last one ends the iteration)
+    // persistent closure kernel: grid barrier and per-parity iteration counters
+    uint32_t bar_count, bar_gen;
+    uint32_t pitem_count[2][2], pitem_next[2][2];  // [iteration parity][list]
+    uint32_t pchanged[2];
     unsigned long long tile_triples;
     unsigned long long items_total;
     unsigned long long products;      // non-empty product terms over all iterations
@@ -82,6 +86,14 @@ struct IterState {
     unsigned long long bytes_staged;  // operand bytes copied global -> shared by product kernels
     unsigned long long out_words;     // non-zero accumulator words merged into heads
     unsigned long long new_words;     // words that received new bits
+};
+
+// A matrix and the prefix sum of tile-rows over a list of matrices (kernels
+// with one warp per (matrix, tile-row)).
+struct MatRows {
+    DevMat m;
+    uint32_t row_start;
+    uint32_t pad;
 };
 
 // Per-query bookkeeping of a batched closure (device arrays of nqueries).
@@ -202,6 +214,38 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t phase)
 }
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31; }
+
+// One warp: clear tile-row ti of D -- zero every occupied tile and its
+// population, then the occupancy row (tiles without an occupancy bit hold no
+// bit and have population 0).
+__device__ __forceinline__ void clear_tile_row(const DevMat &D, uint32_t ti) {
+    const uint32_t lane = threadIdx.x & 31;
+    uint32_t *orow = D.occ + (size_t)ti * D.ow;
+    for (uint32_t w = 0; w < D.ow; ++w) {
+        uint32_t bits = orow[w];
+        while (bits) {
+            const uint32_t tj = w * 32 + (__ffs(bits) - 1);
+            bits &= bits - 1;
+            uint4 *tile = reinterpret_cast<uint4 *>(D.bits + tile_offset(D.T, ti, tj));
+            tile[lane] = make_uint4(0, 0, 0, 0);
+            if (lane == 0) D.nnz[(size_t)ti * D.T + tj] = 0;
+        }
+    }
+    __syncwarp();
+    for (uint32_t w = lane; w < D.ow; w += 32) orow[w] = 0;
+}
+
+// One warp: clear tile-row `row` (over all slots, slot tile-rows in order) of
+// the delta buffer dlt[parity].
+__device__ __forceinline__ void clear_delta_row(const MatSlot *__restrict__ slots, uint32_t nslots, uint32_t row,
+                                                uint32_t parity) {
+    uint32_t lo = 0, hi = nslots;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (slots[mid].row_start <= row) lo = mid; else hi = mid;
+    }
+    clear_tile_row(slots[lo].dlt[parity], row - slots[lo].row_start);
+}
 
 #endif  // __CUDACC__
 

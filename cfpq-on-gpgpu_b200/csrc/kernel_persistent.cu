@@ -1,0 +1,305 @@
+// Persistent closure kernel: the whole semi-naive fixpoint of a closure whose
+// products all use the word-level variants (LOP3 / M4R) in ONE cooperative
+// launch (every CTA resident), iterations separated by grid barriers instead
+// of kernel boundaries.
+//
+// Iteration t (parity par = t & 1), every CTA:
+//   phase A  warps take units round-robin: the product tile-rows (plan::plan_row
+//            emits the iteration's work items into the item lists of parity
+//            par) and, for t >= 1, the slot tile-rows of the delta read in
+//            iteration t-1 (dlt[par ^ 1], cleared: the products of iteration t
+//            write their new bits there).  CTA 0 also folds the counters of
+//            parity par ^ 1 (iteration t-1) into the statistics and zeroes them.
+//   barrier
+//   phase B  CTAs take work items (LOP3 list, then M4R list) and run
+//            tiled::process_item; new bits set changed[par].
+//   barrier
+//   decision every CTA reads changed[par] (final after the barrier) and the
+//            error word: continue while something changed, no wait gave up
+//            and the iteration limit is not reached.  CTA 0 records the
+//            per-query convergence data.
+// After the loop the delta read in the last iteration is cleared, so the
+// delta buffers go back to the pool zeroed.
+//
+// The same plan and item code as the multi-kernel iteration runs here; only
+// the sequencing differs.  Barrier waits are bounded: a CTA that gives up sets
+// the error word and leaves the loop, and every other wait then gives up too.
+#include "launch.h"
+#include "plan_device.cuh"
+#include "product_tiled.cuh"
+
+namespace cfpq {
+
+namespace {
+
+using tiled::ItemCounters;
+using tiled::kThreads;
+
+constexpr uint32_t kBarrierSpinLimit = 1u << 25;  // ~1 s of polling
+
+// Word-level products only: output blocks of 16 tiles, at most 128 per
+// tile-row.  The planner areas do not alias the product layout (its mbarriers
+// live across phases).
+constexpr uint32_t kWordBlocks = 128;
+
+// Slot and product tables are copied into shared memory when they fit (one
+// query or a small batch), saving two dependent global loads per item.
+constexpr uint32_t kTableBytes = 8192;
+
+template <bool kM4R>
+struct PersistSmem {
+    tiled::TiledSmem<kM4R> prod;
+    plan::WarpArea<kWordBlocks> plan[kThreads / 32];
+    alignas(16) unsigned char tables[kTableBytes];
+};
+
+struct PersistArgs {
+    const ProdDesc *prods;
+    uint32_t nprods, prod_rows;
+    const MatSlot *slots;
+    uint32_t nslots, slot_rows;
+    IterState *st;
+    uint64_t *items;  // 4 lists: (parity, list) at items + (2 * parity + list) * list_cap
+    size_t list_cap;
+    uint32_t *prod_seen;
+    QueryTrack qt;
+    int tpb;
+    unsigned long long *phase_log;  // 3 %globaltimer stamps per iteration (may be null)
+    uint32_t phase_log_iters;
+};
+
+// Grid barrier (all CTAs of the cooperative launch): arrival counter plus a
+// generation word; `gen` is the CTA's copy of the generation.  Returns false
+// when the wait gave up.
+__device__ __forceinline__ bool grid_barrier(IterState *st, uint32_t &gen) {
+    __shared__ uint32_t s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t ok = 1;
+        __threadfence();
+        if (atomicAdd(&st->bar_count, 1u) + 1 == gridDim.x) {
+            st->bar_count = 0;
+            __threadfence();
+            atomicAdd(&st->bar_gen, 1u);
+        } else {
+            uint32_t i = 0;
+            while (*reinterpret_cast<volatile uint32_t *>(&st->bar_gen) == gen) {
+                if (++i > kBarrierSpinLimit) {
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+        s_ok = ok;
+    }
+    ++gen;
+    __syncthreads();
+    return s_ok != 0;
+}
+
+template <bool kHasM4R>
+__global__ void __launch_bounds__(kThreads, 3) k_closure_persistent(PersistArgs a) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    PersistSmem<kHasM4R> &S = *reinterpret_cast<PersistSmem<kHasM4R> *>(smem_raw);
+    IterState *st = a.st;
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t gwarp = blockIdx.x * (kThreads / 32) + warp, nwarps = gridDim.x * (kThreads / 32);
+    __shared__ uint32_t s_gen0, s_go;
+
+    if (tid == 0) {
+        for (uint32_t i = 0; i < tiled::kStages; ++i) mbar_init(&S.prod.bar[i], 1);
+        fence_mbar_init();
+        s_gen0 = st->bar_gen;
+    }
+    const size_t slot_bytes = (size_t)a.nslots * sizeof(MatSlot), prod_bytes = (size_t)a.nprods * sizeof(ProdDesc);
+    const bool cached = slot_bytes + prod_bytes <= kTableBytes;
+    const MatSlot *slots = a.slots;
+    const ProdDesc *prods = a.prods;
+    if (cached) {
+        uint32_t *dst = reinterpret_cast<uint32_t *>(S.tables);
+        const uint32_t *s0 = reinterpret_cast<const uint32_t *>(a.slots);
+        const uint32_t *p0 = reinterpret_cast<const uint32_t *>(a.prods);
+        for (size_t i = tid; i < slot_bytes / 4; i += kThreads) dst[i] = s0[i];
+        for (size_t i = tid; i < prod_bytes / 4; i += kThreads) dst[slot_bytes / 4 + i] = p0[i];
+        slots = reinterpret_cast<const MatSlot *>(S.tables);
+        prods = reinterpret_cast<const ProdDesc *>(S.tables + slot_bytes);
+    }
+    __syncthreads();
+    uint32_t gen = s_gen0, phase = 0;
+    bool timed_out = false;
+    ItemCounters ctr;
+    const uint32_t iter0 = st->iter, max_iter = st->max_iter;
+    uint32_t t = iter0;
+
+    for (;; ++t) {
+        const uint32_t par = t & 1;
+        if (blockIdx.x == 0 && tid == 0) {
+            if (a.phase_log && t - iter0 < a.phase_log_iters) a.phase_log[3 * (t - iter0)] = globaltimer_ns();
+            if (t > iter0) {  // counters of iteration t-1 -> statistics, then reset for iteration t+1
+                const uint32_t q = par ^ 1;
+                const uint32_t c0 = st->pitem_count[q][0], c1 = st->pitem_count[q][1];
+                st->items_total += c0 + c1;
+                st->items_by_variant[2] += c0;
+                st->items_by_variant[3] += c1;
+                st->pitem_count[q][0] = st->pitem_count[q][1] = 0;
+                st->pitem_next[q][0] = st->pitem_next[q][1] = 0;
+                st->pchanged[q] = 0;
+            }
+        }
+        // ---- phase A: plan of iteration t + clear of the delta read in t-1 ----
+        {
+            const uint32_t clear_rows = t > 0 ? a.slot_rows : 0u;
+            const uint32_t units = a.prod_rows + clear_rows;
+            for (uint32_t u = gwarp; u < units; u += nwarps) {
+                if (u < a.prod_rows) {
+                    plan::plan_row(u, prods, a.nprods, slots, t, st, st->pitem_count[par],
+                                   a.items + (size_t)(2 * par) * a.list_cap, a.list_cap, a.tpb, a.prod_seen, 0,
+                                   S.plan[warp].cnt, S.plan[warp].bnd);
+                } else {
+                    clear_delta_row(slots, a.nslots, u - a.prod_rows, par ^ 1);
+                }
+                __syncwarp();
+            }
+        }
+        if (!grid_barrier(st, gen)) timed_out = true;
+        if (blockIdx.x == 0 && tid == 0 && a.phase_log && t - iter0 < a.phase_log_iters)
+            a.phase_log[3 * (t - iter0) + 1] = globaltimer_ns();
+        if (timed_out) break;
+
+        // ---- phase B: products ----
+        {
+            const uint64_t *items = a.items + (size_t)(2 * par) * a.list_cap;
+            const uint32_t n0 = st->pitem_count[par][0];
+            for (;;) {
+                if (tid == 0) S.prod.item = atomicAdd(&st->pitem_next[par][0], 1u);
+                __syncthreads();
+                const uint32_t idx = S.prod.item;
+                __syncthreads();
+                if (idx >= n0) break;
+                tiled::process_item<false>(S.prod, items[idx], prods, slots, t, &st->pchanged[par], a.qt.changed,
+                                           phase, timed_out, ctr);
+            }
+            if constexpr (kHasM4R) {
+                const uint32_t n1 = st->pitem_count[par][1];
+                for (;;) {
+                    if (tid == 0) S.prod.item = atomicAdd(&st->pitem_next[par][1], 1u);
+                    __syncthreads();
+                    const uint32_t idx = S.prod.item;
+                    __syncthreads();
+                    if (idx >= n1) break;
+                    tiled::process_item<true>(S.prod, items[a.list_cap + idx], prods, slots, t,
+                                              &st->pchanged[par], a.qt.changed, phase, timed_out, ctr);
+                }
+            }
+        }
+        if (!grid_barrier(st, gen)) timed_out = true;
+        if (timed_out) break;
+
+        // ---- decision ----
+        if (tid == 0) {
+            const uint32_t changed = *reinterpret_cast<volatile uint32_t *>(&st->pchanged[par]);
+            const uint32_t err = *reinterpret_cast<volatile uint32_t *>(&st->error);
+            s_go = changed && err == 0 && (max_iter == 0 || t + 1 < max_iter);
+        }
+        __syncthreads();
+        const bool go = s_go != 0;
+        if (blockIdx.x == 0) {
+            if (tid == 0 && a.phase_log && t - iter0 < a.phase_log_iters)
+                a.phase_log[3 * (t - iter0) + 2] = globaltimer_ns();
+            if (a.qt.changed) {
+                const unsigned long long now = globaltimer_ns();
+                for (uint32_t q = tid; q < st->nqueries; q += kThreads) {
+                    if (a.qt.changed[q]) {
+                        a.qt.changed[q] = 0;
+                        a.qt.last_iter[q] = t + 1;
+                        a.qt.done_ns[q] = now;
+                    }
+                }
+            }
+        }
+        if (!go) break;
+    }
+
+    // ---- exit: clear the delta read in the last iteration; final state ----
+    if (!timed_out) {
+        const uint32_t par = t & 1;
+        for (uint32_t u = gwarp; u < a.slot_rows; u += nwarps) {
+            clear_delta_row(slots, a.nslots, u, par);
+            __syncwarp();
+        }
+    }
+    unsigned long long triples = ctr.triples, outw = ctr.outw, neww = ctr.neww;
+    for (int o = 16; o > 0; o >>= 1) {
+        triples += __shfl_down_sync(tiled::kFull, triples, o);
+        outw += __shfl_down_sync(tiled::kFull, outw, o);
+        neww += __shfl_down_sync(tiled::kFull, neww, o);
+    }
+    if (lane == 0) {
+        if (triples) atomicAdd(&st->tile_triples, triples);
+        if (outw) atomicAdd(&st->out_words, outw);
+        if (neww) atomicAdd(&st->new_words, neww);
+    }
+    if (tid == 0 && ctr.staged) atomicAdd(&st->bytes_staged, ctr.staged);
+    if (tid == 0 && timed_out) atomicExch(&st->error, (uint32_t)5);
+    if (blockIdx.x == 0 && tid == 0 && !timed_out) {
+        const uint32_t par = t & 1;
+        const uint32_t c0 = st->pitem_count[par][0], c1 = st->pitem_count[par][1];
+        st->items_total += c0 + c1;
+        st->items_by_variant[2] += c0;
+        st->items_by_variant[3] += c1;
+        st->last_changed = st->pchanged[par];
+        st->iter = t + 1;
+        st->active = 0;
+    }
+}
+
+template <bool kHasM4R>
+int persistent_blocks_per_sm_impl() {
+    const int smem = (int)sizeof(PersistSmem<kHasM4R>);
+    if (cudaFuncSetAttribute(k_closure_persistent<kHasM4R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+        cudaSuccess)
+        return 0;
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_closure_persistent<kHasM4R>, kThreads, smem) !=
+        cudaSuccess)
+        return 0;
+    return nb;
+}
+
+}  // namespace
+
+int persistent_blocks_per_sm(int has_m4r) {
+    return has_m4r ? persistent_blocks_per_sm_impl<true>() : persistent_blocks_per_sm_impl<false>();
+}
+
+cudaError_t launch_closure_persistent(int has_m4r, int grid, const ProdDesc *prods, uint32_t nprods,
+                                      uint32_t prod_rows, const MatSlot *slots, uint32_t nslots, uint32_t slot_rows,
+                                      IterState *st, uint64_t *items, size_t list_cap, uint32_t *prod_seen,
+                                      const QueryTrack &qt, int tpb, unsigned long long *phase_log,
+                                      uint32_t phase_log_iters, cudaStream_t s) {
+    PersistArgs a;
+    a.prods = prods;
+    a.nprods = nprods;
+    a.prod_rows = prod_rows;
+    a.slots = slots;
+    a.nslots = nslots;
+    a.slot_rows = slot_rows;
+    a.st = st;
+    a.items = items;
+    a.list_cap = list_cap;
+    a.prod_seen = prod_seen;
+    a.qt = qt;
+    a.tpb = tpb;
+    a.phase_log = phase_log;
+    a.phase_log_iters = phase_log_iters;
+    void *args[] = {&a};
+    if (has_m4r)
+        return cudaLaunchCooperativeKernel((const void *)k_closure_persistent<true>, dim3(grid), dim3(kThreads), args,
+                                           sizeof(PersistSmem<true>), s);
+    return cudaLaunchCooperativeKernel((const void *)k_closure_persistent<false>, dim3(grid), dim3(kThreads), args,
+                                       sizeof(PersistSmem<false>), s);
+}
+
+}  // namespace cfpq

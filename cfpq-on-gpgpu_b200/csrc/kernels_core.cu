@@ -2,6 +2,7 @@
 // bit scatter, result hash, the plain dense product, and the plan / advance
 // steps of the device-resident closure iteration.
 #include "launch.h"
+#include "plan_device.cuh"
 
 namespace cfpq {
 
@@ -269,195 +270,45 @@ __global__ void __launch_bounds__(64) k_merge_or(DevMat dst, DevMat src, uint32_
 }
 
 // ---- closure iteration: plan ---------------------------------------------------
-// One warp per (product, output tile-row ti) (a group of 4 tile-rows for
-// tensor-core products).  For every block of `tpb` output tiles the warp counts
-// the contributing k-tiles tk (occupied P tile (ti, tk) and a non-empty Q
-// block (tk, block)) in increasing tk order and cuts them into chunks of E
-// (item_entries of the row's occupied P tile count, so at most
-// kMaxChunksPerBlock chunks; tensor-core items take one chunk).  Chunk j of a
-// block becomes the item with k-tile range [first tk of chunk j, first tk of
-// chunk j+1), the first range starting at 0 and the last ending at T: the
-// ranges partition [0, T).  Skipping is exact: a tile pair contributes only if
-// both tiles are occupied.
-// The k-tiles of one P occupancy word go to the lanes (lane l takes the l-th
-// set bit), so the Q occupancy loads of a word are issued together; per-block
-// counts and chunk boundaries live in shared memory (one region per warp).
-__device__ __forceinline__ DevMat resolve_operand(const MatSlot &s, uint8_t use_delta, uint32_t iter) {
-    if (!use_delta || iter == 0) return s.cur;
-    return s.dlt[iter & 1];
-}
-
-// Position of the n-th (0-based) set bit of x (x has more than n set bits).
-__device__ __forceinline__ uint32_t nth_set_bit(uint32_t x, uint32_t n) {
-    uint32_t pos = 0;
-#pragma unroll
-    for (uint32_t s = 16; s > 0; s >>= 1) {
-        const uint32_t c = __popc(x & ((1u << s) - 1));
-        if (n >= c) {
-            n -= c;
-            x >>= s;
-            pos += s;
-        }
-    }
-    return pos;
-}
-
+// One warp per (product, tile-row); the planner itself is plan::plan_row.
 constexpr int kPlanThreads = 128;
-constexpr uint32_t kPlanMaxBlocks = 512;  // T <= 2048 tiles, blocks of >= 4 tiles
 
-// Items go to list 0 (LOP3 inner loop), 1 (Four Russians) or 2 (tensor cores)
-// by the product's variant; list l starts at items + l * list_cap.
 __global__ void __launch_bounds__(kPlanThreads)
     k_plan(const ProdDesc *__restrict__ prods, uint32_t nprods, uint32_t row_begin, uint32_t total_rows,
            const MatSlot *__restrict__ slots, IterState *st, uint64_t *__restrict__ items_all, size_t list_cap,
            int tpb, uint32_t *prod_seen, int tc_mode) {
-    __shared__ uint32_t counts[kPlanThreads / 32][kPlanMaxBlocks];
-    __shared__ uint16_t bounds[kPlanThreads / 32][kPlanMaxBlocks][kMaxChunksPerBlock - 1];
+    __shared__ plan::WarpArea<plan::kPlanMaxBlocks> areas[kPlanThreads / 32];
     const uint32_t gw = row_begin + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-    const uint32_t lane = threadIdx.x & 31;
-    uint32_t *cnt = counts[threadIdx.x >> 5];
-    uint16_t(*bnd)[kMaxChunksPerBlock - 1] = bounds[threadIdx.x >> 5];
     if (gw >= total_rows || !st->active) return;
-    uint32_t lo = 0, hi = nprods;  // product: last p with row_start <= gw
-    while (hi - lo > 1) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (prods[mid].row_start <= gw) lo = mid; else hi = mid;
-    }
-    const ProdDesc pd = prods[lo];
-    const uint32_t iter = st->iter;
-    if (pd.term == 1 && iter == 0) return;  // first iteration: delta(A) = A, one term covers A*B
-    const bool tc = pd.variant == 4;                         // CFPQ_VARIANT_TC
-    if (tc != (tc_mode != 0)) return;  // word-level and tensor-core products are planned by separate launches
-    const uint32_t list = tc ? 2u : (pd.variant == 3 ? 1u : 0u);  // CFPQ_VARIANT_M4R
-    if (tc) tpb = 4;
-    const uint32_t rows_per_item = tc ? 4u : 1u;
-    uint64_t *items = items_all + list * list_cap;
-    const uint32_t ti = gw - pd.row_start;  // tile-row, or group of 4 tile-rows for tc
-    const DevMat P = resolve_operand(slots[pd.pslot], pd.p_delta, iter);
-    const DevMat Q = resolve_operand(slots[pd.qslot], pd.q_delta, iter);
-    const uint32_t T = pd.T, ow = P.ow;
-    const uint32_t bpw = 32 / tpb;  // blocks per occupancy word
-    const uint32_t bmask = tpb == 32 ? 0xffffffffu : ((1u << tpb) - 1);
-    const uint32_t nblocks = (T + tpb - 1) / tpb;
-    auto prow_word = [&](uint32_t w) {
-        uint32_t bits = 0;
-        for (uint32_t g = 0; g < rows_per_item && ti * rows_per_item + g < T; ++g)
-            bits |= P.occ[(size_t)(ti * rows_per_item + g) * ow + w];
-        return bits;
-    };
-    uint32_t np = 0;  // occupied P tiles of the row (group)
-    for (uint32_t base = 0; base < ow; base += 32)
-        np += __reduce_add_sync(kFull, base + lane < ow ? (uint32_t)__popc(prow_word(base + lane)) : 0u);
-    if (!np) return;
-    const uint32_t E = tc ? T : item_entries(np);
-    for (uint32_t b = lane; b < nblocks; b += 32) cnt[b] = 0;
-    __syncwarp();
-
-    for (uint32_t pw = 0; pw < ow; ++pw) {
-        const uint32_t bits = prow_word(pw);  // warp-uniform
-        if (!bits) continue;
-        const bool valid = lane < (uint32_t)__popc(bits);
-        const uint32_t tk = valid ? pw * 32 + nth_set_bit(bits, lane) : 0u;  // increasing with the lane
-        const uint32_t *qrow = Q.occ + (size_t)tk * ow;
-        for (uint32_t w0 = 0; w0 < ow; w0 += 4) {
-            uint32_t m[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) m[u] = (valid && w0 + u < ow) ? qrow[w0 + u] : 0u;
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                if (w0 + u >= ow) break;
-                if (!__ballot_sync(kFull, m[u] != 0)) continue;
-                for (uint32_t h = 0; h < bpw; ++h) {
-                    const unsigned bal = __ballot_sync(kFull, ((m[u] >> (h * tpb)) & bmask) != 0);
-                    if (!bal) continue;
-                    const uint32_t b = (w0 + u) * bpw + h, c = __popc(bal), cb = cnt[b];
-                    // chunk boundaries: ranks j*E (j >= 1) among this ballot's ranks cb .. cb+c-1
-                    for (uint32_t j = (cb + E - 1) / E; j < kMaxChunksPerBlock && j * E < cb + c; ++j) {
-                        if (j == 0) continue;
-                        const uint32_t src = nth_set_bit(bal, j * E - cb);
-                        const uint32_t tkj = __shfl_sync(kFull, tk, src);
-                        if (lane == 0) bnd[b][j - 1] = (uint16_t)tkj;
-                    }
-                    __syncwarp();
-                    if (lane == 0) cnt[b] = cb + c;
-                    __syncwarp();
-                }
-            }
-        }
-    }
-
-    auto nchunks = [&](uint32_t c) { return c ? (c + E - 1) / E : 0u; };
-    uint32_t total = 0;
-    for (uint32_t base = 0; base < nblocks; base += 32) {
-        const uint32_t b = base + lane;
-        total += __reduce_add_sync(kFull, b < nblocks ? nchunks(cnt[b]) : 0u);
-    }
-    if (!total) return;
-    uint32_t pos0 = 0;
-    if (lane == 0) pos0 = atomicAdd(&st->item_count[list], total);
-    pos0 = __shfl_sync(kFull, pos0, 0);
-    for (uint32_t base = 0; base < nblocks; base += 32) {
-        const uint32_t b = base + lane;
-        const uint32_t nitem = b < nblocks ? nchunks(cnt[b]) : 0u;
-        uint32_t pre = nitem;  // inclusive scan over lanes
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t v = __shfl_up_sync(kFull, pre, o);
-            if (lane >= (uint32_t)o) pre += v;
-        }
-        for (uint32_t j = 0; j < nitem; ++j) {
-            const uint32_t klo = j ? bnd[b][j - 1] : 0u, khi = j + 1 < nitem ? bnd[b][j] : T;
-            items[pos0 + pre - nitem + j] = make_item(lo, ti, b, klo, khi);
-        }
-        pos0 += __shfl_sync(kFull, pre, 31);
-    }
-    if (lane == 0 && prod_seen) {
-        if (atomicExch(&prod_seen[lo], iter + 1) != iter + 1) {
-            atomicAdd(&st->products, 1ULL);
-            atomicAdd(&st->dense_bitops, (unsigned long long)pd.n * pd.n * pd.n);
-        }
-    }
+    plan::plan_row(gw, prods, nprods, slots, st->iter, st, st->item_count, items_all, list_cap, tpb, prod_seen,
+                   tc_mode, areas[threadIdx.x >> 5].cnt, areas[threadIdx.x >> 5].bnd);
 }
 
-// ---- closure iteration: advance -------------------------------------------------
+// ---- closure iteration: advance + end ----------------------------------------
 // Clears the delta buffer that was read in this iteration (it receives the next
 // iteration's new bits): zero every occupied tile and its population, then the
-// occupancy row.  One warp per (slot, tile-row).
-__global__ void k_advance(const MatSlot *__restrict__ slots, uint32_t nslots, uint32_t total_rows, IterState *st) {
-    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t lane = threadIdx.x & 31;
-    if (gw >= total_rows) return;
-    uint32_t lo = 0, hi = nslots;
-    while (hi - lo > 1) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (slots[mid].row_start <= gw) lo = mid; else hi = mid;
-    }
-    const uint32_t ti = gw - slots[lo].row_start;
-    const DevMat D = slots[lo].dlt[st->iter & 1];
-    uint32_t *orow = D.occ + (size_t)ti * D.ow;
-    for (uint32_t w = 0; w < D.ow; ++w) {
-        uint32_t bits = orow[w];
-        while (bits) {
-            const uint32_t tj = w * 32 + (__ffs(bits) - 1);
-            bits &= bits - 1;
-            uint4 *tile = reinterpret_cast<uint4 *>(D.bits + tile_offset(D.T, ti, tj));
-            tile[lane] = make_uint4(0, 0, 0, 0);
-            if (lane == 0) D.nnz[(size_t)ti * D.T + tj] = 0;
-        }
-    }
-    __syncwarp();
-    for (uint32_t w = lane; w < D.ow; w += 32) orow[w] = 0;
-}
-
-__global__ void k_mark_start(IterState *st) { st->t_start_ns = globaltimer_ns(); }
-
-// End of one iteration: publish the changed flag, advance the iteration index,
-// decide whether to continue, and record per-query convergence.  A call after
-// the loop has stopped is a no-op (the host may run a few iterations
+// occupancy row.  One warp per (slot, tile-row).  The last block to finish
+// (counter in IterState) then ends the iteration: publishes the changed flag,
+// advances the iteration index, decides whether to continue (the graph's
+// while-node condition) and records per-query convergence.  A launch after the
+// loop has stopped only clears (the host may run a few iterations
 // speculatively between checks).
-__global__ void k_iter_end(IterState *st, QueryTrack qt, cudaGraphConditionalHandle handle, int use_handle) {
-    __shared__ uint32_t s_run, s_iter, s_go;
+__global__ void k_advance_end(const MatSlot *__restrict__ slots, uint32_t nslots, uint32_t total_rows,
+                              IterState *st, QueryTrack qt, cudaGraphConditionalHandle handle, int use_handle) {
+    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (gw < total_rows && nslots > 0) clear_delta_row(slots, nslots, gw, st->iter & 1);
+
+    __shared__ uint32_t s_last, s_run, s_iter, s_go;
+    __syncthreads();
     if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(&st->blocks_done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    if (threadIdx.x == 0) {
+        st->blocks_done = 0;
         s_run = st->active;
         s_go = 0;
         if (s_run) {
@@ -488,6 +339,20 @@ __global__ void k_iter_end(IterState *st, QueryTrack qt, cudaGraphConditionalHan
         }
     }
     if (threadIdx.x == 0 && use_handle) cudaGraphSetConditional(handle, s_go ? 1u : 0u);
+}
+
+__global__ void k_mark_start(IterState *st) { st->t_start_ns = globaltimer_ns(); }
+
+// Clear a list of matrices: one warp per (matrix, tile-row), occupied tiles only.
+__global__ void k_clear_rows(const MatRows *__restrict__ tab, uint32_t nmats, uint32_t total_rows) {
+    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (gw >= total_rows) return;
+    uint32_t lo = 0, hi = nmats;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (tab[mid].row_start <= gw) lo = mid; else hi = mid;
+    }
+    clear_tile_row(tab[lo].m, gw - tab[lo].row_start);
 }
 
 }  // namespace
@@ -596,21 +461,22 @@ cudaError_t launch_plan(const ProdDesc *d_prods, uint32_t nprods, uint32_t row_b
     return cudaGetLastError();
 }
 
-cudaError_t launch_advance(const MatSlot *d_slots, uint32_t nslots, uint32_t total_rows, IterState *d_st,
-                           cudaStream_t s) {
-    if (total_rows == 0 || nslots == 0) return cudaSuccess;
-    k_advance<<<grid_for((size_t)total_rows * 32, 256), 256, 0, s>>>(d_slots, nslots, total_rows, d_st);
+cudaError_t launch_advance_end(const MatSlot *d_slots, uint32_t nslots, uint32_t total_rows, IterState *d_st,
+                               const QueryTrack &qt, cudaGraphConditionalHandle handle, int use_handle,
+                               cudaStream_t s) {
+    k_advance_end<<<grid_for((size_t)total_rows * 32, 256), 256, 0, s>>>(d_slots, nslots, total_rows, d_st, qt,
+                                                                         handle, use_handle);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_clear_rows(const MatRows *d_tab, uint32_t nmats, uint32_t total_rows, cudaStream_t s) {
+    if (total_rows == 0 || nmats == 0) return cudaSuccess;
+    k_clear_rows<<<grid_for((size_t)total_rows * 32, 256), 256, 0, s>>>(d_tab, nmats, total_rows);
     return cudaGetLastError();
 }
 
 cudaError_t launch_mark_start(IterState *d_st, cudaStream_t s) {
     k_mark_start<<<1, 1, 0, s>>>(d_st);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_iter_end(IterState *d_st, const QueryTrack &qt, cudaGraphConditionalHandle handle, int use_handle,
-                            cudaStream_t s) {
-    k_iter_end<<<1, 256, 0, s>>>(d_st, qt, handle, use_handle);
     return cudaGetLastError();
 }
 

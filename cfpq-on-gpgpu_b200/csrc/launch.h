@@ -20,6 +20,8 @@ cudaError_t launch_rows_to_tiles(const DevMat &m, const uint64_t *d_rows, cudaSt
 cudaError_t launch_tiles_to_rows(const DevMat &m, uint64_t *d_rows, cudaStream_t s);
 cudaError_t launch_copy_matrix(const DevMat &dst, const DevMat &src, cudaStream_t s);
 cudaError_t launch_clear_matrix(const DevMat &m, cudaStream_t s);
+// Clear the matrices of d_tab (occupied tiles only; relies on the occupancy invariant).
+cudaError_t launch_clear_rows(const MatRows *d_tab, uint32_t nmats, uint32_t total_rows, cudaStream_t s);
 
 // Result hash / count (cfpq-cpp/Grammar.cpp:81-100 on the device)
 cudaError_t launch_hash_count(const DevMat &m, const uint32_t *d_pow11, const uint32_t *d_pow13,
@@ -60,13 +62,23 @@ int product_lop3_max_tiles();
 // Called once per context before any capture: sets kernel attributes, returns
 // resident CTAs per SM of the given inner loop.
 int product_tiled_blocks_per_sm(int m4r);
-cudaError_t launch_advance(const MatSlot *d_slots, uint32_t nslots, uint32_t total_rows, IterState *d_st,
-                           cudaStream_t s);
+// Clears the deltas read in this iteration, then (last block) ends the
+// iteration: changed flag, iteration index, loop condition, per-query records.
+cudaError_t launch_advance_end(const MatSlot *d_slots, uint32_t nslots, uint32_t total_rows, IterState *d_st,
+                               const QueryTrack &qt, cudaGraphConditionalHandle handle, int use_handle,
+                               cudaStream_t s);
 cudaError_t launch_mark_start(IterState *d_st, cudaStream_t s);
+// Persistent closure (word-level variants only): the whole fixpoint in one
+// cooperative launch of `grid` CTAs (at most persistent_blocks_per_sm() per
+// SM); items: 4 lists of list_cap; phase_log: 3 timestamps per iteration.
+int persistent_blocks_per_sm(int has_m4r);
+cudaError_t launch_closure_persistent(int has_m4r, int grid, const ProdDesc *prods, uint32_t nprods,
+                                      uint32_t prod_rows, const MatSlot *slots, uint32_t nslots, uint32_t slot_rows,
+                                      IterState *st, uint64_t *items, size_t list_cap, uint32_t *prod_seen,
+                                      const QueryTrack &qt, int tpb, unsigned long long *phase_log,
+                                      uint32_t phase_log_iters, cudaStream_t s);
 // Calibration: logic instructions per second of the whole GPU (d_out: 8*256*num_sms words).
 cudaError_t measure_logic_rate(int num_sms, uint32_t *d_out, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1,
                                double *ops_per_s, double *ms_out);
-cudaError_t launch_iter_end(IterState *d_st, const QueryTrack &qt, cudaGraphConditionalHandle handle, int use_handle,
-                            cudaStream_t s);
 
 }  // namespace cfpq

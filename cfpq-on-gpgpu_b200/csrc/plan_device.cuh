@@ -1,0 +1,173 @@
+// Closure plan: per (product, tile-row) the work items of one iteration.
+// Used by the plan kernel (kernels_core.cu) and the persistent closure kernel
+// (kernel_persistent.cu).
+#pragma once
+
+#include "common.cuh"
+
+namespace cfpq {
+namespace plan {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+// One warp per (product, output tile-row ti) (a group of 4 tile-rows for
+// tensor-core products).  For every block of `tpb` output tiles the warp counts
+// the contributing k-tiles tk (occupied P tile (ti, tk) and a non-empty Q
+// block (tk, block)) in increasing tk order and cuts them into chunks of E
+// (item_entries of the row's occupied P tile count, so at most
+// kMaxChunksPerBlock chunks; tensor-core items take one chunk).  Chunk j of a
+// block becomes the item with k-tile range [first tk of chunk j, first tk of
+// chunk j+1), the first range starting at 0 and the last ending at T: the
+// ranges partition [0, T).  Skipping is exact: a tile pair contributes only if
+// both tiles are occupied.
+// The k-tiles of one P occupancy word go to the lanes (lane l takes the l-th
+// set bit), so the Q occupancy loads of a word are issued together; per-block
+// counts and chunk boundaries live in shared memory (one region per warp).
+__device__ __forceinline__ DevMat resolve_operand(const MatSlot &s, uint8_t use_delta, uint32_t iter) {
+    if (!use_delta || iter == 0) return s.cur;
+    return s.dlt[iter & 1];
+}
+
+// Position of the n-th (0-based) set bit of x (x has more than n set bits).
+__device__ __forceinline__ uint32_t nth_set_bit(uint32_t x, uint32_t n) {
+    uint32_t pos = 0;
+#pragma unroll
+    for (uint32_t s = 16; s > 0; s >>= 1) {
+        const uint32_t c = __popc(x & ((1u << s) - 1));
+        if (n >= c) {
+            n -= c;
+            x >>= s;
+            pos += s;
+        }
+    }
+    return pos;
+}
+
+constexpr uint32_t kPlanMaxBlocks = 512;  // T <= 2048 tiles, blocks of >= 4 tiles
+
+// Per-warp shared memory of the planner for up to kBlocks output blocks per
+// tile-row (512: any product; 128: word-level products, blocks of 16 tiles).
+template <uint32_t kBlocks>
+struct WarpArea {
+    uint32_t cnt[kBlocks];
+    uint16_t bnd[kBlocks][kMaxChunksPerBlock - 1];
+};
+
+// Plan product row gw (one warp): items go to list 0 (LOP3 inner loop), 1
+// (Four Russians) or 2 (tensor cores) by the product's variant, list l at
+// items_all + l * list_cap, counted in item_count[l]; st receives the
+// product statistics.  tc_mode 0 plans word-level products, 1 tensor-core ones.
+__device__ __forceinline__ void plan_row(uint32_t gw, const ProdDesc *__restrict__ prods, uint32_t nprods,
+                                         const MatSlot *__restrict__ slots, uint32_t iter, IterState *st,
+                                         uint32_t *item_count, uint64_t *__restrict__ items_all, size_t list_cap,
+                                         int tpb, uint32_t *prod_seen, int tc_mode, uint32_t *cnt,
+                                         uint16_t (*bnd)[kMaxChunksPerBlock - 1]) {
+    const uint32_t lane = threadIdx.x & 31;
+    uint32_t lo = 0, hi = nprods;  // product: last p with row_start <= gw
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (prods[mid].row_start <= gw) lo = mid; else hi = mid;
+    }
+    const ProdDesc pd = prods[lo];
+    if (pd.term == 1 && iter == 0) return;  // first iteration: delta(A) = A, one term covers A*B
+    const bool tc = pd.variant == 4;                         // CFPQ_VARIANT_TC
+    if (tc != (tc_mode != 0)) return;  // word-level and tensor-core products are planned by separate launches
+    const uint32_t list = tc ? 2u : (pd.variant == 3 ? 1u : 0u);  // CFPQ_VARIANT_M4R
+    if (tc) tpb = 4;
+    const uint32_t rows_per_item = tc ? 4u : 1u;
+    uint64_t *items = items_all + list * list_cap;
+    const uint32_t ti = gw - pd.row_start;  // tile-row, or group of 4 tile-rows for tc
+    const DevMat P = resolve_operand(slots[pd.pslot], pd.p_delta, iter);
+    const DevMat Q = resolve_operand(slots[pd.qslot], pd.q_delta, iter);
+    const uint32_t T = pd.T, ow = P.ow;
+    const uint32_t bpw = 32 / tpb;  // blocks per occupancy word
+    const uint32_t bmask = tpb == 32 ? 0xffffffffu : ((1u << tpb) - 1);
+    const uint32_t nblocks = (T + tpb - 1) / tpb;
+    auto prow_word = [&](uint32_t w) {
+        uint32_t bits = 0;
+        for (uint32_t g = 0; g < rows_per_item && ti * rows_per_item + g < T; ++g)
+            bits |= P.occ[(size_t)(ti * rows_per_item + g) * ow + w];
+        return bits;
+    };
+    // occupied P tiles of the row (group); the first 32 occupancy words stay
+    // in registers (one per lane) for the main loop
+    const uint32_t first = lane < ow ? prow_word(lane) : 0u;
+    uint32_t np = __reduce_add_sync(kFull, (uint32_t)__popc(first));
+    for (uint32_t base = 32; base < ow; base += 32)
+        np += __reduce_add_sync(kFull, base + lane < ow ? (uint32_t)__popc(prow_word(base + lane)) : 0u);
+    if (!np) return;
+    const uint32_t E = tc ? T : item_entries(np);
+    for (uint32_t b = lane; b < nblocks; b += 32) cnt[b] = 0;
+    __syncwarp();
+    uint32_t mine = first;
+
+    for (uint32_t pw = 0; pw < ow; ++pw) {
+        // P occupancy words come 32 at a time, one per lane
+        if (pw > 0 && (pw & 31) == 0) mine = pw + lane < ow ? prow_word(pw + lane) : 0u;
+        const uint32_t bits = __shfl_sync(kFull, mine, pw & 31);  // warp-uniform
+        if (!bits) continue;
+        const bool valid = lane < (uint32_t)__popc(bits);
+        const uint32_t tk = valid ? pw * 32 + nth_set_bit(bits, lane) : 0u;  // increasing with the lane
+        const uint32_t *qrow = Q.occ + (size_t)tk * ow;
+        for (uint32_t w0 = 0; w0 < ow; w0 += 4) {
+            uint32_t m[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) m[u] = (valid && w0 + u < ow) ? qrow[w0 + u] : 0u;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if (w0 + u >= ow) break;
+                if (!__ballot_sync(kFull, m[u] != 0)) continue;
+                for (uint32_t h = 0; h < bpw; ++h) {
+                    const unsigned bal = __ballot_sync(kFull, ((m[u] >> (h * tpb)) & bmask) != 0);
+                    if (!bal) continue;
+                    const uint32_t b = (w0 + u) * bpw + h, c = __popc(bal), cb = cnt[b];
+                    // chunk boundaries: ranks j*E (j >= 1) among this ballot's ranks cb .. cb+c-1
+                    for (uint32_t j = (cb + E - 1) / E; j < kMaxChunksPerBlock && j * E < cb + c; ++j) {
+                        if (j == 0) continue;
+                        const uint32_t src = nth_set_bit(bal, j * E - cb);
+                        const uint32_t tkj = __shfl_sync(kFull, tk, src);
+                        if (lane == 0) bnd[b][j - 1] = (uint16_t)tkj;
+                    }
+                    __syncwarp();
+                    if (lane == 0) cnt[b] = cb + c;
+                    __syncwarp();
+                }
+            }
+        }
+    }
+
+    auto nchunks = [&](uint32_t c) { return c ? (c + E - 1) / E : 0u; };
+    uint32_t total = 0;
+    for (uint32_t base = 0; base < nblocks; base += 32) {
+        const uint32_t b = base + lane;
+        total += __reduce_add_sync(kFull, b < nblocks ? nchunks(cnt[b]) : 0u);
+    }
+    if (!total) return;
+    uint32_t pos0 = 0;
+    if (lane == 0) pos0 = atomicAdd(&item_count[list], total);
+    pos0 = __shfl_sync(kFull, pos0, 0);
+    for (uint32_t base = 0; base < nblocks; base += 32) {
+        const uint32_t b = base + lane;
+        const uint32_t nitem = b < nblocks ? nchunks(cnt[b]) : 0u;
+        uint32_t pre = nitem;  // inclusive scan over lanes
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(kFull, pre, o);
+            if (lane >= (uint32_t)o) pre += v;
+        }
+        for (uint32_t j = 0; j < nitem; ++j) {
+            const uint32_t klo = j ? bnd[b][j - 1] : 0u, khi = j + 1 < nitem ? bnd[b][j] : T;
+            items[pos0 + pre - nitem + j] = make_item(lo, ti, b, klo, khi);
+        }
+        pos0 += __shfl_sync(kFull, pre, 31);
+    }
+    if (lane == 0 && prod_seen) {
+        if (atomicExch(&prod_seen[lo], iter + 1) != iter + 1) {
+            atomicAdd(&st->products, 1ULL);
+            atomicAdd(&st->dense_bitops, (unsigned long long)pd.n * pd.n * pd.n);
+        }
+    }
+}
+
+}  // namespace plan
+}  // namespace cfpq

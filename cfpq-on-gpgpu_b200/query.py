@@ -153,8 +153,7 @@ class PreparedQuery:
 
     def load(self) -> None:
         """Clear and initialise from the edge list (one H2D copy, one scatter)."""
-        for m in self.mats:
-            m.clear()
+        self.ctx.clear_many(self.mats)
         if self.graph.nedges and self.mats:
             self.ctx.load_edges(self.mats, self.graph.src, self.graph.label, self.graph.dst, self.off, self.lm)
         for e in self.grammar.epsilon:

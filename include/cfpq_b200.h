@@ -72,12 +72,21 @@ typedef struct cfpq_rule {
     uint32_t body2;
 } cfpq_rule;
 
+#define CFPQ_LOOP_HOST 0
+#define CFPQ_LOOP_DEVICE 1
+#define CFPQ_LOOP_GRAPH 2
+
 typedef struct cfpq_closure_opts {
     int32_t driver;          /* cfpq_driver */
     int32_t variant;         /* cfpq_variant used for every product, or AUTO */
     int32_t max_iterations;  /* 0 = until the fixpoint */
-    int32_t use_graph;       /* 1 = run the iteration loop as one CUDA graph with a
-                                device-side while condition (ENGINE driver only) */
+    int32_t use_graph;       /* ENGINE driver, how the iterations are sequenced:
+                                0 (CFPQ_LOOP_HOST)   kernels launched from a host loop
+                                1 (CFPQ_LOOP_DEVICE) no host round trip: one persistent
+                                   cooperative kernel for the whole fixpoint when every
+                                   product is word-level, else the CUDA-graph loop
+                                2 (CFPQ_LOOP_GRAPH)  one CUDA graph with a device-side
+                                   while condition, one node per kernel */
     int32_t log_products;    /* 1 = record a per-product timing log (see cfpq_product_log) */
     int32_t reserved[3];
 } cfpq_closure_opts;
@@ -111,7 +120,8 @@ int cfpq_calibrate(cfpq_ctx *ctx, cfpq_calibration *out);
 /* Per-kernel device times of the last closure run with
  * opts->log_products & CFPQ_LOG_KERNELS (every launch bracketed by CUDA events
  * on the context's stream; the iteration loop then runs from the host instead
- * of a CUDA graph). */
+ * of a CUDA graph).  The delta clear and the iteration end are one kernel
+ * (advance_*); iter_end_* stay zero. */
 #define CFPQ_LOG_KERNELS 1
 #define CFPQ_LOG_PRODUCTS 2
 typedef struct cfpq_kernel_profile {
@@ -205,6 +215,10 @@ int cfpq_load_edges_device(cfpq_ctx *ctx, cfpq_matrix *const *mats, size_t nmats
 int cfpq_matrix_set_diagonal(cfpq_ctx *ctx, cfpq_matrix *m);
 /* Clears all bits. */
 int cfpq_matrix_clear(cfpq_ctx *ctx, cfpq_matrix *m);
+/* Clear `count` matrices with one kernel that zeroes only their occupied
+ * tiles (the occupancy invariant holds at every API boundary), so the cost
+ * follows the number of set tiles, not n^2. */
+int cfpq_matrices_clear(cfpq_ctx *ctx, cfpq_matrix *const *mats, size_t count);
 /* Copies all bits of src into dst (same n). */
 int cfpq_matrix_copy(cfpq_ctx *ctx, cfpq_matrix *dst, const cfpq_matrix *src);
 
@@ -307,6 +321,14 @@ typedef struct cfpq_product_record {
     float reserved;
 } cfpq_product_record;
 size_t cfpq_product_log(cfpq_ctx *ctx, cfpq_product_record *out, size_t cap);
+
+/* Phase timestamps of the last closure that ran as one persistent kernel
+ * (use_graph = CFPQ_LOOP_DEVICE, every product word-level): per iteration
+ * three %globaltimer values in ns -- iteration start, end of the plan phase,
+ * end of the product phase (both after the grid barrier).  Copies
+ * min(cap, 3 * iterations) values and returns the number of iterations logged
+ * (at most 4096; 0 when the last closure did not run persistently). */
+size_t cfpq_last_phase_log(cfpq_ctx *ctx, uint64_t *out, size_t cap);
 
 #ifdef __cplusplus
 }

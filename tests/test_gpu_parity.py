@@ -221,6 +221,38 @@ def test_closure_random_cnf(ctx, pkg, oracle, tmp_path, seed, variant):
     _check_query(ctx, pkg, oracle, wl, tmp_path, variant=variant)
 
 
+@pytest.mark.parametrize("loop", ["device", "graph", "host"])
+@pytest.mark.parametrize("variant", ["lop3", "m4r"])
+def test_closure_loop_modes(ctx, pkg, oracle, tmp_path, loop, variant):
+    """The persistent kernel (device), the CUDA-graph loop and the host loop
+    sequence the same plan / product code and agree with the oracle."""
+    labels = ["x", "y", "z"]
+    g = pkg.workloads.uniform_graph(900, 2000, labels, 11)
+    gram = pkg.workloads.random_cnf(8, 20, labels, 11)
+    wl = pkg.workloads.Workload("random_cnf", gram, g, {})
+    res = _check_query(ctx, pkg, oracle, wl, tmp_path, variant=variant, use_graph=loop)
+    assert res.stats["iterations"] > 1
+    if loop == "device":
+        assert res.stats["kernel_launches"] == 2  # mark + one persistent launch
+
+
+def test_closure_iteration_limit_then_full(ctx, pkg, oracle, tmp_path):
+    """A closure cut off by max_iterations leaves the context usable: the
+    next full closure of the same query is exact."""
+    wl = pkg.workloads.ontology_query(2048, 7)
+    gp, rp = _write(wl, tmp_path)
+    exp_lines, _, _ = _oracle_run(oracle, gp, rp)
+    q = pkg.query.PreparedQuery(ctx, wl.grammar, wl.graph)
+    try:
+        for loop in ("device", "graph", "host"):
+            q.load()
+            st = ctx.closure(wl.grammar.rules, q.mats, use_graph=loop, max_iterations=2)
+            assert st["iterations"] == 2
+            assert q.run(use_graph=loop).lines == exp_lines
+    finally:
+        q.close()
+
+
 def test_closure_epsilon_and_self_loops(ctx, pkg, oracle, tmp_path):
     gram = "S\nS S S\nS A S\nA a\nB S B\nB b\n"
     g = pkg.workloads.uniform_graph(150, 200, ["a", "b"], 9)
@@ -240,6 +272,62 @@ def test_closure_repeated_runs_are_identical(ctx, pkg, oracle, tmp_path):
         q.close()
 
 
+def test_plan_reuse_across_interleaved_work(ctx, pkg, oracle, tmp_path):
+    """Closures of two prepared queries, interleaved with a product that
+    reuses the context's tables, stay exact (the cached plan of the last
+    closure is only reused for the same rules and matrices)."""
+    wl1 = pkg.workloads.ontology_query(1024, 5)
+    labels = ["x", "y", "z"]
+    wl2 = pkg.workloads.Workload("random_cnf", pkg.workloads.random_cnf(8, 20, labels, 4),
+                                 pkg.workloads.uniform_graph(700, 1400, labels, 4), {})
+    exps = []
+    for i, wl in enumerate((wl1, wl2)):
+        d = tmp_path / f"q{i}"
+        d.mkdir()
+        exps.append(_oracle_run(oracle, *_write(wl, d))[0])
+    q1 = pkg.query.PreparedQuery(ctx, wl1.grammar, wl1.graph)
+    q2 = pkg.query.PreparedQuery(ctx, wl2.grammar, wl2.graph)
+    a, b, c = ctx.matrix(300), ctx.matrix(300), ctx.matrix(300)
+    try:
+        for loop in ("device", "graph", "device"):
+            assert q1.run(use_graph=loop).lines == exps[0]
+            assert q1.run(use_graph=loop).lines == exps[0]
+            assert q2.run(use_graph=loop).lines == exps[1]
+            a.set_diagonal()
+            b.set_diagonal()
+            ctx.add_mul(c, a, b, "lop3")
+            assert q2.run(use_graph=loop).lines == exps[1]
+            assert q1.run(use_graph=loop).lines == exps[0]
+    finally:
+        q1.close()
+        q2.close()
+        for m in (a, b, c):
+            m.destroy()
+
+
+def test_clear_many(ctx, pkg):
+    rng = np.random.default_rng(3)
+    mats = [ctx.matrix(n) for n in (1, 64, 200, 1000)]
+    order = ctx.order(rng.permutation(333).astype(np.uint32))
+    mats.append(ctx.matrix(333, order))
+    try:
+        for m in mats:
+            n = m.n
+            k = max(1, n * 3)
+            m.set_bits(rng.integers(0, n, k).astype(np.uint32), rng.integers(0, n, k).astype(np.uint32))
+            assert m.hash_count()[1] > 0
+        ctx.clear_many(mats)
+        for m in mats:
+            assert m.hash_count() == (0, 0)
+            assert not m.download_rows().any()
+            occ, nnz = m.tile_stats()
+            assert not occ.any() and not nnz.any()
+    finally:
+        for m in mats:
+            m.destroy()
+        order.destroy()
+
+
 def test_batch_matches_single_queries(ctx, pkg, oracle, tmp_path):
     wls = [w for w in pkg.workloads.batch_queries(24, seed=5, n_min=64, n_max=900)]
     qs, exps = [], []
@@ -251,13 +339,16 @@ def test_batch_matches_single_queries(ctx, pkg, oracle, tmp_path):
         q = pkg.query.PreparedQuery(ctx, wl.grammar, wl.graph)
         q.load()
         qs.append(q)
-    stats, iters, done = ctx.closure_batch([(q.grammar.rules, q.mats) for q in qs])
     try:
-        for q, exp in zip(qs, exps):
-            got = dict(zip(q.grammar.nonterminals, ctx.hash_count_many(q.mats)))
-            assert got == exp
-        assert stats["iterations"] >= int(iters.max())
-        assert (done >= 0).all()
+        for loop in ("device", "graph"):
+            for q in qs:
+                q.load()
+            stats, iters, done = ctx.closure_batch([(q.grammar.rules, q.mats) for q in qs], use_graph=loop)
+            for q, exp in zip(qs, exps):
+                got = dict(zip(q.grammar.nonterminals, ctx.hash_count_many(q.mats)))
+                assert got == exp
+            assert stats["iterations"] >= int(iters.max())
+            assert (done >= 0).all()
     finally:
         for q in qs:
             q.close()
