@@ -132,8 +132,9 @@ def measured_peaks() -> dict:
 
 
 def committed_traffic() -> dict:
-    """ncu DRAM traffic per launch of the product kernel, scaled to the bench
-    workload (profiles/traffic.json, written from an ncu capture)."""
+    """ncu DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) per
+    launch of the dominant kernels on the bench workload (profiles/traffic.json,
+    copied from an ncu capture)."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(p):
         with open(p) as f:
@@ -276,6 +277,7 @@ def ours_arm(args, world, rank, local):
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > 126 MB L2
 
     launches = {"n": 0}
+    device_ms: list[float] = []
 
     def step_value():
         ctx.clear_many(q.mats)
@@ -284,7 +286,8 @@ def ours_arm(args, world, rank, local):
         for e in grammar.epsilon:
             q.mats[e].set_diagonal()
         st = ctx.closure(grammar.rules, q.mats, use_graph=not args.no_graph)
-        launches["n"] += 1 + len(grammar.epsilon) + st["kernel_launches"]
+        launches["n"] += 2 + len(grammar.epsilon) + st["kernel_launches"]  # clear + edge scatter + closure
+        device_ms.append(st["device_ms"])
         return st
 
     def step_e2e():
@@ -328,6 +331,7 @@ def ours_arm(args, world, rank, local):
     sampler = ClockSampler(local)
     sampler.start()
     launches["n"] = 0
+    device_ms.clear()
     times, st = timed(step_value, args.steps)
     clocks = sampler.stop()
     barrier()
@@ -348,25 +352,30 @@ def ours_arm(args, world, rank, local):
     d2h = 16 * len(q.mats)
 
     # per-kernel device times (instrumented pass: every launch bracketed by events)
-    roofline, prof = None, None
+    # roofline of the dominant kernel: the persistent closure kernel (one
+    # launch per step; its duration is the library's event pair around it)
+    peaks = measured_peaks()
+    dev_ms = statistics.mean(device_ms) if device_ms else 0.0
+    alg_bytes = st["bytes_staged"] + 16 * st["out_words"] + 8 * st["new_words"]
+    achieved = alg_bytes / (dev_ms / 1e3) / 1e9 if dev_ms > 0 else 0.0
+    tr = committed_traffic().get("k_closure_persistent", {}).get("dram_bytes_per_launch")
+    roofline = {"kernel": "k_closure_persistent" if len(phases) else "closure iteration kernels", "bound": "hbm",
+                "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"], "traffic": tr, "peak_source": peaks["source"],
+                "avg_launch_ms": dev_ms, "algorithmic_bytes_per_launch": alg_bytes,
+                "algorithmic_bytes": "operand tiles staged global->shared + 16 B per merged output word "
+                                     "(read + atomic) + 8 B per delta word written",
+                "note": "latency-bound: a few hundred short work items per iteration; see phase_us_per_iteration "
+                        "and the dense_product_kernels rooflines"}
     if not args.no_profile:
+        # per-kernel times of the multi-kernel iteration (host loop, every launch bracketed by events)
         ctx.clear_many(q.mats)
         ctx.load_edges_device(q.mats, d_src.data_ptr(), d_lab.data_ptr(), d_dst.data_ptr(), graph.nedges,
                               q.off, q.lm)
-        pst = ctx.closure(grammar.rules, q.mats, use_graph=False, log_products=capi.LOG_KERNELS)
+        ctx.closure(grammar.rules, q.mats, use_graph=False, log_products=capi.LOG_KERNELS)
         prof = ctx.kernel_profile()
-        peaks = measured_peaks()
-        kern = {"product": prof["product_ms"], "plan": prof["plan_ms"], "advance_end": prof["advance_ms"]}
-        launches_p = max(1, prof["product_launches"])
-        avg_ms = prof["product_ms"] / launches_p
-        alg_bytes = (pst["bytes_staged"] + 16 * pst["out_words"] + 8 * pst["new_words"]) / launches_p
-        achieved = alg_bytes / (avg_ms / 1e3) / 1e9 if avg_ms > 0 else 0.0
-        tr = committed_traffic().get("product_bytes_per_launch")
-        roofline = {"kernel": "k_product_lop3", "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
-                    "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": tr,
-                    "peak_source": peaks["source"], "avg_launch_ms": avg_ms,
-                    "algorithmic_bytes_per_launch": alg_bytes,
-                    "kernel_ms": kern, "dominant": max(kern, key=kern.get)}
+        roofline["multi_kernel_path_ms"] = {"plan": prof["plan_ms"], "product": prof["product_ms"],
+                                            "advance_end": prof["advance_ms"]}
 
     out = None
     if rank == 0:
@@ -380,7 +389,9 @@ def ours_arm(args, world, rank, local):
                        "nonterminals": len(grammar.nonterminals), "rules": len(grammar.rules),
                        "seed": args.seed, "l2": "flushed between steps (256 MiB write)",
                        "parallelism": f"query-partitioned x{world}",
-                       "launch": "host loop" if args.no_graph else "CUDA graph (conditional while node)"},
+                       "launch": "host loop" if args.no_graph else
+                       ("one persistent cooperative kernel per closure" if len(phases) else
+                        "CUDA graph (conditional while node)")},
             "clocks": clocks,
             "e2e": {"value": e2e_value, "unit": "closures/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
