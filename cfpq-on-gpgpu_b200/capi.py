@@ -33,7 +33,9 @@ EXPORTED = (
     "cfpq_product_log", "cfpq_last_kernel_profile", "cfpq_ctx_stream", "cfpq_load_edges_device",
     "cfpq_matrix_tile_stats", "cfpq_order_create", "cfpq_order_destroy", "cfpq_order_suggest",
     "cfpq_matrix_create_ordered", "cfpq_hash_count_rows_noalloc", "cfpq_noalloc_last_error", "cfpq_calibrate",
-    "cfpq_last_phase_log", "cfpq_matrices_clear",
+    "cfpq_last_phase_log", "cfpq_matrices_clear", "cfpq_selector_configure", "cfpq_selector_get_config",
+    "cfpq_selector_weight_count", "cfpq_selector_set_weights", "cfpq_selector_get_weights", "cfpq_selector_train",
+    "cfpq_selector_loss_grad", "cfpq_selector_predict", "cfpq_autotune",
 )
 
 
@@ -88,11 +90,53 @@ class Query(ctypes.Structure):
                 ("mats", ctypes.POINTER(ctypes.c_void_p)), ("nmats", ctypes.c_size_t)]
 
 
+SEL_FEATURES, SEL_OUTPUTS = 16, 3
+SELECT_FIXED, SELECT_HEURISTIC, SELECT_MLP = 0, 1, 2
+LOG_SELECTION = 4
+
+
 class ProductRecord(ctypes.Structure):
     _fields_ = [("iteration", ctypes.c_uint32), ("query", ctypes.c_uint32), ("rule", ctypes.c_uint32),
                 ("term", ctypes.c_uint32), ("n", ctypes.c_uint32), ("variant", ctypes.c_uint32),
-                ("p_tiles", ctypes.c_uint64), ("q_tiles", ctypes.c_uint64), ("c_tiles", ctypes.c_uint64),
-                ("tile_triples", ctypes.c_uint64), ("usec", ctypes.c_float), ("reserved", ctypes.c_float)]
+                ("flags", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
+                ("features", ctypes.c_float * SEL_FEATURES), ("predicted", ctypes.c_float * SEL_OUTPUTS),
+                ("usec", ctypes.c_float * 5)]
+
+
+# numpy view of an array of cfpq_product_record
+PRODUCT_RECORD_DTYPE = np.dtype([("iteration", np.uint32), ("query", np.uint32), ("rule", np.uint32),
+                                 ("term", np.uint32), ("n", np.uint32), ("variant", np.uint32),
+                                 ("flags", np.uint32), ("reserved", np.uint32),
+                                 ("features", np.float32, (SEL_FEATURES,)), ("predicted", np.float32, (SEL_OUTPUTS,)),
+                                 ("usec", np.float32, (5,))])
+
+
+class SelectorConfig(ctypes.Structure):
+    _fields_ = [("mode", ctypes.c_int32), ("allowed", ctypes.c_uint32), ("tc_min_tiles", ctypes.c_uint32),
+                ("tc_min_occ", ctypes.c_float), ("tc_min_pop", ctypes.c_float), ("m4r_min_dense", ctypes.c_float),
+                ("conf_margin", ctypes.c_float), ("range_margin", ctypes.c_float), ("min_tiles", ctypes.c_uint32)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class TrainOpts(ctypes.Structure):
+    _fields_ = [("epochs", ctypes.c_int32), ("learning_rate", ctypes.c_float), ("weight_decay", ctypes.c_float),
+                ("seed", ctypes.c_uint32), ("keep_weights", ctypes.c_int32)]
+
+
+class TrainReport(ctypes.Structure):
+    _fields_ = [("loss_first", ctypes.c_float), ("loss_last", ctypes.c_float), ("samples", ctypes.c_uint32),
+                ("epochs", ctypes.c_uint32), ("ms", ctypes.c_double)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class AutotuneOpts(ctypes.Structure):
+    _fields_ = [("sizes", ctypes.POINTER(ctypes.c_uint32)), ("nsizes", ctypes.c_size_t),
+                ("densities", ctypes.POINTER(ctypes.c_float)), ("ndensities", ctypes.c_size_t),
+                ("reps", ctypes.c_uint32), ("seed", ctypes.c_uint32)]
 
 
 _lib = None
@@ -146,6 +190,15 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "cfpq_load_edges_device": ([vp, P(vp), sz, vp, vp, vp, sz, vp, vp, u32], i32),
         "cfpq_last_phase_log": ([vp, P(u64), sz], sz),
         "cfpq_matrices_clear": ([vp, P(vp), sz], i32),
+        "cfpq_selector_configure": ([vp, P(SelectorConfig)], i32),
+        "cfpq_selector_get_config": ([vp, P(SelectorConfig)], i32),
+        "cfpq_selector_weight_count": ([], sz),
+        "cfpq_selector_set_weights": ([vp, vp, sz], i32),
+        "cfpq_selector_get_weights": ([vp, vp, sz], i32),
+        "cfpq_selector_train": ([vp, vp, sz, P(TrainOpts), P(TrainReport)], i32),
+        "cfpq_selector_loss_grad": ([vp, vp, vp, vp, vp, sz, P(ctypes.c_float), vp], i32),
+        "cfpq_selector_predict": ([vp, vp, sz, vp], i32),
+        "cfpq_autotune": ([vp, P(AutotuneOpts), P(SelectorConfig), vp], i32),
     }
     for name, (args, res) in sigs.items():
         f = getattr(lib, name)
@@ -320,7 +373,7 @@ class Context:
         return st.as_dict()
 
     def closure_batch(self, queries: Sequence[tuple[Sequence[tuple[int, int, int]], Sequence[Matrix]]],
-                      variant="auto", use_graph: bool = True, max_iterations: int = 0):
+                      variant="auto", use_graph: bool = True, max_iterations: int = 0, log_products: int = 0):
         keep = []
         qs = (Query * max(len(queries), 1))()
         for i, (rules, mats) in enumerate(queries):
@@ -331,7 +384,7 @@ class Context:
             qs[i].nrules = len(rules)
             qs[i].mats = ctypes.cast(hs, ctypes.POINTER(ctypes.c_void_p))
             qs[i].nmats = len(mats)
-        o = self._opts("engine", variant, use_graph, max_iterations, False)
+        o = self._opts("engine", variant, use_graph, max_iterations, log_products)
         st = ClosureStats()
         iters = np.zeros(max(len(queries), 1), dtype=np.uint32)
         done = np.zeros(max(len(queries), 1), dtype=np.float64)
@@ -386,6 +439,78 @@ class Context:
         self.lib.cfpq_last_phase_log(self.handle, buf.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), buf.size)
         t = buf.reshape(n, 3).astype(np.float64)
         return np.stack([t[:, 1] - t[:, 0], t[:, 2] - t[:, 1]], axis=1) / 1e3
+
+    # ---- variant selector -------------------------------------------------
+    def selector_config(self) -> dict:
+        c = SelectorConfig()
+        _check(self.lib, self.lib.cfpq_selector_get_config(self.handle, ctypes.byref(c)))
+        return c.as_dict()
+
+    def selector_configure(self, **kw) -> dict:
+        """Change selector settings (keys of cfpq_selector_config; mode may be
+        "fixed" / "heuristic" / "mlp", allowed a list of variant names)."""
+        cur = self.selector_config()
+        if isinstance(kw.get("mode"), str):
+            kw["mode"] = {"fixed": SELECT_FIXED, "heuristic": SELECT_HEURISTIC, "mlp": SELECT_MLP}[kw["mode"]]
+        if isinstance(kw.get("allowed"), (list, tuple)):
+            kw["allowed"] = sum(1 << VARIANTS[v] for v in kw["allowed"])
+        cur.update(kw)
+        c = SelectorConfig(**cur)
+        _check(self.lib, self.lib.cfpq_selector_configure(self.handle, ctypes.byref(c)))
+        return self.selector_config()
+
+    def selector_weights(self) -> np.ndarray:
+        w = np.zeros(self.lib.cfpq_selector_weight_count(), dtype=np.float32)
+        _check(self.lib, self.lib.cfpq_selector_get_weights(self.handle, _ptr(w), w.size))
+        return w
+
+    def selector_set_weights(self, w: np.ndarray) -> None:
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        _check(self.lib, self.lib.cfpq_selector_set_weights(self.handle, _ptr(w), w.size))
+
+    def selector_train(self, records: np.ndarray, epochs: int = 2000, learning_rate: float = 3e-3,
+                       weight_decay: float = 1e-4, seed: int = 1, keep_weights: bool = False) -> dict:
+        rec = np.ascontiguousarray(records, dtype=PRODUCT_RECORD_DTYPE)
+        o = TrainOpts(epochs, learning_rate, weight_decay, seed, int(keep_weights))
+        r = TrainReport()
+        _check(self.lib, self.lib.cfpq_selector_train(self.handle, _ptr(rec), rec.size, ctypes.byref(o),
+                                                      ctypes.byref(r)))
+        return r.as_dict()
+
+    def selector_loss_grad(self, weights: np.ndarray, x: np.ndarray, y: np.ndarray, m: np.ndarray):
+        w = np.ascontiguousarray(weights, dtype=np.float32)
+        x, y, m = (np.ascontiguousarray(a, dtype=np.float32) for a in (x, y, m))
+        loss = ctypes.c_float()
+        grad = np.zeros_like(w)
+        _check(self.lib, self.lib.cfpq_selector_loss_grad(self.handle, _ptr(w), _ptr(x), _ptr(y), _ptr(m),
+                                                          x.shape[0], ctypes.byref(loss), _ptr(grad)))
+        return float(loss.value), grad
+
+    def selector_predict(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        out = np.zeros((x.shape[0], SEL_OUTPUTS), dtype=np.float32)
+        _check(self.lib, self.lib.cfpq_selector_predict(self.handle, _ptr(x), x.shape[0], _ptr(out)))
+        return out
+
+    def autotune(self, sizes=(2048, 8192), densities=(0.002, 0.02, 0.1, 0.3, 0.6), reps: int = 3, seed: int = 1):
+        """Time LOP3 / M4R / TC on random matrices and set the selector's
+        thresholds.  Returns (config dict, timings [sizes][densities][3] ms)."""
+        sz = np.ascontiguousarray(sizes, dtype=np.uint32)
+        de = np.ascontiguousarray(densities, dtype=np.float32)
+        o = AutotuneOpts(sz.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), sz.size,
+                         de.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), de.size, reps, seed)
+        c = SelectorConfig()
+        t = np.zeros((sz.size, de.size, 3), dtype=np.float32)
+        _check(self.lib, self.lib.cfpq_autotune(self.handle, ctypes.byref(o), ctypes.byref(c), _ptr(t)))
+        return c.as_dict(), t
+
+    def product_log(self) -> np.ndarray:
+        """Records of the last closure run with LOG_PRODUCTS / LOG_SELECTION."""
+        n = self.lib.cfpq_product_log(self.handle, None, 0)
+        out = np.zeros(n, dtype=PRODUCT_RECORD_DTYPE)
+        if n:
+            self.lib.cfpq_product_log(self.handle, out.ctypes.data_as(ctypes.POINTER(ProductRecord)), n)
+        return out
 
     def kernel_profile(self) -> dict:
         p = KernelProfile()

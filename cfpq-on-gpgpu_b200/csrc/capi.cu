@@ -27,17 +27,16 @@
 #include <unordered_map>
 #include <vector>
 
-#include "cfpq_b200.h"
-#include "launch.h"
+#include "ctx.h"
 
-using namespace cfpq;
+static void free_plan_cache(cfpq_ctx *ctx);
 
 // ---------------------------------------------------------------------------
 // errors
 
 static thread_local std::string g_last_error;
 
-static int set_error(int code, const char *fmt, ...) {
+int set_error(int code, const char *fmt, ...) {
     char buf[512];
     va_list ap;
     va_start(ap, fmt);
@@ -47,121 +46,6 @@ static int set_error(int code, const char *fmt, ...) {
     return code;
 }
 
-#define CUDA_TRY(call)                                                                                \
-    do {                                                                                              \
-        cudaError_t e_ = (call);                                                                      \
-        if (e_ != cudaSuccess)                                                                        \
-            return set_error(e_ == cudaErrorMemoryAllocation ? CFPQ_ERR_OOM : CFPQ_ERR_CUDA,          \
-                             "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__);    \
-    } while (0)
-
-#define TRY(call)                   \
-    do {                            \
-        int r_ = (call);            \
-        if (r_ != CFPQ_OK) return r_; \
-    } while (0)
-
-// ---------------------------------------------------------------------------
-// types
-
-namespace {
-
-struct DevBuf {
-    void *p = nullptr;
-    size_t cap = 0;
-    int ensure(size_t bytes) {
-        if (bytes <= cap) return CFPQ_OK;
-        if (p) cudaFree(p);
-        p = nullptr;
-        cap = 0;
-        size_t want = std::max<size_t>(bytes, 256);
-        want = (want + 4095) & ~(size_t)4095;
-        cudaError_t e = cudaMalloc(&p, want);
-        if (e != cudaSuccess) {
-            p = nullptr;
-            return set_error(CFPQ_ERR_OOM, "device allocation of %zu bytes failed: %s", want, cudaGetErrorString(e));
-        }
-        cap = want;
-        return CFPQ_OK;
-    }
-    void release() {
-        if (p) cudaFree(p);
-        p = nullptr;
-        cap = 0;
-    }
-    template <class T> T *as() const { return reinterpret_cast<T *>(p); }
-};
-
-struct PowTables {
-    uint32_t *d_pow11 = nullptr;
-    uint32_t *d_pow13 = nullptr;
-};
-
-struct GraphCache {
-    cudaGraphExec_t exec = nullptr;
-    cudaGraph_t graph = nullptr;
-    std::vector<uint64_t> key;
-    void release() {
-        if (exec) cudaGraphExecDestroy(exec);
-        if (graph) cudaGraphDestroy(graph);
-        exec = nullptr;
-        graph = nullptr;
-        key.clear();
-    }
-};
-
-}  // namespace
-
-struct cfpq_order {
-    uint32_t n = 0;
-    uint32_t *d_perm = nullptr;
-    PowTables pow;  // hash powers indexed by internal id
-};
-
-struct cfpq_matrix {
-    cfpq_ctx *ctx;
-    DevMat d;
-    cfpq_order *order = nullptr;
-};
-
-struct PlanCache;
-static void free_plan_cache(cfpq_ctx *ctx);
-
-struct cfpq_ctx {
-    int device = 0;
-    int num_sms = 0;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    // small device scratch
-    IterState *d_st = nullptr;
-    uint32_t *d_flag = nullptr;
-    unsigned long long *d_hash = nullptr;  // 2 per matrix for hash_count_many
-    size_t d_hash_cap = 0;
-    uint32_t *d_bad = nullptr;
-    // pinned host scratch
-    IterState *h_st = nullptr;
-    uint32_t *h_flag = nullptr;
-    unsigned long long *h_hash = nullptr;
-    size_t h_hash_cap = 0;
-    // growable device scratch
-    DevBuf stage, items, prods, slots, qtrack, prod_seen, mats_desc, edge_buf, xbuf, clear_desc;
-    std::unordered_map<uint32_t, PowTables> pow;
-    std::vector<cfpq_matrix *> pool;  // zeroed spare matrices (deltas, alias copies)
-    GraphCache gcache;
-    PlanCache *pcache = nullptr;  // created by the first closure
-    uint64_t plan_ids = 0;
-    uint64_t tables_owner = 0;  // plan id whose slot / product tables are in `slots` / `prods`
-    int lop3_grid = 0, m4r_grid = 0, tc_grid = 0;  // tc_grid 0: tensor-core variant unavailable
-    int persist_grid[2] = {0, 0};  // persistent closure CTAs [with M4R items]; 0: unavailable
-    DevBuf phase_log;              // persistent closure: 3 timestamps per iteration
-    uint32_t phase_log_iters = 0;  // iterations logged by the last closure
-    std::vector<cfpq_product_record> log;
-    cudaEvent_t kev[5] = {};
-    cfpq_kernel_profile prof = {};
-    void *h_small = nullptr;
-    size_t h_small_cap = 0;
-};
-
 // ---------------------------------------------------------------------------
 // helpers
 
@@ -169,6 +53,8 @@ static inline uint32_t tiles_for(uint32_t n) { return (n + 63) / 64; }
 
 // Iterations of a persistent closure whose phase timestamps are kept.
 constexpr uint32_t kPhaseLogIters = 4096;
+// Iterations of a closure whose selection rows are kept.
+constexpr uint32_t kSelLogIters = 128;
 
 // Upper bound of the work items one product term can emit per iteration:
 // tile-rows x column blocks x chunks per block (tensor-core items: fewer).
@@ -375,6 +261,8 @@ extern "C" int cfpq_ctx_create(int device, cfpq_ctx **out) {
     int coop = 0;
     cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
     for (int m = 0; m < 2; ++m) c->persist_grid[m] = coop ? persistent_blocks_per_sm(m) * c->num_sms : 0;
+    selector_defaults(&c->sel);
+    if (!c->tc_grid) c->sel.allowed &= ~(1u << CFPQ_VARIANT_TC);
     *out = c;
     return CFPQ_OK;
 }
@@ -394,7 +282,10 @@ extern "C" int cfpq_ctx_destroy(cfpq_ctx *ctx) {
         cudaFree(kv.second.d_pow13);
     }
     for (DevBuf *b : {&ctx->stage, &ctx->items, &ctx->prods, &ctx->slots, &ctx->qtrack, &ctx->prod_seen,
-                      &ctx->mats_desc, &ctx->edge_buf, &ctx->xbuf, &ctx->phase_log, &ctx->clear_desc})
+                      &ctx->mats_desc, &ctx->edge_buf, &ctx->xbuf, &ctx->phase_log, &ctx->clear_desc,
+                      &ctx->d_sel, &ctx->cnts, &ctx->choice, &ctx->tc_ok, &ctx->sel_log, &ctx->mlp_w, &ctx->mlp_x,
+                      &ctx->mlp_y, &ctx->mlp_m, &ctx->mlp_grad, &ctx->mlp_m1, &ctx->mlp_v2, &ctx->mlp_loss,
+                      &ctx->mlp_out})
         b->release();
     cudaFree(ctx->d_st);
     cudaFree(ctx->d_flag);
@@ -407,6 +298,7 @@ extern "C" int cfpq_ctx_destroy(cfpq_ctx *ctx) {
     cudaEventDestroy(ctx->ev0);
     cudaEventDestroy(ctx->ev1);
     for (auto &e : ctx->kev) cudaEventDestroy(e);
+    for (auto &e : ctx->tev) cudaEventDestroy(e);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     return CFPQ_OK;
@@ -713,7 +605,8 @@ static int read_flag(cfpq_ctx *ctx, uint32_t *dflag, int *changed) {
     return CFPQ_OK;
 }
 
-static int launch_products(cfpq_ctx *ctx, size_t list_cap, bool lop3, bool m4r, uint32_t *qchanged, cudaStream_t s);
+static int launch_products(cfpq_ctx *ctx, size_t list_cap, bool lop3, bool m4r, uint32_t *qchanged,
+                           BufCounters *cnts, cudaStream_t s);
 
 // A tensor-core product term of a closure plan.
 struct TcProduct {
@@ -728,19 +621,21 @@ static int ensure_expand_scratch(cfpq_ctx *ctx, uint32_t T) {
 }
 
 // One tensor-core product: expand its operands, plan its items, run the
-// tensor-core kernel, close the item list.
+// tensor-core kernel, close the item list.  With a choice array every step is
+// a no-op unless this iteration's variant of the product is TC.
 static int launch_tc_product(cfpq_ctx *ctx, const TcProduct &tp, uint32_t nprods, size_t list_cap,
-                             uint32_t *prod_seen, uint32_t *qchanged, cudaStream_t s) {
+                             uint32_t *prod_seen, uint32_t *qchanged, const uint8_t *choice, BufCounters *cnts,
+                             cudaStream_t s) {
     uint8_t *xp = ctx->xbuf.as<uint8_t>();
     uint8_t *xq = xp + (size_t)tp.T * tp.T * 4096;
     const ProdDesc *pr = ctx->prods.as<ProdDesc>();
     const MatSlot *sl = ctx->slots.as<MatSlot>();
-    CUDA_TRY(launch_expand_operand(pr, tp.index, tp.T, sl, ctx->d_st, 0, xp, ctx->num_sms, s));
-    CUDA_TRY(launch_expand_operand(pr, tp.index, tp.T, sl, ctx->d_st, 1, xq, ctx->num_sms, s));
+    CUDA_TRY(launch_expand_operand(pr, tp.index, tp.T, sl, ctx->d_st, 0, xp, ctx->num_sms, choice, s));
+    CUDA_TRY(launch_expand_operand(pr, tp.index, tp.T, sl, ctx->d_st, 1, xq, ctx->num_sms, choice, s));
     CUDA_TRY(launch_plan(pr, nprods, tp.row_start, tp.row_start + tp.rows, sl, ctx->d_st, ctx->items.as<uint64_t>(),
-                         list_cap, product_lop3_tiles_per_block(), prod_seen, 1, s));
+                         list_cap, product_lop3_tiles_per_block(), prod_seen, 1, choice, s));
     CUDA_TRY(launch_product_tc(pr, sl, ctx->d_st, ctx->items.as<uint64_t>(), list_cap, qchanged, ctx->tc_grid, xp, xq,
-                               s));
+                               cnts, s));
     CUDA_TRY(launch_reset_list(ctx->d_st, 2, s));
     return CFPQ_OK;
 }
@@ -777,23 +672,26 @@ static int enqueue_tiled_product(cfpq_ctx *ctx, const DevMat &a, const DevMat &b
     CUDA_TRY(cudaMemcpyAsync(ctx->d_st, ctx->h_st, sizeof(IterState), cudaMemcpyHostToDevice, ctx->stream));
     if (variant == CFPQ_VARIANT_TC) {
         TRY(ensure_expand_scratch(ctx, T));
-        return launch_tc_product(ctx, TcProduct{0, T, 0, (T + 3) / 4}, 1, cap, nullptr, nullptr, ctx->stream);
+        return launch_tc_product(ctx, TcProduct{0, T, 0, (T + 3) / 4}, 1, cap, nullptr, nullptr, nullptr, nullptr,
+                                 ctx->stream);
     }
     CUDA_TRY(launch_plan(ctx->prods.as<ProdDesc>(), 1, 0, T, ctx->slots.as<MatSlot>(), ctx->d_st,
-                         ctx->items.as<uint64_t>(), cap, tpb, nullptr, 0, ctx->stream));
-    TRY(launch_products(ctx, cap, variant == CFPQ_VARIANT_LOP3, variant == CFPQ_VARIANT_M4R, nullptr, ctx->stream));
+                         ctx->items.as<uint64_t>(), cap, tpb, nullptr, 0, nullptr, ctx->stream));
+    TRY(launch_products(ctx, cap, variant == CFPQ_VARIANT_LOP3, variant == CFPQ_VARIANT_M4R, nullptr, nullptr,
+                        ctx->stream));
     return CFPQ_OK;
 }
 
 // Word-level product kernels of one closure iteration: one launch per item
 // list in use.
-static int launch_products(cfpq_ctx *ctx, size_t list_cap, bool lop3, bool m4r, uint32_t *qchanged, cudaStream_t s) {
+static int launch_products(cfpq_ctx *ctx, size_t list_cap, bool lop3, bool m4r, uint32_t *qchanged,
+                           BufCounters *cnts, cudaStream_t s) {
     if (lop3)
         CUDA_TRY(launch_product_tiled(0, ctx->prods.as<ProdDesc>(), ctx->slots.as<MatSlot>(), ctx->d_st,
-                                      ctx->items.as<uint64_t>(), list_cap, qchanged, ctx->lop3_grid, s));
+                                      ctx->items.as<uint64_t>(), list_cap, qchanged, ctx->lop3_grid, cnts, s));
     if (m4r)
         CUDA_TRY(launch_product_tiled(1, ctx->prods.as<ProdDesc>(), ctx->slots.as<MatSlot>(), ctx->d_st,
-                                      ctx->items.as<uint64_t>(), list_cap, qchanged, ctx->m4r_grid, s));
+                                      ctx->items.as<uint64_t>(), list_cap, qchanged, ctx->m4r_grid, cnts, s));
     return CFPQ_OK;
 }
 
@@ -874,6 +772,9 @@ struct ClosurePlan {
     bool uses_lop3 = false, uses_m4r = false, uses_tc = false;
     std::vector<TcProduct> tc_prods;
     uint32_t tc_max_T = 0;
+    bool auto_select = false;     // variants chosen on the device every iteration
+    uint8_t fixed_variant = 0;    // otherwise: every product's variant
+    std::vector<uint8_t> tc_ok;   // per product: has a tensor-core launch sequence
 };
 
 
@@ -924,6 +825,27 @@ static int validate_query(const QueryIn &q, size_t qi) {
 
 static int build_plan(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, int variant, ClosurePlan *pl) {
     const int tpb = product_lop3_tiles_per_block();
+    // AUTO with a selector: chosen per term and iteration among the allowed
+    // variants; else one variant for every term (PLAIN and fixed-mode AUTO
+    // run the LOP3 kernel)
+    const uint32_t allowed = ctx->sel.allowed & ((1u << CFPQ_VARIANT_LOP3) | (1u << CFPQ_VARIANT_M4R) |
+                                                 (ctx->tc_grid ? 1u << CFPQ_VARIANT_TC : 0u));
+    uint32_t max_T = 0;
+    for (const QueryIn &q : qs)
+        if (q.nmats && q.nrules) max_T = std::max(max_T, q.mats[0]->d.T);
+    pl->auto_select = variant == CFPQ_VARIANT_AUTO && ctx->sel.mode != CFPQ_SELECT_FIXED &&
+                      (allowed & ~(1u << CFPQ_VARIANT_LOP3)) != 0 && max_T >= ctx->sel.min_tiles;
+    pl->fixed_variant = (uint8_t)(variant == CFPQ_VARIANT_M4R || variant == CFPQ_VARIANT_TC ? variant
+                                                                                           : CFPQ_VARIANT_LOP3);
+    const bool tc_auto = (allowed & (1u << CFPQ_VARIANT_TC)) != 0;
+    if (pl->auto_select) {
+        pl->uses_lop3 = (allowed & (1u << CFPQ_VARIANT_LOP3)) != 0;
+        pl->uses_m4r = (allowed & (1u << CFPQ_VARIANT_M4R)) != 0;
+        if (!pl->uses_lop3 && !pl->uses_m4r) pl->uses_lop3 = true;  // the heuristic's last resort
+    } else {
+        pl->uses_lop3 = pl->fixed_variant == CFPQ_VARIANT_LOP3;
+        pl->uses_m4r = pl->fixed_variant == CFPQ_VARIANT_M4R;
+    }
     for (size_t qi = 0; qi < qs.size(); ++qi) {
         const QueryIn &q = qs[qi];
         const uint32_t base = (uint32_t)pl->slots.size();
@@ -955,26 +877,30 @@ static int build_plan(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, int variant
                 pd.p_delta = term == 0;
                 pd.q_delta = term == 1;
                 pd.term = term;
-                pd.variant = (uint8_t)(variant == CFPQ_VARIANT_M4R || variant == CFPQ_VARIANT_TC ? variant
-                                                                                                    : CFPQ_VARIANT_LOP3);
-                (pd.variant == CFPQ_VARIANT_M4R ? pl->uses_m4r
-                                                : pd.variant == CFPQ_VARIANT_TC ? pl->uses_tc : pl->uses_lop3) = true;
+                pd.variant = pl->auto_select ? (uint8_t)CFPQ_VARIANT_AUTO : pl->fixed_variant;
                 pd.query = (uint32_t)qi;
                 pd.rule = (uint32_t)r;
                 pd.T = T;
                 pd.n = n;
+                // plan rows: T tile-rows for the word-level kernels; a term that
+                // may run on tensor cores also plans ceil(T/4) groups of 4
+                // tile-rows from the same start in its own launch
                 pd.row_start = pl->prod_rows;
-                if (pd.variant == CFPQ_VARIANT_TC) {  // plan rows: tile-row groups of 4 for tc
+                const bool tc = pl->auto_select ? tc_auto && T >= ctx->sel.tc_min_tiles
+                                                : pl->fixed_variant == CFPQ_VARIANT_TC;
+                if (tc) {
                     pl->tc_prods.push_back(TcProduct{(uint32_t)pl->prods.size(), T, pl->prod_rows, (T + 3) / 4});
                     pl->tc_max_T = std::max(pl->tc_max_T, T);
                 }
-                pl->prod_rows += pd.variant == CFPQ_VARIANT_TC ? (T + 3) / 4 : T;
+                pl->tc_ok.push_back(tc ? 1 : 0);
+                pl->prod_rows += T;
                 pl->item_cap += item_capacity(T, tpb);
                 pl->prods.push_back(pd);
             }
         }
     }
     pl->item_cap = std::max<size_t>(pl->item_cap, 1);
+    pl->uses_tc = !pl->tc_prods.empty();
     if (pl->prods.size() > kMaxItemProducts)
         return set_error(CFPQ_ERR_INVALID, "%zu rule products in one closure (at most %u)", pl->prods.size(),
                          kMaxItemProducts);
@@ -983,9 +909,13 @@ static int build_plan(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, int variant
 
 // Cache key of a closure: variant, and per query its rules and the device
 // layout of its matrices.
-static void plan_key(const std::vector<QueryIn> &qs, int variant, std::vector<uint64_t> *key) {
+static void plan_key(const cfpq_ctx *ctx, const std::vector<QueryIn> &qs, int variant,
+                     std::vector<uint64_t> *key) {
     key->clear();
     key->push_back(((uint64_t)(uint32_t)variant << 32) | (uint64_t)qs.size());
+    key->push_back(((uint64_t)(uint32_t)ctx->sel.mode << 40) | ((uint64_t)ctx->sel.allowed << 32) |
+                   ctx->sel.tc_min_tiles);
+    key->push_back(ctx->sel.min_tiles);
     for (const QueryIn &q : qs) {
         key->push_back(((uint64_t)q.nrules << 32) | (uint64_t)q.nmats);
         for (size_t r = 0; r < q.nrules; ++r)
@@ -1010,37 +940,54 @@ static void drop_plan_cache(cfpq_ctx *ctx, bool dirty) {
     pc.valid = false;
 }
 
-static int enqueue_iteration(cfpq_ctx *ctx, const ClosurePlan &pl, const QueryTrack &qt,
-                             cudaGraphConditionalHandle handle, int use_handle) {
-    const int tpb = product_lop3_tiles_per_block();
+// Buffer counters of a closure: kept (and read) only when the selector runs.
+static BufCounters *closure_counters(cfpq_ctx *ctx, const ClosurePlan &) {
+    return ctx->cnts_on ? ctx->cnts.as<BufCounters>() : nullptr;
+}
+
+// Plan of one iteration; in AUTO closures the planner also chooses every
+// term's variant (PlanSelect).
+static int enqueue_select_plan(cfpq_ctx *ctx, const ClosurePlan &pl, cudaStream_t s) {
+    const PlanSelect ps = {ctx->d_sel.as<SelectorParams>(), ctx->cnts.as<BufCounters>(), ctx->tc_ok.as<uint8_t>(),
+                           ctx->choice.as<uint8_t>(), ctx->sel_log_iters ? ctx->sel_log.as<SelLogRow>() : nullptr,
+                           ctx->sel_log_iters};
     CUDA_TRY(launch_plan(ctx->prods.as<ProdDesc>(), (uint32_t)pl.prods.size(), 0, pl.prod_rows,
-                         ctx->slots.as<MatSlot>(), ctx->d_st, ctx->items.as<uint64_t>(), pl.item_cap, tpb,
-                         ctx->prod_seen.as<uint32_t>(), 0, ctx->stream));
-    TRY(launch_products(ctx, pl.item_cap, pl.uses_lop3, pl.uses_m4r, qt.changed, ctx->stream));
-    for (const TcProduct &tp : pl.tc_prods)
-        TRY(launch_tc_product(ctx, tp, (uint32_t)pl.prods.size(), pl.item_cap, ctx->prod_seen.as<uint32_t>(),
-                              qt.changed, ctx->stream));
-    CUDA_TRY(launch_advance_end(ctx->slots.as<MatSlot>(), (uint32_t)pl.slots.size(), pl.slot_rows, ctx->d_st, qt,
-                                handle, use_handle, ctx->stream));
+                         ctx->slots.as<MatSlot>(), ctx->d_st, ctx->items.as<uint64_t>(), pl.item_cap,
+                         product_lop3_tiles_per_block(), ctx->prod_seen.as<uint32_t>(), 0, ctx->choice.as<uint8_t>(),
+                         s, pl.auto_select ? &ps : nullptr));
     return CFPQ_OK;
 }
 
-// One iteration with every kernel bracketed by events (profiling mode).
-static int enqueue_iteration_timed(cfpq_ctx *ctx, const ClosurePlan &pl, const QueryTrack &qt) {
-    const int tpb = product_lop3_tiles_per_block();
-    cudaStream_t s = ctx->stream;
-    CUDA_TRY(cudaEventRecord(ctx->kev[0], s));
-    CUDA_TRY(launch_plan(ctx->prods.as<ProdDesc>(), (uint32_t)pl.prods.size(), 0, pl.prod_rows,
-                         ctx->slots.as<MatSlot>(), ctx->d_st, ctx->items.as<uint64_t>(), pl.item_cap, tpb,
-                         ctx->prod_seen.as<uint32_t>(), 0, s));
-    CUDA_TRY(cudaEventRecord(ctx->kev[1], s));
-    TRY(launch_products(ctx, pl.item_cap, pl.uses_lop3, pl.uses_m4r, qt.changed, s));
+// Product kernels of one iteration: the word-level lists, then the tensor-core
+// sequence of every term that may run on tensor cores.
+static int enqueue_products(cfpq_ctx *ctx, const ClosurePlan &pl, const QueryTrack &qt, cudaStream_t s) {
+    BufCounters *cnts = closure_counters(ctx, pl);
+    TRY(launch_products(ctx, pl.item_cap, pl.uses_lop3, pl.uses_m4r, qt.changed, cnts, s));
     for (const TcProduct &tp : pl.tc_prods)
         TRY(launch_tc_product(ctx, tp, (uint32_t)pl.prods.size(), pl.item_cap, ctx->prod_seen.as<uint32_t>(),
-                              qt.changed, s));
+                              qt.changed, ctx->choice.as<uint8_t>(), cnts, s));
+    return CFPQ_OK;
+}
+
+static int enqueue_iteration(cfpq_ctx *ctx, const ClosurePlan &pl, const QueryTrack &qt,
+                             cudaGraphConditionalHandle handle, int use_handle) {
+    TRY(enqueue_select_plan(ctx, pl, ctx->stream));
+    TRY(enqueue_products(ctx, pl, qt, ctx->stream));
+    CUDA_TRY(launch_advance_end(ctx->slots.as<MatSlot>(), (uint32_t)pl.slots.size(), pl.slot_rows, ctx->d_st, qt,
+                                handle, use_handle, closure_counters(ctx, pl), ctx->stream));
+    return CFPQ_OK;
+}
+
+// One iteration with every phase bracketed by events (profiling mode).
+static int enqueue_iteration_timed(cfpq_ctx *ctx, const ClosurePlan &pl, const QueryTrack &qt) {
+    cudaStream_t s = ctx->stream;
+    CUDA_TRY(cudaEventRecord(ctx->kev[0], s));
+    TRY(enqueue_select_plan(ctx, pl, s));
+    CUDA_TRY(cudaEventRecord(ctx->kev[1], s));
+    TRY(enqueue_products(ctx, pl, qt, s));
     CUDA_TRY(cudaEventRecord(ctx->kev[2], s));
     CUDA_TRY(launch_advance_end(ctx->slots.as<MatSlot>(), (uint32_t)pl.slots.size(), pl.slot_rows, ctx->d_st, qt, 0, 0,
-                                s));
+                                closure_counters(ctx, pl), s));
     CUDA_TRY(cudaEventRecord(ctx->kev[3], s));
     return CFPQ_OK;
 }
@@ -1088,7 +1035,10 @@ static int get_loop_graph(cfpq_ctx *ctx, const ClosurePlan &pl, const QueryTrack
                                  (uint64_t)(uintptr_t)qt.changed,     (uint64_t)(uintptr_t)qt.last_iter,
                                  (uint64_t)(uintptr_t)qt.done_ns,     (uint64_t)ctx->lop3_grid,
                                  (uint64_t)pl.item_cap,               (uint64_t)(pl.uses_lop3 + 2 * pl.uses_m4r + 4 * pl.uses_tc),
-                                 (uint64_t)(uintptr_t)ctx->xbuf.p};
+                                 (uint64_t)(uintptr_t)ctx->xbuf.p,    (uint64_t)(uintptr_t)ctx->choice.p,
+                                 (uint64_t)(uintptr_t)ctx->cnts.p,    (uint64_t)(uintptr_t)ctx->d_sel.p,
+                                 (uint64_t)(uintptr_t)ctx->tc_ok.p,   (uint64_t)(uintptr_t)ctx->sel_log.p,
+                                 (uint64_t)ctx->sel_log_iters,        (uint64_t)pl.auto_select};
     for (const TcProduct &tp : pl.tc_prods) {  // kernel arguments of the tensor-core launches
         key.push_back(((uint64_t)tp.index << 32) | tp.T);
         key.push_back(((uint64_t)tp.row_start << 32) | tp.rows);
@@ -1135,11 +1085,135 @@ static int get_loop_graph(cfpq_ctx *ctx, const ClosurePlan &pl, const QueryTrack
     return CFPQ_OK;
 }
 
+// Product records (features and the selector's decision, no timings) of the
+// iterations the selection log holds.
+static int collect_selection_log(cfpq_ctx *ctx, const ClosurePlan &pl, uint32_t iterations) {
+    const uint32_t np = (uint32_t)pl.prods.size(), its = std::min(iterations, ctx->sel_log_iters);
+    if (!np || !its) return CFPQ_OK;
+    std::vector<SelLogRow> rows((size_t)its * np);
+    CUDA_TRY(cudaMemcpy(rows.data(), ctx->sel_log.p, rows.size() * sizeof(SelLogRow), cudaMemcpyDeviceToHost));
+    for (uint32_t it = 0; it < its; ++it)
+        for (uint32_t p = 0; p < np; ++p) {
+            const ProdDesc &pd = pl.prods[p];
+            if (pd.term == 1 && it == 0) continue;  // the first iteration runs term 0 only
+            const SelLogRow &r = rows[(size_t)it * np + p];
+            cfpq_product_record rec;
+            memset(&rec, 0, sizeof(rec));
+            rec.iteration = it;
+            rec.query = pd.query;
+            rec.rule = pd.rule;
+            rec.term = pd.term;
+            rec.n = pd.n;
+            rec.variant = r.choice & 0xFF;
+            rec.flags = r.choice & ~0xFFu;
+            memcpy(rec.features, r.f, sizeof(rec.features));
+            memcpy(rec.predicted, r.pred, sizeof(rec.predicted));
+            for (float &u : rec.usec) u = -1.f;
+            ctx->log.push_back(rec);
+        }
+    return CFPQ_OK;
+}
+
+// CFPQ_LOG_PRODUCTS: iterations from the host.  Each iteration: the selector
+// (features and decision of every term), the real work with the chosen
+// variants, then every term alone with every candidate variant, timed with
+// events (the state no longer changes: all bits are already there), then the
+// iteration end.
+static int run_logged_iterations(cfpq_ctx *ctx, const ClosurePlan &pl, const QueryTrack &qt) {
+    cudaStream_t s = ctx->stream;
+    const uint32_t np = (uint32_t)pl.prods.size();
+    const int tpb = product_lop3_tiles_per_block();
+    const size_t need_ev = (size_t)np * 3 * 2;
+    while (ctx->tev.size() < need_ev) {
+        cudaEvent_t e;
+        CUDA_TRY(cudaEventCreate(&e));
+        ctx->tev.push_back(e);
+    }
+    std::vector<int> tc_index(np, -1);
+    for (size_t i = 0; i < pl.tc_prods.size(); ++i) tc_index[pl.tc_prods[i].index] = (int)i;
+    std::vector<SelLogRow> rows(np);
+    for (uint32_t it = 0;; ++it) {
+        if (it > (1u << 20)) return set_error(CFPQ_ERR_CUDA, "closure did not converge");
+        // features + decisions (always logged in this mode)
+        CUDA_TRY(launch_select(ctx->prods.as<ProdDesc>(), np, ctx->cnts.as<BufCounters>(), ctx->d_st,
+                               ctx->d_sel.as<SelectorParams>(), ctx->choice.as<uint8_t>(), ctx->tc_ok.as<uint8_t>(),
+                               ctx->sel_log.as<SelLogRow>(), ctx->sel_log_iters, s));
+        if (!pl.auto_select) CUDA_TRY(launch_fill_choice(ctx->choice.as<uint8_t>(), np, pl.fixed_variant, s));
+        // the real work
+        CUDA_TRY(launch_plan(ctx->prods.as<ProdDesc>(), np, 0, pl.prod_rows, ctx->slots.as<MatSlot>(), ctx->d_st,
+                             ctx->items.as<uint64_t>(), pl.item_cap, tpb, ctx->prod_seen.as<uint32_t>(), 0,
+                             ctx->choice.as<uint8_t>(), s));
+        TRY(enqueue_products(ctx, pl, qt, s));
+        CUDA_TRY(launch_reset_list(ctx->d_st, 0, s));
+        CUDA_TRY(launch_reset_list(ctx->d_st, 1, s));
+        // every term alone with every candidate variant
+        std::vector<std::pair<uint32_t, int>> timed;  // (product, variant)
+        size_t ev = 0;
+        for (uint32_t p = 0; p < np; ++p) {
+            const ProdDesc &pd = pl.prods[p];
+            if (pd.term == 1 && it == 0) continue;
+            for (int v = CFPQ_VARIANT_LOP3; v <= CFPQ_VARIANT_TC; ++v) {
+                if (v == CFPQ_VARIANT_TC && tc_index[p] < 0) continue;
+                CUDA_TRY(cudaMemsetAsync(ctx->choice.as<uint8_t>() + p, v, 1, s));
+                CUDA_TRY(cudaEventRecord(ctx->tev[ev], s));
+                if (v == CFPQ_VARIANT_TC) {
+                    TRY(launch_tc_product(ctx, pl.tc_prods[tc_index[p]], np, pl.item_cap, nullptr, qt.changed,
+                                          ctx->choice.as<uint8_t>(), ctx->cnts.as<BufCounters>(), s));
+                } else {
+                    CUDA_TRY(launch_plan(ctx->prods.as<ProdDesc>(), np, pd.row_start, pd.row_start + pd.T,
+                                         ctx->slots.as<MatSlot>(), ctx->d_st, ctx->items.as<uint64_t>(), pl.item_cap,
+                                         tpb, nullptr, 0, ctx->choice.as<uint8_t>(), s));
+                    TRY(launch_products(ctx, pl.item_cap, v == CFPQ_VARIANT_LOP3, v == CFPQ_VARIANT_M4R, qt.changed,
+                                        ctx->cnts.as<BufCounters>(), s));
+                    CUDA_TRY(launch_reset_list(ctx->d_st, v == CFPQ_VARIANT_LOP3 ? 0 : 1, s));
+                }
+                CUDA_TRY(cudaEventRecord(ctx->tev[ev + 1], s));
+                ev += 2;
+                timed.push_back({p, v});
+            }
+        }
+        CUDA_TRY(launch_advance_end(ctx->slots.as<MatSlot>(), (uint32_t)pl.slots.size(), pl.slot_rows, ctx->d_st, qt, 0,
+                                    0, ctx->cnts.as<BufCounters>(), s));
+        CUDA_TRY(cudaMemcpyAsync(ctx->h_st, ctx->d_st, sizeof(IterState), cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+        if (it < ctx->sel_log_iters)
+            CUDA_TRY(cudaMemcpy(rows.data(), ctx->sel_log.as<SelLogRow>() + (size_t)it * np, np * sizeof(SelLogRow),
+                                cudaMemcpyDeviceToHost));
+        std::vector<int> rec_of(np, -1);
+        for (uint32_t p = 0; p < np; ++p) {
+            const ProdDesc &pd = pl.prods[p];
+            if (pd.term == 1 && it == 0) continue;
+            cfpq_product_record rec;
+            memset(&rec, 0, sizeof(rec));
+            rec.iteration = it;
+            rec.query = pd.query;
+            rec.rule = pd.rule;
+            rec.term = pd.term;
+            rec.n = pd.n;
+            const SelLogRow &r = rows[p];
+            rec.variant = pl.auto_select ? (r.choice & 0xFF) : pl.fixed_variant;
+            rec.flags = r.choice & ~0xFFu;
+            memcpy(rec.features, r.f, sizeof(rec.features));
+            memcpy(rec.predicted, r.pred, sizeof(rec.predicted));
+            for (float &u : rec.usec) u = -1.f;
+            rec_of[p] = (int)ctx->log.size();
+            ctx->log.push_back(rec);
+        }
+        for (size_t i = 0; i < timed.size(); ++i) {
+            float ms = 0;
+            CUDA_TRY(cudaEventElapsedTime(&ms, ctx->tev[2 * i], ctx->tev[2 * i + 1]));
+            ctx->log[rec_of[timed[i].first]].usec[timed[i].second] = ms * 1e3f;
+        }
+        if (!ctx->h_st->active) break;
+    }
+    return CFPQ_OK;
+}
+
 static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_closure_opts &o,
                       cfpq_closure_stats *stats, uint32_t *iters_out, double *done_ms_out) {
     for (size_t qi = 0; qi < qs.size(); ++qi) TRY(validate_query(qs[qi], qi));
     std::vector<uint64_t> key;
-    plan_key(qs, o.variant, &key);
+    plan_key(ctx, qs, o.variant, &key);
     if (!ctx->pcache) ctx->pcache = new PlanCache();
     PlanCache &pc = *ctx->pcache;
     if (!pc.valid || pc.key != key) {
@@ -1170,9 +1244,21 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
     const bool tables_current =
         ctx->tables_owner == pc.id && ctx->slots.p == slots_before && ctx->prods.p == prods_before;
     const bool timed = (o.log_products & CFPQ_LOG_KERNELS) != 0;
+    const bool log_products = (o.log_products & CFPQ_LOG_PRODUCTS) != 0;
     const int persist_grid = ctx->persist_grid[pl.uses_m4r ? 1 : 0];
-    const bool persistent = o.use_graph == CFPQ_LOOP_DEVICE && !timed && !pl.uses_tc && persist_grid > 0;
+    const bool persistent =
+        o.use_graph == CFPQ_LOOP_DEVICE && !timed && !log_products && !pl.uses_tc && persist_grid > 0;
+    const uint32_t nprods = (uint32_t)pl.prods.size(), nslots = (uint32_t)pl.slots.size();
     TRY(ctx->items.ensure((persistent ? 4 : 3) * pl.item_cap * 8));
+    TRY(ctx->choice.ensure(nprods));
+    TRY(ctx->tc_ok.ensure(nprods));
+    TRY(ctx->cnts.ensure((size_t)nslots * 3 * sizeof(BufCounters)));
+    ctx->cnts_on = pl.auto_select || log_products;
+    if (ctx->cnts_on) TRY(selector_sync(ctx));
+    ctx->sel_log_iters = (log_products || (o.log_products & CFPQ_LOG_SELECTION)) ? kSelLogIters : 0;
+    ctx->sel_log_prods = nprods;
+    if (ctx->sel_log_iters) TRY(ctx->sel_log.ensure((size_t)kSelLogIters * nprods * sizeof(SelLogRow)));
+    ctx->log.clear();
     TRY(ctx->prod_seen.ensure(pl.prods.size() * 4));
     if (pl.tc_max_T) TRY(ensure_expand_scratch(ctx, pl.tc_max_T));
     if (persistent) TRY(ctx->phase_log.ensure(kPhaseLogIters * 3 * 8));
@@ -1187,8 +1273,15 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
                                  cudaMemcpyHostToDevice, ctx->stream));
         CUDA_TRY(cudaMemcpyAsync(ctx->prods.p, pl.prods.data(), pl.prods.size() * sizeof(ProdDesc),
                                  cudaMemcpyHostToDevice, ctx->stream));
+        CUDA_TRY(cudaMemcpyAsync(ctx->tc_ok.p, pl.tc_ok.data(), nprods, cudaMemcpyHostToDevice, ctx->stream));
         ctx->tables_owner = pc.id;
     }
+    CUDA_TRY(launch_fill_choice(ctx->choice.as<uint8_t>(), nprods,
+                                pl.auto_select ? (uint8_t)CFPQ_VARIANT_LOP3 : pl.fixed_variant, ctx->stream));
+    if (ctx->cnts_on) CUDA_TRY(launch_counters_init(ctx->slots.as<MatSlot>(), nslots, ctx->cnts.as<BufCounters>(),
+                                                    ctx->stream));
+    if (ctx->sel_log_iters)
+        CUDA_TRY(cudaMemsetAsync(ctx->sel_log.p, 0, (size_t)kSelLogIters * nprods * sizeof(SelLogRow), ctx->stream));
     CUDA_TRY(cudaMemsetAsync(ctx->prod_seen.p, 0, pl.prods.size() * 4, ctx->stream));
     CUDA_TRY(cudaMemsetAsync(ctx->qtrack.p, 0, qbytes, ctx->stream));
     IterState st;
@@ -1200,12 +1293,14 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
     CUDA_TRY(cudaMemcpyAsync(ctx->d_st, ctx->h_st, sizeof(IterState), cudaMemcpyHostToDevice, ctx->stream));
 
     cudaGraphExec_t exec = nullptr;
-    if (o.use_graph && !timed && !persistent) TRY(get_loop_graph(ctx, pl, qt, &exec));
+    if (o.use_graph && !timed && !log_products && !persistent) TRY(get_loop_graph(ctx, pl, qt, &exec));
     if (timed) memset(&ctx->prof, 0, sizeof(ctx->prof));
 
     CUDA_TRY(launch_mark_start(ctx->d_st, ctx->stream));
     CUDA_TRY(cudaEventRecord(ctx->ev0, ctx->stream));
-    if (timed) {
+    if (log_products) {
+        TRY(run_logged_iterations(ctx, pl, qt));
+    } else if (timed) {
         for (uint32_t it = 0;; ++it) {
             TRY(enqueue_iteration_timed(ctx, pl, qt));
             CUDA_TRY(cudaMemcpyAsync(ctx->h_st, ctx->d_st, sizeof(IterState), cudaMemcpyDeviceToHost, ctx->stream));
@@ -1220,7 +1315,11 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
                                            (uint32_t)pl.slots.size(), pl.slot_rows, ctx->d_st,
                                            ctx->items.as<uint64_t>(), pl.item_cap, ctx->prod_seen.as<uint32_t>(), qt,
                                            product_lop3_tiles_per_block(),
-                                           ctx->phase_log.as<unsigned long long>(), kPhaseLogIters, ctx->stream));
+                                           ctx->phase_log.as<unsigned long long>(), kPhaseLogIters,
+                                           closure_counters(ctx, pl), ctx->choice.as<uint8_t>(),
+                                           pl.auto_select ? ctx->d_sel.as<SelectorParams>() : nullptr,
+                                           ctx->sel_log_iters ? ctx->sel_log.as<SelLogRow>() : nullptr,
+                                           ctx->sel_log_iters, ctx->stream));
     } else if (exec) {
         CUDA_TRY(cudaGraphLaunch(exec, ctx->stream));
     } else {
@@ -1275,6 +1374,7 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
         if (iters_out) iters_out[q] = h_last[q];
         if (done_ms_out) done_ms_out[q] = h_last[q] ? (double)(h_done[q] - hs.t_start_ns) / 1e6 : 0.0;
     }
+    if (ctx->sel_log_iters && !log_products) TRY(collect_selection_log(ctx, pl, hs.iter));
     return CFPQ_OK;
 }
 

@@ -96,6 +96,60 @@ struct MatRows {
     uint32_t pad;
 };
 
+// Statistics of one buffer of a closure (a slot's current matrix or one of
+// its two deltas), kept exact by the product epilogues and reset when a delta
+// is cleared: population, occupied tiles (occupancy bits), dense tiles
+// (population > kDenseTilePop).  Buffer b of slot s is counters[3*s + b]
+// (b = 0: current matrix, 1 + d: delta d).  They are the selector's features.
+struct BufCounters {
+    unsigned long long nnz;
+    uint32_t occ_tiles;
+    uint32_t dense_tiles;
+};
+constexpr uint32_t kDenseTilePop = 96;
+
+// Variant selector (device-resident).  Feature vector of a product term,
+// predicted log-microseconds per candidate variant (LOP3, M4R, TC).
+constexpr int kSelFeatures = 16;
+constexpr int kSelHidden = 64;
+constexpr int kSelOutputs = 3;
+constexpr int kSelWeights = kSelFeatures * kSelHidden + kSelHidden + kSelHidden * kSelHidden + kSelHidden +
+                            kSelHidden * kSelOutputs + kSelOutputs;
+struct SelectorParams {
+    int32_t mode;           // 0 fixed, 1 heuristic, 2 MLP with heuristic fallback
+    uint32_t allowed;       // bit v: variant v may be chosen
+    uint32_t tc_min_tiles;  // tensor cores only for products with T >= tc_min_tiles
+    float tc_min_occ, tc_min_pop, m4r_min_dense;
+    float conf_margin, range_margin;
+    uint32_t min_tiles;     // closures whose largest term has fewer tile-rows run LOP3 throughout
+    int32_t has_weights;
+    float feat_lo[kSelFeatures], feat_hi[kSelFeatures];  // training range of every feature
+    float w[kSelWeights];   // W1 [F][H], b1 [H], W2 [H][H], b2 [H], W3 [H][O], b3 [O]
+};
+
+// One row of the selection log: the features of (iteration, product), the
+// MLP's predictions (if it ran) and the choice (bits 0-7 variant, bit 8: the
+// MLP decided, bit 9: the MLP ran but fell back to the heuristic).
+struct SelLogRow {
+    float f[kSelFeatures];
+    float pred[kSelOutputs];
+    uint32_t choice;
+};
+
+// Variant source of the planner.  sel non-null: the planner's warps decide
+// every word-level plan's variant themselves from the buffer counters (every
+// row of a product gets the same answer; the warp of tile-row 0 stores it in
+// choice[] and the selection log), and the tensor-core plan reads choice[].
+// sel null: choice[] (or, if null too, the product's own variant).
+struct PlanSelect {
+    const SelectorParams *sel;
+    const BufCounters *cnts;
+    const uint8_t *tc_ok;
+    uint8_t *choice;
+    SelLogRow *log;
+    uint32_t log_iters;
+};
+
 // Per-query bookkeeping of a batched closure (device arrays of nqueries).
 struct QueryTrack {
     uint32_t *changed;              // set by product kernels in the current iteration
@@ -214,6 +268,38 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t phase)
 }
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31; }
+
+// Lanes 0..3 of a warp, lane j for tile tj0 + j (add[j] new bits, 0: none):
+// tile populations and occupancy bits of m, then (cnt non-null) the buffer
+// counters, aggregated over the 4 tiles into one update per counter.
+__device__ __forceinline__ void tiles_gain(const DevMat &m, uint32_t ti, uint32_t tj0, uint32_t add,
+                                           BufCounters *cnt) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t tj = tj0 + lane;
+    uint32_t gained = 0, dense = 0;
+    if (lane < 4 && add) {
+        const size_t t = (size_t)ti * m.T + tj;
+        const uint32_t bit = 1u << (tj & 31);
+        if (cnt) {
+            const uint32_t old_pop = atomicAdd(m.nnz + t, add);
+            const uint32_t old_occ = atomicOr(m.occ + (size_t)ti * m.ow + (tj >> 5), bit);
+            gained = (old_occ & bit) ? 0u : 1u;
+            dense = (old_pop <= kDenseTilePop && old_pop + add > kDenseTilePop) ? 1u : 0u;
+        } else {
+            atomicAdd(m.nnz + t, add);
+            atomicOr(m.occ + (size_t)ti * m.ow + (tj >> 5), bit);
+        }
+    }
+    if (!cnt) return;
+    const uint32_t sum_add = __reduce_add_sync(0xffffffffu, lane < 4 ? add : 0u);
+    const uint32_t sum_gained = __reduce_add_sync(0xffffffffu, gained);
+    const uint32_t sum_dense = __reduce_add_sync(0xffffffffu, dense);
+    if (lane == 0) {
+        if (sum_add) atomicAdd(&cnt->nnz, sum_add);
+        if (sum_gained) atomicAdd(&cnt->occ_tiles, sum_gained);
+        if (sum_dense) atomicAdd(&cnt->dense_tiles, sum_dense);
+    }
+}
 
 // One warp: clear tile-row ti of D -- zero every occupied tile and its
 // population, then the occupancy row (tiles without an occupancy bit hold no

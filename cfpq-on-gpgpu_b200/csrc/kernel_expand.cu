@@ -62,7 +62,9 @@ __device__ __forceinline__ void transpose64(uint64_t &lo, uint64_t &hi, uint32_t
 // per tile (grid-stride); lane l writes operand rows l and l+32.
 __global__ void __launch_bounds__(256) k_expand_operand(const ProdDesc *__restrict__ prods, uint32_t p,
                                                         const MatSlot *__restrict__ slots, const IterState *st,
-                                                        int side, uint8_t *__restrict__ out) {
+                                                        int side, uint8_t *__restrict__ out,
+                                                        const uint8_t *__restrict__ choice) {
+    if (choice && choice[p] != 4) return;  // this iteration runs the product on the word-level kernels
     const ProdDesc pd = prods[p];
     const uint32_t iter = st->iter;
     if (!st->active || (pd.term == 1 && iter == 0)) return;  // the plan emits nothing for this product
@@ -91,12 +93,13 @@ __global__ void k_reset_list(IterState *st, int list) {
 }  // namespace
 
 cudaError_t launch_expand_operand(const ProdDesc *d_prods, uint32_t p, uint32_t T, const MatSlot *d_slots,
-                                  const IterState *d_st, int side, uint8_t *out, int num_sms, cudaStream_t s) {
+                                  const IterState *d_st, int side, uint8_t *out, int num_sms,
+                                  const uint8_t *d_choice, cudaStream_t s) {
     if (T == 0) return cudaSuccess;
     size_t blocks = ((size_t)T * T + 7) / 8;
     const size_t cap = (size_t)num_sms * 16;
     if (blocks > cap) blocks = cap;
-    k_expand_operand<<<(unsigned)blocks, 256, 0, s>>>(d_prods, p, d_slots, d_st, side, out);
+    k_expand_operand<<<(unsigned)blocks, 256, 0, s>>>(d_prods, p, d_slots, d_st, side, out, d_choice);
     return cudaGetLastError();
 }
 

@@ -52,7 +52,7 @@ using namespace tiled;
 template <bool kM4R>
 __global__ void __launch_bounds__(kThreads, 4)
     k_product_tiled(const ProdDesc *__restrict__ prods, const MatSlot *__restrict__ slots, IterState *st,
-                    const uint64_t *__restrict__ items_all, size_t list_cap, uint32_t *qchanged) {
+                    const uint64_t *__restrict__ items_all, size_t list_cap, uint32_t *qchanged, BufCounters *cnts) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     TiledSmem<kM4R> &S = *reinterpret_cast<TiledSmem<kM4R> *>(smem_raw);
     const uint32_t tid = threadIdx.x, lane = tid & 31;
@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(kThreads, 4)
         __syncthreads();
         const uint32_t idx = S.item;
         if (idx >= nitems) break;
-        process_item<kM4R>(S, items[idx], prods, slots, iter, &st->changed, qchanged, phase, timed_out, ctr);
+        process_item<kM4R>(S, items[idx], prods, slots, iter, &st->changed, qchanged, phase, timed_out, ctr, cnts);
     }
     // per-CTA counters (warp-reduced) for statistics and the roofline report
     unsigned long long triples = ctr.triples, outw = ctr.outw, neww = ctr.neww;
@@ -115,13 +115,13 @@ int product_tiled_blocks_per_sm(int m4r) {
 
 cudaError_t launch_product_tiled(int m4r, const ProdDesc *d_prods, const MatSlot *d_slots, IterState *d_st,
                                  const uint64_t *d_items, size_t list_cap, uint32_t *d_qchanged, int grid,
-                                 cudaStream_t s) {
+                                 BufCounters *d_cnts, cudaStream_t s) {
     if (m4r)
         k_product_tiled<true><<<grid, kThreads, sizeof(TiledSmem<true>), s>>>(d_prods, d_slots, d_st, d_items, list_cap,
-                                                                              d_qchanged);
+                                                                              d_qchanged, d_cnts);
     else
         k_product_tiled<false><<<grid, kThreads, sizeof(TiledSmem<false>), s>>>(d_prods, d_slots, d_st, d_items,
-                                                                                list_cap, d_qchanged);
+                                                                                list_cap, d_qchanged, d_cnts);
     return cudaGetLastError();
 }
 

@@ -6,7 +6,8 @@
 // Iteration t (parity par = t & 1), every CTA:
 //   phase A  warps take units round-robin: the product tile-rows (plan::plan_row
 //            emits the iteration's work items into the item lists of parity
-//            par) and, for t >= 1, the slot tile-rows of the delta read in
+//            par; AUTO closures: the planner also chooses each term's variant,
+//            select_device.cuh) and, for t >= 1, the slot tile-rows of the delta read in
 //            iteration t-1 (dlt[par ^ 1], cleared: the products of iteration t
 //            write their new bits there).  CTA 0 also folds the counters of
 //            parity par ^ 1 (iteration t-1) into the statistics and zeroes them.
@@ -66,6 +67,11 @@ struct PersistArgs {
     int tpb;
     unsigned long long *phase_log;  // 3 %globaltimer stamps per iteration (may be null)
     uint32_t phase_log_iters;
+    BufCounters *cnts;              // 3 per slot
+    uint8_t *choice;                // variant of every product in the current iteration
+    const SelectorParams *sel;      // non-null: choose per iteration (selection phase)
+    SelLogRow *sel_log;
+    uint32_t sel_log_iters;
 };
 
 // Grid barrier (all CTAs of the cooperative launch): arrival counter plus a
@@ -127,6 +133,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_closure_persistent(PersistArgs 
         prods = reinterpret_cast<const ProdDesc *>(S.tables + slot_bytes);
     }
     __syncthreads();
+    const PlanSelect psel = {a.sel && a.cnts ? a.sel : nullptr, a.cnts, nullptr, a.choice, a.sel_log, a.sel_log_iters};
     uint32_t gen = s_gen0, phase = 0;
     bool timed_out = false;
     ItemCounters ctr;
@@ -149,6 +156,8 @@ __global__ void __launch_bounds__(kThreads, 3) k_closure_persistent(PersistArgs 
             }
         }
         // ---- phase A: plan of iteration t + clear of the delta read in t-1 ----
+        if (a.cnts && blockIdx.x == 0 && t > 0)  // that delta's counters restart at zero
+            for (uint32_t sl = tid; sl < a.nslots; sl += kThreads) a.cnts[3 * sl + 1 + (par ^ 1)] = BufCounters{0, 0, 0};
         {
             const uint32_t clear_rows = t > 0 ? a.slot_rows : 0u;
             const uint32_t units = a.prod_rows + clear_rows;
@@ -156,7 +165,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_closure_persistent(PersistArgs 
                 if (u < a.prod_rows) {
                     plan::plan_row(u, prods, a.nprods, slots, t, st, st->pitem_count[par],
                                    a.items + (size_t)(2 * par) * a.list_cap, a.list_cap, a.tpb, a.prod_seen, 0,
-                                   S.plan[warp].cnt, S.plan[warp].bnd);
+                                   psel, S.plan[warp].cnt, S.plan[warp].bnd);
                 } else {
                     clear_delta_row(slots, a.nslots, u - a.prod_rows, par ^ 1);
                 }
@@ -179,7 +188,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_closure_persistent(PersistArgs 
                 __syncthreads();
                 if (idx >= n0) break;
                 tiled::process_item<false>(S.prod, items[idx], prods, slots, t, &st->pchanged[par], a.qt.changed,
-                                           phase, timed_out, ctr);
+                                           phase, timed_out, ctr, a.cnts);
             }
             if constexpr (kHasM4R) {
                 const uint32_t n1 = st->pitem_count[par][1];
@@ -190,7 +199,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_closure_persistent(PersistArgs 
                     __syncthreads();
                     if (idx >= n1) break;
                     tiled::process_item<true>(S.prod, items[a.list_cap + idx], prods, slots, t,
-                                              &st->pchanged[par], a.qt.changed, phase, timed_out, ctr);
+                                              &st->pchanged[par], a.qt.changed, phase, timed_out, ctr, a.cnts);
                 }
             }
         }
@@ -278,7 +287,9 @@ cudaError_t launch_closure_persistent(int has_m4r, int grid, const ProdDesc *pro
                                       uint32_t prod_rows, const MatSlot *slots, uint32_t nslots, uint32_t slot_rows,
                                       IterState *st, uint64_t *items, size_t list_cap, uint32_t *prod_seen,
                                       const QueryTrack &qt, int tpb, unsigned long long *phase_log,
-                                      uint32_t phase_log_iters, cudaStream_t s) {
+                                      uint32_t phase_log_iters, BufCounters *cnts, uint8_t *choice,
+                                      const SelectorParams *sel, SelLogRow *sel_log, uint32_t sel_log_iters,
+                                      cudaStream_t s) {
     PersistArgs a;
     a.prods = prods;
     a.nprods = nprods;
@@ -294,6 +305,11 @@ cudaError_t launch_closure_persistent(int has_m4r, int grid, const ProdDesc *pro
     a.tpb = tpb;
     a.phase_log = phase_log;
     a.phase_log_iters = phase_log_iters;
+    a.cnts = cnts;
+    a.choice = choice;
+    a.sel = sel;
+    a.sel_log = sel_log;
+    a.sel_log_iters = sel_log_iters;
     void *args[] = {&a};
     if (has_m4r)
         return cudaLaunchCooperativeKernel((const void *)k_closure_persistent<true>, dim3(grid), dim3(kThreads), args,

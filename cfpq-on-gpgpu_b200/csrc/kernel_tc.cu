@@ -105,7 +105,7 @@ __device__ __forceinline__ void tmem_ld64(uint32_t taddr, uint32_t (&r)[64]) {
 __global__ void __launch_bounds__(kThreads, 1)
     k_product_tc(const ProdDesc *__restrict__ prods, const MatSlot *__restrict__ slots, IterState *st,
                  const uint64_t *__restrict__ items_all, size_t list_cap, uint32_t *qchanged,
-                 const uint8_t *__restrict__ xp, const uint8_t *__restrict__ xq) {
+                 const uint8_t *__restrict__ xp, const uint8_t *__restrict__ xq, BufCounters *cnts) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     TcSmem &S = *reinterpret_cast<TcSmem *>(smem_raw);
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -265,6 +265,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         // ---- epilogue ----
         bool any_new = false;
         if (nk > 0) {
+            uint32_t tile_new[4] = {0, 0, 0, 0};
             const uint32_t h = warp >> 2, q = warp & 3;
             const uint32_t m = 128 * h + 32 * q + lane;  // output row within the 256-row block
             const uint32_t ti = ti0 + (m >> 6), r = m & 63;
@@ -293,18 +294,14 @@ __global__ void __launch_bounds__(kThreads, 1)
                         }
                     }
                 }
-                const uint32_t tile_new = __reduce_add_sync(kFull, newcnt);  // the warp's 32 rows share (ti, tj)
-                if (tile_new) {
-                    any_new = true;
-                    if (lane == 0) {
-                        atomicAdd(C.nnz + (size_t)ti * T + tj, tile_new);
-                        atomicOr(C.occ + (size_t)ti * C.ow + (tj >> 5), 1u << (tj & 31));
-                        if (D.bits) {
-                            atomicAdd(D.nnz + (size_t)ti * T + tj, tile_new);
-                            atomicOr(D.occ + (size_t)ti * D.ow + (tj >> 5), 1u << (tj & 31));
-                        }
-                    }
-                }
+                tile_new[jt] = __reduce_add_sync(kFull, newcnt);  // the warp's 32 rows share (ti, tj)
+            }
+            any_new = (tile_new[0] | tile_new[1] | tile_new[2] | tile_new[3]) != 0;
+            if (any_new && ti < T) {  // lane j: tile tj0 + j (populations, occupancy, buffer counters)
+                const uint32_t mine = lane == 0 ? tile_new[0] : lane == 1 ? tile_new[1] : lane == 2 ? tile_new[2]
+                                    : lane == 3 ? tile_new[3] : 0u;
+                tiles_gain(C, ti, tj0, mine, cnts ? cnts + 3 * pd.head : nullptr);
+                if (D.bits) tiles_gain(D, ti, tj0, mine, cnts ? cnts + 3 * pd.head + 1 + ((iter & 1) ^ 1) : nullptr);
             }
         }
         if (any_new && lane == 0) {
@@ -343,9 +340,9 @@ int product_tc_blocks_per_sm() {
 
 cudaError_t launch_product_tc(const ProdDesc *d_prods, const MatSlot *d_slots, IterState *d_st,
                               const uint64_t *d_items, size_t list_cap, uint32_t *d_qchanged, int grid,
-                              const uint8_t *xp, const uint8_t *xq, cudaStream_t s) {
+                              const uint8_t *xp, const uint8_t *xq, BufCounters *cnts, cudaStream_t s) {
     k_product_tc<<<grid, kThreads, sizeof(TcSmem), s>>>(d_prods, d_slots, d_st, d_items, list_cap, d_qchanged, xp,
-                                                        xq);
+                                                        xq, cnts);
     return cudaGetLastError();
 }
 

@@ -104,6 +104,31 @@ __global__ void k_tile_stats(DevMat m) {
     if (lane == 0) m.occ[(size_t)ti * m.ow + w] = word;
 }
 
+// Seeded random matrix (autotuner inputs): bit (r, c) set with probability
+// thresh / 2^32 from a hash of (seed, r, c); padding rows/columns stay zero.
+__device__ __forceinline__ uint32_t hash3(uint64_t seed, uint32_t r, uint32_t c) {
+    uint64_t x = seed ^ ((uint64_t)r << 32 | c);
+    x += 0x9E3779B97F4A7C15ULL;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBULL;
+    return (uint32_t)((x ^ (x >> 31)) >> 32);
+}
+
+__global__ void k_random_fill(DevMat m, uint32_t thresh, uint64_t seed) {
+    const size_t total = (size_t)m.T * m.T * 64;
+    for (size_t x = blockIdx.x * (size_t)blockDim.x + threadIdx.x; x < total; x += (size_t)gridDim.x * blockDim.x) {
+        const size_t tile = x >> 6;
+        const uint32_t row = (uint32_t)(tile / m.T) * 64 + (uint32_t)(x & 63), tj = (uint32_t)(tile % m.T);
+        uint64_t w = 0;
+        if (row < m.n)
+            for (uint32_t b = 0; b < 64; ++b) {
+                const uint32_t c = tj * 64 + b;
+                if (c < m.n && hash3(seed, row, c) < thresh) w |= 1ULL << b;
+            }
+        m.bits[x] = w;
+    }
+}
+
 // Row-major staging (n rows x T words) -> tiles.
 __global__ void k_rows_to_tiles(DevMat m, const uint64_t *__restrict__ rows) {
     const size_t total = (size_t)m.T * m.T * 64;
@@ -276,12 +301,12 @@ constexpr int kPlanThreads = 128;
 __global__ void __launch_bounds__(kPlanThreads)
     k_plan(const ProdDesc *__restrict__ prods, uint32_t nprods, uint32_t row_begin, uint32_t total_rows,
            const MatSlot *__restrict__ slots, IterState *st, uint64_t *__restrict__ items_all, size_t list_cap,
-           int tpb, uint32_t *prod_seen, int tc_mode) {
+           int tpb, uint32_t *prod_seen, int tc_mode, PlanSelect ps) {
     __shared__ plan::WarpArea<plan::kPlanMaxBlocks> areas[kPlanThreads / 32];
     const uint32_t gw = row_begin + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     if (gw >= total_rows || !st->active) return;
     plan::plan_row(gw, prods, nprods, slots, st->iter, st, st->item_count, items_all, list_cap, tpb, prod_seen,
-                   tc_mode, areas[threadIdx.x >> 5].cnt, areas[threadIdx.x >> 5].bnd);
+                   tc_mode, ps, areas[threadIdx.x >> 5].cnt, areas[threadIdx.x >> 5].bnd);
 }
 
 // ---- closure iteration: advance + end ----------------------------------------
@@ -294,7 +319,8 @@ __global__ void __launch_bounds__(kPlanThreads)
 // loop has stopped only clears (the host may run a few iterations
 // speculatively between checks).
 __global__ void k_advance_end(const MatSlot *__restrict__ slots, uint32_t nslots, uint32_t total_rows,
-                              IterState *st, QueryTrack qt, cudaGraphConditionalHandle handle, int use_handle) {
+                              IterState *st, QueryTrack qt, cudaGraphConditionalHandle handle, int use_handle,
+                              BufCounters *cnts) {
     const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (gw < total_rows && nslots > 0) clear_delta_row(slots, nslots, gw, st->iter & 1);
 
@@ -307,6 +333,11 @@ __global__ void k_advance_end(const MatSlot *__restrict__ slots, uint32_t nslots
     __syncthreads();
     if (!s_last) return;
     __threadfence();
+    if (cnts) {  // the delta just cleared starts the next iteration empty
+        const uint32_t b = 1 + (st->iter & 1);
+        for (uint32_t sl = threadIdx.x; sl < nslots; sl += blockDim.x) cnts[3 * sl + b] = BufCounters{0, 0, 0};
+    }
+    __syncthreads();
     if (threadIdx.x == 0) {
         st->blocks_done = 0;
         s_run = st->active;
@@ -388,6 +419,15 @@ cudaError_t launch_occ_rebuild(const DevMat &m, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+cudaError_t launch_random_fill(const DevMat &m, double density, uint64_t seed, cudaStream_t s) {
+    if (m.T == 0) return cudaSuccess;
+    const double t = density <= 0 ? 0.0 : (density >= 1 ? 4294967295.0 : density * 4294967296.0);
+    k_random_fill<<<capped_grid((size_t)m.T * m.T * 64, 256, 1u << 16), 256, 0, s>>>(m, (uint32_t)t, seed);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return launch_occ_rebuild(m, s);
+}
+
 cudaError_t launch_rows_to_tiles(const DevMat &m, const uint64_t *d_rows, cudaStream_t s) {
     if (m.T == 0) return cudaSuccess;
     if (m.perm) {
@@ -454,18 +494,21 @@ cudaError_t launch_merge_or(const DevMat &dst, const DevMat &src, uint32_t *d_fl
 
 cudaError_t launch_plan(const ProdDesc *d_prods, uint32_t nprods, uint32_t row_begin, uint32_t row_end,
                         const MatSlot *d_slots, IterState *d_st, uint64_t *d_items, size_t list_cap,
-                        int tiles_per_block, uint32_t *d_prod_seen, int tc_mode, cudaStream_t s) {
+                        int tiles_per_block, uint32_t *d_prod_seen, int tc_mode, const uint8_t *d_choice,
+                        cudaStream_t s, const PlanSelect *sel) {
     if (row_end <= row_begin || nprods == 0) return cudaSuccess;
+    PlanSelect ps = sel ? *sel : PlanSelect{nullptr, nullptr, nullptr, const_cast<uint8_t *>(d_choice), nullptr, 0};
     k_plan<<<grid_for((size_t)(row_end - row_begin) * 32, kPlanThreads), kPlanThreads, 0, s>>>(
-        d_prods, nprods, row_begin, row_end, d_slots, d_st, d_items, list_cap, tiles_per_block, d_prod_seen, tc_mode);
+        d_prods, nprods, row_begin, row_end, d_slots, d_st, d_items, list_cap, tiles_per_block, d_prod_seen, tc_mode,
+        ps);
     return cudaGetLastError();
 }
 
 cudaError_t launch_advance_end(const MatSlot *d_slots, uint32_t nslots, uint32_t total_rows, IterState *d_st,
                                const QueryTrack &qt, cudaGraphConditionalHandle handle, int use_handle,
-                               cudaStream_t s) {
+                               BufCounters *d_cnts, cudaStream_t s) {
     k_advance_end<<<grid_for((size_t)total_rows * 32, 256), 256, 0, s>>>(d_slots, nslots, total_rows, d_st, qt,
-                                                                         handle, use_handle);
+                                                                         handle, use_handle, d_cnts);
     return cudaGetLastError();
 }
 

@@ -20,6 +20,8 @@ cudaError_t launch_rows_to_tiles(const DevMat &m, const uint64_t *d_rows, cudaSt
 cudaError_t launch_tiles_to_rows(const DevMat &m, uint64_t *d_rows, cudaStream_t s);
 cudaError_t launch_copy_matrix(const DevMat &dst, const DevMat &src, cudaStream_t s);
 cudaError_t launch_clear_matrix(const DevMat &m, cudaStream_t s);
+// Seeded random matrix with the given bit density (not for ordered matrices).
+cudaError_t launch_random_fill(const DevMat &m, double density, uint64_t seed, cudaStream_t s);
 // Clear the matrices of d_tab (occupied tiles only; relies on the occupancy invariant).
 cudaError_t launch_clear_rows(const MatRows *d_tab, uint32_t nmats, uint32_t total_rows, cudaStream_t s);
 
@@ -37,24 +39,29 @@ cudaError_t launch_merge_or(const DevMat &dst, const DevMat &src, uint32_t *d_fl
 // Closure iteration
 cudaError_t launch_plan(const ProdDesc *d_prods, uint32_t nprods, uint32_t row_begin, uint32_t row_end,
                         const MatSlot *d_slots, IterState *d_st, uint64_t *d_items, size_t list_cap,
-                        int tiles_per_block, uint32_t *d_prod_seen, int tc_mode, cudaStream_t s);
-// (tc_mode 0 plans the word-level products of the row range, 1 the tensor-core ones.)
+                        int tiles_per_block, uint32_t *d_prod_seen, int tc_mode, const uint8_t *d_choice,
+                        cudaStream_t s, const PlanSelect *sel = nullptr);
+// (tc_mode 0 plans the word-level products of the row range, 1 the tensor-core
+// ones; the variant of product p is d_choice[p], or its descriptor's when
+// null; with sel, the word-level plan decides the variants, PlanSelect.)
 // Tiled product over item list `m4r` (0: LOP3 inner loop, 1: Four Russians
 // inner loop); items of list l start at d_items + l * list_cap.
 cudaError_t launch_product_tiled(int m4r, const ProdDesc *d_prods, const MatSlot *d_slots, IterState *d_st,
                                  const uint64_t *d_items, size_t list_cap, uint32_t *d_qchanged, int grid,
-                                 cudaStream_t s);
+                                 BufCounters *d_cnts, cudaStream_t s);
 // Tensor-core product over item list 2 (d_items + 2 * list_cap) of one
 // product whose operands were expanded into xp (P by rows) and xq (Q
 // transposed); one CTA per SM (it owns all 512 TMEM columns).
 cudaError_t launch_product_tc(const ProdDesc *d_prods, const MatSlot *d_slots, IterState *d_st,
                               const uint64_t *d_items, size_t list_cap, uint32_t *d_qchanged, int grid,
-                              const uint8_t *xp, const uint8_t *xq, cudaStream_t s);
+                              const uint8_t *xp, const uint8_t *xq, BufCounters *d_cnts, cudaStream_t s);
 int product_tc_blocks_per_sm();
 // Operand expansion for the tensor-core product (4 KiB of 0/1 bytes per tile,
 // canonical layout): side 0 = P of product p by rows, side 1 = Q transposed.
 cudaError_t launch_expand_operand(const ProdDesc *d_prods, uint32_t p, uint32_t T, const MatSlot *d_slots,
-                                  const IterState *d_st, int side, uint8_t *out, int num_sms, cudaStream_t s);
+                                  const IterState *d_st, int side, uint8_t *out, int num_sms,
+                                  const uint8_t *d_choice, cudaStream_t s);
+// (does nothing when d_choice is given and d_choice[p] is not the tensor-core variant)
 // Closes a tensor-core product's item list (counts it, resets the counters).
 cudaError_t launch_reset_list(IterState *st, int list, cudaStream_t s);
 int product_lop3_tiles_per_block();
@@ -66,7 +73,7 @@ int product_tiled_blocks_per_sm(int m4r);
 // iteration: changed flag, iteration index, loop condition, per-query records.
 cudaError_t launch_advance_end(const MatSlot *d_slots, uint32_t nslots, uint32_t total_rows, IterState *d_st,
                                const QueryTrack &qt, cudaGraphConditionalHandle handle, int use_handle,
-                               cudaStream_t s);
+                               BufCounters *d_cnts, cudaStream_t s);
 cudaError_t launch_mark_start(IterState *d_st, cudaStream_t s);
 // Persistent closure (word-level variants only): the whole fixpoint in one
 // cooperative launch of `grid` CTAs (at most persistent_blocks_per_sm() per
@@ -76,7 +83,26 @@ cudaError_t launch_closure_persistent(int has_m4r, int grid, const ProdDesc *pro
                                       uint32_t prod_rows, const MatSlot *slots, uint32_t nslots, uint32_t slot_rows,
                                       IterState *st, uint64_t *items, size_t list_cap, uint32_t *prod_seen,
                                       const QueryTrack &qt, int tpb, unsigned long long *phase_log,
-                                      uint32_t phase_log_iters, cudaStream_t s);
+                                      uint32_t phase_log_iters, BufCounters *cnts, uint8_t *choice,
+                                      const SelectorParams *sel, SelLogRow *sel_log, uint32_t sel_log_iters,
+                                      cudaStream_t s);
+// (sel non-null: every iteration starts with a selection phase writing choice[];
+// else choice[] is fixed for the closure)
+
+// Variant selection (kernel_select.cu): one warp per product per iteration.
+cudaError_t launch_select(const ProdDesc *d_prods, uint32_t nprods, const BufCounters *d_cnts, const IterState *d_st,
+                          const SelectorParams *d_params, uint8_t *d_choice, const uint8_t *d_tc_ok,
+                          SelLogRow *d_log, uint32_t log_iters, cudaStream_t s);
+// Buffer counters at closure start (current matrices measured, deltas zero).
+cudaError_t launch_counters_init(const MatSlot *d_slots, uint32_t nslots, BufCounters *d_cnts, cudaStream_t s);
+cudaError_t launch_fill_choice(uint8_t *d_choice, uint32_t n, uint8_t v, cudaStream_t s);
+
+// Cost-model training and inference (kernel_mlp.cu); weights: kSelWeights floats.
+cudaError_t mlp_loss_grad(const float *d_w, const float *d_x, const float *d_y, const float *d_m, uint32_t n,
+                          float inv_msum, float *d_grad, float *d_loss, cudaStream_t s);
+cudaError_t mlp_adam_step(float *d_w, float *d_grad, float *d_m, float *d_v, float lr, float wd, uint32_t step,
+                          cudaStream_t s);
+cudaError_t mlp_predict(const float *d_w, const float *d_x, uint32_t n, float *d_out, cudaStream_t s);
 // Calibration: logic instructions per second of the whole GPU (d_out: 8*256*num_sms words).
 cudaError_t measure_logic_rate(int num_sms, uint32_t *d_out, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1,
                                double *ops_per_s, double *ms_out);

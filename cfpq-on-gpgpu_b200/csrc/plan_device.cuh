@@ -4,6 +4,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "select_device.cuh"
 
 namespace cfpq {
 namespace plan {
@@ -60,8 +61,8 @@ struct WarpArea {
 __device__ __forceinline__ void plan_row(uint32_t gw, const ProdDesc *__restrict__ prods, uint32_t nprods,
                                          const MatSlot *__restrict__ slots, uint32_t iter, IterState *st,
                                          uint32_t *item_count, uint64_t *__restrict__ items_all, size_t list_cap,
-                                         int tpb, uint32_t *prod_seen, int tc_mode, uint32_t *cnt,
-                                         uint16_t (*bnd)[kMaxChunksPerBlock - 1]) {
+                                         int tpb, uint32_t *prod_seen, int tc_mode, const PlanSelect &ps,
+                                         uint32_t *cnt, uint16_t (*bnd)[kMaxChunksPerBlock - 1]) {
     const uint32_t lane = threadIdx.x & 31;
     uint32_t lo = 0, hi = nprods;  // product: last p with row_start <= gw
     while (hi - lo > 1) {
@@ -70,9 +71,26 @@ __device__ __forceinline__ void plan_row(uint32_t gw, const ProdDesc *__restrict
     }
     const ProdDesc pd = prods[lo];
     if (pd.term == 1 && iter == 0) return;  // first iteration: delta(A) = A, one term covers A*B
-    const bool tc = pd.variant == 4;                         // CFPQ_VARIANT_TC
+    uint32_t variant;  // this iteration's variant of the product
+    if (ps.sel && !tc_mode) {
+        float f[kSelFeatures], pred[kSelOutputs] = {0.f, 0.f, 0.f};
+        uint32_t flags = 0;
+        variant = sel::select_product(pd, ps.cnts, iter, ps.sel, ps.tc_ok && ps.tc_ok[lo], f, pred, &flags);
+        if (gw == pd.row_start && (threadIdx.x & 31) == 0) {
+            ps.choice[lo] = (uint8_t)variant;
+            if (ps.log && iter < ps.log_iters) {
+                SelLogRow &r = ps.log[(size_t)iter * nprods + lo];
+                for (int i = 0; i < kSelFeatures; ++i) r.f[i] = f[i];
+                for (int o = 0; o < kSelOutputs; ++o) r.pred[o] = pred[o];
+                r.choice = variant | flags;
+            }
+        }
+    } else {
+        variant = ps.choice ? ps.choice[lo] : pd.variant;
+    }
+    const bool tc = variant == 4;                                // CFPQ_VARIANT_TC
     if (tc != (tc_mode != 0)) return;  // word-level and tensor-core products are planned by separate launches
-    const uint32_t list = tc ? 2u : (pd.variant == 3 ? 1u : 0u);  // CFPQ_VARIANT_M4R
+    const uint32_t list = tc ? 2u : (variant == 3 ? 1u : 0u);   // CFPQ_VARIANT_M4R
     if (tc) tpb = 4;
     const uint32_t rows_per_item = tc ? 4u : 1u;
     uint64_t *items = items_all + list * list_cap;

@@ -77,7 +77,7 @@ template <bool kM4R, class Smem>
 __device__ __forceinline__ void process_item(Smem &S, uint64_t it, const ProdDesc *__restrict__ prods,
                                              const MatSlot *__restrict__ slots, uint32_t iter, uint32_t *changed,
                                              uint32_t *qchanged, uint32_t &phase, bool &timed_out,
-                                             ItemCounters &ctr) {
+                                             ItemCounters &ctr, BufCounters *cnts) {
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     unsigned long long &triples = ctr.triples, &staged = ctr.staged, &outw = ctr.outw, &neww = ctr.neww;
     const ProdDesc pd = prods[item_prod(it)];
@@ -339,10 +339,9 @@ __device__ __forceinline__ void process_item(Smem &S, uint64_t it, const ProdDes
         prev[k] = (av[k] & ~seen[k]) ? atomicOr(reinterpret_cast<unsigned long long *>(C.bits + off[k]),
                                                 (unsigned long long)av[k])
                                      : ~0ULL;
-    bool any_new = false;
+    uint32_t tile_new[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-        const uint32_t tj = tj0 + 4 * warp + j;
         uint32_t newcnt = 0;
 #pragma unroll
         for (int rr = 0; rr < 2; ++rr) {
@@ -354,18 +353,14 @@ __device__ __forceinline__ void process_item(Smem &S, uint64_t it, const ProdDes
                 if (D.bits) atomicOr(reinterpret_cast<unsigned long long *>(D.bits + off[k]), (unsigned long long)nw);
             }
         }
-        const uint32_t tile_new = __reduce_add_sync(kFull, newcnt);
-        if (tile_new) {
-            any_new = true;
-            if (lane == 0) {
-                atomicAdd(C.nnz + (size_t)ti * T + tj, tile_new);
-                atomicOr(C.occ + (size_t)ti * C.ow + (tj >> 5), 1u << (tj & 31));
-                if (D.bits) {
-                    atomicAdd(D.nnz + (size_t)ti * T + tj, tile_new);
-                    atomicOr(D.occ + (size_t)ti * D.ow + (tj >> 5), 1u << (tj & 31));
-                }
-            }
-        }
+        tile_new[j] = __reduce_add_sync(kFull, newcnt);  // the warp's rows of tile tj0 + 4*warp + j
+    }
+    const bool any_new = (tile_new[0] | tile_new[1] | tile_new[2] | tile_new[3]) != 0;
+    if (any_new) {  // lane j updates tile j of the warp (populations, occupancy, buffer counters)
+        const uint32_t mine = lane == 0 ? tile_new[0] : lane == 1 ? tile_new[1] : lane == 2 ? tile_new[2]
+                            : lane == 3 ? tile_new[3] : 0u;
+        tiles_gain(C, ti, tj0 + 4 * warp, mine, cnts ? cnts + 3 * pd.head : nullptr);
+        if (D.bits) tiles_gain(D, ti, tj0 + 4 * warp, mine, cnts ? cnts + 3 * pd.head + 1 + ((iter & 1) ^ 1) : nullptr);
     }
     if (any_new && lane == 0) {
         *changed = 1u;

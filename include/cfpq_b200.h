@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define CFPQ_B200_ABI_VERSION 1
+#define CFPQ_B200_ABI_VERSION 2
 
 typedef enum cfpq_status {
     CFPQ_OK = 0,
@@ -87,7 +87,7 @@ typedef struct cfpq_closure_opts {
                                    product is word-level, else the CUDA-graph loop
                                 2 (CFPQ_LOOP_GRAPH)  one CUDA graph with a device-side
                                    while condition, one node per kernel */
-    int32_t log_products;    /* 1 = record a per-product timing log (see cfpq_product_log) */
+    int32_t log_products;    /* CFPQ_LOG_* flags (cfpq_last_kernel_profile, cfpq_product_log) */
     int32_t reserved[3];
 } cfpq_closure_opts;
 
@@ -124,6 +124,7 @@ int cfpq_calibrate(cfpq_ctx *ctx, cfpq_calibration *out);
  * (advance_*); iter_end_* stay zero. */
 #define CFPQ_LOG_KERNELS 1
 #define CFPQ_LOG_PRODUCTS 2
+#define CFPQ_LOG_SELECTION 4 /* AUTO closures: keep the selector's features and choices (cfpq_product_log) */
 typedef struct cfpq_kernel_profile {
     double plan_ms, product_ms, advance_ms, iter_end_ms;
     uint64_t plan_launches, product_launches, advance_launches, iter_end_launches;
@@ -302,25 +303,106 @@ int cfpq_closure_batch(cfpq_ctx *ctx, const cfpq_query *queries, size_t nqueries
                        const cfpq_closure_opts *opts, cfpq_closure_stats *stats,
                        uint32_t *iterations_out, double *done_ms_out);
 
-/* Per-product log of the last cfpq_closure / cfpq_closure_batch call with
- * opts->log_products = 1: one record per work-item group.  Returns the number
- * of records available; copies at most cap records.  No reference
- * counterpart (the reference only times the whole closure, Grammar.h:53-80). */
+/* Per-product log of the last cfpq_closure / cfpq_closure_batch call run with
+ * opts->log_products & CFPQ_LOG_PRODUCTS (engine driver): one record per
+ * (iteration, product term).  In that mode the iterations run from the host;
+ * each term first runs once with the selected variant (the real work), then
+ * is timed again with every candidate variant on the same state (bits only
+ * ever get added, so the re-runs change nothing): usec[v] is the device time
+ * of variant v (CUDA events around its plan and product launches, tensor
+ * cores including operand expansion), or < 0 where v was not timed.  These
+ * records are the cost model's training data and the ground truth of its
+ * regret.  Returns the number of records available; copies at most cap.
+ * No reference counterpart (the reference only times the whole closure,
+ * cfpq-cpp/Grammar.h:53-80). */
+#define CFPQ_SEL_FEATURES 16
+#define CFPQ_SEL_OUTPUTS 3 /* LOP3, M4R, TC */
 typedef struct cfpq_product_record {
     uint32_t iteration;
     uint32_t query;
     uint32_t rule;
     uint32_t term;          /* 0: delta(body1) * body2, 1: body1 * delta(body2) */
     uint32_t n;
-    uint32_t variant;
-    uint64_t p_tiles;       /* occupied tiles of the left operand */
-    uint64_t q_tiles;       /* occupied tiles of the right operand */
-    uint64_t c_tiles;       /* occupied tiles of the head before the product */
-    uint64_t tile_triples;  /* tile products executed */
-    float usec;             /* device time of the product (CUDA events) */
-    float reserved;
+    uint32_t variant;       /* variant that did the real work (the selector's choice) */
+    uint32_t flags;         /* bit 8: the MLP chose; bit 9: the MLP ran but was not confident */
+    uint32_t reserved;
+    float features[CFPQ_SEL_FEATURES];  /* the selector's feature vector (kernel_select.cu) */
+    float predicted[CFPQ_SEL_OUTPUTS];  /* MLP prediction, log microseconds (0 if it did not run) */
+    float usec[5];                      /* index = cfpq_variant */
 } cfpq_product_record;
 size_t cfpq_product_log(cfpq_ctx *ctx, cfpq_product_record *out, size_t cap);
+
+/* ---- Variant selector -------------------------------------------------------
+ * With opts->variant = CFPQ_VARIANT_AUTO the engine chooses, on the device and
+ * for every product term in every iteration, which exact variant runs it
+ * (LOP3, M4R or TC).  The choice never changes a result.  No reference
+ * counterpart: the reference binds one Matrix implementation per executable
+ * (cfpq-cpp/Grammar.h:23). */
+#define CFPQ_SELECT_FIXED 0     /* AUTO behaves like LOP3 */
+#define CFPQ_SELECT_HEURISTIC 1 /* autotuned density thresholds */
+#define CFPQ_SELECT_MLP 2       /* cost model, heuristic when it is not confident */
+typedef struct cfpq_selector_config {
+    int32_t mode;
+    uint32_t allowed;       /* bit v set: variant v may be chosen (bits 2, 3, 4) */
+    uint32_t tc_min_tiles;  /* tensor cores only for n >= 64 * tc_min_tiles */
+    float tc_min_occ;       /* TC: minimum occupied-tile fraction of P */
+    float tc_min_pop;       /* TC: minimum mean tile population / 4096 of P and Q */
+    float m4r_min_dense;    /* M4R: minimum fraction of dense P tiles (population > 96) */
+    float conf_margin;      /* MLP: best prediction ahead of the second by this (log us) */
+    float range_margin;     /* MLP: features within the training range widened by this fraction */
+    uint32_t min_tiles;     /* selection runs only in closures with a term of n >= 64 * min_tiles;
+                               smaller closures are latency-bound and run LOP3 throughout */
+} cfpq_selector_config;
+int cfpq_selector_configure(cfpq_ctx *ctx, const cfpq_selector_config *cfg);
+int cfpq_selector_get_config(cfpq_ctx *ctx, cfpq_selector_config *cfg);
+
+/* Cost model weights: W1[16][64], b1[64], W2[64][64], b2[64], W3[64][3], b3[3]
+ * (row-major, input index first), then the training range of the features
+ * (lo[16], hi[16]).  cfpq_selector_weight_count() floats in total. */
+size_t cfpq_selector_weight_count(void);
+int cfpq_selector_set_weights(cfpq_ctx *ctx, const float *w, size_t count);
+int cfpq_selector_get_weights(cfpq_ctx *ctx, float *w, size_t count); /* CFPQ_ERR_INVALID if untrained */
+
+/* Train the cost model on the GPU (hand-written forward/backward kernels,
+ * full-batch Adam) from product records: targets log(usec[v]) of the timed
+ * variants, loss = mean squared error over timed entries.  Sets the weights
+ * and the feature ranges; does not change the mode. */
+typedef struct cfpq_train_opts {
+    int32_t epochs;         /* default 2000 */
+    float learning_rate;    /* default 3e-3 */
+    float weight_decay;     /* default 1e-4 */
+    uint32_t seed;          /* weight initialisation */
+    int32_t keep_weights;   /* 1: continue from the current weights */
+} cfpq_train_opts;
+typedef struct cfpq_train_report {
+    float loss_first, loss_last;
+    uint32_t samples, epochs;
+    double ms;
+} cfpq_train_report;
+int cfpq_selector_train(cfpq_ctx *ctx, const cfpq_product_record *recs, size_t count, const cfpq_train_opts *opts,
+                        cfpq_train_report *report);
+
+/* The training kernels' loss and gradient for explicit weights (count =
+ * cfpq_selector_weight_count() - 32 floats, no feature ranges) on samples
+ * x[n][16], targets y[n][3], mask m[n][3] (host arrays): the gradient check. */
+int cfpq_selector_loss_grad(cfpq_ctx *ctx, const float *weights, const float *x, const float *y, const float *m,
+                            size_t n, float *loss, float *grad);
+/* Predictions of the current weights for x[n][16] (host), out[n][3]. */
+int cfpq_selector_predict(cfpq_ctx *ctx, const float *x, size_t n, float *out);
+
+/* Autotuner: times C |= A * B with LOP3, M4R and TC on seeded random
+ * matrices (every tile populated) for the given sizes and densities, finds the
+ * crossovers and stores them in the context's selector thresholds (and in
+ * *result).  timings (optional, [nsizes][ndensities][3] ms, < 0 = not run). */
+typedef struct cfpq_autotune_opts {
+    const uint32_t *sizes;
+    size_t nsizes;
+    const float *densities;
+    size_t ndensities;
+    uint32_t reps;
+    uint32_t seed;
+} cfpq_autotune_opts;
+int cfpq_autotune(cfpq_ctx *ctx, const cfpq_autotune_opts *opts, cfpq_selector_config *result, float *timings);
 
 /* Phase timestamps of the last closure that ran as one persistent kernel
  * (use_graph = CFPQ_LOOP_DEVICE, every product word-level): per iteration

@@ -29,7 +29,10 @@ def test_library_exports_every_declared_function(pkg):
 
 def test_abi_version(pkg):
     lib = pkg.capi.load_library()
-    assert lib.cfpq_abi_version() == 1
+    header = open(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include",
+                               "cfpq_b200.h")).read()
+    declared = int(re.search(r"#define CFPQ_B200_ABI_VERSION (\d+)", header).group(1))
+    assert lib.cfpq_abi_version() == declared
 
 
 def test_null_arguments_are_errors_not_crashes(pkg):

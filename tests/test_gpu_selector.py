@@ -1,0 +1,171 @@
+"""Variant selector on the GPU: every selection mode gives the oracle's
+closure, the cost model's kernels match the CPU oracle (oracle/mlp_ref.py),
+the product timing log and the autotuner work."""
+import numpy as np
+import pytest
+
+import mlp_ref
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture
+def sctx(pkg):
+    """A context of its own: selector settings do not leak between tests."""
+    c = pkg.capi.Context(0)
+    yield c
+    c.close()
+
+
+def _random_cnf(pkg, n=900, edges=2000, seed=11):
+    labels = ["x", "y", "z"]
+    g = pkg.workloads.uniform_graph(n, edges, labels, seed)
+    gram = pkg.workloads.random_cnf(8, 20, labels, seed)
+    return pkg.workloads.Workload("random_cnf", gram, g, {})
+
+
+def _expected(oracle, wl, tmp_path):
+    gp, rp = str(tmp_path / "g.txt"), str(tmp_path / "r.txt")
+    wl.write(gp, rp)
+    with oracle.Problem(gp, rp) as p:
+        p.closure(oracle.M4RM, 0)
+        return p.results()
+
+
+def _random_weights(seed=3):
+    rng = np.random.default_rng(seed)
+    w = rng.normal(0, 0.3, mlp_ref.N_WEIGHTS).astype(np.float32)
+    lo = np.full(16, -10.0, np.float32)
+    hi = np.full(16, 10.0, np.float32)
+    return np.concatenate([w, lo, hi])
+
+
+def test_loss_and_gradient_match_cpu_oracle(sctx):
+    rng = np.random.default_rng(1)
+    n = 203  # not a multiple of the kernel's 64 samples per block
+    w = rng.normal(0, 0.3, mlp_ref.N_WEIGHTS).astype(np.float32)
+    x = rng.random((n, 16)).astype(np.float32)
+    y = rng.normal(2.0, 1.0, (n, 3)).astype(np.float32)
+    m = (rng.random((n, 3)) < 0.7).astype(np.float32)
+    loss, grad = sctx.selector_loss_grad(w, x, y, m)
+    ref_loss, ref_grad = mlp_ref.loss_grad(w.astype(np.float64), x, y, m)
+    assert loss == pytest.approx(ref_loss, rel=1e-4)
+    # float32 sums in a different order: 1e-3 of the largest gradient entry
+    assert np.allclose(grad, ref_grad, rtol=1e-3, atol=1e-3 * np.abs(ref_grad).max())
+
+
+def test_training_fits_and_predicts_like_the_oracle(pkg, sctx):
+    rng = np.random.default_rng(2)
+    n = 600
+    recs = np.zeros(n, dtype=pkg.capi.PRODUCT_RECORD_DTYPE)
+    f = rng.random((n, 16)).astype(np.float32)
+    recs["features"] = f
+    # three smooth "variant costs" of the features, in microseconds
+    t = np.stack([20 + 300 * f[:, 2] * f[:, 4], 25 + 120 * f[:, 2] * f[:, 4], 60 + 40 * f[:, 2]], axis=1)
+    recs["usec"][:, 2:5] = t
+    recs["usec"][:, :2] = -1
+    rep = sctx.selector_train(recs, epochs=1500, learning_rate=3e-3, seed=5)
+    assert rep["samples"] == n
+    assert rep["loss_last"] < rep["loss_first"] / 10
+    w = sctx.selector_weights()
+    pred = sctx.selector_predict(f)
+    ref = mlp_ref.forward(w[:mlp_ref.N_WEIGHTS].astype(np.float64), f)
+    assert np.allclose(pred, ref, rtol=1e-4, atol=1e-4)
+    # the model ranks the variants like the true costs on most samples
+    agree = (np.argmin(pred, axis=1) == np.argmin(np.log(t), axis=1)).mean()
+    assert agree > 0.85, agree
+    # feature range = training range
+    assert np.allclose(w[mlp_ref.N_WEIGHTS:mlp_ref.N_WEIGHTS + 16], f.min(axis=0))
+    assert np.allclose(w[mlp_ref.N_WEIGHTS + 16:], f.max(axis=0))
+
+
+@pytest.mark.parametrize("mode", ["fixed", "heuristic", "mlp"])
+@pytest.mark.parametrize("loop", ["device", "graph", "host"])
+def test_auto_closure_is_exact_in_every_mode(pkg, oracle, sctx, tmp_path, mode, loop):
+    wl = _random_cnf(pkg)
+    exp = _expected(oracle, wl, tmp_path)
+    if mode == "mlp":
+        sctx.selector_set_weights(_random_weights())
+        sctx.selector_configure(mode="mlp", conf_margin=0.0, min_tiles=1)
+    else:
+        # M4R whenever a P tile is dense, so both word-level kernels run
+        sctx.selector_configure(mode=mode, m4r_min_dense=0.01, min_tiles=1)
+    q = pkg.query.PreparedQuery(sctx, wl.grammar, wl.graph)
+    try:
+        res = q.run(variant="auto", use_graph=loop)
+        assert res.lines == exp
+    finally:
+        q.close()
+
+
+@pytest.mark.parametrize("loop", ["graph", "host"])
+def test_auto_closure_with_tensor_core_terms(pkg, oracle, sctx, tmp_path, loop):
+    """Thresholds that send every term to the tensor cores when its operands
+    are populated: the per-iteration choice switches terms between the
+    word-level and tensor-core launch sequences."""
+    wl = pkg.workloads.ontology_query(1024, 3)
+    exp = _expected(oracle, wl, tmp_path)
+    sctx.selector_configure(mode="heuristic", tc_min_tiles=1, tc_min_occ=0.0, tc_min_pop=0.001, min_tiles=1)
+    q = pkg.query.PreparedQuery(sctx, wl.grammar, wl.graph)
+    try:
+        res = q.run(variant="auto", use_graph=loop)
+        assert res.lines == exp
+        assert res.stats["variant_items"][pkg.capi.VARIANT_TC] > 0
+    finally:
+        q.close()
+
+
+def test_product_log_times_every_candidate(pkg, oracle, sctx, tmp_path):
+    wl = pkg.workloads.ontology_query(1024, 4)
+    exp = _expected(oracle, wl, tmp_path)
+    sctx.selector_configure(mode="heuristic", tc_min_tiles=8, min_tiles=1)
+    q = pkg.query.PreparedQuery(sctx, wl.grammar, wl.graph)
+    try:
+        q.load()
+        st = sctx.closure(wl.grammar.rules, q.mats, variant="auto", log_products=pkg.capi.LOG_PRODUCTS)
+        got = dict(zip(wl.grammar.nonterminals, sctx.hash_count_many(q.mats)))
+        assert got == exp
+        recs = sctx.product_log()
+        assert len(recs) > 0
+        assert recs["iteration"].max() + 1 == st["iterations"]
+        assert (recs["usec"][:, 2] > 0).all() and (recs["usec"][:, 3] > 0).all()
+        assert (recs["usec"][:, 4] > 0).all()  # n = 1024: 16 tiles >= tc_min_tiles
+        assert np.isin(recs["variant"], [2, 3, 4]).all()
+        assert np.isfinite(recs["features"]).all()
+    finally:
+        q.close()
+
+
+def test_counters_track_the_closure(pkg, sctx):
+    """The selector's features come from counters that the product epilogues
+    keep exact: at the last iteration the population feature of a term's
+    current left operand equals that matrix's final population."""
+    wl = pkg.workloads.ontology_query(2048, 5)
+    sctx.selector_configure(mode="heuristic", min_tiles=1)
+    q = pkg.query.PreparedQuery(sctx, wl.grammar, wl.graph, order=None)
+    try:
+        q.load()
+        st = sctx.closure(wl.grammar.rules, q.mats, variant="auto", use_graph="graph",
+                          log_products=pkg.capi.LOG_SELECTION)
+        recs = sctx.product_log()
+        last = recs[recs["iteration"] == st["iterations"] - 1]
+        assert len(last)
+        counts = [c for _, c in sctx.hash_count_many(q.mats)]
+        for r in last[last["term"] == 1]:  # term 1: body1 (current) x delta(body2)
+            body1 = wl.grammar.rules[r["rule"]][1]
+            nnz = counts[body1]
+            assert r["features"][8] == pytest.approx(np.log2(1 + nnz) / 34, rel=1e-5)
+            occ, _ = q.mats[body1].tile_stats()
+            T = (q.mats[body1].n + 63) // 64
+            occupied = int(sum(bin(int(v)).count("1") for v in occ.ravel()))
+            assert r["features"][2] == pytest.approx(occupied / (T * T), rel=1e-5)
+    finally:
+        q.close()
+
+
+def test_autotune_sets_thresholds(sctx):
+    cfg, t = sctx.autotune(sizes=(512, 1024), densities=(0.01, 0.4), reps=1)
+    assert t.shape == (2, 2, 3)
+    assert (t[:, :, :2] > 0).all()
+    assert cfg["mode"] == 1
+    assert sctx.selector_config() == cfg
