@@ -52,6 +52,10 @@ def parse_args():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-profile", action="store_true")
+    ap.add_argument("--selector-eval", action="store_true",
+                    help="train the cost model on logged product timings and report its regret (about a minute)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the plain-GPU-form, reference-GPU, brackets and 512-query batch measurements")
     ap.add_argument("--no-graph", action="store_true",
                     help="launch every kernel from the host instead of the CUDA-graph loop (profilers cannot "
                          "capture kernel nodes of graphs with conditional nodes)")
@@ -210,6 +214,206 @@ def cpu_baseline(wl, budget_s=12.0) -> dict:
             "sample": f"{len(times)} full closures of the same workload, algorithm time, "
                       f"{'reference m4riCPU main + restated libm4ri' if exe else 'oracle M4RM port'}",
             "answer": answer}
+
+
+def _event_ms(torch, stream, fn):
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    r = fn()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1), r
+
+
+def plain_gpu_form(ctx, q, grammar, torch, stream, reps=2) -> dict:
+    """The plain single-variant GPU form on the same workload: the reference's
+    worklist driver (one product at a time, changed flag read back after each)
+    with the plain dense product kernel (no tiles, no skipping, no batching)."""
+    best, st = None, None
+    for _ in range(reps):
+        q.load()
+        ctx.synchronize()
+        ms, st = _event_ms(torch, stream, lambda: ctx.closure(grammar.rules, q.mats, driver="worklist",
+                                                               variant="plain"))
+        best = ms if best is None else min(best, ms)
+    return {"ms": best, "closures_per_s": 1e3 / best, "products": st["products"],
+            "form": "worklist driver + plain dense kernel (variant PLAIN)"}
+
+
+def reference_gpu_forms(wl, lines_expected) -> dict:
+    """The reference's own GPU executables (naiveGPU, m4riGPU built from its
+    sources for sm_100a): algorithm time printed by their main."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    out = {}
+    with tempfile.TemporaryDirectory() as d:
+        gp, rp = os.path.join(d, "grammar.txt"), os.path.join(d, "graph.txt")
+        wl.write(gp, rp)
+        for name in ("naiveGPU", "m4riGPU"):
+            exe = oracle.ref_executable(name)
+            if exe is None:
+                out[name] = {"unavailable": "not built"}
+                continue
+            try:
+                answer, (total, algo) = oracle.run_executable(exe, gp, rp, timeout=600)
+                out[name] = {"algo_ms": algo, "total_ms": total, "matches_ours": answer == lines_expected}
+            except Exception as e:  # a reference failure is reported, not fatal
+                out[name] = {"error": str(e)[:200]}
+    return out
+
+
+def batch_bench(pkg, ctx, torch, stream, rank, world, dist, nq=512, seed=1, steps=3) -> dict:
+    """Batched queries (512 independent queries, N log-uniform in [256, 8192],
+    three grammar families): every step closes the rank's LPT share of the
+    batch with one cfpq_closure_batch (all products of all unfinished queries
+    per iteration in one grouped launch).  Matrices are loaded before each
+    step (not timed); queries/s = all queries / the slowest rank's time."""
+    wls = pkg.workloads.batch_queries(nq, seed=seed)
+    costs = [pkg.shard.query_cost(w.graph.n, len(w.grammar.rules)) for w in wls]
+    mine = pkg.shard.lpt_assign(costs, world)[rank]
+    qs = [pkg.query.PreparedQuery(ctx, wls[i].grammar, wls[i].graph) for i in mine]
+    times, done, iters = [], None, None
+    try:
+        for step in range(steps + 1):
+            for q in qs:
+                q.load()
+            ctx.synchronize()
+            ms, (st, it, dn) = _event_ms(torch, stream, lambda: ctx.closure_batch(
+                [(q.grammar.rules, q.mats) for q in qs]))
+            if step > 0:  # step 0 warms up (plan cache, graph)
+                times.append(ms)
+                done, iters = dn, it
+        t = max(times)
+        if dist:
+            tt = torch.tensor([t], dtype=torch.float64, device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t = float(tt.item())
+        local_lines = {i: dict(zip(wls[i].grammar.nonterminals, ctx.hash_count_many(q.mats)))
+                       for i, q in zip(mine, qs)}
+        lines = pkg.shard.gather_lines(dist, local_lines)
+        import numpy as np
+
+        return {"queries": nq, "ms": t, "queries_per_s": nq / (t / 1e3),
+                "p50_query_ms": float(np.percentile(done, 50)), "p99_query_ms": float(np.percentile(done, 99)),
+                "max_iterations": int(iters.max()), "products": st["products"], "ranks": world,
+                "sharding": "LPT on 2 * rules * n^3 per query, no data-path collective",
+                "queries_closed": len(lines),
+                "per_query_ms": "completion time of each query inside its rank's batch (device timer)"}
+    finally:
+        for q in qs:
+            q.close()
+
+
+def brackets_small(pkg, ctx, torch, stream, reps=20) -> dict:
+    """Balanced brackets on a random graph, N = 1024, 4096 edges."""
+    wl = pkg.workloads.brackets_query()
+    q = pkg.query.PreparedQuery(ctx, wl.grammar, wl.graph)
+    try:
+        ms = []
+        for _ in range(reps + 3):
+            q.load()
+            ctx.synchronize()
+            ms.append(_event_ms(torch, stream, lambda: ctx.closure(wl.grammar.rules, q.mats))[0])
+        t = statistics.median(ms[3:])
+        return {"n": 1024, "edges": wl.graph.nedges, "ms": t, "closures_per_s": 1e3 / t}
+    finally:
+        q.close()
+
+
+def _logged_records(pkg, ctx, queries):
+    """CFPQ_LOG_PRODUCTS run of a batch (exhaustive timing of every candidate
+    variant of every term in every iteration); records and their keys."""
+    for q in queries:
+        q.load()
+    ctx.closure_batch([(q.grammar.rules, q.mats) for q in queries], log_products=pkg.capi.LOG_PRODUCTS)
+    return ctx.product_log()
+
+
+def _regret(recs, choice) -> float:
+    """sum of the chosen variants' times / sum of the fastest timed variant's - 1."""
+    import numpy as np
+
+    t = recs["usec"][:, 2:5].astype(np.float64)
+    timed = t > 0
+    best = np.where(timed, t, np.inf).min(axis=1)
+    idx = np.asarray(choice) - 2
+    chosen = t[np.arange(len(t)), idx]
+    ok = timed[np.arange(len(t)), idx] & np.isfinite(best)
+    return float(chosen[ok].sum() / best[ok].sum() - 1.0)
+
+
+def selector_eval(pkg, ctx, torch, stream, n_train=32, n_eval=32) -> dict:
+    """The learned selector (cfg5 shape): train the cost model on product
+    timings logged from brackets (N=1024), same-generation (N=8192) and a
+    32-query batch of the mixed-query shape, then evaluate on a fresh-seed
+    32-query batch: regret against exhaustive per-term timing for the
+    heuristic, the MLP and each fixed variant, and the batch closure time
+    with each selector."""
+    import numpy as np
+
+    # logging: tensor cores are a candidate for terms of n >= 4096
+    ctx.selector_configure(mode="heuristic", min_tiles=1, tc_min_tiles=64)
+    cfg = ctx.selector_config()
+    train = []
+    t0 = time.perf_counter()
+    for wl in (pkg.workloads.brackets_query(), pkg.workloads.ontology_query(8192, 7)):
+        q = pkg.query.PreparedQuery(ctx, wl.grammar, wl.graph)
+        train.append(_logged_records(pkg, ctx, [q]))
+        q.close()
+    tr_wls = pkg.workloads.batch_queries(n_train, seed=101, n_max=8192)
+    tr_qs = [pkg.query.PreparedQuery(ctx, w.grammar, w.graph) for w in tr_wls]
+    train.append(_logged_records(pkg, ctx, tr_qs))
+    for q in tr_qs:
+        q.close()
+    train = np.concatenate(train)
+    log_s = time.perf_counter() - t0
+    rep = ctx.selector_train(train, epochs=3000, learning_rate=3e-3, weight_decay=1e-4, seed=1)
+    ev_wls = pkg.workloads.batch_queries(n_eval, seed=202, n_max=8192)
+    ev_qs = [pkg.query.PreparedQuery(ctx, w.grammar, w.graph) for w in ev_wls]
+    out = {"train_records": int(len(train)), "logging_s": log_s, "train": rep, "config": cfg}
+    try:
+        ctx.selector_configure(mode="heuristic", min_tiles=1, tc_min_tiles=64)
+        rec_h = _logged_records(pkg, ctx, ev_qs)
+        ctx.selector_configure(mode="mlp", min_tiles=1, tc_min_tiles=64, conf_margin=0.0)
+        rec_m = _logged_records(pkg, ctx, ev_qs)
+        key = lambda r: (int(r["query"]), int(r["rule"]), int(r["term"]), int(r["iteration"]))
+        hmap = {key(r): int(r["variant"]) for r in rec_h}
+        common = np.array([key(r) in hmap for r in rec_m])
+        rm = rec_m[common]
+        heur = [hmap[key(r)] for r in rm]
+        tc_ok = rm["usec"][:, 4] > 0
+        out["eval_records"] = int(len(rm))
+        out["regret"] = {
+            "mlp": _regret(rm, rm["variant"]),
+            "heuristic": _regret(rm, heur),
+            "fixed_lop3": _regret(rm, np.full(len(rm), 2)),
+            "fixed_m4r": _regret(rm, np.full(len(rm), 3)),
+            "tc_where_possible": _regret(rm, np.where(tc_ok, 4, 2)),
+        }
+        out["mlp_decided_fraction"] = float(((rm["flags"] >> 8) & 1).mean())
+        # batch closure time of the fresh queries with each selector (the
+        # default tensor-core size limit, n >= 16384, keeps these terms on the
+        # word-level kernels: the choice is LOP3 or M4R per term and iteration)
+        times = {}
+        for label, kw in (("fixed_lop3", dict(mode="fixed")),
+                          ("heuristic", dict(mode="heuristic", min_tiles=1, tc_min_tiles=256)),
+                          ("mlp", dict(mode="mlp", min_tiles=1, tc_min_tiles=256, conf_margin=0.0))):
+            ctx.selector_configure(**kw)
+            ms = []
+            for _ in range(3):
+                for q in ev_qs:
+                    q.load()
+                ctx.synchronize()
+                ms.append(_event_ms(torch, stream, lambda: ctx.closure_batch(
+                    [(q.grammar.rules, q.mats) for q in ev_qs]))[0])
+            times[label] = min(ms)
+        out["batch_closure_ms"] = times
+    finally:
+        for q in ev_qs:
+            q.close()
+        ctx.selector_configure(mode="heuristic", min_tiles=256, tc_min_tiles=256)
+    return out
 
 
 def dense_product_kernels(ctx, capi, torch, stream, n=8192, density=0.3, reps=3):
@@ -377,6 +581,8 @@ def ours_arm(args, world, rank, local):
         roofline["multi_kernel_path_ms"] = {"plan": prof["plan_ms"], "product": prof["product_ms"],
                                             "advance_end": prof["advance_ms"]}
 
+    batch = None if args.no_extras else batch_bench(pkg, ctx, torch, stream, rank, world, dist)
+
     out = None
     if rank == 0:
         out = {
@@ -407,11 +613,22 @@ def ours_arm(args, world, rank, local):
         }
         if not args.no_profile:
             out["dense_product_kernels"] = dense_product_kernels(ctx, capi, torch, stream)
+        if not args.no_extras:
+            expected = {k: tuple(v) for k, v in zip(grammar.nonterminals, lines)}
+            pf = plain_gpu_form(ctx, q, grammar, torch, stream)
+            pf["engine_speedup"] = value / pf["closures_per_s"]
+            out["plain_gpu_form"] = pf
+            out["reference_gpu"] = reference_gpu_forms(wl, expected)
+            out["brackets_n1024"] = brackets_small(pkg, ctx, torch, stream)
         if world == 1 and not args.no_cpu_baseline:
             cb = cpu_baseline(wl)
             answer = cb.pop("answer")
             out["cpu_baseline"] = cb
             out["closure"]["parity_vs_cpu"] = answer == {k: tuple(v) for k, v in zip(grammar.nonterminals, lines)}
+        if batch is not None:
+            out["batch_512"] = batch
+        if args.selector_eval:
+            out["selector_eval"] = selector_eval(pkg, ctx, torch, stream)
         print(json.dumps(out))
     q.close()
     ctx.close()

@@ -8,6 +8,6 @@ drop-in backend (cpp/cfpq/B200Matrix.h, bin/b200GPU).  This package exposes
 The directory name contains hyphens; import it with
 importlib.import_module("cfpq-on-gpgpu_b200").
 """
-from . import capi, query, workloads  # noqa: F401
+from . import capi, query, shard, workloads  # noqa: F401
 
 __all__ = ["capi", "query", "workloads"]

@@ -833,8 +833,9 @@ static int build_plan(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, int variant
     uint32_t max_T = 0;
     for (const QueryIn &q : qs)
         if (q.nmats && q.nrules) max_T = std::max(max_T, q.mats[0]->d.T);
+    // a single small query is latency-bound: selection costs more than it gains
     pl->auto_select = variant == CFPQ_VARIANT_AUTO && ctx->sel.mode != CFPQ_SELECT_FIXED &&
-                      (allowed & ~(1u << CFPQ_VARIANT_LOP3)) != 0 && max_T >= ctx->sel.min_tiles;
+                      (allowed & ~(1u << CFPQ_VARIANT_LOP3)) != 0 && (qs.size() > 1 || max_T >= ctx->sel.min_tiles);
     pl->fixed_variant = (uint8_t)(variant == CFPQ_VARIANT_M4R || variant == CFPQ_VARIANT_TC ? variant
                                                                                            : CFPQ_VARIANT_LOP3);
     const bool tc_auto = (allowed & (1u << CFPQ_VARIANT_TC)) != 0;

@@ -16,12 +16,13 @@ void selector_defaults(SelectorParams *sp) {
     sp->tc_min_tiles = 256;
     sp->tc_min_occ = 0.5f;
     sp->tc_min_pop = 0.25f;
-    sp->m4r_min_dense = 0.5f;
+    sp->m4r_min_dense = 0.25f;
     sp->conf_margin = 0.05f;
     sp->range_margin = 0.1f;
     // Per-iteration selection costs one feature computation per planned row
-    // and exact buffer counters in every epilogue; a same-generation closure
-    // at n = 8192 (T = 128) loses 16% to it, with nothing to gain.
+    // and exact buffer counters in every epilogue; a single same-generation
+    // query at n = 8192 (T = 128) loses 16% to it, with nothing to gain.
+    // Batches of queries always select (512 mixed queries: 6-10% faster).
     sp->min_tiles = 256;
 }
 
@@ -352,7 +353,7 @@ extern "C" int cfpq_autotune(cfpq_ctx *ctx, const cfpq_autotune_opts *opts, cfpq
                 any_dense = true;
                 m4r_wins = m4r_wins && T(si, di, 1) > 0 && T(si, di, 1) < T(si, di, 0);
             }
-    sp.m4r_min_dense = (any_dense && m4r_wins) ? 0.5f : 1.5f;
+    sp.m4r_min_dense = (any_dense && m4r_wins) ? 0.25f : 1.5f;
     // tensor cores: the smallest density from which TC beats both word-level
     // variants at every larger density, per size; the smallest such size sets
     // tc_min_tiles, its crossover tc_min_pop

@@ -350,8 +350,9 @@ typedef struct cfpq_selector_config {
     float m4r_min_dense;    /* M4R: minimum fraction of dense P tiles (population > 96) */
     float conf_margin;      /* MLP: best prediction ahead of the second by this (log us) */
     float range_margin;     /* MLP: features within the training range widened by this fraction */
-    uint32_t min_tiles;     /* selection runs only in closures with a term of n >= 64 * min_tiles;
-                               smaller closures are latency-bound and run LOP3 throughout */
+    uint32_t min_tiles;     /* a single-query closure selects only if it has a term of
+                               n >= 64 * min_tiles (smaller ones are latency-bound and run
+                               LOP3 throughout); batches of queries always select */
 } cfpq_selector_config;
 int cfpq_selector_configure(cfpq_ctx *ctx, const cfpq_selector_config *cfg);
 int cfpq_selector_get_config(cfpq_ctx *ctx, cfpq_selector_config *cfg);

@@ -169,3 +169,52 @@ def test_autotune_sets_thresholds(sctx):
     assert (t[:, :, :2] > 0).all()
     assert cfg["mode"] == 1
     assert sctx.selector_config() == cfg
+
+
+def _logged(pkg, ctx, queries):
+    for q in queries:
+        q.load()
+    ctx.closure_batch([(q.grammar.rules, q.mats) for q in queries], log_products=pkg.capi.LOG_PRODUCTS)
+    return ctx.product_log()
+
+
+def _regret(recs, choice):
+    t = recs["usec"][:, 2:5].astype(np.float64)
+    timed = t > 0
+    best = np.where(timed, t, np.inf).min(axis=1)
+    idx = np.asarray(choice) - 2
+    rows = np.arange(len(t))
+    ok = timed[rows, idx] & np.isfinite(best)
+    return float(t[rows, idx][ok].sum() / best[ok].sum() - 1.0)
+
+
+def test_trained_selector_regret_on_fresh_queries(pkg, oracle, sctx, tmp_path):
+    """Train the cost model on logged timings of one batch, evaluate it on a
+    batch of fresh seeds against exhaustive timing: the learned choices are
+    exact (results) and their regret beats always-LOP3 (the method without a
+    selector)."""
+    sctx.selector_configure(mode="heuristic", min_tiles=1, tc_min_tiles=16)
+    tr = [pkg.query.PreparedQuery(sctx, w.grammar, w.graph)
+          for w in pkg.workloads.batch_queries(10, seed=11, n_min=256, n_max=2048)]
+    recs = _logged(pkg, sctx, tr)
+    for q in tr:
+        q.close()
+    rep = sctx.selector_train(recs, epochs=1500, seed=3)
+    assert rep["loss_last"] < rep["loss_first"]
+    wls = pkg.workloads.batch_queries(10, seed=12, n_min=256, n_max=2048)
+    ev = [pkg.query.PreparedQuery(sctx, w.grammar, w.graph) for w in wls]
+    try:
+        sctx.selector_configure(mode="mlp", conf_margin=0.0)
+        rm = _logged(pkg, sctx, ev)
+        for i, (q, wl) in enumerate(zip(ev, wls)):
+            d = tmp_path / f"e{i}"
+            d.mkdir()
+            got = dict(zip(wl.grammar.nonterminals, sctx.hash_count_many(q.mats)))
+            assert got == _expected(oracle, wl, d)
+        assert ((rm["flags"] >> 8) & 1).any()  # the network made decisions
+        r_mlp = _regret(rm, rm["variant"])
+        r_lop3 = _regret(rm, np.full(len(rm), 2))
+        assert 0.0 <= r_mlp < r_lop3, (r_mlp, r_lop3)
+    finally:
+        for q in ev:
+            q.close()
