@@ -218,3 +218,24 @@ def test_trained_selector_regret_on_fresh_queries(pkg, oracle, sctx, tmp_path):
     finally:
         for q in ev:
             q.close()
+
+
+@pytest.mark.parametrize("n", [1024, 2048, 4096])
+@pytest.mark.parametrize("variant", ["auto", "lop3", "tc"])
+def test_chain_workload_dense_closure(pkg, oracle, sctx, tmp_path, n, variant):
+    """The N=65536 chain workload's generator at sizes the CPU oracle closes in
+    seconds: its closure turns about half dense, where the selector sends dense
+    terms to M4R or the tensor cores and keeps sparse deltas on the
+    word-level kernels."""
+    wl = pkg.workloads.chain_query(n, 1)
+    exp = _expected(oracle, wl, tmp_path)
+    sctx.selector_configure(mode="heuristic", min_tiles=1, tc_min_tiles=16)
+    q = pkg.query.PreparedQuery(sctx, wl.grammar, wl.graph)
+    try:
+        res = q.run(variant=variant)
+        assert res.lines == exp
+        if variant == "auto":
+            items = res.stats["variant_items"]
+            assert items[pkg.capi.VARIANT_M4R] + items[pkg.capi.VARIANT_TC] > 0
+    finally:
+        q.close()
