@@ -14,7 +14,8 @@
 //
 // Configuration (environment variables): CFPQ_DEVICE (default 0),
 // CFPQ_DRIVER = engine | worklist (default engine), CFPQ_VARIANT = auto |
-// plain | lop3 (default auto), CFPQ_GRAPH = 0 | 1 (default 1).
+// plain | lop3 | m4r | tc (default auto), CFPQ_GRAPH = 0 (host loop) | 1
+// (device: persistent kernel or CUDA graph) | 2 (CUDA graph), default 1.
 //
 // Errors throw std::runtime_error with the library's message (the reference
 // prints and exits, cuda/naive-gpu/Multiplication.cu:10-17).
