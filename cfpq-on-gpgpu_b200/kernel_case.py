@@ -3,10 +3,16 @@
 
   python cfpq-on-gpgpu_b200/kernel_case.py dense --variant tc --n 8192 --density 0.3 --reps 3
   python cfpq-on-gpgpu_b200/kernel_case.py closure --n 8192 --reps 3
+  python cfpq-on-gpgpu_b200/kernel_case.py batch --queries 64 --reps 2
+  python cfpq-on-gpgpu_b200/kernel_case.py chain --n 16384 --reps 1
 
 `dense` runs C |= A * B on two seeded random n x n bit matrices (every tile
 populated) `reps` times with one variant; `closure` runs the same-generation
-ontology query (seeded, n vertices) `reps` times.  Each prints one JSON line
+ontology query (seeded, n vertices) `reps` times; `batch` closes a seeded
+mixed batch of `queries` queries (N log-uniform in [256, 8192]) with one
+cfpq_closure_batch per repetition; `chain` closes the chain workload (mean
+out-degree 2, 90% local edges, random CNF with 10 nonterminals and 24 rules)
+at n vertices with the selector (variant AUTO, every size selects).  Each prints one JSON line
 with the device time of every repetition (CUDA events on the library's
 stream), so the same command can run with and without a profiler.
 """
@@ -23,13 +29,14 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["dense", "closure"])
+    ap.add_argument("case", choices=["dense", "closure", "batch", "chain"])
+    ap.add_argument("--queries", type=int, default=64)
     ap.add_argument("--variant", default="lop3", choices=["plain", "lop3", "m4r", "tc"])
     ap.add_argument("--n", type=int, default=8192)
     ap.add_argument("--density", type=float, default=0.3)
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--seed", type=int, default=1)
-    ap.add_argument("--no-graph", action="store_true", help="closure: host-launched iterations, no CUDA graph")
+    ap.add_argument("--no-graph", action="store_true", help="closure, chain: host-launched iterations, no CUDA graph")
     args = ap.parse_args()
 
     import numpy as np
@@ -64,6 +71,39 @@ def main():
                    tbitmac_per_s=[n ** 3 / (t / 1e3) / 1e12 for t in times])
         for m in mats + [c]:
             m.destroy()
+    elif args.case == "batch":
+        wls = pkg.workloads.batch_queries(args.queries, seed=args.seed)
+        qs = [pkg.query.PreparedQuery(ctx, w.grammar, w.graph) for w in wls]
+        for _ in range(args.reps):
+            for q in qs:
+                q.load()
+            ctx.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            st, iters, _ = ctx.closure_batch([(q.grammar.rules, q.mats) for q in qs])
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        out.update(queries=args.queries, iterations=int(iters.max()), items=st["work_items"],
+                   dense_bitops=st["dense_bitops"], tile_triples=st["tile_triples"], variant_items=st["variant_items"])
+        for q in qs:
+            q.close()
+    elif args.case == "chain":
+        wl = pkg.workloads.chain_query(args.n, args.seed)
+        ctx.selector_configure(min_tiles=1)
+        q = pkg.query.PreparedQuery(ctx, wl.grammar, wl.graph)
+        for _ in range(args.reps):
+            q.load()
+            ctx.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            st = ctx.closure(wl.grammar.rules, q.mats, variant="auto", use_graph=not args.no_graph)
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        out.update(iterations=st["iterations"], tile_triples=st["tile_triples"], variant_items=st["variant_items"],
+                   lines={k: list(v) for k, v in zip(wl.grammar.nonterminals, ctx.hash_count_many(q.mats))})
+        q.close()
     else:
         wl = pkg.workloads.ontology_query(args.n, args.seed)
         q = pkg.query.PreparedQuery(ctx, wl.grammar, wl.graph)
