@@ -285,7 +285,7 @@ extern "C" int cfpq_ctx_destroy(cfpq_ctx *ctx) {
                       &ctx->mats_desc, &ctx->edge_buf, &ctx->xbuf, &ctx->phase_log, &ctx->clear_desc,
                       &ctx->d_sel, &ctx->cnts, &ctx->choice, &ctx->tc_ok, &ctx->sel_log, &ctx->mlp_w, &ctx->mlp_x,
                       &ctx->mlp_y, &ctx->mlp_m, &ctx->mlp_grad, &ctx->mlp_m1, &ctx->mlp_v2, &ctx->mlp_loss,
-                      &ctx->mlp_out})
+                      &ctx->mlp_out, &ctx->qranges})
         b->release();
     cudaFree(ctx->d_st);
     cudaFree(ctx->d_flag);
@@ -775,6 +775,7 @@ struct ClosurePlan {
     bool auto_select = false;     // variants chosen on the device every iteration
     uint8_t fixed_variant = 0;    // otherwise: every product's variant
     std::vector<uint8_t> tc_ok;   // per product: has a tensor-core launch sequence
+    std::vector<QueryRange> qranges;  // per query: its plan rows, slot rows, slots and products
 };
 
 
@@ -850,6 +851,11 @@ static int build_plan(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, int variant
     for (size_t qi = 0; qi < qs.size(); ++qi) {
         const QueryIn &q = qs[qi];
         const uint32_t base = (uint32_t)pl->slots.size();
+        QueryRange qrange;
+        qrange.prow0 = pl->prod_rows;
+        qrange.srow0 = pl->slot_rows;
+        qrange.slot0 = base;
+        qrange.prod0 = (uint32_t)pl->prods.size();
         for (size_t i = 0; i < q.nmats; ++i) {
             MatSlot s;
             memset(&s, 0, sizeof(s));
@@ -865,10 +871,8 @@ static int build_plan(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, int variant
             pl->slot_rows += s.cur.T;
             pl->slots.push_back(s);
         }
-        if (q.nmats == 0) continue;
-        const uint32_t T = q.mats[0]->d.T, n = q.mats[0]->d.n;
-        if (T == 0) continue;
-        for (size_t r = 0; r < q.nrules; ++r) {
+        const uint32_t T = q.nmats ? q.mats[0]->d.T : 0, n = q.nmats ? q.mats[0]->d.n : 0;
+        for (size_t r = 0; r < q.nrules && T; ++r) {
             for (uint8_t term = 0; term < 2; ++term) {
                 ProdDesc pd;
                 memset(&pd, 0, sizeof(pd));
@@ -899,6 +903,11 @@ static int build_plan(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, int variant
                 pl->prods.push_back(pd);
             }
         }
+        qrange.nprow = pl->prod_rows - qrange.prow0;
+        qrange.nsrow = pl->slot_rows - qrange.srow0;
+        qrange.nslot = (uint32_t)pl->slots.size() - qrange.slot0;
+        qrange.nprod = (uint32_t)pl->prods.size() - qrange.prod0;
+        pl->qranges.push_back(qrange);
     }
     pl->item_cap = std::max<size_t>(pl->item_cap, 1);
     pl->uses_tc = !pl->tc_prods.empty();
@@ -1239,11 +1248,12 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
         return CFPQ_OK;
     }
     // device tables
-    void *const slots_before = ctx->slots.p, *const prods_before = ctx->prods.p;
+    void *const slots_before = ctx->slots.p, *const prods_before = ctx->prods.p, *const qr_before = ctx->qranges.p;
     TRY(ctx->slots.ensure(pl.slots.size() * sizeof(MatSlot)));
     TRY(ctx->prods.ensure(pl.prods.size() * sizeof(ProdDesc)));
-    const bool tables_current =
-        ctx->tables_owner == pc.id && ctx->slots.p == slots_before && ctx->prods.p == prods_before;
+    TRY(ctx->qranges.ensure(pl.qranges.size() * sizeof(QueryRange)));
+    const bool tables_current = ctx->tables_owner == pc.id && ctx->slots.p == slots_before &&
+                                ctx->prods.p == prods_before && ctx->qranges.p == qr_before;
     const bool timed = (o.log_products & CFPQ_LOG_KERNELS) != 0;
     const bool log_products = (o.log_products & CFPQ_LOG_PRODUCTS) != 0;
     const int persist_grid = ctx->persist_grid[pl.uses_m4r ? 1 : 0];
@@ -1263,18 +1273,21 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
     TRY(ctx->prod_seen.ensure(pl.prods.size() * 4));
     if (pl.tc_max_T) TRY(ensure_expand_scratch(ctx, pl.tc_max_T));
     if (persistent) TRY(ctx->phase_log.ensure(kPhaseLogIters * 3 * 8));
-    const size_t qbytes = nq * (4 + 4 + 8) + 64;
+    // done_ns, changed flags (three rotating arrays in the persistent kernel), last_iter
+    const size_t qbytes = nq * (8 + 3 * 4 + 4) + 64;
     TRY(ctx->qtrack.ensure(qbytes));
     QueryTrack qt;
     qt.done_ns = ctx->qtrack.as<unsigned long long>();
     qt.changed = reinterpret_cast<uint32_t *>(qt.done_ns + nq);
-    qt.last_iter = qt.changed + nq;
+    qt.last_iter = qt.changed + 3 * nq;
     if (!tables_current) {
         CUDA_TRY(cudaMemcpyAsync(ctx->slots.p, pl.slots.data(), pl.slots.size() * sizeof(MatSlot),
                                  cudaMemcpyHostToDevice, ctx->stream));
         CUDA_TRY(cudaMemcpyAsync(ctx->prods.p, pl.prods.data(), pl.prods.size() * sizeof(ProdDesc),
                                  cudaMemcpyHostToDevice, ctx->stream));
         CUDA_TRY(cudaMemcpyAsync(ctx->tc_ok.p, pl.tc_ok.data(), nprods, cudaMemcpyHostToDevice, ctx->stream));
+        CUDA_TRY(cudaMemcpyAsync(ctx->qranges.p, pl.qranges.data(), pl.qranges.size() * sizeof(QueryRange),
+                                 cudaMemcpyHostToDevice, ctx->stream));
         ctx->tables_owner = pc.id;
     }
     CUDA_TRY(launch_fill_choice(ctx->choice.as<uint8_t>(), nprods,
@@ -1320,7 +1333,10 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
                                            closure_counters(ctx, pl), ctx->choice.as<uint8_t>(),
                                            pl.auto_select ? ctx->d_sel.as<SelectorParams>() : nullptr,
                                            ctx->sel_log_iters ? ctx->sel_log.as<SelLogRow>() : nullptr,
-                                           ctx->sel_log_iters, ctx->stream));
+                                           ctx->sel_log_iters,
+                                           nq >= 2 && nq <= kMaxActiveQueries ? ctx->qranges.as<QueryRange>()
+                                                                              : nullptr,
+                                           ctx->stream));
     } else if (exec) {
         CUDA_TRY(cudaGraphLaunch(exec, ctx->stream));
     } else {

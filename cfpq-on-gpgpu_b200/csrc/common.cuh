@@ -150,6 +150,16 @@ struct PlanSelect {
     uint32_t log_iters;
 };
 
+// Rows, slots and products of one query of a closure (all contiguous): plan
+// rows [prow0, prow0 + nprow), slot tile-rows [srow0, srow0 + nsrow), slots
+// [slot0, slot0 + nslot), products [prod0, prod0 + nprod).
+struct QueryRange {
+    uint32_t prow0, nprow, srow0, nsrow, slot0, nslot, prod0, nprod;
+};
+
+// Largest batch whose persistent closure plans over active queries only.
+constexpr uint32_t kMaxActiveQueries = 512;
+
 // Per-query bookkeeping of a batched closure (device arrays of nqueries).
 struct QueryTrack {
     uint32_t *changed;              // set by product kernels in the current iteration
@@ -324,8 +334,8 @@ __device__ __forceinline__ void clear_tile_row(const DevMat &D, uint32_t ti) {
 // One warp: clear tile-row `row` (over all slots, slot tile-rows in order) of
 // the delta buffer dlt[parity].
 __device__ __forceinline__ void clear_delta_row(const MatSlot *__restrict__ slots, uint32_t nslots, uint32_t row,
-                                                uint32_t parity) {
-    uint32_t lo = 0, hi = nslots;
+                                                uint32_t parity, uint32_t slo = 0, uint32_t shi = 0xFFFFFFFFu) {
+    uint32_t lo = slo, hi = shi < nslots ? shi : nslots;  // slot search range (a query's slots if known)
     while (hi - lo > 1) {
         const uint32_t mid = (lo + hi) >> 1;
         if (slots[mid].row_start <= row) lo = mid; else hi = mid;

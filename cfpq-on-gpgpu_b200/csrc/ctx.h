@@ -130,6 +130,7 @@ struct cfpq_ctx {
     int lop3_grid = 0, m4r_grid = 0, tc_grid = 0;  // tc_grid 0: tensor-core variant unavailable
     int persist_grid[2] = {0, 0};  // persistent closure CTAs [with M4R items]; 0: unavailable
     DevBuf phase_log;              // persistent closure: 3 timestamps per iteration
+    DevBuf qranges;                // persistent closure of a batch: QueryRange per query
     uint32_t phase_log_iters = 0;  // iterations logged by the last closure
     std::vector<cfpq_product_record> log;
     cudaEvent_t kev[5] = {};

@@ -11,9 +11,16 @@
 //            iteration t-1 (dlt[par ^ 1], cleared: the products of iteration t
 //            write their new bits there).  CTA 0 also folds the counters of
 //            parity par ^ 1 (iteration t-1) into the statistics and zeroes them.
+//            Batches of at most kMaxActive queries plan only the queries that
+//            changed in iteration t-1 and clear only those that changed in
+//            t-2 (the deltas of the others are empty): every CTA compacts
+//            the per-query changed flags into its own active lists first, so
+//            converged queries cost nothing in the tail of a batch.
 //   barrier
 //   phase B  CTAs take work items (LOP3 list, then M4R list) and run
-//            tiled::process_item; new bits set changed[par].
+//            tiled::process_item; new bits set changed[par] and the query's
+//            flag in qt.changed[t % 3] (three rotating flag arrays: iteration
+//            t reads those of t-1 and t-2; CTA 0 zeroes those of t+1 here).
 //   barrier
 //   decision every CTA reads changed[par] (final after the barrier) and the
 //            error word: continue while something changed, no wait gave up
@@ -47,11 +54,25 @@ constexpr uint32_t kWordBlocks = 128;
 // query or a small batch), saving two dependent global loads per item.
 constexpr uint32_t kTableBytes = 8192;
 
+constexpr uint32_t kMaxActive = kMaxActiveQueries;
+constexpr uint32_t kActivePerThread = kMaxActive / kThreads;
+static_assert(kMaxActive % kThreads == 0, "active-list build: whole queries per thread");
+
+// Queries of one phase-A unit set with the prefix sum of their row counts:
+// unit u belongs to q[i] for the last i with pref[i] <= u.
+struct ActiveList {
+    uint32_t n;
+    uint32_t pref[kMaxActive + 1];
+    uint16_t q[kMaxActive];
+};
+
 template <bool kM4R>
 struct PersistSmem {
     tiled::TiledSmem<kM4R> prod;
     plan::WarpArea<kWordBlocks> plan[kThreads / 32];
     alignas(16) unsigned char tables[kTableBytes];
+    ActiveList act_plan, act_clear;
+    uint32_t wtot[kThreads / 32][2];
 };
 
 struct PersistArgs {
@@ -72,7 +93,67 @@ struct PersistArgs {
     const SelectorParams *sel;      // non-null: choose per iteration (selection phase)
     SelLogRow *sel_log;
     uint32_t sel_log_iters;
+    const QueryRange *qr;           // non-null (batches of 2..kMaxActive queries): active-query phase A
 };
+
+// Block-wide compaction of the queries whose flag is set (every query when
+// flags is null) into L, with the prefix sum of their plan rows (slot rows
+// when srows).  Called by all threads; ends synchronised.
+__device__ void build_active(ActiveList &L, const uint32_t *flags, const QueryRange *qr, uint32_t nq, bool srows,
+                             uint32_t (*wtot)[2]) {
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t q0 = tid * kActivePerThread;
+    uint32_t rows[kActivePerThread], c = 0, r = 0;
+#pragma unroll
+    for (uint32_t k = 0; k < kActivePerThread; ++k) {
+        const uint32_t q = q0 + k;
+        const bool on = q < nq && (!flags || __ldcg(flags + q) != 0);
+        rows[k] = on ? (srows ? qr[q].nsrow : qr[q].nprow) : 0xFFFFFFFFu;
+        c += on;
+        r += on ? rows[k] : 0;
+    }
+    uint32_t ic = c, ir = r;
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t xc = __shfl_up_sync(tiled::kFull, ic, o), xr = __shfl_up_sync(tiled::kFull, ir, o);
+        if (lane >= (uint32_t)o) {
+            ic += xc;
+            ir += xr;
+        }
+    }
+    if (lane == 31) {
+        wtot[warp][0] = ic;
+        wtot[warp][1] = ir;
+    }
+    __syncthreads();
+    uint32_t ec = ic - c, er = ir - r;
+    for (uint32_t w = 0; w < warp; ++w) {
+        ec += wtot[w][0];
+        er += wtot[w][1];
+    }
+#pragma unroll
+    for (uint32_t k = 0; k < kActivePerThread; ++k) {
+        if (rows[k] == 0xFFFFFFFFu) continue;
+        L.q[ec] = (uint16_t)(q0 + k);
+        L.pref[ec] = er;
+        ++ec;
+        er += rows[k];
+    }
+    if (tid == kThreads - 1) {
+        L.n = ec;
+        L.pref[ec] = er;
+    }
+    __syncthreads();
+}
+
+// Index i of the last pref[i] <= u in L (u below the list's total).
+__device__ __forceinline__ uint32_t active_find(const ActiveList &L, uint32_t u) {
+    uint32_t lo = 0, hi = L.n;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (L.pref[mid] <= u) lo = mid; else hi = mid;
+    }
+    return lo;
+}
 
 // Grid barrier (all CTAs of the cooperative launch): arrival counter plus a
 // generation word; `gen` is the CTA's copy of the generation.  Returns false
@@ -158,7 +239,32 @@ __global__ void __launch_bounds__(kThreads, 3) k_closure_persistent(PersistArgs 
         // ---- phase A: plan of iteration t + clear of the delta read in t-1 ----
         if (a.cnts && blockIdx.x == 0 && t > 0)  // that delta's counters restart at zero
             for (uint32_t sl = tid; sl < a.nslots; sl += kThreads) a.cnts[3 * sl + 1 + (par ^ 1)] = BufCounters{0, 0, 0};
-        {
+        if (a.qr) {
+            // plan: queries that changed in t-1 (all in iteration 0); clear:
+            // queries that changed in t-2 (all in iteration 1, none in 0)
+            const uint32_t nq = st->nqueries;
+            build_active(S.act_plan, t > 0 ? a.qt.changed + ((t - 1) % 3) * nq : nullptr, a.qr, nq, false, S.wtot);
+            if (t > 0)
+                build_active(S.act_clear, t > 1 ? a.qt.changed + ((t - 2) % 3) * nq : nullptr, a.qr, nq, true,
+                             S.wtot);
+            const uint32_t np = S.act_plan.pref[S.act_plan.n], ns = t > 0 ? S.act_clear.pref[S.act_clear.n] : 0u;
+            for (uint32_t u = gwarp; u < np + ns; u += nwarps) {
+                if (u < np) {
+                    const uint32_t i = active_find(S.act_plan, u);
+                    const QueryRange qr = a.qr[S.act_plan.q[i]];
+                    plan::plan_row(qr.prow0 + (u - S.act_plan.pref[i]), prods, a.nprods, slots, t, st,
+                                   st->pitem_count[par], a.items + (size_t)(2 * par) * a.list_cap, a.list_cap, a.tpb,
+                                   a.prod_seen, 0, psel, S.plan[warp].cnt, S.plan[warp].bnd, qr.prod0,
+                                   qr.prod0 + qr.nprod);
+                } else {
+                    const uint32_t i = active_find(S.act_clear, u - np);
+                    const QueryRange qr = a.qr[S.act_clear.q[i]];
+                    clear_delta_row(slots, a.nslots, qr.srow0 + (u - np - S.act_clear.pref[i]), par ^ 1, qr.slot0,
+                                    qr.slot0 + qr.nslot);
+                }
+                __syncwarp();
+            }
+        } else {
             const uint32_t clear_rows = t > 0 ? a.slot_rows : 0u;
             const uint32_t units = a.prod_rows + clear_rows;
             for (uint32_t u = gwarp; u < units; u += nwarps) {
@@ -178,6 +284,11 @@ __global__ void __launch_bounds__(kThreads, 3) k_closure_persistent(PersistArgs 
         if (timed_out) break;
 
         // ---- phase B: products ----
+        uint32_t *const qchanged = a.qt.changed ? a.qt.changed + (t % 3) * st->nqueries : nullptr;
+        if (blockIdx.x == 0 && a.qt.changed) {  // flags of iteration t+1 (last read in phase A of t)
+            uint32_t *next = a.qt.changed + ((t + 1) % 3) * st->nqueries;
+            for (uint32_t q = tid; q < st->nqueries; q += kThreads) next[q] = 0;
+        }
         {
             const uint64_t *items = a.items + (size_t)(2 * par) * a.list_cap;
             const uint32_t n0 = st->pitem_count[par][0];
@@ -187,8 +298,8 @@ __global__ void __launch_bounds__(kThreads, 3) k_closure_persistent(PersistArgs 
                 const uint32_t idx = S.prod.item;
                 __syncthreads();
                 if (idx >= n0) break;
-                tiled::process_item<false>(S.prod, items[idx], prods, slots, t, &st->pchanged[par], a.qt.changed,
-                                           phase, timed_out, ctr, a.cnts);
+                tiled::process_item<false>(S.prod, items[idx], prods, slots, t, &st->pchanged[par], qchanged, phase,
+                                           timed_out, ctr, a.cnts);
             }
             if constexpr (kHasM4R) {
                 const uint32_t n1 = st->pitem_count[par][1];
@@ -199,7 +310,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_closure_persistent(PersistArgs 
                     __syncthreads();
                     if (idx >= n1) break;
                     tiled::process_item<true>(S.prod, items[a.list_cap + idx], prods, slots, t,
-                                              &st->pchanged[par], a.qt.changed, phase, timed_out, ctr, a.cnts);
+                                              &st->pchanged[par], qchanged, phase, timed_out, ctr, a.cnts);
                 }
             }
         }
@@ -217,11 +328,10 @@ __global__ void __launch_bounds__(kThreads, 3) k_closure_persistent(PersistArgs 
         if (blockIdx.x == 0) {
             if (tid == 0 && a.phase_log && t - iter0 < a.phase_log_iters)
                 a.phase_log[3 * (t - iter0) + 2] = globaltimer_ns();
-            if (a.qt.changed) {
+            if (qchanged) {
                 const unsigned long long now = globaltimer_ns();
                 for (uint32_t q = tid; q < st->nqueries; q += kThreads) {
-                    if (a.qt.changed[q]) {
-                        a.qt.changed[q] = 0;
+                    if (__ldcg(qchanged + q)) {
                         a.qt.last_iter[q] = t + 1;
                         a.qt.done_ns[q] = now;
                     }
@@ -234,9 +344,22 @@ __global__ void __launch_bounds__(kThreads, 3) k_closure_persistent(PersistArgs 
     // ---- exit: clear the delta read in the last iteration; final state ----
     if (!timed_out) {
         const uint32_t par = t & 1;
-        for (uint32_t u = gwarp; u < a.slot_rows; u += nwarps) {
-            clear_delta_row(slots, a.nslots, u, par);
-            __syncwarp();
+        if (a.qr) {  // queries planned in iteration t
+            const uint32_t nq = st->nqueries;
+            build_active(S.act_clear, t > 0 ? a.qt.changed + ((t - 1) % 3) * nq : nullptr, a.qr, nq, true, S.wtot);
+            const uint32_t ns = S.act_clear.pref[S.act_clear.n];
+            for (uint32_t u = gwarp; u < ns; u += nwarps) {
+                const uint32_t i = active_find(S.act_clear, u);
+                const QueryRange qr = a.qr[S.act_clear.q[i]];
+                clear_delta_row(slots, a.nslots, qr.srow0 + (u - S.act_clear.pref[i]), par, qr.slot0,
+                                qr.slot0 + qr.nslot);
+                __syncwarp();
+            }
+        } else {
+            for (uint32_t u = gwarp; u < a.slot_rows; u += nwarps) {
+                clear_delta_row(slots, a.nslots, u, par);
+                __syncwarp();
+            }
         }
     }
     unsigned long long triples = ctr.triples, outw = ctr.outw, neww = ctr.neww;
@@ -289,7 +412,7 @@ cudaError_t launch_closure_persistent(int has_m4r, int grid, const ProdDesc *pro
                                       const QueryTrack &qt, int tpb, unsigned long long *phase_log,
                                       uint32_t phase_log_iters, BufCounters *cnts, uint8_t *choice,
                                       const SelectorParams *sel, SelLogRow *sel_log, uint32_t sel_log_iters,
-                                      cudaStream_t s) {
+                                      const QueryRange *qr, cudaStream_t s) {
     PersistArgs a;
     a.prods = prods;
     a.nprods = nprods;
@@ -310,6 +433,7 @@ cudaError_t launch_closure_persistent(int has_m4r, int grid, const ProdDesc *pro
     a.sel = sel;
     a.sel_log = sel_log;
     a.sel_log_iters = sel_log_iters;
+    a.qr = qr;
     void *args[] = {&a};
     if (has_m4r)
         return cudaLaunchCooperativeKernel((const void *)k_closure_persistent<true>, dim3(grid), dim3(kThreads), args,

@@ -62,9 +62,12 @@ __device__ __forceinline__ void plan_row(uint32_t gw, const ProdDesc *__restrict
                                          const MatSlot *__restrict__ slots, uint32_t iter, IterState *st,
                                          uint32_t *item_count, uint64_t *__restrict__ items_all, size_t list_cap,
                                          int tpb, uint32_t *prod_seen, int tc_mode, const PlanSelect &ps,
-                                         uint32_t *cnt, uint16_t (*bnd)[kMaxChunksPerBlock - 1]) {
+                                         uint32_t *cnt, uint16_t (*bnd)[kMaxChunksPerBlock - 1],
+                                         uint32_t plo = 0, uint32_t phi = 0xFFFFFFFFu) {
     const uint32_t lane = threadIdx.x & 31;
-    uint32_t lo = 0, hi = nprods;  // product: last p with row_start <= gw
+    // product: last p with row_start <= gw, searched in [plo, phi) (a query's
+    // products when the caller knows the query)
+    uint32_t lo = plo, hi = phi < nprods ? phi : nprods;
     while (hi - lo > 1) {
         const uint32_t mid = (lo + hi) >> 1;
         if (prods[mid].row_start <= gw) lo = mid; else hi = mid;

@@ -354,6 +354,48 @@ def test_batch_matches_single_queries(ctx, pkg, oracle, tmp_path):
             q.close()
 
 
+def test_batch_active_queries(ctx, pkg, oracle, tmp_path):
+    """Batches plan only the queries still changing (persistent loop): empty
+    queries in the mix, and an iteration limit followed by a full closure.
+    Iteration counts are not compared with each query closed alone: products
+    of one iteration may already see bits other products set in it, so the
+    count depends on scheduling; the fixpoint does not."""
+    wls = pkg.workloads.batch_queries(12, seed=11, n_min=64, n_max=700)
+    qs, exps = [], []
+    for i, wl in enumerate(wls):
+        d = tmp_path / f"q{i}"
+        d.mkdir()
+        gp, rp = _write(wl, d)
+        exps.append(_oracle_run(oracle, gp, rp)[0])
+        qs.append(pkg.query.PreparedQuery(ctx, wl.grammar, wl.graph))
+    spare = ctx.matrix(128)
+    try:
+        batch = [(q.grammar.rules, q.mats) for q in qs]
+        batch.insert(3, ([], []))          # no matrices
+        batch.insert(7, ([], [spare]))     # a matrix, no rules
+        for limit in (2, 0):
+            for q in qs:
+                q.load()
+            st, it, done = ctx.closure_batch(batch, use_graph="device", max_iterations=limit)
+            assert int(it[3]) == 0 and int(it[7]) == 0
+            if limit:
+                assert int(it.max()) <= limit
+                continue
+            assert 1 <= int(it.min(initial=99, where=it > 0)) and int(it.max()) < st["iterations"]
+            for q, exp in zip(qs, exps):
+                assert dict(zip(q.grammar.nonterminals, ctx.hash_count_many(q.mats))) == exp
+        for q in qs:  # after the limited run the next closure restarts from scratch
+            q.load()
+        ctx.closure_batch(batch, use_graph="device", max_iterations=3)
+        ctx.closure_batch(batch, use_graph="device")
+        for q, exp in zip(qs, exps):
+            assert dict(zip(q.grammar.nonterminals, ctx.hash_count_many(q.mats))) == exp
+    finally:
+        spare.destroy()
+        for q in qs:
+            q.close()
+
+
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 GOLDEN_CASES = sorted(d for d in os.listdir(GOLDEN) if os.path.isdir(os.path.join(GOLDEN, d)))
 
