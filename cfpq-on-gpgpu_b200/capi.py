@@ -35,7 +35,7 @@ EXPORTED = (
     "cfpq_matrix_create_ordered", "cfpq_hash_count_rows_noalloc", "cfpq_noalloc_last_error", "cfpq_calibrate",
     "cfpq_last_phase_log", "cfpq_matrices_clear", "cfpq_selector_configure", "cfpq_selector_get_config",
     "cfpq_selector_weight_count", "cfpq_selector_set_weights", "cfpq_selector_get_weights", "cfpq_selector_train",
-    "cfpq_selector_loss_grad", "cfpq_selector_predict", "cfpq_autotune",
+    "cfpq_selector_loss_grad", "cfpq_selector_predict", "cfpq_autotune", "cfpq_item_log",
 )
 
 
@@ -93,6 +93,11 @@ class Query(ctypes.Structure):
 SEL_FEATURES, SEL_OUTPUTS = 16, 3
 SELECT_FIXED, SELECT_HEURISTIC, SELECT_MLP = 0, 1, 2
 LOG_SELECTION = 4
+LOG_ITEMS = 8
+
+# numpy view of an array of cfpq_item_record
+ITEM_RECORD_DTYPE = np.dtype([("item", np.uint64), ("iteration", np.uint32), ("cta", np.uint16),
+                              ("list", np.uint16), ("start_ns", np.uint64), ("end_ns", np.uint64)])
 
 
 class ProductRecord(ctypes.Structure):
@@ -189,6 +194,7 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "cfpq_calibrate": ([vp, P(Calibration)], i32),
         "cfpq_load_edges_device": ([vp, P(vp), sz, vp, vp, vp, sz, vp, vp, u32], i32),
         "cfpq_last_phase_log": ([vp, P(u64), sz], sz),
+        "cfpq_item_log": ([vp, vp, sz], sz),
         "cfpq_matrices_clear": ([vp, P(vp), sz], i32),
         "cfpq_selector_configure": ([vp, P(SelectorConfig)], i32),
         "cfpq_selector_get_config": ([vp, P(SelectorConfig)], i32),
@@ -510,6 +516,23 @@ class Context:
         out = np.zeros(n, dtype=PRODUCT_RECORD_DTYPE)
         if n:
             self.lib.cfpq_product_log(self.handle, out.ctypes.data_as(ctypes.POINTER(ProductRecord)), n)
+        return out
+
+    def item_log(self) -> np.ndarray:
+        """Work items of the last persistent closure run with LOG_ITEMS: the
+        records plus decoded fields product, ti, block, klo, khi."""
+        n = self.lib.cfpq_item_log(self.handle, None, 0)
+        raw = np.zeros(n, dtype=ITEM_RECORD_DTYPE)
+        if n:
+            self.lib.cfpq_item_log(self.handle, raw.ctypes.data, n)
+        it = raw["item"]
+        dec = {"product": it >> 48, "ti": (it >> 37) & 0x7FF, "block": (it >> 28) & 0x1FF,
+               "klo": (it >> 16) & 0xFFF, "khi": (it >> 4) & 0xFFF}
+        out = np.zeros(n, dtype=ITEM_RECORD_DTYPE.descr + [(k, np.uint32) for k in dec])
+        for k in ITEM_RECORD_DTYPE.names:
+            out[k] = raw[k]
+        for k, v in dec.items():
+            out[k] = v.astype(np.uint32)
         return out
 
     def kernel_profile(self) -> dict:

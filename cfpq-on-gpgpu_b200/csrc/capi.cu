@@ -285,7 +285,7 @@ extern "C" int cfpq_ctx_destroy(cfpq_ctx *ctx) {
                       &ctx->mats_desc, &ctx->edge_buf, &ctx->xbuf, &ctx->phase_log, &ctx->clear_desc,
                       &ctx->d_sel, &ctx->cnts, &ctx->choice, &ctx->tc_ok, &ctx->sel_log, &ctx->mlp_w, &ctx->mlp_x,
                       &ctx->mlp_y, &ctx->mlp_m, &ctx->mlp_grad, &ctx->mlp_m1, &ctx->mlp_v2, &ctx->mlp_loss,
-                      &ctx->mlp_out, &ctx->qranges})
+                      &ctx->mlp_out, &ctx->qranges, &ctx->item_trace})
         b->release();
     cudaFree(ctx->d_st);
     cudaFree(ctx->d_flag);
@@ -1273,6 +1273,14 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
     TRY(ctx->prod_seen.ensure(pl.prods.size() * 4));
     if (pl.tc_max_T) TRY(ensure_expand_scratch(ctx, pl.tc_max_T));
     if (persistent) TRY(ctx->phase_log.ensure(kPhaseLogIters * 3 * 8));
+    static_assert(sizeof(ItemTrace) == sizeof(cfpq_item_record), "item trace layout");
+    const bool trace = persistent && (o.log_products & CFPQ_LOG_ITEMS) != 0;
+    const size_t trace_bytes = (size_t)kItemTraceCap * sizeof(ItemTrace);
+    ctx->item_trace_n = 0;
+    if (trace) {
+        TRY(ctx->item_trace.ensure(trace_bytes + 64));
+        CUDA_TRY(cudaMemsetAsync(static_cast<char *>(ctx->item_trace.p) + trace_bytes, 0, 4, ctx->stream));
+    }
     // done_ns, changed flags (three rotating arrays in the persistent kernel), last_iter
     const size_t qbytes = nq * (8 + 3 * 4 + 4) + 64;
     TRY(ctx->qtrack.ensure(qbytes));
@@ -1336,6 +1344,10 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
                                            ctx->sel_log_iters,
                                            nq >= 2 && nq <= kMaxActiveQueries ? ctx->qranges.as<QueryRange>()
                                                                               : nullptr,
+                                           trace ? ctx->item_trace.as<ItemTrace>() : nullptr,
+                                           trace ? reinterpret_cast<uint32_t *>(
+                                                       static_cast<char *>(ctx->item_trace.p) + trace_bytes)
+                                                 : nullptr,
                                            ctx->stream));
     } else if (exec) {
         CUDA_TRY(cudaGraphLaunch(exec, ctx->stream));
@@ -1357,6 +1369,9 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
     CUDA_TRY(cudaMemcpyAsync(ctx->h_st, ctx->d_st, sizeof(IterState), cudaMemcpyDeviceToHost, ctx->stream));
     std::vector<unsigned long long> h_done(nq);
     std::vector<uint32_t> h_last(nq);
+    if (trace)
+        CUDA_TRY(cudaMemcpyAsync(&ctx->item_trace_n, static_cast<char *>(ctx->item_trace.p) + trace_bytes, 4,
+                                 cudaMemcpyDeviceToHost, ctx->stream));
     CUDA_TRY(cudaMemcpyAsync(h_done.data(), qt.done_ns, nq * 8, cudaMemcpyDeviceToHost, ctx->stream));
     CUDA_TRY(cudaMemcpyAsync(h_last.data(), qt.last_iter, nq * 4, cudaMemcpyDeviceToHost, ctx->stream));
     CUDA_TRY(cudaStreamSynchronize(ctx->stream));
@@ -1491,6 +1506,16 @@ extern "C" size_t cfpq_last_phase_log(cfpq_ctx *ctx, uint64_t *out, size_t cap) 
     if (out && k) {
         if (cudaMemcpy(out, ctx->phase_log.p, k * 8, cudaMemcpyDeviceToHost) != cudaSuccess) return 0;
     }
+    return n;
+}
+
+extern "C" size_t cfpq_item_log(cfpq_ctx *ctx, cfpq_item_record *out, size_t cap) {
+    if (!ctx) return 0;
+    const size_t n = std::min<size_t>(ctx->item_trace_n, kItemTraceCap);
+    const size_t k = std::min(cap, n);
+    if (out && k && cudaMemcpy(out, ctx->item_trace.p, k * sizeof(cfpq_item_record), cudaMemcpyDeviceToHost) !=
+                        cudaSuccess)
+        return 0;
     return n;
 }
 

@@ -157,6 +157,15 @@ struct QueryRange {
     uint32_t prow0, nprow, srow0, nsrow, slot0, nslot, prod0, nprod;
 };
 
+// One traced work item of a persistent closure (layout of cfpq_item_record).
+struct ItemTrace {
+    uint64_t item;
+    uint32_t iteration;
+    uint16_t cta, list;
+    unsigned long long start_ns, end_ns;
+};
+constexpr uint32_t kItemTraceCap = 65536;
+
 // Largest batch whose persistent closure plans over active queries only.
 constexpr uint32_t kMaxActiveQueries = 512;
 

@@ -131,6 +131,8 @@ struct cfpq_ctx {
     int persist_grid[2] = {0, 0};  // persistent closure CTAs [with M4R items]; 0: unavailable
     DevBuf phase_log;              // persistent closure: 3 timestamps per iteration
     DevBuf qranges;                // persistent closure of a batch: QueryRange per query
+    DevBuf item_trace;             // CFPQ_LOG_ITEMS: ItemTrace records, then the record count
+    uint32_t item_trace_n = 0;     // records of the last closure
     uint32_t phase_log_iters = 0;  // iterations logged by the last closure
     std::vector<cfpq_product_record> log;
     cudaEvent_t kev[5] = {};

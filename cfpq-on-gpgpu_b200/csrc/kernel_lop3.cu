@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(kThreads, 4)
         __syncthreads();
         const uint32_t idx = S.item;
         if (idx >= nitems) break;
-        process_item<kM4R>(S, items[idx], prods, slots, iter, &st->changed, qchanged, phase, timed_out, ctr, cnts);
+        process_item<kM4R, kThreads / 32>(S, items[idx], prods, slots, iter, &st->changed, qchanged, phase, timed_out, ctr, cnts);
     }
     // per-CTA counters (warp-reduced) for statistics and the roofline report
     unsigned long long triples = ctr.triples, outw = ctr.outw, neww = ctr.neww;

@@ -41,7 +41,12 @@ namespace cfpq {
 namespace {
 
 using tiled::ItemCounters;
-using tiled::kThreads;
+
+// 8 warps per CTA: an item's 16 output tiles are spread 2 per warp (twice the
+// threads of the product kernels on one item: most iterations of a single
+// closure have fewer items than CTAs, so item latency is the phase length).
+constexpr int kPW = 8;
+constexpr uint32_t kThreads = 32 * kPW;
 
 constexpr uint32_t kBarrierSpinLimit = 1u << 25;  // ~1 s of polling
 
@@ -66,14 +71,22 @@ struct ActiveList {
     uint16_t q[kMaxActive];
 };
 
+// Phase-A scratch.  It lives in the Q staging buffers of the product layout:
+// no bulk copy is in flight outside phase B (every item waits for all the
+// k-tiles it staged), and the mbarriers lie outside the staging buffers.
+struct PlanScratch {
+    plan::WarpArea<kWordBlocks> plan[kPW];
+    ActiveList act_plan, act_clear;
+    uint32_t wtot[kPW][2];
+};
+
 template <bool kM4R>
 struct PersistSmem {
     tiled::TiledSmem<kM4R> prod;
-    plan::WarpArea<kWordBlocks> plan[kThreads / 32];
     alignas(16) unsigned char tables[kTableBytes];
-    ActiveList act_plan, act_clear;
-    uint32_t wtot[kThreads / 32][2];
+    __device__ PlanScratch &scratch() { return *reinterpret_cast<PlanScratch *>(&prod.q[0][0]); }
 };
+static_assert(sizeof(PlanScratch) <= sizeof(tiled::TiledSmem<false>::q), "phase-A scratch fits the staging buffers");
 
 struct PersistArgs {
     const ProdDesc *prods;
@@ -94,7 +107,16 @@ struct PersistArgs {
     SelLogRow *sel_log;
     uint32_t sel_log_iters;
     const QueryRange *qr;           // non-null (batches of 2..kMaxActive queries): active-query phase A
+    ItemTrace *trace;               // non-null: one record per processed item (first kItemTraceCap)
+    uint32_t *trace_count;
 };
+
+// Records one processed item (thread 0 of the CTA).
+__device__ __forceinline__ void trace_item(const PersistArgs &a, uint64_t it, uint32_t iter, uint32_t list,
+                                           unsigned long long t0) {
+    const uint32_t k = atomicAdd(a.trace_count, 1u);
+    if (k < kItemTraceCap) a.trace[k] = ItemTrace{it, iter, (uint16_t)blockIdx.x, (uint16_t)list, t0, globaltimer_ns()};
+}
 
 // Block-wide compaction of the queries whose flag is set (every query when
 // flags is null) into L, with the prefix sum of their plan rows (slot rows
@@ -187,9 +209,10 @@ __device__ __forceinline__ bool grid_barrier(IterState *st, uint32_t &gen) {
 }
 
 template <bool kHasM4R>
-__global__ void __launch_bounds__(kThreads, 3) k_closure_persistent(PersistArgs a) {
+__global__ void __launch_bounds__(kThreads, 2) k_closure_persistent(PersistArgs a) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     PersistSmem<kHasM4R> &S = *reinterpret_cast<PersistSmem<kHasM4R> *>(smem_raw);
+    PlanScratch &X = S.scratch();
     IterState *st = a.st;
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t gwarp = blockIdx.x * (kThreads / 32) + warp, nwarps = gridDim.x * (kThreads / 32);
@@ -243,23 +266,23 @@ __global__ void __launch_bounds__(kThreads, 3) k_closure_persistent(PersistArgs 
             // plan: queries that changed in t-1 (all in iteration 0); clear:
             // queries that changed in t-2 (all in iteration 1, none in 0)
             const uint32_t nq = st->nqueries;
-            build_active(S.act_plan, t > 0 ? a.qt.changed + ((t - 1) % 3) * nq : nullptr, a.qr, nq, false, S.wtot);
+            build_active(X.act_plan, t > 0 ? a.qt.changed + ((t - 1) % 3) * nq : nullptr, a.qr, nq, false, X.wtot);
             if (t > 0)
-                build_active(S.act_clear, t > 1 ? a.qt.changed + ((t - 2) % 3) * nq : nullptr, a.qr, nq, true,
-                             S.wtot);
-            const uint32_t np = S.act_plan.pref[S.act_plan.n], ns = t > 0 ? S.act_clear.pref[S.act_clear.n] : 0u;
+                build_active(X.act_clear, t > 1 ? a.qt.changed + ((t - 2) % 3) * nq : nullptr, a.qr, nq, true,
+                             X.wtot);
+            const uint32_t np = X.act_plan.pref[X.act_plan.n], ns = t > 0 ? X.act_clear.pref[X.act_clear.n] : 0u;
             for (uint32_t u = gwarp; u < np + ns; u += nwarps) {
                 if (u < np) {
-                    const uint32_t i = active_find(S.act_plan, u);
-                    const QueryRange qr = a.qr[S.act_plan.q[i]];
-                    plan::plan_row(qr.prow0 + (u - S.act_plan.pref[i]), prods, a.nprods, slots, t, st,
+                    const uint32_t i = active_find(X.act_plan, u);
+                    const QueryRange qr = a.qr[X.act_plan.q[i]];
+                    plan::plan_row(qr.prow0 + (u - X.act_plan.pref[i]), prods, a.nprods, slots, t, st,
                                    st->pitem_count[par], a.items + (size_t)(2 * par) * a.list_cap, a.list_cap, a.tpb,
-                                   a.prod_seen, 0, psel, S.plan[warp].cnt, S.plan[warp].bnd, qr.prod0,
+                                   a.prod_seen, 0, psel, X.plan[warp].cnt, X.plan[warp].bnd, qr.prod0,
                                    qr.prod0 + qr.nprod);
                 } else {
-                    const uint32_t i = active_find(S.act_clear, u - np);
-                    const QueryRange qr = a.qr[S.act_clear.q[i]];
-                    clear_delta_row(slots, a.nslots, qr.srow0 + (u - np - S.act_clear.pref[i]), par ^ 1, qr.slot0,
+                    const uint32_t i = active_find(X.act_clear, u - np);
+                    const QueryRange qr = a.qr[X.act_clear.q[i]];
+                    clear_delta_row(slots, a.nslots, qr.srow0 + (u - np - X.act_clear.pref[i]), par ^ 1, qr.slot0,
                                     qr.slot0 + qr.nslot);
                 }
                 __syncwarp();
@@ -271,13 +294,14 @@ __global__ void __launch_bounds__(kThreads, 3) k_closure_persistent(PersistArgs 
                 if (u < a.prod_rows) {
                     plan::plan_row(u, prods, a.nprods, slots, t, st, st->pitem_count[par],
                                    a.items + (size_t)(2 * par) * a.list_cap, a.list_cap, a.tpb, a.prod_seen, 0,
-                                   psel, S.plan[warp].cnt, S.plan[warp].bnd);
+                                   psel, X.plan[warp].cnt, X.plan[warp].bnd);
                 } else {
                     clear_delta_row(slots, a.nslots, u - a.prod_rows, par ^ 1);
                 }
                 __syncwarp();
             }
         }
+        fence_proxy_async_smem();  // the scratch writes come before the next bulk copies into the same bytes
         if (!grid_barrier(st, gen)) timed_out = true;
         if (blockIdx.x == 0 && tid == 0 && a.phase_log && t - iter0 < a.phase_log_iters)
             a.phase_log[3 * (t - iter0) + 1] = globaltimer_ns();
@@ -298,8 +322,10 @@ __global__ void __launch_bounds__(kThreads, 3) k_closure_persistent(PersistArgs 
                 const uint32_t idx = S.prod.item;
                 __syncthreads();
                 if (idx >= n0) break;
-                tiled::process_item<false>(S.prod, items[idx], prods, slots, t, &st->pchanged[par], qchanged, phase,
+                const unsigned long long t0 = a.trace ? globaltimer_ns() : 0ull;
+                tiled::process_item<false, kPW>(S.prod, items[idx], prods, slots, t, &st->pchanged[par], qchanged, phase,
                                            timed_out, ctr, a.cnts);
+                if (a.trace && tid == 0) trace_item(a, items[idx], t, 0, t0);
             }
             if constexpr (kHasM4R) {
                 const uint32_t n1 = st->pitem_count[par][1];
@@ -309,8 +335,10 @@ __global__ void __launch_bounds__(kThreads, 3) k_closure_persistent(PersistArgs 
                     const uint32_t idx = S.prod.item;
                     __syncthreads();
                     if (idx >= n1) break;
-                    tiled::process_item<true>(S.prod, items[a.list_cap + idx], prods, slots, t,
+                    const unsigned long long t0 = a.trace ? globaltimer_ns() : 0ull;
+                    tiled::process_item<true, kPW>(S.prod, items[a.list_cap + idx], prods, slots, t,
                                               &st->pchanged[par], qchanged, phase, timed_out, ctr, a.cnts);
+                    if (a.trace && tid == 0) trace_item(a, items[a.list_cap + idx], t, 1, t0);
                 }
             }
         }
@@ -346,12 +374,12 @@ __global__ void __launch_bounds__(kThreads, 3) k_closure_persistent(PersistArgs 
         const uint32_t par = t & 1;
         if (a.qr) {  // queries planned in iteration t
             const uint32_t nq = st->nqueries;
-            build_active(S.act_clear, t > 0 ? a.qt.changed + ((t - 1) % 3) * nq : nullptr, a.qr, nq, true, S.wtot);
-            const uint32_t ns = S.act_clear.pref[S.act_clear.n];
+            build_active(X.act_clear, t > 0 ? a.qt.changed + ((t - 1) % 3) * nq : nullptr, a.qr, nq, true, X.wtot);
+            const uint32_t ns = X.act_clear.pref[X.act_clear.n];
             for (uint32_t u = gwarp; u < ns; u += nwarps) {
-                const uint32_t i = active_find(S.act_clear, u);
-                const QueryRange qr = a.qr[S.act_clear.q[i]];
-                clear_delta_row(slots, a.nslots, qr.srow0 + (u - S.act_clear.pref[i]), par, qr.slot0,
+                const uint32_t i = active_find(X.act_clear, u);
+                const QueryRange qr = a.qr[X.act_clear.q[i]];
+                clear_delta_row(slots, a.nslots, qr.srow0 + (u - X.act_clear.pref[i]), par, qr.slot0,
                                 qr.slot0 + qr.nslot);
                 __syncwarp();
             }
@@ -412,7 +440,8 @@ cudaError_t launch_closure_persistent(int has_m4r, int grid, const ProdDesc *pro
                                       const QueryTrack &qt, int tpb, unsigned long long *phase_log,
                                       uint32_t phase_log_iters, BufCounters *cnts, uint8_t *choice,
                                       const SelectorParams *sel, SelLogRow *sel_log, uint32_t sel_log_iters,
-                                      const QueryRange *qr, cudaStream_t s) {
+                                      const QueryRange *qr, ItemTrace *trace, uint32_t *trace_count,
+                                      cudaStream_t s) {
     PersistArgs a;
     a.prods = prods;
     a.nprods = nprods;
@@ -434,6 +463,8 @@ cudaError_t launch_closure_persistent(int has_m4r, int grid, const ProdDesc *pro
     a.sel_log = sel_log;
     a.sel_log_iters = sel_log_iters;
     a.qr = qr;
+    a.trace = trace;
+    a.trace_count = trace_count;
     void *args[] = {&a};
     if (has_m4r)
         return cudaLaunchCooperativeKernel((const void *)k_closure_persistent<true>, dim3(grid), dim3(kThreads), args,

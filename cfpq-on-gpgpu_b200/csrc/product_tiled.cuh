@@ -10,10 +10,10 @@ namespace cfpq {
 namespace tiled {
 
 
-constexpr int kBJ = 16;
+constexpr int kBJ = 16;              // output tiles per work item (1024 columns)
 constexpr uint32_t kStages = 4;      // staged k-tiles in flight per CTA
-constexpr uint32_t kLaneBits = 4;    // sparse loop: bits per row a lane walks before the warp helps              // output tiles per work item (1024 columns)
-constexpr int kThreads = 128;        // 4 warps
+constexpr uint32_t kLaneBits = 4;    // sparse loop: bits per row a lane walks before the warp helps
+constexpr int kThreads = 128;        // 4 warps (product kernels; the persistent kernel runs 8)
 constexpr int kMaxTiles = 2048;      // k-list capacity (n <= 131072)
 constexpr uint32_t kSparseMax = 96;  // P-tile population up to which the sparse loop runs
 constexpr int kTabRow = kBJ + 1;     // padded table row (uint64 words)
@@ -69,15 +69,20 @@ struct ItemCounters {
     unsigned long long triples = 0, staged = 0, outw = 0, neww = 0;
 };
 
-// Process work item `it` (all threads of the CTA).  `phase` is the CTA's
-// mbarrier parity state (bit s = next parity of stage s), `timed_out` is set
-// (CTA-uniformly) when a bounded wait gave up; new bits set *changed and
-// qchanged[query].  Ends with the CTA synchronised.
-template <bool kM4R, class Smem>
+// Process work item `it` (all kW warps of the CTA; warp w owns output tiles
+// kTPW*w .. kTPW*w + kTPW-1 of the block, lane l rows 2l and 2l+1).  `phase`
+// is the CTA's mbarrier parity state (bit s = next parity of stage s),
+// `timed_out` is set (CTA-uniformly) when a bounded wait gave up; new bits
+// set *changed and qchanged[query].  Ends with the CTA synchronised.
+template <bool kM4R, int kW, class Smem>
 __device__ __forceinline__ void process_item(Smem &S, uint64_t it, const ProdDesc *__restrict__ prods,
                                              const MatSlot *__restrict__ slots, uint32_t iter, uint32_t *changed,
                                              uint32_t *qchanged, uint32_t &phase, bool &timed_out,
                                              ItemCounters &ctr, BufCounters *cnts) {
+    static_assert(kBJ % kW == 0 && kBJ / kW <= 4, "whole tiles per warp, at most 4");
+    constexpr int kTPW = kBJ / kW;             // output tiles per warp
+    constexpr uint32_t kNT = 32u * kW;         // threads
+    constexpr uint32_t kWMask = (1u << kTPW) - 1;
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     unsigned long long &triples = ctr.triples, &staged = ctr.staged, &outw = ctr.outw, &neww = ctr.neww;
     const ProdDesc pd = prods[item_prod(it)];
@@ -119,7 +124,7 @@ __device__ __forceinline__ void process_item(Smem &S, uint64_t it, const ProdDes
     // rank the candidates with a non-empty Q block in increasing tk order
     // (ballot per round of 32)
     const uint32_t nc = S.nc, rounds = (nc + 31) / 32;
-    for (uint32_t r = warp; r < rounds; r += kThreads / 32) {
+    for (uint32_t r = warp; r < rounds; r += kW) {
         const uint32_t c = r * 32 + lane;
         uint32_t mask = 0;
         bool dense = false;
@@ -152,7 +157,7 @@ __device__ __forceinline__ void process_item(Smem &S, uint64_t it, const ProdDes
         }
     }
     __syncthreads();
-    for (uint32_t c = tid; c < nc; c += kThreads) {
+    for (uint32_t c = tid; c < nc; c += kNT) {
         const uint32_t mask = S.cmask[c];
         if (!mask) continue;
         const uint32_t rank = S.roff[c >> 5] + __popc(S.rball[c >> 5] & ((1u << (c & 31)) - 1));
@@ -164,9 +169,9 @@ __device__ __forceinline__ void process_item(Smem &S, uint64_t it, const ProdDes
     __syncthreads();
     const uint32_t nk = S.nk;
 
-    uint2 acc0[4], acc1[4];
+    uint2 acc0[kTPW], acc1[kTPW];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) acc0[j] = acc1[j] = make_uint2(0, 0);
+    for (int j = 0; j < kTPW; ++j) acc0[j] = acc1[j] = make_uint2(0, 0);
 
     // ---- staged k-tiles ----
     auto issue = [&](uint32_t e, uint32_t stage) -> uint32_t {
@@ -192,7 +197,7 @@ __device__ __forceinline__ void process_item(Smem &S, uint64_t it, const ProdDes
         if (!timed_out && !mbar_wait_bounded(&S.bar[stage], (phase >> stage) & 1u)) timed_out = true;
         phase ^= 1u << stage;
         const bool dense = (S.ktile[e] & 0x8000u) != 0;
-        const uint32_t wmask = ((uint32_t)S.kmask[e] >> (4 * warp)) & 0xFu;
+        const uint32_t wmask = ((uint32_t)S.kmask[e] >> (kTPW * warp)) & kWMask;
         const uint4 pp = *reinterpret_cast<const uint4 *>(&S.p[stage][2 * lane]);
         if (!dense) {
             // sparse P tile, only the occupied Q tiles staged.  Each lane
@@ -201,7 +206,7 @@ __device__ __forceinline__ void process_item(Smem &S, uint64_t it, const ProdDes
             // at a time by the whole warp: lane i takes the i-th remaining
             // bit, and the partial ORs meet in a warp OR-reduction.
             if (wmask && !timed_out) {
-                const uint64_t *q = &S.q[stage][(4 * warp) * 64];
+                const uint64_t *q = &S.q[stage][(kTPW * warp) * 64];
                 uint64_t xa = ((uint64_t)pp.y << 32) | pp.x;
                 uint64_t xb = ((uint64_t)pp.w << 32) | pp.z;
 #pragma unroll 1
@@ -210,14 +215,14 @@ __device__ __forceinline__ void process_item(Smem &S, uint64_t it, const ProdDes
                         const int k = __ffsll((long long)xa) - 1;
                         xa &= xa - 1;
 #pragma unroll
-                        for (int j = 0; j < 4; ++j)
+                        for (int j = 0; j < kTPW; ++j)
                             if ((wmask >> j) & 1u) or64(acc0[j], q[j * 64 + k]);
                     }
                     if (xb) {
                         const int k = __ffsll((long long)xb) - 1;
                         xb &= xb - 1;
 #pragma unroll
-                        for (int j = 0; j < 4; ++j)
+                        for (int j = 0; j < kTPW; ++j)
                             if ((wmask >> j) & 1u) or64(acc1[j], q[j * 64 + k]);
                     }
                 }
@@ -231,29 +236,31 @@ __device__ __forceinline__ void process_item(Smem &S, uint64_t it, const ProdDes
                         const uint64_t x = __shfl_sync(kFull, xr, src);
                         const uint32_t lo = (uint32_t)x, hi = (uint32_t)(x >> 32), nlo = __popc(lo);
                         const uint32_t cnt = nlo + __popc(hi);
-                        uint64_t o[4] = {0, 0, 0, 0};
+                        uint64_t o[kTPW];
+#pragma unroll
+                        for (int j = 0; j < kTPW; ++j) o[j] = 0;
                         for (uint32_t b = lane; b < cnt; b += 32) {
                             const uint32_t k = b < nlo ? nth_bit(lo, b) : 32 + nth_bit(hi, b - nlo);
 #pragma unroll
-                            for (int j = 0; j < 4; ++j)
+                            for (int j = 0; j < kTPW; ++j)
                                 if ((wmask >> j) & 1u) o[j] |= q[j * 64 + k];
                         }
 #pragma unroll
-                        for (int j = 0; j < 4; ++j) {
+                        for (int j = 0; j < kTPW; ++j) {
                             if (!((wmask >> j) & 1u)) continue;
 #pragma unroll
                             for (int d = 16; d > 0; d >>= 1) o[j] |= __shfl_xor_sync(kFull, o[j], d);
                         }
                         if ((int)lane == src) {
 #pragma unroll
-                            for (int j = 0; j < 4; ++j) or64(half ? acc1[j] : acc0[j], o[j]);
+                            for (int j = 0; j < kTPW; ++j) or64(half ? acc1[j] : acc0[j], o[j]);
                         }
                     }
                 }
             }
         } else if constexpr (kM4R) {
             // build: (slab s, tile j) pairs over the CTA; 16 keys each
-            for (uint32_t pr = tid; pr < 16 * kBJ; pr += kThreads) {
+            for (uint32_t pr = tid; pr < 16 * kBJ; pr += kNT) {
                 const uint32_t s = pr / kBJ, j = pr % kBJ;
                 const uint64_t *qr = &S.q[stage][j * 64 + 4 * s];
                 const uint64_t q0 = qr[0], q1 = qr[1], q2 = qr[2], q3 = qr[3];
@@ -282,10 +289,10 @@ __device__ __forceinline__ void process_item(Smem &S, uint64_t it, const ProdDes
                 const uint64_t pb = ((uint64_t)pp.w << 32) | pp.z;  // row 2l+1
 #pragma unroll
                 for (int s = 0; s < 16; ++s) {
-                    const uint64_t *ta = &S.tab[(s * 16 + (uint32_t)((pa >> (4 * s)) & 15u)) * kTabRow + 4 * warp];
-                    const uint64_t *tb = &S.tab[(s * 16 + (uint32_t)((pb >> (4 * s)) & 15u)) * kTabRow + 4 * warp];
+                    const uint64_t *ta = &S.tab[(s * 16 + (uint32_t)((pa >> (4 * s)) & 15u)) * kTabRow + kTPW * warp];
+                    const uint64_t *tb = &S.tab[(s * 16 + (uint32_t)((pb >> (4 * s)) & 15u)) * kTabRow + kTPW * warp];
 #pragma unroll
-                    for (int j = 0; j < 4; ++j) {
+                    for (int j = 0; j < kTPW; ++j) {
                         or64(acc0[j], ta[j]);
                         or64(acc1[j], tb[j]);
                     }
@@ -293,7 +300,7 @@ __device__ __forceinline__ void process_item(Smem &S, uint64_t it, const ProdDes
             }
         } else {
             if (wmask && !timed_out) {
-                const uint64_t *q = &S.q[stage][(4 * warp) * 64];
+                const uint64_t *q = &S.q[stage][(kTPW * warp) * 64];
 #pragma unroll
                 for (int kk = 0; kk < 64; kk += 2) {
                     const uint32_t pa = kk < 32 ? pp.x : pp.y;  // row 2l
@@ -302,7 +309,7 @@ __device__ __forceinline__ void process_item(Smem &S, uint64_t it, const ProdDes
                     const uint32_t ma0 = bitmask(pa, b), ma1 = bitmask(pa, b + 1);
                     const uint32_t mb0 = bitmask(pb, b), mb1 = bitmask(pb, b + 1);
 #pragma unroll
-                    for (int j = 0; j < 4; ++j) {
+                    for (int j = 0; j < kTPW; ++j) {
                         const uint4 qv = *reinterpret_cast<const uint4 *>(q + j * 64 + kk);
                         acc0[j].x |= (qv.x & ma0) | (qv.z & ma1);
                         acc0[j].y |= (qv.y & ma0) | (qv.w & ma1);
@@ -320,28 +327,29 @@ __device__ __forceinline__ void process_item(Smem &S, uint64_t it, const ProdDes
     // ---- epilogue: the 8 words of the thread in three batches (loads of C,
     // then the atomics that can add bits, then D / populations), so that
     // their global round trips overlap ----
-    uint64_t av[8], seen[8], prev[8];
-    size_t off[8];
+    constexpr int kWords = 2 * kTPW;
+    uint64_t av[kWords], seen[kWords], prev[kWords];
+    size_t off[kWords];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
+    for (int k = 0; k < kWords; ++k) {
         const int j = k >> 1, rr = k & 1;
         const uint2 a2 = rr ? acc1[j] : acc0[j];
-        const uint32_t tj = tj0 + 4 * warp + j;
+        const uint32_t tj = tj0 + kTPW * warp + j;
         av[k] = tj < T ? (((uint64_t)a2.y << 32) | a2.x) : 0ULL;
         off[k] = tile_offset(T, ti, tj < T ? tj : 0) + 2 * lane + rr;
         outw += av[k] != 0;
     }
 #pragma unroll
-    for (int k = 0; k < 8; ++k)
+    for (int k = 0; k < kWords; ++k)
         seen[k] = av[k] ? __ldcg(reinterpret_cast<const unsigned long long *>(C.bits + off[k])) : ~0ULL;
 #pragma unroll
-    for (int k = 0; k < 8; ++k)
+    for (int k = 0; k < kWords; ++k)
         prev[k] = (av[k] & ~seen[k]) ? atomicOr(reinterpret_cast<unsigned long long *>(C.bits + off[k]),
                                                 (unsigned long long)av[k])
                                      : ~0ULL;
-    uint32_t tile_new[4];
+    uint32_t tile_new[kTPW];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
+    for (int j = 0; j < kTPW; ++j) {
         uint32_t newcnt = 0;
 #pragma unroll
         for (int rr = 0; rr < 2; ++rr) {
@@ -353,14 +361,18 @@ __device__ __forceinline__ void process_item(Smem &S, uint64_t it, const ProdDes
                 if (D.bits) atomicOr(reinterpret_cast<unsigned long long *>(D.bits + off[k]), (unsigned long long)nw);
             }
         }
-        tile_new[j] = __reduce_add_sync(kFull, newcnt);  // the warp's rows of tile tj0 + 4*warp + j
+        tile_new[j] = __reduce_add_sync(kFull, newcnt);  // the warp's rows of tile tj0 + kTPW*warp + j
     }
-    const bool any_new = (tile_new[0] | tile_new[1] | tile_new[2] | tile_new[3]) != 0;
-    if (any_new) {  // lane j updates tile j of the warp (populations, occupancy, buffer counters)
-        const uint32_t mine = lane == 0 ? tile_new[0] : lane == 1 ? tile_new[1] : lane == 2 ? tile_new[2]
-                            : lane == 3 ? tile_new[3] : 0u;
-        tiles_gain(C, ti, tj0 + 4 * warp, mine, cnts ? cnts + 3 * pd.head : nullptr);
-        if (D.bits) tiles_gain(D, ti, tj0 + 4 * warp, mine, cnts ? cnts + 3 * pd.head + 1 + ((iter & 1) ^ 1) : nullptr);
+    uint32_t mine = 0, any = 0;  // lane j updates tile j of the warp (populations, occupancy, buffer counters)
+#pragma unroll
+    for (int j = 0; j < kTPW; ++j) {
+        any |= tile_new[j];
+        if (lane == (uint32_t)j) mine = tile_new[j];
+    }
+    const bool any_new = any != 0;
+    if (any_new) {
+        tiles_gain(C, ti, tj0 + kTPW * warp, mine, cnts ? cnts + 3 * pd.head : nullptr);
+        if (D.bits) tiles_gain(D, ti, tj0 + kTPW * warp, mine, cnts ? cnts + 3 * pd.head + 1 + ((iter & 1) ^ 1) : nullptr);
     }
     if (any_new && lane == 0) {
         *changed = 1u;

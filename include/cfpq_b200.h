@@ -413,6 +413,23 @@ int cfpq_autotune(cfpq_ctx *ctx, const cfpq_autotune_opts *opts, cfpq_selector_c
  * (at most 4096; 0 when the last closure did not run persistently). */
 size_t cfpq_last_phase_log(cfpq_ctx *ctx, uint64_t *out, size_t cap);
 
+/* Work-item trace of the last persistent closure run with
+ * opts->log_products & CFPQ_LOG_ITEMS: one record per processed work item
+ * (the first 65536), in no particular order.  `item` is the item's encoding
+ * (bits 48-63 product index in the closure, 37-47 tile-row, 28-36 block of 16
+ * output tiles, 16-27 first k-tile, 4-15 end k-tile), `list` 0 for the LOP3
+ * inner loop and 1 for Four Russians; times are %globaltimer ns taken by the
+ * CTA around the item.  Copies min(cap, count) records and returns the count
+ * (0 when the last closure was not traced). */
+#define CFPQ_LOG_ITEMS 8
+typedef struct cfpq_item_record {
+    uint64_t item;
+    uint32_t iteration;
+    uint16_t cta, list;
+    uint64_t start_ns, end_ns;
+} cfpq_item_record;
+size_t cfpq_item_log(cfpq_ctx *ctx, cfpq_item_record *out, size_t cap);
+
 #ifdef __cplusplus
 }
 #endif

@@ -396,6 +396,31 @@ def test_batch_active_queries(ctx, pkg, oracle, tmp_path):
             q.close()
 
 
+def test_item_trace(ctx, pkg, oracle, tmp_path):
+    """LOG_ITEMS records every work item of a persistent closure once, and
+    tracing does not change the result."""
+    wl = pkg.workloads.ontology_query(1024, 2)
+    gp, rp = _write(wl, tmp_path)
+    exp = _oracle_run(oracle, gp, rp)[0]
+    q = pkg.query.PreparedQuery(ctx, wl.grammar, wl.graph)
+    try:
+        q.load()
+        st = ctx.closure(wl.grammar.rules, q.mats, use_graph="device", log_products=pkg.capi.LOG_ITEMS)
+        assert dict(zip(q.grammar.nonterminals, ctx.hash_count_many(q.mats))) == exp
+        tr = ctx.item_log()
+        assert len(tr) == st["work_items"] > 0
+        assert (tr["end_ns"] >= tr["start_ns"]).all()
+        assert (tr["iteration"] < st["iterations"]).all()
+        assert (tr["product"] < 2 * len(wl.grammar.rules)).all()
+        assert (tr["klo"] < tr["khi"]).all() and (tr["khi"] <= (1024 + 63) // 64).all()
+        assert set(np.unique(tr["list"])) <= {0, 1}
+        q.load()
+        ctx.closure(wl.grammar.rules, q.mats, use_graph="device")
+        assert len(ctx.item_log()) == 0
+    finally:
+        q.close()
+
+
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 GOLDEN_CASES = sorted(d for d in os.listdir(GOLDEN) if os.path.isdir(os.path.join(GOLDEN, d)))
 
