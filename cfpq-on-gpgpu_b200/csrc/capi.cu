@@ -1332,6 +1332,9 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
             if (it > (1u << 24)) return set_error(CFPQ_ERR_CUDA, "closure did not converge");
         }
     } else if (persistent) {
+        // the kernel's item lists (one per iteration parity, at 0 and 2 * item_cap)
+        // start empty: a zero entry means "not yet written"
+        CUDA_TRY(cudaMemsetAsync(ctx->items.p, 0, 3 * pl.item_cap * 8, ctx->stream));
         CUDA_TRY(launch_closure_persistent(pl.uses_m4r ? 1 : 0, persist_grid, ctx->prods.as<ProdDesc>(),
                                            (uint32_t)pl.prods.size(), pl.prod_rows, ctx->slots.as<MatSlot>(),
                                            (uint32_t)pl.slots.size(), pl.slot_rows, ctx->d_st,

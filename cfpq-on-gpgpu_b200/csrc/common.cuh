@@ -73,10 +73,16 @@ struct IterState {
     uint32_t active;        // loop condition mirror (1 while iterating)
     uint32_t nqueries;
     uint32_t blocks_done;   // blocks of the advance kernel that finished (the last one ends the iteration)
-    // persistent closure kernel: grid barrier and per-parity iteration counters
-    uint32_t bar_count, bar_gen;
-    uint32_t pitem_count[2][2], pitem_next[2][2];  // [iteration parity][list]
-    uint32_t pchanged[2];
+    // persistent closure kernel: per-parity iteration counters
+    uint32_t pitem_count[2][2];  // [iteration parity][list]
+    uint32_t pitem_m4r[2];       // Four Russians items among pitem_count[.][0]
+    // polled by every CTA of the persistent kernel: own cache lines
+    alignas(128) uint32_t plan_done[2];  // CTAs done with the plan/clear units of the iteration (per parity)
+    alignas(128) uint32_t pitem_next[2][2];
+    // grid barrier of the iterations of parity p: low 32 bits count the CTAs'
+    // arrivals (cumulative over the closure), high 32 bits are the
+    // iteration's flags (kBarChanged, kBarAbort), read with the count
+    alignas(128) unsigned long long pbar[2];
     unsigned long long tile_triples;
     unsigned long long items_total;
     unsigned long long products;      // non-empty product terms over all iterations
@@ -149,6 +155,9 @@ struct PlanSelect {
     SelLogRow *log;
     uint32_t log_iters;
 };
+
+constexpr uint32_t kBarChanged = 1u;  // some product set a new bit
+constexpr uint32_t kBarAbort = 2u;    // a CTA gave up a bounded wait
 
 // Rows, slots and products of one query of a closure (all contiguous): plan
 // rows [prow0, prow0 + nprow), slot tile-rows [srow0, srow0 + nsrow), slots

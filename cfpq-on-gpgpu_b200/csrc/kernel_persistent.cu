@@ -1,26 +1,30 @@
 // Persistent closure kernel: the whole semi-naive fixpoint of a closure whose
 // products all use the word-level variants (LOP3 / M4R) in ONE cooperative
-// launch (every CTA resident), iterations separated by grid barriers instead
-// of kernel boundaries.
+// launch (every CTA resident), one grid barrier per iteration instead of
+// kernel boundaries.
 //
 // Iteration t (parity par = t & 1), every CTA:
-//   phase A  warps take units round-robin: the product tile-rows (plan::plan_row
-//            emits the iteration's work items into the item lists of parity
-//            par; AUTO closures: the planner also chooses each term's variant,
-//            select_device.cuh) and, for t >= 1, the slot tile-rows of the delta read in
-//            iteration t-1 (dlt[par ^ 1], cleared: the products of iteration t
-//            write their new bits there).  CTA 0 also folds the counters of
-//            parity par ^ 1 (iteration t-1) into the statistics and zeroes them.
-//            Batches of at most kMaxActive queries plan only the queries that
-//            changed in iteration t-1 and clear only those that changed in
-//            t-2 (the deltas of the others are empty): every CTA compacts
-//            the per-query changed flags into its own active lists first, so
-//            converged queries cost nothing in the tail of a batch.
-//   barrier
-//   phase B  CTAs take work items (LOP3 list, then M4R list) and run
-//            tiled::process_item; new bits set changed[par] and the query's
-//            flag in qt.changed[t % 3] (three rotating flag arrays: iteration
-//            t reads those of t-1 and t-2; CTA 0 zeroes those of t+1 here).
+//   plan     warps take units round-robin: the product tile-rows (plan::plan_row
+//            appends the iteration's work items to the item list of parity
+//            par, Four Russians items marked by bit 0; AUTO closures: the
+//            planner also chooses each term's variant, select_device.cuh) and,
+//            for t >= 1, the slot tile-rows of the delta read in iteration t-1
+//            (dlt[par ^ 1], cleared: the products of iteration t write their
+//            new bits there).  CTA 0 also folds the counters of parity par ^ 1
+//            (iteration t-1) into the statistics and zeroes them.  Batches of
+//            at most kMaxActive queries plan only the queries that changed in
+//            iteration t-1 and clear only those that changed in t-2 (the
+//            deltas of the others are empty): every CTA compacts the
+//            per-query changed flags into its own active lists first, so
+//            converged queries cost nothing in the tail of a batch.  The CTA
+//            then counts itself in plan_done[par].
+//   products the CTA takes items from the list as soon as they are written
+//            (no barrier after the plan) and runs tiled::process_item; an
+//            item merges its results only once every CTA is done planning
+//            and clearing (plan_done[par] == grid).  New bits set
+//            changed[par] and the query's flag in qt.changed[t % 3] (three
+//            rotating flag arrays: iteration t reads those of t-1 and t-2;
+//            CTA 0 zeroes those of t+1 after the barrier of t).
 //   barrier
 //   decision every CTA reads changed[par] (final after the barrier) and the
 //            error word: continue while something changed, no wait gave up
@@ -29,8 +33,14 @@
 // After the loop the delta read in the last iteration is cleared, so the
 // delta buffers go back to the pool zeroed.
 //
+// Overlapping the plan with the products is exact: an item's operands only
+// grow after its planner read them (its k-tile range is a fixed part of
+// [0, T) and the item re-reads the occupancy), so it covers at least the
+// semi-naive terms of its planner, and bits it finds beyond those are true
+// and recorded in the delta like any other.
+//
 // The same plan and item code as the multi-kernel iteration runs here; only
-// the sequencing differs.  Barrier waits are bounded: a CTA that gives up sets
+// the sequencing differs.  Every wait is bounded: a CTA that gives up sets
 // the error word and leaves the loop, and every other wait then gives up too.
 #include "launch.h"
 #include "plan_device.cuh"
@@ -177,34 +187,33 @@ __device__ __forceinline__ uint32_t active_find(const ActiveList &L, uint32_t u)
     return lo;
 }
 
-// Grid barrier (all CTAs of the cooperative launch): arrival counter plus a
-// generation word; `gen` is the CTA's copy of the generation.  Returns false
-// when the wait gave up.
-__device__ __forceinline__ bool grid_barrier(IterState *st, uint32_t &gen) {
-    __shared__ uint32_t s_ok;
+// Grid barrier of an iteration (all CTAs of the cooperative launch) on the
+// 64-bit word w: every CTA adds one arrival to the low half and polls the
+// word until the count reaches `target`; the high half, final by then, comes
+// with the same load.  Returns false when the wait gave up; *flags receives
+// the high half.
+__device__ __forceinline__ bool grid_barrier(unsigned long long *w, uint32_t target, bool abort, uint32_t *flags) {
+    __shared__ uint32_t s_ok, s_flags;
     __syncthreads();
     if (threadIdx.x == 0) {
         uint32_t ok = 1;
         __threadfence();
-        if (atomicAdd(&st->bar_count, 1u) + 1 == gridDim.x) {
-            st->bar_count = 0;
-            __threadfence();
-            atomicAdd(&st->bar_gen, 1u);
-        } else {
-            uint32_t i = 0;
-            while (*reinterpret_cast<volatile uint32_t *>(&st->bar_gen) == gen) {
-                if (++i > kBarrierSpinLimit) {
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(32);
+        if (abort) atomicOr(reinterpret_cast<uint32_t *>(w) + 1, kBarAbort);
+        unsigned long long v = atomicAdd(w, 1ull) + 1ull;
+        uint32_t i = 0;
+        while ((uint32_t)v < target) {
+            if (++i > kBarrierSpinLimit) {
+                ok = 0;
+                break;
             }
+            v = *reinterpret_cast<volatile unsigned long long *>(w);
         }
         __threadfence();
         s_ok = ok;
+        s_flags = (uint32_t)(v >> 32);
     }
-    ++gen;
     __syncthreads();
+    *flags = s_flags;
     return s_ok != 0;
 }
 
@@ -216,12 +225,12 @@ __global__ void __launch_bounds__(kThreads, 2) k_closure_persistent(PersistArgs 
     IterState *st = a.st;
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t gwarp = blockIdx.x * (kThreads / 32) + warp, nwarps = gridDim.x * (kThreads / 32);
-    __shared__ uint32_t s_gen0, s_go;
+    __shared__ uint32_t s_stop;
+    __shared__ unsigned long long s_item;
 
     if (tid == 0) {
         for (uint32_t i = 0; i < tiled::kStages; ++i) mbar_init(&S.prod.bar[i], 1);
         fence_mbar_init();
-        s_gen0 = st->bar_gen;
     }
     const size_t slot_bytes = (size_t)a.nslots * sizeof(MatSlot), prod_bytes = (size_t)a.nprods * sizeof(ProdDesc);
     const bool cached = slot_bytes + prod_bytes <= kTableBytes;
@@ -238,7 +247,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_closure_persistent(PersistArgs 
     }
     __syncthreads();
     const PlanSelect psel = {a.sel && a.cnts ? a.sel : nullptr, a.cnts, nullptr, a.choice, a.sel_log, a.sel_log_iters};
-    uint32_t gen = s_gen0, phase = 0;
+    uint32_t phase = 0, bar_uses[2] = {0, 0};
     bool timed_out = false;
     ItemCounters ctr;
     const uint32_t iter0 = st->iter, max_iter = st->max_iter;
@@ -246,20 +255,26 @@ __global__ void __launch_bounds__(kThreads, 2) k_closure_persistent(PersistArgs 
 
     for (;; ++t) {
         const uint32_t par = t & 1;
+        uint64_t *const items = a.items + (size_t)(2 * par) * a.list_cap;  // one list per parity
         if (blockIdx.x == 0 && tid == 0) {
             if (a.phase_log && t - iter0 < a.phase_log_iters) a.phase_log[3 * (t - iter0)] = globaltimer_ns();
+            // flags of this iteration's barrier word (last read before the
+            // barrier of t-1; next set after every CTA's plan of t)
+            if (t > iter0 + 1) reinterpret_cast<uint32_t *>(&st->pbar[par])[1] = 0;
             if (t > iter0) {  // counters of iteration t-1 -> statistics, then reset for iteration t+1
                 const uint32_t q = par ^ 1;
-                const uint32_t c0 = st->pitem_count[q][0], c1 = st->pitem_count[q][1];
-                st->items_total += c0 + c1;
-                st->items_by_variant[2] += c0;
-                st->items_by_variant[3] += c1;
+                const uint32_t c0 = st->pitem_count[q][0], m4r = st->pitem_m4r[q];
+                st->items_total += c0;
+                st->items_by_variant[2] += c0 - m4r;
+                st->items_by_variant[3] += m4r;
                 st->pitem_count[q][0] = st->pitem_count[q][1] = 0;
                 st->pitem_next[q][0] = st->pitem_next[q][1] = 0;
-                st->pchanged[q] = 0;
+                st->plan_done[q] = 0;
+                st->pitem_m4r[q] = 0;
             }
         }
-        // ---- phase A: plan of iteration t + clear of the delta read in t-1 ----
+        // ---- plan of iteration t + clear of the delta read in t-1 ----
+        const unsigned long long plan_t0 = a.trace && tid == 0 ? globaltimer_ns() : 0ull;
         if (a.cnts && blockIdx.x == 0 && t > 0)  // that delta's counters restart at zero
             for (uint32_t sl = tid; sl < a.nslots; sl += kThreads) a.cnts[3 * sl + 1 + (par ^ 1)] = BufCounters{0, 0, 0};
         if (a.qr) {
@@ -276,9 +291,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_closure_persistent(PersistArgs 
                     const uint32_t i = active_find(X.act_plan, u);
                     const QueryRange qr = a.qr[X.act_plan.q[i]];
                     plan::plan_row(qr.prow0 + (u - X.act_plan.pref[i]), prods, a.nprods, slots, t, st,
-                                   st->pitem_count[par], a.items + (size_t)(2 * par) * a.list_cap, a.list_cap, a.tpb,
-                                   a.prod_seen, 0, psel, X.plan[warp].cnt, X.plan[warp].bnd, qr.prod0,
-                                   qr.prod0 + qr.nprod);
+                                   st->pitem_count[par], items, a.list_cap, a.tpb, a.prod_seen, 0, psel,
+                                   X.plan[warp].cnt, X.plan[warp].bnd, qr.prod0, qr.prod0 + qr.nprod,
+                                   &st->pitem_m4r[par]);
                 } else {
                     const uint32_t i = active_find(X.act_clear, u - np);
                     const QueryRange qr = a.qr[X.act_clear.q[i]];
@@ -292,9 +307,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_closure_persistent(PersistArgs 
             const uint32_t units = a.prod_rows + clear_rows;
             for (uint32_t u = gwarp; u < units; u += nwarps) {
                 if (u < a.prod_rows) {
-                    plan::plan_row(u, prods, a.nprods, slots, t, st, st->pitem_count[par],
-                                   a.items + (size_t)(2 * par) * a.list_cap, a.list_cap, a.tpb, a.prod_seen, 0,
-                                   psel, X.plan[warp].cnt, X.plan[warp].bnd);
+                    plan::plan_row(u, prods, a.nprods, slots, t, st, st->pitem_count[par], items, a.list_cap, a.tpb,
+                                   a.prod_seen, 0, psel, X.plan[warp].cnt, X.plan[warp].bnd, 0u, 0xFFFFFFFFu,
+                                   &st->pitem_m4r[par]);
                 } else {
                     clear_delta_row(slots, a.nslots, u - a.prod_rows, par ^ 1);
                 }
@@ -302,67 +317,93 @@ __global__ void __launch_bounds__(kThreads, 2) k_closure_persistent(PersistArgs 
             }
         }
         fence_proxy_async_smem();  // the scratch writes come before the next bulk copies into the same bytes
-        if (!grid_barrier(st, gen)) timed_out = true;
-        if (blockIdx.x == 0 && tid == 0 && a.phase_log && t - iter0 < a.phase_log_iters)
-            a.phase_log[3 * (t - iter0) + 1] = globaltimer_ns();
-        if (timed_out) break;
-
-        // ---- phase B: products ----
-        uint32_t *const qchanged = a.qt.changed ? a.qt.changed + (t % 3) * st->nqueries : nullptr;
-        if (blockIdx.x == 0 && a.qt.changed) {  // flags of iteration t+1 (last read in phase A of t)
-            uint32_t *next = a.qt.changed + ((t + 1) % 3) * st->nqueries;
-            for (uint32_t q = tid; q < st->nqueries; q += kThreads) next[q] = 0;
-        }
-        {
-            const uint64_t *items = a.items + (size_t)(2 * par) * a.list_cap;
-            const uint32_t n0 = st->pitem_count[par][0];
-            for (;;) {
-                if (tid == 0) S.prod.item = atomicAdd(&st->pitem_next[par][0], 1u);
-                __syncthreads();
-                const uint32_t idx = S.prod.item;
-                __syncthreads();
-                if (idx >= n0) break;
-                const unsigned long long t0 = a.trace ? globaltimer_ns() : 0ull;
-                tiled::process_item<false, kPW>(S.prod, items[idx], prods, slots, t, &st->pchanged[par], qchanged, phase,
-                                           timed_out, ctr, a.cnts);
-                if (a.trace && tid == 0) trace_item(a, items[idx], t, 0, t0);
-            }
-            if constexpr (kHasM4R) {
-                const uint32_t n1 = st->pitem_count[par][1];
-                for (;;) {
-                    if (tid == 0) S.prod.item = atomicAdd(&st->pitem_next[par][1], 1u);
-                    __syncthreads();
-                    const uint32_t idx = S.prod.item;
-                    __syncthreads();
-                    if (idx >= n1) break;
-                    const unsigned long long t0 = a.trace ? globaltimer_ns() : 0ull;
-                    tiled::process_item<true, kPW>(S.prod, items[a.list_cap + idx], prods, slots, t,
-                                              &st->pchanged[par], qchanged, phase, timed_out, ctr, a.cnts);
-                    if (a.trace && tid == 0) trace_item(a, items[a.list_cap + idx], t, 1, t0);
-                }
-            }
-        }
-        if (!grid_barrier(st, gen)) timed_out = true;
-        if (timed_out) break;
-
-        // ---- decision ----
-        if (tid == 0) {
-            const uint32_t changed = *reinterpret_cast<volatile uint32_t *>(&st->pchanged[par]);
-            const uint32_t err = *reinterpret_cast<volatile uint32_t *>(&st->error);
-            s_go = changed && err == 0 && (max_iter == 0 || t + 1 < max_iter);
-        }
         __syncthreads();
-        const bool go = s_go != 0;
+        if (tid == 0) {  // this CTA's items, clears and counter resets are all published
+            __threadfence();
+            atomicAdd(&st->plan_done[par], 1u);
+            if (blockIdx.x == 0 && a.phase_log && t - iter0 < a.phase_log_iters)
+                a.phase_log[3 * (t - iter0) + 1] = globaltimer_ns();
+            if (a.trace) trace_item(a, 0, t, 2, plan_t0);
+        }
+
+        // ---- products: items as the planners publish them ----
+        // A CTA takes the next list index and waits (bounded) until that item
+        // is written or every CTA is done planning with fewer items; it
+        // zeroes the slot again for the iteration after next.  Items may run
+        // while other CTAs still plan (operands only grow: an item sees at
+        // least what its planner saw) but their results wait for every
+        // CTA's delta clear (the gate before the epilogue).
+        uint32_t *const qchanged = a.qt.changed ? a.qt.changed + (t % 3) * st->nqueries : nullptr;
+        uint32_t *const changed = reinterpret_cast<uint32_t *>(&st->pbar[par]) + 1;  // kBarChanged
+        const uint32_t *gate = &st->plan_done[par];  // cleared by the first item that passes it
+        while (!timed_out) {
+            if (tid == 0) {
+                const uint32_t idx = atomicAdd(&st->pitem_next[par][0], 1u);
+                volatile uint64_t *slot = items + idx;
+                unsigned long long v = 0;
+                uint32_t stop = 0, spins = 0;
+                for (;;) {
+                    if (idx < a.list_cap && (v = *slot) != 0) break;
+                    if (*reinterpret_cast<volatile uint32_t *>(&st->plan_done[par]) == gridDim.x) {
+                        __threadfence();
+                        if (idx >= *reinterpret_cast<volatile uint32_t *>(&st->pitem_count[par][0])) {
+                            stop = 1;
+                            break;
+                        }
+                    }
+                    if (++spins > kBarrierSpinLimit) {
+                        stop = 2;
+                        break;
+                    }
+                    __nanosleep(32);
+                }
+                if (v) *slot = 0;
+                s_item = v;
+                s_stop = stop;
+            }
+            __syncthreads();
+            const unsigned long long v = s_item;
+            const uint32_t stop = s_stop;
+            __syncthreads();
+            if (stop) {
+                if (stop == 2) timed_out = true;
+                break;
+            }
+            const unsigned long long t0 = a.trace ? globaltimer_ns() : 0ull;
+            const uint64_t item = v & ~1ull;
+            bool m4r_item = false;
+            if constexpr (kHasM4R) m4r_item = (v & 1ull) != 0;
+            if constexpr (kHasM4R) {
+                if (m4r_item)
+                    tiled::process_item<true, kPW>(S.prod, item, prods, slots, t, changed, qchanged,
+                                                   phase, timed_out, ctr, a.cnts, &gate, gridDim.x);
+            }
+            if (!m4r_item)
+                tiled::process_item<false, kPW>(S.prod, item, prods, slots, t, changed, qchanged, phase,
+                                                timed_out, ctr, a.cnts, &gate, gridDim.x);
+            if (a.trace && tid == 0) trace_item(a, item, t, (uint32_t)(v & 1ull), t0);
+        }
+        uint32_t flags = 0;
+        if (!grid_barrier(&st->pbar[par], ++bar_uses[par] * gridDim.x, timed_out, &flags)) timed_out = true;
+        if (flags & kBarAbort) timed_out = true;
+        if (timed_out) break;
+
+        // ---- decision (the same on every CTA: the flags are final) ----
+        const bool go = (flags & kBarChanged) && (max_iter == 0 || t + 1 < max_iter);
         if (blockIdx.x == 0) {
             if (tid == 0 && a.phase_log && t - iter0 < a.phase_log_iters)
                 a.phase_log[3 * (t - iter0) + 2] = globaltimer_ns();
             if (qchanged) {
                 const unsigned long long now = globaltimer_ns();
+                // flags of iteration t+1: last read by the plan of t, next
+                // written after this CTA's plan of t+1 is published
+                uint32_t *next = a.qt.changed + ((t + 1) % 3) * st->nqueries;
                 for (uint32_t q = tid; q < st->nqueries; q += kThreads) {
                     if (__ldcg(qchanged + q)) {
                         a.qt.last_iter[q] = t + 1;
                         a.qt.done_ns[q] = now;
                     }
+                    next[q] = 0;
                 }
             }
         }
@@ -405,11 +446,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_closure_persistent(PersistArgs 
     if (tid == 0 && timed_out) atomicExch(&st->error, (uint32_t)5);
     if (blockIdx.x == 0 && tid == 0 && !timed_out) {
         const uint32_t par = t & 1;
-        const uint32_t c0 = st->pitem_count[par][0], c1 = st->pitem_count[par][1];
-        st->items_total += c0 + c1;
-        st->items_by_variant[2] += c0;
-        st->items_by_variant[3] += c1;
-        st->last_changed = st->pchanged[par];
+        const uint32_t c0 = st->pitem_count[par][0], m4r = st->pitem_m4r[par];
+        st->items_total += c0;
+        st->items_by_variant[2] += c0 - m4r;
+        st->items_by_variant[3] += m4r;
+        st->last_changed = (uint32_t)(st->pbar[par] >> 32) & kBarChanged;
         st->iter = t + 1;
         st->active = 0;
     }

@@ -58,12 +58,15 @@ struct WarpArea {
 // (Four Russians) or 2 (tensor cores) by the product's variant, list l at
 // items_all + l * list_cap, counted in item_count[l]; st receives the
 // product statistics.  tc_mode 0 plans word-level products, 1 tensor-core ones.
+// unified_m4r non-null: every word-level item goes to list 0, Four Russians
+// items marked by bit 0 of the item and also counted in *unified_m4r.
 __device__ __forceinline__ void plan_row(uint32_t gw, const ProdDesc *__restrict__ prods, uint32_t nprods,
                                          const MatSlot *__restrict__ slots, uint32_t iter, IterState *st,
                                          uint32_t *item_count, uint64_t *__restrict__ items_all, size_t list_cap,
                                          int tpb, uint32_t *prod_seen, int tc_mode, const PlanSelect &ps,
                                          uint32_t *cnt, uint16_t (*bnd)[kMaxChunksPerBlock - 1],
-                                         uint32_t plo = 0, uint32_t phi = 0xFFFFFFFFu) {
+                                         uint32_t plo = 0, uint32_t phi = 0xFFFFFFFFu,
+                                         uint32_t *unified_m4r = nullptr) {
     const uint32_t lane = threadIdx.x & 31;
     // product: last p with row_start <= gw, searched in [plo, phi) (a query's
     // products when the caller knows the query)
@@ -93,7 +96,9 @@ __device__ __forceinline__ void plan_row(uint32_t gw, const ProdDesc *__restrict
     }
     const bool tc = variant == 4;                                // CFPQ_VARIANT_TC
     if (tc != (tc_mode != 0)) return;  // word-level and tensor-core products are planned by separate launches
-    const uint32_t list = tc ? 2u : (variant == 3 ? 1u : 0u);   // CFPQ_VARIANT_M4R
+    const bool m4r = !tc && variant == 3;                        // CFPQ_VARIANT_M4R
+    const uint32_t list = tc ? 2u : (m4r && !unified_m4r ? 1u : 0u);
+    const uint64_t vbit = m4r && unified_m4r ? 1u : 0u;
     if (tc) tpb = 4;
     const uint32_t rows_per_item = tc ? 4u : 1u;
     uint64_t *items = items_all + list * list_cap;
@@ -165,7 +170,10 @@ __device__ __forceinline__ void plan_row(uint32_t gw, const ProdDesc *__restrict
     }
     if (!total) return;
     uint32_t pos0 = 0;
-    if (lane == 0) pos0 = atomicAdd(&item_count[list], total);
+    if (lane == 0) {
+        pos0 = atomicAdd(&item_count[list], total);
+        if (vbit) atomicAdd(unified_m4r, total);
+    }
     pos0 = __shfl_sync(kFull, pos0, 0);
     for (uint32_t base = 0; base < nblocks; base += 32) {
         const uint32_t b = base + lane;
@@ -178,7 +186,7 @@ __device__ __forceinline__ void plan_row(uint32_t gw, const ProdDesc *__restrict
         }
         for (uint32_t j = 0; j < nitem; ++j) {
             const uint32_t klo = j ? bnd[b][j - 1] : 0u, khi = j + 1 < nitem ? bnd[b][j] : T;
-            items[pos0 + pre - nitem + j] = make_item(lo, ti, b, klo, khi);
+            items[pos0 + pre - nitem + j] = make_item(lo, ti, b, klo, khi) | vbit;
         }
         pos0 += __shfl_sync(kFull, pre, 31);
     }

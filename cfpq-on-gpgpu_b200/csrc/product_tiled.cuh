@@ -18,6 +18,7 @@ constexpr int kMaxTiles = 2048;      // k-list capacity (n <= 131072)
 constexpr uint32_t kSparseMax = 96;  // P-tile population up to which the sparse loop runs
 constexpr int kTabRow = kBJ + 1;     // padded table row (uint64 words)
 constexpr unsigned kFull = 0xffffffffu;
+constexpr uint32_t kGateSpinLimit = 1u << 24;  // ~1 s of polling
 
 template <bool kM4R>
 struct __align__(128) TiledSmem {
@@ -73,12 +74,16 @@ struct ItemCounters {
 // kTPW*w .. kTPW*w + kTPW-1 of the block, lane l rows 2l and 2l+1).  `phase`
 // is the CTA's mbarrier parity state (bit s = next parity of stage s),
 // `timed_out` is set (CTA-uniformly) when a bounded wait gave up; new bits
-// set *changed and qchanged[query].  Ends with the CTA synchronised.
+// set *changed and qchanged[query].  gate and *gate non-null: the results
+// are merged only once **gate reaches gate_target (bounded wait; on timeout
+// the item merges nothing), after which *gate is cleared so that the CTA's
+// later items skip the check.  Ends with the CTA synchronised.
 template <bool kM4R, int kW, class Smem>
 __device__ __forceinline__ void process_item(Smem &S, uint64_t it, const ProdDesc *__restrict__ prods,
                                              const MatSlot *__restrict__ slots, uint32_t iter, uint32_t *changed,
                                              uint32_t *qchanged, uint32_t &phase, bool &timed_out,
-                                             ItemCounters &ctr, BufCounters *cnts) {
+                                             ItemCounters &ctr, BufCounters *cnts,
+                                             const uint32_t **gate = nullptr, uint32_t gate_target = 0) {
     static_assert(kBJ % kW == 0 && kBJ / kW <= 4, "whole tiles per warp, at most 4");
     constexpr int kTPW = kBJ / kW;             // output tiles per warp
     constexpr uint32_t kNT = 32u * kW;         // threads
@@ -324,7 +329,24 @@ __device__ __forceinline__ void process_item(Smem &S, uint64_t it, const ProdDes
         timed_out = __syncthreads_or(timed_out) != 0;
         if (tid == 0 && !timed_out && e + kStages < nk) staged += issue(e + kStages, stage);
     }
-    // ---- epilogue: the 8 words of the thread in three batches (loads of C,
+    if (gate && *gate) {
+        bool gave_up = false;
+        if (tid == 0 && !timed_out) {
+            uint32_t spins = 0;
+            while (*reinterpret_cast<const volatile uint32_t *>(*gate) < gate_target) {
+                if (++spins > kGateSpinLimit) {
+                    gave_up = true;
+                    break;
+                }
+                __nanosleep(64);
+            }
+            __threadfence();
+        }
+        timed_out = __syncthreads_or(timed_out || gave_up) != 0;
+        if (timed_out) return;
+        *gate = nullptr;
+    }
+    // ---- epilogue: the 2*kTPW words of the thread in three batches (loads of C,
     // then the atomics that can add bits, then D / populations), so that
     // their global round trips overlap ----
     constexpr int kWords = 2 * kTPW;

@@ -419,7 +419,10 @@ size_t cfpq_last_phase_log(cfpq_ctx *ctx, uint64_t *out, size_t cap);
  * (bits 48-63 product index in the closure, 37-47 tile-row, 28-36 block of 16
  * output tiles, 16-27 first k-tile, 4-15 end k-tile), `list` 0 for the LOP3
  * inner loop and 1 for Four Russians; times are %globaltimer ns taken by the
- * CTA around the item.  Copies min(cap, count) records and returns the count
+ * CTA around the item.  Records with list 2 (item 0) are the CTA's plan and
+ * delta-clear span of the iteration, from its start to the moment the CTA
+ * published its items (results of the iteration's items merge only after
+ * every CTA has).  Copies min(cap, count) records and returns the count
  * (0 when the last closure was not traced). */
 #define CFPQ_LOG_ITEMS 8
 typedef struct cfpq_item_record {

@@ -407,13 +407,16 @@ def test_item_trace(ctx, pkg, oracle, tmp_path):
         q.load()
         st = ctx.closure(wl.grammar.rules, q.mats, use_graph="device", log_products=pkg.capi.LOG_ITEMS)
         assert dict(zip(q.grammar.nonterminals, ctx.hash_count_many(q.mats))) == exp
-        tr = ctx.item_log()
+        log = ctx.item_log()
+        plans, tr = log[log["list"] == 2], log[log["list"] < 2]
         assert len(tr) == st["work_items"] > 0
+        assert len(plans) == st["iterations"] * len(np.unique(plans["cta"]))  # every CTA plans every iteration
         assert (tr["end_ns"] >= tr["start_ns"]).all()
         assert (tr["iteration"] < st["iterations"]).all()
         assert (tr["product"] < 2 * len(wl.grammar.rules)).all()
         assert (tr["klo"] < tr["khi"]).all() and (tr["khi"] <= (1024 + 63) // 64).all()
         assert set(np.unique(tr["list"])) <= {0, 1}
+        assert (plans["end_ns"] >= plans["start_ns"]).all()
         q.load()
         ctx.closure(wl.grammar.rules, q.mats, use_graph="device")
         assert len(ctx.item_log()) == 0
