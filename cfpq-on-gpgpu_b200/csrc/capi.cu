@@ -824,6 +824,10 @@ static int validate_query(const QueryIn &q, size_t qi) {
     return CFPQ_OK;
 }
 
+// Largest tile count (n / 64) of a single closure whose persistent kernel
+// merges item results without reading C first.
+static constexpr uint32_t kDirectMergeMaxTiles = 256;
+
 static int build_plan(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, int variant, ClosurePlan *pl) {
     const int tpb = product_lop3_tiles_per_block();
     // AUTO with a selector: chosen per term and iteration among the allowed
@@ -1351,6 +1355,8 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
                                            trace ? reinterpret_cast<uint32_t *>(
                                                        static_cast<char *>(ctx->item_trace.p) + trace_bytes)
                                                  : nullptr,
+                                           // one small closure: latency-bound, merge without the read of C
+                                           nq == 1 && pl.prods[0].T <= kDirectMergeMaxTiles ? 1 : 0,
                                            ctx->stream));
     } else if (exec) {
         CUDA_TRY(cudaGraphLaunch(exec, ctx->stream));

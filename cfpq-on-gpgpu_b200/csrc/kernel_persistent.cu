@@ -118,6 +118,7 @@ struct PersistArgs {
     uint32_t sel_log_iters;
     const QueryRange *qr;           // non-null (batches of 2..kMaxActive queries): active-query phase A
     ItemTrace *trace;               // non-null: one record per processed item (first kItemTraceCap)
+    int direct_merge;               // items merge without reading C first (small single closures)
     uint32_t *trace_count;
 };
 
@@ -376,11 +377,13 @@ __global__ void __launch_bounds__(kThreads, 2) k_closure_persistent(PersistArgs 
             if constexpr (kHasM4R) {
                 if (m4r_item)
                     tiled::process_item<true, kPW>(S.prod, item, prods, slots, t, changed, qchanged,
-                                                   phase, timed_out, ctr, a.cnts, &gate, gridDim.x);
+                                                   phase, timed_out, ctr, a.cnts, &gate, gridDim.x,
+                                                a.direct_merge != 0);
             }
             if (!m4r_item)
                 tiled::process_item<false, kPW>(S.prod, item, prods, slots, t, changed, qchanged, phase,
-                                                timed_out, ctr, a.cnts, &gate, gridDim.x);
+                                                timed_out, ctr, a.cnts, &gate, gridDim.x,
+                                                a.direct_merge != 0);
             if (a.trace && tid == 0) trace_item(a, item, t, (uint32_t)(v & 1ull), t0);
         }
         uint32_t flags = 0;
@@ -482,7 +485,7 @@ cudaError_t launch_closure_persistent(int has_m4r, int grid, const ProdDesc *pro
                                       uint32_t phase_log_iters, BufCounters *cnts, uint8_t *choice,
                                       const SelectorParams *sel, SelLogRow *sel_log, uint32_t sel_log_iters,
                                       const QueryRange *qr, ItemTrace *trace, uint32_t *trace_count,
-                                      cudaStream_t s) {
+                                      int direct_merge, cudaStream_t s) {
     PersistArgs a;
     a.prods = prods;
     a.nprods = nprods;
@@ -506,6 +509,7 @@ cudaError_t launch_closure_persistent(int has_m4r, int grid, const ProdDesc *pro
     a.qr = qr;
     a.trace = trace;
     a.trace_count = trace_count;
+    a.direct_merge = direct_merge;
     void *args[] = {&a};
     if (has_m4r)
         return cudaLaunchCooperativeKernel((const void *)k_closure_persistent<true>, dim3(grid), dim3(kThreads), args,

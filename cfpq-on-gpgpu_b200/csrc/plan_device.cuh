@@ -125,39 +125,62 @@ __device__ __forceinline__ void plan_row(uint32_t gw, const ProdDesc *__restrict
     const uint32_t E = tc ? T : item_entries(np);
     for (uint32_t b = lane; b < nblocks; b += 32) cnt[b] = 0;
     __syncwarp();
-    uint32_t mine = first;
-
-    for (uint32_t pw = 0; pw < ow; ++pw) {
-        // P occupancy words come 32 at a time, one per lane
-        if (pw > 0 && (pw & 31) == 0) mine = pw + lane < ow ? prow_word(pw + lane) : 0u;
-        const uint32_t bits = __shfl_sync(kFull, mine, pw & 31);  // warp-uniform
-        if (!bits) continue;
-        const bool valid = lane < (uint32_t)__popc(bits);
-        const uint32_t tk = valid ? pw * 32 + nth_set_bit(bits, lane) : 0u;  // increasing with the lane
-        const uint32_t *qrow = Q.occ + (size_t)tk * ow;
-        for (uint32_t w0 = 0; w0 < ow; w0 += 4) {
-            uint32_t m[4];
+    // Q occupancy words m[0..3] (words w0.. of Q row tk, tk the lane's
+    // candidate) -> per output block b the count of candidate k-tiles and the
+    // chunk boundaries
+    auto scan = [&](uint32_t w0, const uint32_t (&m)[4], uint32_t tk) {
 #pragma unroll
-            for (int u = 0; u < 4; ++u) m[u] = (valid && w0 + u < ow) ? qrow[w0 + u] : 0u;
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                if (w0 + u >= ow) break;
-                if (!__ballot_sync(kFull, m[u] != 0)) continue;
-                for (uint32_t h = 0; h < bpw; ++h) {
-                    const unsigned bal = __ballot_sync(kFull, ((m[u] >> (h * tpb)) & bmask) != 0);
-                    if (!bal) continue;
-                    const uint32_t b = (w0 + u) * bpw + h, c = __popc(bal), cb = cnt[b];
-                    // chunk boundaries: ranks j*E (j >= 1) among this ballot's ranks cb .. cb+c-1
-                    for (uint32_t j = (cb + E - 1) / E; j < kMaxChunksPerBlock && j * E < cb + c; ++j) {
-                        if (j == 0) continue;
-                        const uint32_t src = nth_set_bit(bal, j * E - cb);
-                        const uint32_t tkj = __shfl_sync(kFull, tk, src);
-                        if (lane == 0) bnd[b][j - 1] = (uint16_t)tkj;
-                    }
-                    __syncwarp();
-                    if (lane == 0) cnt[b] = cb + c;
-                    __syncwarp();
+        for (int u = 0; u < 4; ++u) {
+            if (w0 + u >= ow) break;
+            if (!__ballot_sync(kFull, m[u] != 0)) continue;
+            for (uint32_t h = 0; h < bpw; ++h) {
+                const unsigned bal = __ballot_sync(kFull, ((m[u] >> (h * tpb)) & bmask) != 0);
+                if (!bal) continue;
+                const uint32_t b = (w0 + u) * bpw + h, c = __popc(bal), cb = cnt[b];
+                // chunk boundaries: ranks j*E (j >= 1) among this ballot's ranks cb .. cb+c-1
+                for (uint32_t j = (cb + E - 1) / E; j < kMaxChunksPerBlock && j * E < cb + c; ++j) {
+                    if (j == 0) continue;
+                    const uint32_t src = nth_set_bit(bal, j * E - cb);
+                    const uint32_t tkj = __shfl_sync(kFull, tk, src);
+                    if (lane == 0) bnd[b][j - 1] = (uint16_t)tkj;
                 }
+                __syncwarp();
+                if (lane == 0) cnt[b] = cb + c;
+                __syncwarp();
+            }
+        }
+    };
+    if (ow <= 4) {
+        // at most 128 tiles: the Q words of every candidate load together
+        // (one round trip), lane l holding the l-th candidate of each P word
+        uint32_t pre[4][4], tks[4];
+#pragma unroll
+        for (int pw = 0; pw < 4; ++pw) {
+            const uint32_t bits = __shfl_sync(kFull, first, pw);  // 0 beyond ow
+            const bool valid = lane < (uint32_t)__popc(bits);
+            tks[pw] = valid ? pw * 32 + nth_set_bit(bits, lane) : 0u;
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                pre[pw][u] = (valid && (uint32_t)u < ow) ? Q.occ[(size_t)tks[pw] * ow + u] : 0u;
+        }
+#pragma unroll
+        for (int pw = 0; pw < 4; ++pw)
+            if (__shfl_sync(kFull, first, pw)) scan(0, pre[pw], tks[pw]);
+    } else {
+        uint32_t mine = first;
+        for (uint32_t pw = 0; pw < ow; ++pw) {
+            // P occupancy words come 32 at a time, one per lane
+            if (pw > 0 && (pw & 31) == 0) mine = pw + lane < ow ? prow_word(pw + lane) : 0u;
+            const uint32_t bits = __shfl_sync(kFull, mine, pw & 31);  // warp-uniform
+            if (!bits) continue;
+            const bool valid = lane < (uint32_t)__popc(bits);
+            const uint32_t tk = valid ? pw * 32 + nth_set_bit(bits, lane) : 0u;  // increasing with the lane
+            const uint32_t *qrow = Q.occ + (size_t)tk * ow;
+            for (uint32_t w0 = 0; w0 < ow; w0 += 4) {
+                uint32_t m[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) m[u] = (valid && w0 + u < ow) ? qrow[w0 + u] : 0u;
+                scan(w0, m, tk);
             }
         }
     }

@@ -19,6 +19,7 @@ constexpr uint32_t kSparseMax = 96;  // P-tile population up to which the sparse
 constexpr int kTabRow = kBJ + 1;     // padded table row (uint64 words)
 constexpr unsigned kFull = 0xffffffffu;
 constexpr uint32_t kGateSpinLimit = 1u << 24;  // ~1 s of polling
+constexpr uint32_t kShortRange = 64;            // k ranges up to this length build the k-list in one round trip
 
 template <bool kM4R>
 struct __align__(128) TiledSmem {
@@ -77,14 +78,19 @@ struct ItemCounters {
 // set *changed and qchanged[query].  gate and *gate non-null: the results
 // are merged only once **gate reaches gate_target (bounded wait; on timeout
 // the item merges nothing), after which *gate is cleared so that the CTA's
-// later items skip the check.  Ends with the CTA synchronised.
+// later items skip the check.  direct_merge: every non-zero result word goes
+// straight to its atomic OR (one round trip less per item; for latency-bound
+// closures), else only words with bits C does not hold yet.  Ends with the
+// CTA synchronised.
 template <bool kM4R, int kW, class Smem>
 __device__ __forceinline__ void process_item(Smem &S, uint64_t it, const ProdDesc *__restrict__ prods,
                                              const MatSlot *__restrict__ slots, uint32_t iter, uint32_t *changed,
                                              uint32_t *qchanged, uint32_t &phase, bool &timed_out,
                                              ItemCounters &ctr, BufCounters *cnts,
-                                             const uint32_t **gate = nullptr, uint32_t gate_target = 0) {
+                                             const uint32_t **gate = nullptr, uint32_t gate_target = 0,
+                                             bool direct_merge = false) {
     static_assert(kBJ % kW == 0 && kBJ / kW <= 4, "whole tiles per warp, at most 4");
+    static_assert(kShortRange <= 32u * kW, "one k-tile per thread in the short k-list path");
     constexpr int kTPW = kBJ / kW;             // output tiles per warp
     constexpr uint32_t kNT = 32u * kW;         // threads
     constexpr uint32_t kWMask = (1u << kTPW) - 1;
@@ -101,9 +107,47 @@ __device__ __forceinline__ void process_item(Smem &S, uint64_t it, const ProdDes
     const uint32_t nblk = min((uint32_t)kBJ, T - tj0);
     const uint32_t qword = tj0 >> 5, qshift = tj0 & 31;
 
-    // ---- k-list: warp 0 compacts the occupied P tiles of row ti in
+    // ---- k-list: the item's k-tiles (occupied P tile and non-empty Q
+    // block), increasing, with their Q block masks and P density ----
+    if (khi - klo <= kShortRange) {
+        // short range: thread c loads the P occupancy bit, the Q block
+        // occupancy and the P tile population of k-tile klo + c together
+        // (one round trip instead of two dependent ones; the loads of
+        // unoccupied P tiles are wasted, hence only for short ranges), then a
+        // block-wide ballot compaction
+        const uint32_t tk = klo + tid;
+        uint32_t mask = 0;
+        bool dense = false;
+        if (tk < khi) {
+            const uint32_t pw = P.occ[(size_t)ti * ow + (tk >> 5)];
+            const uint32_t qw = Q.occ[(size_t)tk * ow + qword];
+            const uint32_t pn = P.nnz[(size_t)ti * T + tk];
+            if ((pw >> (tk & 31)) & 1u) {
+                mask = (qw >> qshift) & ((1u << kBJ) - 1);
+                dense = pn > kSparseMax;
+            }
+        }
+        const unsigned ball = __ballot_sync(kFull, mask != 0);
+        if (lane == 0) S.rball[warp] = ball;
+        __syncthreads();
+        uint32_t rank = __popc(ball & ((1u << lane) - 1)), total = 0;
+#pragma unroll
+        for (int w = 0; w < kW; ++w) {
+            const uint32_t c = __popc(S.rball[w]);
+            if ((uint32_t)w < warp) rank += c;
+            total += c;
+        }
+        if (mask) {
+            triples += __popc(mask);
+            S.ktile[rank] = (uint16_t)(tk | (dense ? 0x8000u : 0u));
+            S.kmask[rank] = (uint16_t)mask;
+        }
+        if (tid == 0) S.nk = total;
+        __syncthreads();
+    } else {
+    // long range: warp 0 compacts the occupied P tiles of row ti in
     // [klo, khi) into a candidate list, then all threads classify the
-    // candidates in parallel ----
+    // candidates in parallel
     if (warp == 0) {
         uint32_t nc = 0;
         const uint32_t *prow = P.occ + (size_t)ti * ow;
@@ -172,6 +216,7 @@ __device__ __forceinline__ void process_item(Smem &S, uint64_t it, const ProdDes
     }
     if (tid == 0) S.nk = rounds ? S.roff[rounds - 1] + __popc(S.rball[rounds - 1]) : 0u;
     __syncthreads();
+    }
     const uint32_t nk = S.nk;
 
     uint2 acc0[kTPW], acc1[kTPW];
@@ -363,7 +408,9 @@ __device__ __forceinline__ void process_item(Smem &S, uint64_t it, const ProdDes
     }
 #pragma unroll
     for (int k = 0; k < kWords; ++k)
-        seen[k] = av[k] ? __ldcg(reinterpret_cast<const unsigned long long *>(C.bits + off[k])) : ~0ULL;
+        seen[k] = !av[k] ? ~0ULL
+                  : direct_merge ? 0ULL
+                                 : __ldcg(reinterpret_cast<const unsigned long long *>(C.bits + off[k]));
 #pragma unroll
     for (int k = 0; k < kWords; ++k)
         prev[k] = (av[k] & ~seen[k]) ? atomicOr(reinterpret_cast<unsigned long long *>(C.bits + off[k]),
