@@ -97,7 +97,9 @@ LOG_ITEMS = 8
 
 # numpy view of an array of cfpq_item_record
 ITEM_RECORD_DTYPE = np.dtype([("item", np.uint64), ("iteration", np.uint32), ("cta", np.uint16),
-                              ("list", np.uint16), ("start_ns", np.uint64), ("end_ns", np.uint64)])
+                              ("list", np.uint16), ("start_ns", np.uint64), ("end_ns", np.uint64),
+                              ("klist_ns", np.uint32), ("staged_ns", np.uint32), ("computed_ns", np.uint32),
+                              ("gate_ns", np.uint32)])
 
 
 class ProductRecord(ctypes.Structure):

@@ -295,6 +295,7 @@ extern "C" int cfpq_ctx_destroy(cfpq_ctx *ctx) {
     cudaFreeHost(ctx->h_flag);
     if (ctx->h_hash) cudaFreeHost(ctx->h_hash);
     if (ctx->h_small) cudaFreeHost(ctx->h_small);
+    if (ctx->h_query) cudaFreeHost(ctx->h_query);
     cudaEventDestroy(ctx->ev0);
     cudaEventDestroy(ctx->ev1);
     for (auto &e : ctx->kev) cudaEventDestroy(e);
@@ -662,6 +663,7 @@ static int enqueue_tiled_product(cfpq_ctx *ctx, const DevMat &a, const DevMat &b
     TRY(ctx->slots.ensure(sizeof(hs)));
     TRY(ctx->prods.ensure(sizeof(pd)));
     TRY(ctx->items.ensure(3 * cap * 8));
+    ctx->items_clean_words = 0;
     IterState st;
     memset(&st, 0, sizeof(st));
     st.iter = 1;
@@ -1265,6 +1267,12 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
         o.use_graph == CFPQ_LOOP_DEVICE && !timed && !log_products && !pl.uses_tc && persist_grid > 0;
     const uint32_t nprods = (uint32_t)pl.prods.size(), nslots = (uint32_t)pl.slots.size();
     TRY(ctx->items.ensure((persistent ? 4 : 3) * pl.item_cap * 8));
+    // the persistent kernel's item lists: zero entries mean "not yet written";
+    // a successful persistent closure leaves them zeroed (every item taken is
+    // reset), so only other users of the buffer make a new zeroing necessary
+    const size_t list_words = 3 * pl.item_cap * 2;
+    const bool lists_clean = ctx->items_clean_ptr == ctx->items.p && ctx->items_clean_words >= list_words;
+    ctx->items_clean_words = 0;
     TRY(ctx->choice.ensure(nprods));
     TRY(ctx->tc_ok.ensure(nprods));
     TRY(ctx->cnts.ensure((size_t)nslots * 3 * sizeof(BufCounters)));
@@ -1302,27 +1310,36 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
                                  cudaMemcpyHostToDevice, ctx->stream));
         ctx->tables_owner = pc.id;
     }
-    CUDA_TRY(launch_fill_choice(ctx->choice.as<uint8_t>(), nprods,
-                                pl.auto_select ? (uint8_t)CFPQ_VARIANT_LOP3 : pl.fixed_variant, ctx->stream));
     if (ctx->cnts_on) CUDA_TRY(launch_counters_init(ctx->slots.as<MatSlot>(), nslots, ctx->cnts.as<BufCounters>(),
                                                     ctx->stream));
     if (ctx->sel_log_iters)
         CUDA_TRY(cudaMemsetAsync(ctx->sel_log.p, 0, (size_t)kSelLogIters * nprods * sizeof(SelLogRow), ctx->stream));
-    CUDA_TRY(cudaMemsetAsync(ctx->prod_seen.p, 0, pl.prods.size() * 4, ctx->stream));
-    CUDA_TRY(cudaMemsetAsync(ctx->qtrack.p, 0, qbytes, ctx->stream));
-    IterState st;
-    memset(&st, 0, sizeof(st));
-    st.active = 1;
-    st.max_iter = o.max_iterations > 0 ? (uint32_t)o.max_iterations : 0;
-    st.nqueries = (uint32_t)nq;
-    *ctx->h_st = st;
-    CUDA_TRY(cudaMemcpyAsync(ctx->d_st, ctx->h_st, sizeof(IterState), cudaMemcpyHostToDevice, ctx->stream));
+    {
+        // one launch: product-seen flags, query tracking, the persistent
+        // kernel's item lists (one per iteration parity, at 0 and 2 * item_cap:
+        // a zero entry means "not yet written"), the variant choices and the
+        // iteration state (zeroed, then active, limit, query count, start stamp)
+        ClosureBegin b;
+        memset(&b, 0, sizeof(b));
+        b.zero[0] = ctx->prod_seen.as<uint32_t>();
+        b.nwords[0] = pl.prods.size();
+        b.zero[1] = ctx->qtrack.as<uint32_t>();
+        b.nwords[1] = qbytes / 4;
+        b.zero[2] = ctx->items.as<uint32_t>();
+        b.nwords[2] = persistent && !lists_clean ? list_words : 0;
+        b.choice = ctx->choice.as<uint8_t>();
+        b.nchoice = nprods;
+        b.choice_value = pl.auto_select ? (uint8_t)CFPQ_VARIANT_LOP3 : pl.fixed_variant;
+        b.st = ctx->d_st;
+        b.max_iter = o.max_iterations > 0 ? (uint32_t)o.max_iterations : 0;
+        b.nqueries = (uint32_t)nq;
+        CUDA_TRY(launch_closure_begin(b, ctx->num_sms, ctx->stream));
+    }
 
     cudaGraphExec_t exec = nullptr;
     if (o.use_graph && !timed && !log_products && !persistent) TRY(get_loop_graph(ctx, pl, qt, &exec));
     if (timed) memset(&ctx->prof, 0, sizeof(ctx->prof));
 
-    CUDA_TRY(launch_mark_start(ctx->d_st, ctx->stream));
     CUDA_TRY(cudaEventRecord(ctx->ev0, ctx->stream));
     if (log_products) {
         TRY(run_logged_iterations(ctx, pl, qt));
@@ -1336,9 +1353,6 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
             if (it > (1u << 24)) return set_error(CFPQ_ERR_CUDA, "closure did not converge");
         }
     } else if (persistent) {
-        // the kernel's item lists (one per iteration parity, at 0 and 2 * item_cap)
-        // start empty: a zero entry means "not yet written"
-        CUDA_TRY(cudaMemsetAsync(ctx->items.p, 0, 3 * pl.item_cap * 8, ctx->stream));
         CUDA_TRY(launch_closure_persistent(pl.uses_m4r ? 1 : 0, persist_grid, ctx->prods.as<ProdDesc>(),
                                            (uint32_t)pl.prods.size(), pl.prod_rows, ctx->slots.as<MatSlot>(),
                                            (uint32_t)pl.slots.size(), pl.slot_rows, ctx->d_st,
@@ -1376,13 +1390,27 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
     }
     CUDA_TRY(cudaEventRecord(ctx->ev1, ctx->stream));
     CUDA_TRY(cudaMemcpyAsync(ctx->h_st, ctx->d_st, sizeof(IterState), cudaMemcpyDeviceToHost, ctx->stream));
-    std::vector<unsigned long long> h_done(nq);
-    std::vector<uint32_t> h_last(nq);
     if (trace)
         CUDA_TRY(cudaMemcpyAsync(&ctx->item_trace_n, static_cast<char *>(ctx->item_trace.p) + trace_bytes, 4,
                                  cudaMemcpyDeviceToHost, ctx->stream));
-    CUDA_TRY(cudaMemcpyAsync(h_done.data(), qt.done_ns, nq * 8, cudaMemcpyDeviceToHost, ctx->stream));
-    CUDA_TRY(cudaMemcpyAsync(h_last.data(), qt.last_iter, nq * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    // per-query results (only when asked for), through a pinned block
+    const bool want_q = iters_out || done_ms_out;
+    unsigned long long *h_done = nullptr;
+    uint32_t *h_last = nullptr;
+    if (want_q) {
+        const size_t need = nq * 12;
+        if (ctx->h_query_cap < need) {
+            if (ctx->h_query) cudaFreeHost(ctx->h_query);
+            ctx->h_query = nullptr;
+            ctx->h_query_cap = 0;
+            CUDA_TRY(cudaMallocHost(&ctx->h_query, need));
+            ctx->h_query_cap = need;
+        }
+        h_done = static_cast<unsigned long long *>(ctx->h_query);
+        h_last = reinterpret_cast<uint32_t *>(h_done + nq);
+        CUDA_TRY(cudaMemcpyAsync(h_done, qt.done_ns, nq * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        CUDA_TRY(cudaMemcpyAsync(h_last, qt.last_iter, nq * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    }
     CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     float ms = 0;
     CUDA_TRY(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
@@ -1392,6 +1420,10 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
     if (hs.error) {
         drop_plan_cache(ctx, true);
         return set_error(CFPQ_ERR_TIMEOUT, "a bounded device wait gave up during the closure");
+    }
+    if (persistent) {
+        ctx->items_clean_ptr = ctx->items.p;
+        ctx->items_clean_words = list_words;
     }
     if (!converged)  // stopped by the iteration limit: the deltas still hold bits
         for (auto *m : pl.deltas) CUDA_TRY(launch_clear_matrix(m->d, ctx->stream));
@@ -1411,7 +1443,7 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
         stats->out_words = hs.out_words;
         stats->new_words = hs.new_words;
     }
-    for (size_t q = 0; q < nq; ++q) {
+    for (size_t q = 0; want_q && q < nq; ++q) {
         if (iters_out) iters_out[q] = h_last[q];
         if (done_ms_out) done_ms_out[q] = h_last[q] ? (double)(h_done[q] - hs.t_start_ns) / 1e6 : 0.0;
     }

@@ -172,6 +172,7 @@ struct ItemTrace {
     uint32_t iteration;
     uint16_t cta, list;
     unsigned long long start_ns, end_ns;
+    uint32_t klist_ns, staged_ns, computed_ns, gate_ns;  // after start_ns
 };
 constexpr uint32_t kItemTraceCap = 65536;
 
@@ -218,7 +219,9 @@ __host__ __device__ inline uint32_t item_khi(uint64_t it) { return (uint32_t)((i
 // Chunk length of the word-level items of a tile-row whose P operand has `np`
 // occupied tiles: at most kMaxChunksPerBlock chunks per output block (short
 // chains keep the per-item latency low when an iteration has few blocks; each
-// chunk re-does the block's epilogue).
+// chunk re-does the block's epilogue).  (Finer chunking of small closures,
+// more and shorter items, measured slower: the planner's boundary work and
+// the extra items outweigh the shorter longest item.)
 constexpr uint32_t kMaxChunksPerBlock = 8;
 
 // Bits of occupancy word w (tiles 32w .. 32w+31) that lie in [lo, hi).

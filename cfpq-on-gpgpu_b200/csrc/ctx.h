@@ -139,6 +139,10 @@ struct cfpq_ctx {
     cfpq_kernel_profile prof = {};
     void *h_small = nullptr;
     size_t h_small_cap = 0;
+    void *items_clean_ptr = nullptr;  // items buffer whose first items_clean_words words are zero
+    size_t items_clean_words = 0;
+    void *h_query = nullptr;  // pinned: per-query results of a closure (done_ns, last_iter)
+    size_t h_query_cap = 0;
     // variant selector
     SelectorParams sel;            // host copy of the device parameters
     bool sel_dirty = true;         // host copy changed since the last upload

@@ -122,11 +122,15 @@ struct PersistArgs {
     uint32_t *trace_count;
 };
 
-// Records one processed item (thread 0 of the CTA).
+// Records one processed item (thread 0 of the CTA); sub: the item's
+// sub-phase stamps (process_item), null for plan spans.
 __device__ __forceinline__ void trace_item(const PersistArgs &a, uint64_t it, uint32_t iter, uint32_t list,
-                                           unsigned long long t0) {
+                                           unsigned long long t0, const unsigned long long *sub = nullptr) {
     const uint32_t k = atomicAdd(a.trace_count, 1u);
-    if (k < kItemTraceCap) a.trace[k] = ItemTrace{it, iter, (uint16_t)blockIdx.x, (uint16_t)list, t0, globaltimer_ns()};
+    if (k >= kItemTraceCap) return;
+    auto rel = [&](int i) { return sub ? (uint32_t)(sub[i] - t0) : 0u; };
+    a.trace[k] = ItemTrace{it, iter, (uint16_t)blockIdx.x, (uint16_t)list, t0, globaltimer_ns(), rel(0), rel(1),
+                           rel(2), rel(3)};
 }
 
 // Block-wide compaction of the queries whose flag is set (every query when
@@ -371,6 +375,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_closure_persistent(PersistArgs 
                 break;
             }
             const unsigned long long t0 = a.trace ? globaltimer_ns() : 0ull;
+            unsigned long long sub[4] = {t0, t0, t0, t0};
             const uint64_t item = v & ~1ull;
             bool m4r_item = false;
             if constexpr (kHasM4R) m4r_item = (v & 1ull) != 0;
@@ -378,13 +383,13 @@ __global__ void __launch_bounds__(kThreads, 2) k_closure_persistent(PersistArgs 
                 if (m4r_item)
                     tiled::process_item<true, kPW>(S.prod, item, prods, slots, t, changed, qchanged,
                                                    phase, timed_out, ctr, a.cnts, &gate, gridDim.x,
-                                                a.direct_merge != 0);
+                                                a.direct_merge != 0, a.trace ? sub : nullptr);
             }
             if (!m4r_item)
                 tiled::process_item<false, kPW>(S.prod, item, prods, slots, t, changed, qchanged, phase,
                                                 timed_out, ctr, a.cnts, &gate, gridDim.x,
-                                                a.direct_merge != 0);
-            if (a.trace && tid == 0) trace_item(a, item, t, (uint32_t)(v & 1ull), t0);
+                                                a.direct_merge != 0, a.trace ? sub : nullptr);
+            if (a.trace && tid == 0) trace_item(a, item, t, (uint32_t)(v & 1ull), t0, sub);
         }
         uint32_t flags = 0;
         if (!grid_barrier(&st->pbar[par], ++bar_uses[par] * gridDim.x, timed_out, &flags)) timed_out = true;

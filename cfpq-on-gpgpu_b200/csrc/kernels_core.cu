@@ -1,6 +1,8 @@
 // Core kernels: layout conversion, tile statistics (occupancy + population),
 // bit scatter, result hash, the plain dense product, and the plan / advance
 // steps of the device-resident closure iteration.
+#include <algorithm>
+
 #include "launch.h"
 #include "plan_device.cuh"
 
@@ -374,6 +376,26 @@ __global__ void k_advance_end(const MatSlot *__restrict__ slots, uint32_t nslots
 
 __global__ void k_mark_start(IterState *st) { st->t_start_ns = globaltimer_ns(); }
 
+// Closure prologue in one launch: zero the given word ranges, fill the
+// variant choices, initialise the iteration state and stamp its start.
+__global__ void k_closure_begin(ClosureBegin a) {
+    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x, nt = (size_t)gridDim.x * blockDim.x;
+    for (int r = 0; r < ClosureBegin::kRanges; ++r)
+        for (size_t i = tid; i < a.nwords[r]; i += nt) a.zero[r][i] = 0u;
+    for (size_t i = tid; i < a.nchoice; i += nt) a.choice[i] = a.choice_value;
+    if (blockIdx.x == 0) {
+        uint32_t *w = reinterpret_cast<uint32_t *>(a.st);
+        for (size_t i = threadIdx.x; i < sizeof(IterState) / 4; i += blockDim.x) w[i] = 0u;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            a.st->active = 1;
+            a.st->max_iter = a.max_iter;
+            a.st->nqueries = a.nqueries;
+            a.st->t_start_ns = globaltimer_ns();
+        }
+    }
+}
+
 // Clear a list of matrices: one warp per (matrix, tile-row), occupied tiles only.
 __global__ void k_clear_rows(const MatRows *__restrict__ tab, uint32_t nmats, uint32_t total_rows) {
     const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -515,6 +537,14 @@ cudaError_t launch_advance_end(const MatSlot *d_slots, uint32_t nslots, uint32_t
 cudaError_t launch_clear_rows(const MatRows *d_tab, uint32_t nmats, uint32_t total_rows, cudaStream_t s) {
     if (total_rows == 0 || nmats == 0) return cudaSuccess;
     k_clear_rows<<<grid_for((size_t)total_rows * 32, 256), 256, 0, s>>>(d_tab, nmats, total_rows);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_closure_begin(const ClosureBegin &a, int num_sms, cudaStream_t s) {
+    size_t words = a.nchoice;
+    for (int r = 0; r < ClosureBegin::kRanges; ++r) words = words > a.nwords[r] ? words : a.nwords[r];
+    const unsigned blocks = (unsigned)std::max<size_t>(1, std::min<size_t>((words + 255) / 256, (size_t)num_sms * 4));
+    k_closure_begin<<<blocks, 256, 0, s>>>(a);
     return cudaGetLastError();
 }
 

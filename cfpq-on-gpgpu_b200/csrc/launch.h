@@ -75,6 +75,21 @@ cudaError_t launch_advance_end(const MatSlot *d_slots, uint32_t nslots, uint32_t
                                const QueryTrack &qt, cudaGraphConditionalHandle handle, int use_handle,
                                BufCounters *d_cnts, cudaStream_t s);
 cudaError_t launch_mark_start(IterState *d_st, cudaStream_t s);
+
+// Closure prologue (one launch): zero[r][0 .. nwords[r]) = 0, choice[0 ..
+// nchoice) = choice_value, *st = a fresh iteration state (active, max_iter,
+// nqueries, start stamp).
+struct ClosureBegin {
+    static constexpr int kRanges = 3;
+    uint32_t *zero[kRanges];
+    size_t nwords[kRanges];
+    uint8_t *choice;
+    size_t nchoice;
+    uint8_t choice_value;
+    IterState *st;
+    uint32_t max_iter, nqueries;
+};
+cudaError_t launch_closure_begin(const ClosureBegin &a, int num_sms, cudaStream_t s);
 // Persistent closure (word-level variants only): the whole fixpoint in one
 // cooperative launch of `grid` CTAs (at most persistent_blocks_per_sm() per
 // SM); items: 4 lists of list_cap; phase_log: 3 timestamps per iteration.

@@ -41,6 +41,12 @@ __device__ __forceinline__ DevMat resolve_operand(const MatSlot &s, uint8_t use_
     return s.dlt[iter & 1];
 }
 
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t *p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
 __device__ __forceinline__ uint32_t bitmask(uint32_t word, int b) {
     // all-ones if bit b of word is set, else zero
     return (uint32_t)((int32_t)(word << (31 - b)) >> 31);
@@ -80,15 +86,17 @@ struct ItemCounters {
 // the item merges nothing), after which *gate is cleared so that the CTA's
 // later items skip the check.  direct_merge: every non-zero result word goes
 // straight to its atomic OR (one round trip less per item; for latency-bound
-// closures), else only words with bits C does not hold yet.  Ends with the
-// CTA synchronised.
+// closures), else only words with bits C does not hold yet.  stamps non-null
+// (thread 0): %globaltimer after the k-list, after the first staged k-tile
+// arrived, after the last k-tile and after the gate.  Ends with the CTA
+// synchronised.
 template <bool kM4R, int kW, class Smem>
 __device__ __forceinline__ void process_item(Smem &S, uint64_t it, const ProdDesc *__restrict__ prods,
                                              const MatSlot *__restrict__ slots, uint32_t iter, uint32_t *changed,
                                              uint32_t *qchanged, uint32_t &phase, bool &timed_out,
                                              ItemCounters &ctr, BufCounters *cnts,
                                              const uint32_t **gate = nullptr, uint32_t gate_target = 0,
-                                             bool direct_merge = false) {
+                                             bool direct_merge = false, unsigned long long *stamps = nullptr) {
     static_assert(kBJ % kW == 0 && kBJ / kW <= 4, "whole tiles per warp, at most 4");
     static_assert(kShortRange <= 32u * kW, "one k-tile per thread in the short k-list path");
     constexpr int kTPW = kBJ / kW;             // output tiles per warp
@@ -218,6 +226,10 @@ __device__ __forceinline__ void process_item(Smem &S, uint64_t it, const ProdDes
     __syncthreads();
     }
     const uint32_t nk = S.nk;
+    if (stamps && tid == 0) stamps[0] = stamps[1] = globaltimer_ns();
+    // thread 0 reads the gate early (with the first staged k-tile) so that
+    // the read is usually back, and open, by the time the results are ready
+    uint32_t gate_seen = 0;
 
     uint2 acc0[kTPW], acc1[kTPW];
 #pragma unroll
@@ -246,6 +258,10 @@ __device__ __forceinline__ void process_item(Smem &S, uint64_t it, const ProdDes
         const uint32_t stage = e % kStages;
         if (!timed_out && !mbar_wait_bounded(&S.bar[stage], (phase >> stage) & 1u)) timed_out = true;
         phase ^= 1u << stage;
+        if (tid == 0 && e == 0) {
+            if (gate && *gate) gate_seen = ld_acquire(*gate);
+            if (stamps) stamps[1] = globaltimer_ns();
+        }
         const bool dense = (S.ktile[e] & 0x8000u) != 0;
         const uint32_t wmask = ((uint32_t)S.kmask[e] >> (kTPW * warp)) & kWMask;
         const uint4 pp = *reinterpret_cast<const uint4 *>(&S.p[stage][2 * lane]);
@@ -374,22 +390,23 @@ __device__ __forceinline__ void process_item(Smem &S, uint64_t it, const ProdDes
         timed_out = __syncthreads_or(timed_out) != 0;
         if (tid == 0 && !timed_out && e + kStages < nk) staged += issue(e + kStages, stage);
     }
+    if (stamps && tid == 0) stamps[2] = stamps[3] = globaltimer_ns();
     if (gate && *gate) {
         bool gave_up = false;
-        if (tid == 0 && !timed_out) {
+        if (tid == 0 && !timed_out && gate_seen < gate_target) {
             uint32_t spins = 0;
-            while (*reinterpret_cast<const volatile uint32_t *>(*gate) < gate_target) {
+            while (ld_acquire(*gate) < gate_target) {
                 if (++spins > kGateSpinLimit) {
                     gave_up = true;
                     break;
                 }
                 __nanosleep(64);
             }
-            __threadfence();
         }
         timed_out = __syncthreads_or(timed_out || gave_up) != 0;
         if (timed_out) return;
         *gate = nullptr;
+        if (stamps && tid == 0) stamps[3] = globaltimer_ns();
     }
     // ---- epilogue: the 2*kTPW words of the thread in three batches (loads of C,
     // then the atomics that can add bits, then D / populations), so that

@@ -430,6 +430,9 @@ typedef struct cfpq_item_record {
     uint32_t iteration;
     uint16_t cta, list;
     uint64_t start_ns, end_ns;
+    /* item sub-phases, ns after start_ns: k-list built, first staged k-tile
+     * arrived, last k-tile done, results allowed to merge (0 for list 2) */
+    uint32_t klist_ns, staged_ns, computed_ns, gate_ns;
 } cfpq_item_record;
 size_t cfpq_item_log(cfpq_ctx *ctx, cfpq_item_record *out, size_t cap);
 
