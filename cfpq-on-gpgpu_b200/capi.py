@@ -438,8 +438,10 @@ class Context:
         return {k: getattr(c, k) for k, _ in c._fields_}
 
     def phase_log(self) -> np.ndarray:
-        """Per-iteration phase durations (plan, products) in microseconds of the
-        last persistent closure, shape (iterations, 2); empty if none."""
+        """Per-iteration durations in microseconds of the last persistent
+        closure, shape (iterations, 2): CTA 0's share of the plan, then the
+        rest of the iteration up to its grid barrier (items run while other
+        CTAs still plan); empty if none."""
         n = self.lib.cfpq_last_phase_log(self.handle, None, 0)
         if n == 0:
             return np.zeros((0, 2))

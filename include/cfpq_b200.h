@@ -407,8 +407,9 @@ int cfpq_autotune(cfpq_ctx *ctx, const cfpq_autotune_opts *opts, cfpq_selector_c
 
 /* Phase timestamps of the last closure that ran as one persistent kernel
  * (use_graph = CFPQ_LOOP_DEVICE, every product word-level): per iteration
- * three %globaltimer values in ns -- iteration start, end of the plan phase,
- * end of the product phase (both after the grid barrier).  Copies
+ * three %globaltimer values in ns taken by CTA 0 -- iteration start, CTA 0
+ * done with its share of the plan (other CTAs' items may already run), and
+ * the iteration's grid barrier passed (all products done).  Copies
  * min(cap, 3 * iterations) values and returns the number of iterations logged
  * (at most 4096; 0 when the last closure did not run persistently). */
 size_t cfpq_last_phase_log(cfpq_ctx *ctx, uint64_t *out, size_t cap);
