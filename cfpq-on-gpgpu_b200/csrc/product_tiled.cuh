@@ -11,7 +11,7 @@ namespace tiled {
 
 
 constexpr int kBJ = 16;              // output tiles per work item (1024 columns)
-constexpr uint32_t kStages = 4;      // staged k-tiles in flight per CTA
+constexpr uint32_t kStages = 4;      // staged k-tiles in flight per CTA (product kernels)
 constexpr uint32_t kLaneBits = 4;    // sparse loop: bits per row a lane walks before the warp helps
 constexpr int kThreads = 128;        // 4 warps (product kernels; the persistent kernel runs 8)
 constexpr int kMaxTiles = 2048;      // k-list capacity (n <= 131072)
@@ -21,12 +21,13 @@ constexpr unsigned kFull = 0xffffffffu;
 constexpr uint32_t kGateSpinLimit = 1u << 24;  // ~1 s of polling
 constexpr uint32_t kShortRange = 64;            // k ranges up to this length build the k-list in one round trip
 
-template <bool kM4R>
+template <bool kM4R, uint32_t kS = kStages>
 struct __align__(128) TiledSmem {
-    uint64_t q[kStages][kBJ * 64];  // kStages x 8 KiB
-    uint64_t p[kStages][64];        // kStages x 512 B
+    static constexpr uint32_t kNumStages = kS;
+    uint64_t q[kS][kBJ * 64];  // kS x 8 KiB
+    uint64_t p[kS][64];        // kS x 512 B
     uint64_t tab[kM4R ? 16 * 16 * kTabRow : 1];  // M4R tables [slab][key][tile], 34 KiB
-    uint64_t bar[kStages];
+    uint64_t bar[kS];
     uint16_t cand[kMaxTiles];    // occupied P tiles of the item's tile-row
     uint16_t cmask[kMaxTiles];   // their Q block occupancy
     uint32_t rball[kMaxTiles / 32], roff[kMaxTiles / 32];  // per-round ballots and rank offsets
@@ -102,6 +103,8 @@ __device__ __forceinline__ void process_item(Smem &S, uint64_t it, const ProdDes
     constexpr int kTPW = kBJ / kW;             // output tiles per warp
     constexpr uint32_t kNT = 32u * kW;         // threads
     constexpr uint32_t kWMask = (1u << kTPW) - 1;
+    constexpr uint32_t kSt = Smem::kNumStages;       // staged k-tiles in flight
+    static_assert(kSt <= 32, "one mbarrier parity bit per stage");
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     unsigned long long &triples = ctr.triples, &staged = ctr.staged, &outw = ctr.outw, &neww = ctr.neww;
     const ProdDesc pd = prods[item_prod(it)];
@@ -249,13 +252,13 @@ __device__ __forceinline__ void process_item(Smem &S, uint64_t it, const ProdDes
         bulk_g2s(&S.q[stage][lo * 64], Q.bits + tile_offset(T, tk, tj0 + lo), qbytes, &S.bar[stage]);
         return 512u + qbytes;
     };
-    // k-tile e goes to stage e % kStages; the first kStages are issued up
-    // front, a stage is refilled (k-tile e + kStages) once every thread is
+    // k-tile e goes to stage e % kSt; the first kSt are issued up
+    // front, a stage is refilled (k-tile e + kSt) once every thread is
     // done with it
     if (tid == 0)
-        for (uint32_t e = 0; e < nk && e < kStages; ++e) staged += issue(e, e);
+        for (uint32_t e = 0; e < nk && e < kSt; ++e) staged += issue(e, e);
     for (uint32_t e = 0; e < nk; ++e) {
-        const uint32_t stage = e % kStages;
+        const uint32_t stage = e % kSt;
         if (!timed_out && !mbar_wait_bounded(&S.bar[stage], (phase >> stage) & 1u)) timed_out = true;
         phase ^= 1u << stage;
         if (tid == 0 && e == 0) {
@@ -388,7 +391,7 @@ __device__ __forceinline__ void process_item(Smem &S, uint64_t it, const ProdDes
         // all threads are done with this stage (and the tables) before they
         // are refilled; a timeout anywhere in the CTA stops every later wait
         timed_out = __syncthreads_or(timed_out) != 0;
-        if (tid == 0 && !timed_out && e + kStages < nk) staged += issue(e + kStages, stage);
+        if (tid == 0 && !timed_out && e + kSt < nk) staged += issue(e + kSt, stage);
     }
     if (stamps && tid == 0) stamps[2] = stamps[3] = globaltimer_ns();
     if (gate && *gate) {
