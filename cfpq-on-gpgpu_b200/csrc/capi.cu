@@ -1371,7 +1371,7 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
                                                  : nullptr,
                                            // one small closure: latency-bound, merge without the read of C
                                            nq == 1 && pl.prods[0].T <= kDirectMergeMaxTiles ? 1 : 0,
-                                           ctx->stream));
+                                           nq > 1 ? 1 : 0, ctx->stream));
     } else if (exec) {
         CUDA_TRY(cudaGraphLaunch(exec, ctx->stream));
     } else {

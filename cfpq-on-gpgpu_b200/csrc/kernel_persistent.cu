@@ -59,6 +59,7 @@ constexpr int kPW = 8;
 constexpr uint32_t kThreads = 32 * kPW;
 
 constexpr uint32_t kBarrierSpinLimit = 1u << 25;  // ~1 s of polling
+constexpr uint32_t kNoIndex = 0xFFFFFFFFu;
 
 // Word-level products only: output blocks of 16 tiles, at most 128 per
 // tile-row.  The planner areas do not alias the product layout (its mbarriers
@@ -121,6 +122,7 @@ struct PersistArgs {
     const QueryRange *qr;           // non-null (batches of 2..kMaxActive queries): active-query phase A
     ItemTrace *trace;               // non-null: one record per processed item (first kItemTraceCap)
     int direct_merge;               // items merge without reading C first (small single closures)
+    int prefetch;                   // take the next item index while processing one (batches)
     uint32_t *trace_count;
 };
 
@@ -343,9 +345,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_closure_persistent(PersistArgs 
         uint32_t *const qchanged = a.qt.changed ? a.qt.changed + (t % 3) * st->nqueries : nullptr;
         uint32_t *const changed = reinterpret_cast<uint32_t *>(&st->pbar[par]) + 1;  // kBarChanged
         const uint32_t *gate = &st->plan_done[par];  // cleared by the first item that passes it
+        uint32_t next_idx = kNoIndex;  // (thread 0) list index taken ahead
         while (!timed_out) {
             if (tid == 0) {
-                const uint32_t idx = atomicAdd(&st->pitem_next[par][0], 1u);
+                const uint32_t idx = next_idx != kNoIndex ? next_idx : atomicAdd(&st->pitem_next[par][0], 1u);
+                next_idx = kNoIndex;
                 volatile uint64_t *slot = items + idx;
                 unsigned long long v = 0;
                 uint32_t stop = 0, spins = 0;
@@ -364,7 +368,13 @@ __global__ void __launch_bounds__(kThreads, 2) k_closure_persistent(PersistArgs 
                     }
                     __nanosleep(32);
                 }
-                if (v) *slot = 0;
+                if (v) {
+                    *slot = 0;
+                    // batches: take the next index now, its round trip
+                    // overlaps this item (a single closure keeps items for
+                    // the CTAs that are free first)
+                    if (a.prefetch) next_idx = atomicAdd(&st->pitem_next[par][0], 1u);
+                }
                 s_item = v;
                 s_stop = stop;
             }
@@ -492,7 +502,7 @@ cudaError_t launch_closure_persistent(int has_m4r, int grid, const ProdDesc *pro
                                       uint32_t phase_log_iters, BufCounters *cnts, uint8_t *choice,
                                       const SelectorParams *sel, SelLogRow *sel_log, uint32_t sel_log_iters,
                                       const QueryRange *qr, ItemTrace *trace, uint32_t *trace_count,
-                                      int direct_merge, cudaStream_t s) {
+                                      int direct_merge, int prefetch, cudaStream_t s) {
     PersistArgs a;
     a.prods = prods;
     a.nprods = nprods;
@@ -517,6 +527,7 @@ cudaError_t launch_closure_persistent(int has_m4r, int grid, const ProdDesc *pro
     a.trace = trace;
     a.trace_count = trace_count;
     a.direct_merge = direct_merge;
+    a.prefetch = prefetch;
     void *args[] = {&a};
     if (has_m4r)
         return cudaLaunchCooperativeKernel((const void *)k_closure_persistent<true>, dim3(grid), dim3(kThreads), args,

@@ -101,9 +101,10 @@ cudaError_t launch_closure_persistent(int has_m4r, int grid, const ProdDesc *pro
                                       uint32_t phase_log_iters, BufCounters *cnts, uint8_t *choice,
                                       const SelectorParams *sel, SelLogRow *sel_log, uint32_t sel_log_iters,
                                       const QueryRange *qr, ItemTrace *trace, uint32_t *trace_count,
-                                      int direct_merge, cudaStream_t s);
+                                      int direct_merge, int prefetch, cudaStream_t s);
 // (trace non-null: one ItemTrace per processed item, counted in *trace_count)
 // (direct_merge: result words go to their atomic OR without reading C first)
+// (prefetch: a CTA takes its next item index while it processes one)
 // (qr non-null: per-query ranges of a batch of 2..kMaxActiveQueries queries,
 // whose iterations then plan and clear only the queries still changing; the
 // query-changed flags are then 3 * nqueries words, rotated per iteration)
