@@ -206,18 +206,18 @@ __device__ __forceinline__ bool grid_barrier(unsigned long long *w, uint32_t tar
     __syncthreads();
     if (threadIdx.x == 0) {
         uint32_t ok = 1;
-        __threadfence();
         if (abort) atomicOr(reinterpret_cast<uint32_t *>(w) + 1, kBarAbort);
-        unsigned long long v = atomicAdd(w, 1ull) + 1ull;
+        // release: the CTA's writes (ordered by the __syncthreads above) are
+        // visible before the arrival; acquire: other CTAs' writes before theirs
+        unsigned long long v = atom_add_acq_rel_u64(w, 1ull) + 1ull;
         uint32_t i = 0;
         while ((uint32_t)v < target) {
             if (++i > kBarrierSpinLimit) {
                 ok = 0;
                 break;
             }
-            v = *reinterpret_cast<volatile unsigned long long *>(w);
+            v = ld_acquire_u64(w);
         }
-        __threadfence();
         s_ok = ok;
         s_flags = (uint32_t)(v >> 32);
     }
@@ -328,8 +328,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_closure_persistent(PersistArgs 
         fence_proxy_async_smem();  // the scratch writes come before the next bulk copies into the same bytes
         __syncthreads();
         if (tid == 0) {  // this CTA's items, clears and counter resets are all published
-            __threadfence();
-            atomicAdd(&st->plan_done[par], 1u);
+            red_add_release_u32(&st->plan_done[par], 1u);
             if (blockIdx.x == 0 && a.phase_log && t - iter0 < a.phase_log_iters)
                 a.phase_log[3 * (t - iter0) + 1] = globaltimer_ns();
             if (a.trace) trace_item(a, 0, t, 2, plan_t0);
@@ -355,8 +354,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_closure_persistent(PersistArgs 
                 uint32_t stop = 0, spins = 0;
                 for (;;) {
                     if (idx < a.list_cap && (v = *slot) != 0) break;
-                    if (*reinterpret_cast<volatile uint32_t *>(&st->plan_done[par]) == gridDim.x) {
-                        __threadfence();
+                    if (ld_acquire_u32(&st->plan_done[par]) == gridDim.x) {
                         if (idx >= *reinterpret_cast<volatile uint32_t *>(&st->pitem_count[par][0])) {
                             stop = 1;
                             break;

@@ -42,12 +42,6 @@ __device__ __forceinline__ DevMat resolve_operand(const MatSlot &s, uint8_t use_
     return s.dlt[iter & 1];
 }
 
-__device__ __forceinline__ uint32_t ld_acquire(const uint32_t *p) {
-    uint32_t v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
 __device__ __forceinline__ uint32_t bitmask(uint32_t word, int b) {
     // all-ones if bit b of word is set, else zero
     return (uint32_t)((int32_t)(word << (31 - b)) >> 31);
@@ -262,7 +256,7 @@ __device__ __forceinline__ void process_item(Smem &S, uint64_t it, const ProdDes
         if (!timed_out && !mbar_wait_bounded(&S.bar[stage], (phase >> stage) & 1u)) timed_out = true;
         phase ^= 1u << stage;
         if (tid == 0 && e == 0) {
-            if (gate && *gate) gate_seen = ld_acquire(*gate);
+            if (gate && *gate) gate_seen = ld_acquire_u32(*gate);
             if (stamps) stamps[1] = globaltimer_ns();
         }
         const bool dense = (S.ktile[e] & 0x8000u) != 0;
@@ -398,7 +392,7 @@ __device__ __forceinline__ void process_item(Smem &S, uint64_t it, const ProdDes
         bool gave_up = false;
         if (tid == 0 && !timed_out && gate_seen < gate_target) {
             uint32_t spins = 0;
-            while (ld_acquire(*gate) < gate_target) {
+            while (ld_acquire_u32(*gate) < gate_target) {
                 if (++spins > kGateSpinLimit) {
                     gave_up = true;
                     break;
