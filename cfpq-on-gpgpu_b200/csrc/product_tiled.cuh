@@ -16,7 +16,7 @@ constexpr uint32_t kLaneBits = 4;    // sparse loop: bits per row a lane walks b
 constexpr int kThreads = 128;        // 4 warps (product kernels; the persistent kernel runs 8)
 constexpr int kMaxTiles = 2048;      // k-list capacity (n <= 131072)
 constexpr uint32_t kSparseMax = 96;  // P-tile population up to which the sparse loop runs
-constexpr int kTabRow = kBJ + 1;     // padded table row (uint64 words)
+constexpr int kTabRow = 17;          // padded table row (uint64 words): 16 keys, or kBJ tiles
 constexpr unsigned kFull = 0xffffffffu;
 constexpr uint32_t kGateSpinLimit = 1u << 24;  // ~1 s of polling
 constexpr uint32_t kShortRange = 64;            // k ranges up to this length build the k-list in one round trip
@@ -26,7 +26,9 @@ struct __align__(128) TiledSmem {
     static constexpr uint32_t kNumStages = kS;
     uint64_t q[kS][kBJ * 64];  // kS x 8 KiB
     uint64_t p[kS][64];        // kS x 512 B
-    uint64_t tab[kM4R ? 16 * 16 * kTabRow : 1];  // M4R tables [slab][key][tile], 34 KiB
+    // M4R tables, 34 KiB: [tile][slab][key] when each warp builds its own
+    // tiles' tables (8 warps), [slab][key][tile] when the CTA builds them all
+    uint64_t tab[kM4R ? kBJ * 16 * kTabRow : 1];
     uint64_t bar[kS];
     uint16_t cand[kMaxTiles];    // occupied P tiles of the item's tile-row
     uint16_t cmask[kMaxTiles];   // their Q block occupancy
@@ -321,8 +323,10 @@ __device__ __forceinline__ void process_item(Smem &S, uint64_t it, const ProdDes
                     }
                 }
             }
-        } else if constexpr (kM4R) {
-            // build: (slab s, tile j) pairs over the CTA; 16 keys each
+        } else if constexpr (kM4R && kTPW > 2) {
+            // 4 tiles per warp: the CTA builds every (slab, tile) table
+            // (lanes of a warp on 16 different tiles: conflict-free stores),
+            // then a barrier, then each warp looks up its tiles
             for (uint32_t pr = tid; pr < 16 * kBJ; pr += kNT) {
                 const uint32_t s = pr / kBJ, j = pr % kBJ;
                 const uint64_t *qr = &S.q[stage][j * 64 + 4 * s];
@@ -358,6 +362,53 @@ __device__ __forceinline__ void process_item(Smem &S, uint64_t it, const ProdDes
                     for (int j = 0; j < kTPW; ++j) {
                         or64(acc0[j], ta[j]);
                         or64(acc1[j], tb[j]);
+                    }
+                }
+            }
+        } else if constexpr (kM4R) {
+            // at most 2 tiles per warp: each warp builds the tables of its
+            // own tiles only (the only ones it reads), so no CTA-wide barrier
+            // separates the build from the lookups.  Table (tile, slab) holds
+            // the ORs of the 16 subsets of the slab's 4 Q rows; rows are 17
+            // words apart, so the 16 keys of one lookup hit 16 different bank
+            // pairs.
+            if (wmask && !timed_out) {
+                __syncwarp();  // the warp's lookups of the previous k-tile are done
+                for (uint32_t pr = lane; pr < 16u * kTPW; pr += 32) {
+                    const uint32_t s = pr / kTPW, jj = pr % kTPW;
+                    const uint32_t j = kTPW * warp + jj;
+                    const uint64_t *qr = &S.q[stage][j * 64 + 4 * s];
+                    const uint64_t q0 = qr[0], q1 = qr[1], q2 = qr[2], q3 = qr[3];
+                    uint64_t *t = &S.tab[(j * 16 + s) * kTabRow];
+                    const uint64_t a01 = q0 | q1, a23 = q2 | q3;
+                    t[0] = 0;
+                    t[1] = q0;
+                    t[2] = q1;
+                    t[3] = a01;
+                    t[4] = q2;
+                    t[5] = q0 | q2;
+                    t[6] = q1 | q2;
+                    t[7] = a01 | q2;
+                    t[8] = q3;
+                    t[9] = q0 | q3;
+                    t[10] = q1 | q3;
+                    t[11] = a01 | q3;
+                    t[12] = a23;
+                    t[13] = q0 | a23;
+                    t[14] = q1 | a23;
+                    t[15] = a01 | a23;
+                }
+                __syncwarp();
+                const uint64_t pa = ((uint64_t)pp.y << 32) | pp.x;  // row 2l
+                const uint64_t pb = ((uint64_t)pp.w << 32) | pp.z;  // row 2l+1
+#pragma unroll
+                for (int s = 0; s < 16; ++s) {
+                    const uint32_t ka = (uint32_t)((pa >> (4 * s)) & 15u), kb = (uint32_t)((pb >> (4 * s)) & 15u);
+#pragma unroll
+                    for (int j = 0; j < kTPW; ++j) {
+                        const uint64_t *t = &S.tab[((kTPW * warp + j) * 16 + s) * kTabRow];
+                        or64(acc0[j], t[ka]);
+                        or64(acc1[j], t[kb]);
                     }
                 }
             }
