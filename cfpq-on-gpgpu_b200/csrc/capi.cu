@@ -441,23 +441,41 @@ static int load_edges_impl(cfpq_ctx *ctx, cfpq_matrix *const *mats, size_t nmats
     uint32_t *d_off = reinterpret_cast<uint32_t *>(base + up(bd) + 3 * up(be));
     uint32_t *d_lm = reinterpret_cast<uint32_t *>(base + up(bd) + 3 * up(be) + up(bo));
     // Small tables go through a pinned host block (copied with the call, so the
-    // caller's arrays are free on return and the copy is truly asynchronous).
+    // caller's arrays are free on return and the copy is truly asynchronous);
+    // when they and the buffer layout equal the previous call's (the same
+    // matrices and labels loaded again), the device copies are still there.
+    std::vector<unsigned char> key(6 * sizeof(size_t) + bd + bo + (size_t)nlm * 4);
+    {
+        const size_t head[6] = {bd, be, bo, bl, (size_t)nlm, (size_t)(uintptr_t)ctx->edge_buf.p};
+        unsigned char *k = key.data();
+        memcpy(k, head, sizeof(head));
+        memcpy(k + sizeof(head), descs.data(), bd);
+        memcpy(k + sizeof(head) + bd, label_offsets, bo);
+        if (nlm) memcpy(k + sizeof(head) + bd + bo, label_mats, (size_t)nlm * 4);
+    }
+    const bool tables_loaded = key == ctx->edge_tables_key;
     const size_t small = up(bd) + up(bo) + up(bl);
-    if (ctx->h_small_cap < small) {
+    if (!tables_loaded && ctx->h_small_cap < small) {
         if (ctx->h_small) cudaFreeHost(ctx->h_small);
         ctx->h_small = nullptr;
         ctx->h_small_cap = 0;
         CUDA_TRY(cudaMallocHost(&ctx->h_small, small));
         ctx->h_small_cap = small;
     }
-    CUDA_TRY(cudaStreamSynchronize(ctx->stream));  // previous user of h_small done
-    char *hs = reinterpret_cast<char *>(ctx->h_small);
-    memcpy(hs, descs.data(), bd);
-    memcpy(hs + up(bd), label_offsets, bo);
-    if (nlm) memcpy(hs + up(bd) + up(bo), label_mats, (size_t)nlm * 4);
-    CUDA_TRY(cudaMemcpyAsync(d_desc, hs, bd, cudaMemcpyHostToDevice, ctx->stream));
-    CUDA_TRY(cudaMemcpyAsync(d_off, hs + up(bd), bo, cudaMemcpyHostToDevice, ctx->stream));
-    if (nlm) CUDA_TRY(cudaMemcpyAsync(d_lm, hs + up(bd) + up(bo), (size_t)nlm * 4, cudaMemcpyHostToDevice, ctx->stream));
+    if (!tables_loaded) {
+        ctx->edge_tables_key.clear();
+        CUDA_TRY(cudaStreamSynchronize(ctx->stream));  // previous user of h_small done
+        char *hs = reinterpret_cast<char *>(ctx->h_small);
+        memcpy(hs, descs.data(), bd);
+        memcpy(hs + up(bd), label_offsets, bo);
+        if (nlm) memcpy(hs + up(bd) + up(bo), label_mats, (size_t)nlm * 4);
+        CUDA_TRY(cudaMemcpyAsync(d_desc, hs, bd, cudaMemcpyHostToDevice, ctx->stream));
+        CUDA_TRY(cudaMemcpyAsync(d_off, hs + up(bd), bo, cudaMemcpyHostToDevice, ctx->stream));
+        if (nlm)
+            CUDA_TRY(cudaMemcpyAsync(d_lm, hs + up(bd) + up(bo), (size_t)nlm * 4, cudaMemcpyHostToDevice, ctx->stream));
+        // host-edge loads overwrite the edge arrays only, never the tables
+        ctx->edge_tables_key = std::move(key);
+    }
     if (on_device) {
         d_from = const_cast<uint32_t *>(from);
         d_label = const_cast<uint32_t *>(label);
@@ -499,9 +517,18 @@ extern "C" int cfpq_matrices_clear(cfpq_ctx *ctx, cfpq_matrix *const *mats, size
         tab[i].pad = 0;
         rows += mats[i]->d.T;
     }
+    void *const before = ctx->clear_desc.p;
     TRY(ctx->clear_desc.ensure(count * sizeof(MatRows)));
-    CUDA_TRY(cudaMemcpyAsync(ctx->clear_desc.p, tab.data(), count * sizeof(MatRows), cudaMemcpyHostToDevice,
-                             ctx->stream));
+    // the same list as the previous call (a prepared query cleared again):
+    // its table is still on the device
+    const unsigned char *tb = reinterpret_cast<const unsigned char *>(tab.data());
+    std::vector<unsigned char> key(tb, tb + count * sizeof(MatRows));
+    if (ctx->clear_desc.p != before || key != ctx->clear_desc_key) {
+        ctx->clear_desc_key.clear();
+        CUDA_TRY(cudaMemcpyAsync(ctx->clear_desc.p, tab.data(), count * sizeof(MatRows), cudaMemcpyHostToDevice,
+                                 ctx->stream));
+        ctx->clear_desc_key = std::move(key);
+    }
     CUDA_TRY(launch_clear_rows(ctx->clear_desc.as<MatRows>(), (uint32_t)count, rows, ctx->stream));
     return CFPQ_OK;
 }

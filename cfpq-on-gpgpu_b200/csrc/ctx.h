@@ -139,6 +139,8 @@ struct cfpq_ctx {
     cfpq_kernel_profile prof = {};
     void *h_small = nullptr;
     size_t h_small_cap = 0;
+    std::vector<unsigned char> edge_tables_key;  // small tables of the last edge load still in edge_buf
+    std::vector<unsigned char> clear_desc_key;   // matrix list of the last cfpq_matrices_clear in clear_desc
     void *items_clean_ptr = nullptr;  // items buffer whose first items_clean_words words are zero
     size_t items_clean_words = 0;
     void *h_query = nullptr;  // pinned: per-query results of a closure (done_ns, last_iter)

@@ -396,6 +396,40 @@ def test_batch_active_queries(ctx, pkg, oracle, tmp_path):
             q.close()
 
 
+def test_interleaved_loads_and_clears(ctx, pkg):
+    """Edge loads and clears of alternating matrix sets (host and device edge
+    arrays, the library keeping the small tables of the last load on the
+    device) leave every matrix exactly as a first load does."""
+    import torch
+
+    wls = [pkg.workloads.ontology_query(700, 3), pkg.workloads.brackets_query(), pkg.workloads.ontology_query(700, 4)]
+    qs = [pkg.query.PreparedQuery(ctx, w.grammar, w.graph) for w in wls]
+    try:
+        first = []
+        for q in qs:
+            q.load()
+            first.append(ctx.hash_count_many(q.mats))
+        for order in ([0, 1, 2], [2, 2, 0], [1, 0, 1]):
+            for i in order:
+                qs[i].load()
+                assert ctx.hash_count_many(qs[i].mats) == first[i]
+            for i in order:  # device-resident edge arrays
+                g = qs[i].graph
+                dev = [torch.from_numpy(a.view(np.int32)).cuda() for a in (g.src, g.label, g.dst)]
+                ctx.clear_many(qs[i].mats)
+                ctx.load_edges_device(qs[i].mats, dev[0].data_ptr(), dev[1].data_ptr(), dev[2].data_ptr(),
+                                      g.nedges, qs[i].off, qs[i].lm)
+                for e in qs[i].grammar.epsilon:
+                    qs[i].mats[e].set_diagonal()
+                assert ctx.hash_count_many(qs[i].mats) == first[i]
+        ctx.clear_many(qs[0].mats)
+        assert all(c == 0 for _, c in ctx.hash_count_many(qs[0].mats))
+        assert ctx.hash_count_many(qs[1].mats) == first[1]
+    finally:
+        for q in qs:
+            q.close()
+
+
 def test_item_trace(ctx, pkg, oracle, tmp_path):
     """LOG_ITEMS records every work item of a persistent closure once, and
     tracing does not change the result."""
