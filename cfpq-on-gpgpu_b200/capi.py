@@ -327,6 +327,7 @@ class Context:
         _check(self.lib, self.lib.cfpq_ctx_create(int(device), ctypes.byref(h)))
         self.handle = h
         self.device = device
+        self._closure_args = None  # (key, ctypes arguments) of the last closure() call
 
     def close(self) -> None:
         if self.handle:
@@ -372,10 +373,17 @@ class Context:
 
     def closure(self, rules: Sequence[tuple[int, int, int]], mats: Sequence[Matrix], driver="engine",
                 variant="auto", use_graph: bool = True, max_iterations: int = 0, log_products: bool = False) -> dict:
-        rs = (Rule * max(len(rules), 1))(*[Rule(*map(int, r)) for r in rules])
-        hs = (ctypes.c_void_p * max(len(mats), 1))(*[m.handle for m in mats])
-        o = self._opts(driver, variant, use_graph, max_iterations, log_products)
-        st = ClosureStats()
+        # the ctypes arguments of the last call are kept: a prepared query
+        # closed again (the serving loop) pays no argument marshalling
+        key = (tuple(map(tuple, rules)), tuple(m.handle for m in mats), driver, variant, use_graph,
+               max_iterations, log_products)
+        args = self._closure_args if self._closure_args and self._closure_args[0] == key else None
+        if args is None:
+            rs = (Rule * max(len(rules), 1))(*[Rule(*map(int, r)) for r in rules])
+            hs = (ctypes.c_void_p * max(len(mats), 1))(*[m.handle for m in mats])
+            o = self._opts(driver, variant, use_graph, max_iterations, log_products)
+            args = self._closure_args = (key, rs, hs, o, ClosureStats())
+        _, rs, hs, o, st = args
         _check(self.lib, self.lib.cfpq_closure(self.handle, rs, len(rules), hs, len(mats), ctypes.byref(o),
                                                ctypes.byref(st)))
         return st.as_dict()
