@@ -374,8 +374,6 @@ __global__ void k_advance_end(const MatSlot *__restrict__ slots, uint32_t nslots
     if (threadIdx.x == 0 && use_handle) cudaGraphSetConditional(handle, s_go ? 1u : 0u);
 }
 
-__global__ void k_mark_start(IterState *st) { st->t_start_ns = globaltimer_ns(); }
-
 // Closure prologue in one launch: zero the given word ranges, fill the
 // variant choices, initialise the iteration state and stamp its start.
 __global__ void k_closure_begin(ClosureBegin a) {
@@ -545,11 +543,6 @@ cudaError_t launch_closure_begin(const ClosureBegin &a, int num_sms, cudaStream_
     for (int r = 0; r < ClosureBegin::kRanges; ++r) words = words > a.nwords[r] ? words : a.nwords[r];
     const unsigned blocks = (unsigned)std::max<size_t>(1, std::min<size_t>((words + 255) / 256, (size_t)num_sms * 4));
     k_closure_begin<<<blocks, 256, 0, s>>>(a);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_mark_start(IterState *d_st, cudaStream_t s) {
-    k_mark_start<<<1, 1, 0, s>>>(d_st);
     return cudaGetLastError();
 }
 

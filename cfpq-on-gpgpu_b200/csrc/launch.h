@@ -74,7 +74,6 @@ int product_tiled_blocks_per_sm(int m4r);
 cudaError_t launch_advance_end(const MatSlot *d_slots, uint32_t nslots, uint32_t total_rows, IterState *d_st,
                                const QueryTrack &qt, cudaGraphConditionalHandle handle, int use_handle,
                                BufCounters *d_cnts, cudaStream_t s);
-cudaError_t launch_mark_start(IterState *d_st, cudaStream_t s);
 
 // Closure prologue (one launch): zero[r][0 .. nwords[r]) = 0, choice[0 ..
 // nchoice) = choice_value, *st = a fresh iteration state (active, max_iter,
