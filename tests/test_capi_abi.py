@@ -71,3 +71,29 @@ def test_order_suggest_rejects_out_of_range(pkg):
     out = np.zeros(4, dtype=np.uint32)
     rc = lib.cfpq_order_suggest(4, src.ctypes.data, src.ctypes.data, src.ctypes.data, 2, out.ctypes.data)
     assert rc == pkg.capi.ERR_INVALID
+
+
+def test_python_record_layouts_match_the_header(pkg, tmp_path):
+    """The numpy / ctypes views of the C records have the header's sizes and
+    field offsets (compiled with the host C compiler, no GPU)."""
+    import subprocess
+
+    src = tmp_path / "sizes.c"
+    src.write_text(
+        '#include <stddef.h>\n#include <stdio.h>\n#include "cfpq_b200.h"\n'
+        "int main(void) {\n"
+        '  printf("%zu %zu %zu %zu %zu %zu\\n", sizeof(cfpq_item_record), offsetof(cfpq_item_record, start_ns),\n'
+        "         offsetof(cfpq_item_record, klist_ns), sizeof(cfpq_product_record),\n"
+        "         offsetof(cfpq_product_record, features), offsetof(cfpq_product_record, usec));\n"
+        "  return 0;\n}\n")
+    exe = tmp_path / "sizes"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), "-o", str(exe), str(src)], check=True)
+    item, item_start, item_klist, prod, prod_feat, prod_usec = map(int, subprocess.run(
+        [str(exe)], check=True, capture_output=True, text=True).stdout.split())
+    capi = pkg.capi
+    assert capi.ITEM_RECORD_DTYPE.itemsize == item
+    assert capi.ITEM_RECORD_DTYPE.fields["start_ns"][1] == item_start
+    assert capi.ITEM_RECORD_DTYPE.fields["klist_ns"][1] == item_klist
+    assert capi.PRODUCT_RECORD_DTYPE.itemsize == prod == ctypes.sizeof(capi.ProductRecord)
+    assert capi.PRODUCT_RECORD_DTYPE.fields["features"][1] == prod_feat
+    assert capi.PRODUCT_RECORD_DTYPE.fields["usec"][1] == prod_usec
