@@ -56,6 +56,8 @@ def parse_args():
                     help="train the cost model on logged product timings and report its regret (about a minute)")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the plain-GPU-form, reference-GPU, brackets and 512-query batch measurements")
+    ap.add_argument("--no-chain", action="store_true",
+                    help="skip the N=65536 chain closure (about three minutes)")
     ap.add_argument("--no-graph", action="store_true",
                     help="launch every kernel from the host instead of the CUDA-graph loop (profilers cannot "
                          "capture kernel nodes of graphs with conditional nodes)")
@@ -225,6 +227,59 @@ def _event_ms(torch, stream, fn):
     return e0.elapsed_time(e1), r
 
 
+def tile_model_bytes(ctx, q, grammar, iterations: int) -> dict:
+    """Algorithmic bytes of a closure under the tile model: per product term
+    of every iteration, (occupied P tiles + occupied Q tiles in the rows that
+    P's occupied columns select + 2 x output tiles that some (P, Q) tile pair
+    reaches) x 512 B (one 64x64-bit tile).  P / Q are the full matrix or the
+    previous iteration's delta as the semi-naive term reads them.  The
+    per-iteration tile occupancy comes from closures stopped after k = 0..K
+    iterations (tile statistics downloaded after each; not timed)."""
+    import numpy as np
+
+    occ = []
+    for k in range(iterations + 1):
+        q.load()
+        if k:
+            ctx.closure(grammar.rules, q.mats, max_iterations=k)
+        occ.append([m.tile_stats()[1].astype(np.int64) for m in q.mats])
+    q.load()
+    tiles = {"p": 0, "q": 0, "c": 0}
+    terms = 0
+    for t in range(iterations):
+        cur = occ[t]
+        delta = [cur[i] > occ[t - 1][i] for i in range(len(cur))] if t else None
+        for head, b1, b2 in grammar.rules:
+            pairs = [(cur[b1] > 0, cur[b2] > 0)] if t == 0 else [(delta[b1], cur[b2] > 0), (cur[b1] > 0, delta[b2])]
+            for P, Q in pairs:
+                if not P.any():
+                    continue
+                cols = P.any(axis=0)
+                tiles["p"] += int(P.sum())
+                tiles["q"] += int(Q[cols].sum())
+                tiles["c"] += int(((P.astype(np.float32) @ Q.astype(np.float32)) > 0).sum())
+                terms += 1
+    return {"bytes": 512 * (tiles["p"] + tiles["q"] + 2 * tiles["c"]), "terms": terms,
+            "occupied_p_tiles": tiles["p"], "occupied_q_tiles": tiles["q"], "touched_c_tiles": tiles["c"]}
+
+
+def read_batch_fixture() -> dict:
+    """Answer lines of the 512-query batch (seed 1) from tests/golden/batch512_seed1.txt
+    (oracle M4RM for every query, the reference m4riCPU where it finished)."""
+    out, cur = {}, None
+    path = os.path.join(ROOT, "tests", "golden", "batch512_seed1.txt")
+    if not os.path.exists(path):
+        return {}
+    with open(path) as f:
+        for line in f:
+            parts = line.split()
+            if parts and parts[0] == "query":
+                cur = out.setdefault(int(parts[1]), {})
+            elif parts:
+                cur[parts[0]] = (int(parts[1]), int(parts[2]))
+    return out
+
+
 def plain_gpu_form(ctx, q, grammar, torch, stream, reps=2) -> dict:
     """The plain single-variant GPU form on the same workload: the reference's
     worklist driver (one product at a time, changed flag read back after each)
@@ -291,18 +346,147 @@ def batch_bench(pkg, ctx, torch, stream, rank, world, dist, nq=512, seed=1, step
             t = float(tt.item())
         local_lines = {i: dict(zip(wls[i].grammar.nonterminals, ctx.hash_count_many(q.mats)))
                        for i, q in zip(mine, qs)}
+        # the same queries closed one cfpq_closure at a time on the same
+        # context (the unbatched baseline): sum of the closures' device times
+        seq = 0.0
+        seq_ok = True
+        for i, q in zip(mine, qs):
+            q.load()
+            ctx.synchronize()
+            seq += _event_ms(torch, stream, lambda: ctx.closure(q.grammar.rules, q.mats))[0]
+            seq_ok &= dict(zip(q.grammar.nonterminals, ctx.hash_count_many(q.mats))) == local_lines[i]
+        if dist:
+            tt = torch.tensor([seq, float(seq_ok)], dtype=torch.float64, device="cuda")
+            dist.all_reduce(tt[:1], op=dist.ReduceOp.MAX)
+            dist.all_reduce(tt[1:], op=dist.ReduceOp.MIN)
+            seq, seq_ok = float(tt[0].item()), bool(tt[1].item())
         lines = pkg.shard.gather_lines(dist, local_lines)
         import numpy as np
 
+        expected = read_batch_fixture() if seed == 1 and nq == 512 else {}
+        parity = (len(expected) == nq and all(lines.get(i) == expected[i] for i in range(nq))) if expected else None
         return {"queries": nq, "ms": t, "queries_per_s": nq / (t / 1e3),
                 "p50_query_ms": float(np.percentile(done, 50)), "p99_query_ms": float(np.percentile(done, 99)),
                 "max_iterations": int(iters.max()), "products": st["products"], "ranks": world,
                 "sharding": "LPT on 2 * rules * n^3 per query, no data-path collective",
                 "queries_closed": len(lines),
+                "parity_vs_cpu": parity,
+                "parity_reference": "tests/golden/batch512_seed1.txt: every query's answer lines from the CPU "
+                                    "oracle (restated M4RM), also printed by the reference m4riCPU wherever it "
+                                    "finished within its time budget",
+                "sequential_ms": seq, "sequential_matches_batch": seq_ok,
+                "batch_speedup_vs_sequential": seq / t if t > 0 else None,
+                "sequential": "the same queries, one cfpq_closure each on the same context (default options), "
+                              "sum of device times; loads not timed",
                 "per_query_ms": "completion time of each query inside its rank's batch (device timer)"}
     finally:
         for q in qs:
             q.close()
+
+
+def chain_cpu_check(wl, q, rows_per_rule=16, seed=65536) -> dict:
+    """CPU side of the N=65536 chain workload: the closure property of the
+    device's fixpoint checked with the oracle on a row sample -- for every
+    rule C -> A B, rows R of C | A * B equal rows R of C (a dense CPU closure
+    at this size takes hours).  All host threads."""
+    import numpy as np
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle  # the checker
+
+    n = q.mats[0].n
+    rng = np.random.default_rng(seed)
+    rows = np.unique(np.concatenate([rng.choice(n, rows_per_rule - 2, replace=False), [0, n - 1]]))
+    rows = rows.astype(np.uint32)
+    t0 = time.perf_counter()
+    host = [m.download_rows() for m in q.mats]
+    ok, bad = True, []
+    for r, (head, b1, b2) in enumerate(wl.grammar.rules):
+        got = oracle.add_mul_rows(host[head], host[b1], host[b2], n, rows, os.cpu_count() or 1)
+        if not np.array_equal(got, host[head][rows]):
+            ok = False
+            bad.append(r)
+    return {"closure_property_holds": ok, "rules": len(wl.grammar.rules), "rows_per_rule": int(rows.size),
+            "failing_rules": bad, "cpu_s": time.perf_counter() - t0,
+            "check": "for every rule C -> A B: rows of C | A*B (oracle row gather) == rows of C at the fixpoint"}
+
+
+def reference_naive_product_ms(n: int, log2_inv_density: int = 1, reps: int = 1) -> dict:
+    """The reference's naive GPU product (gpu_lib::matrix_product_add_wrapper,
+    built from its sources for sm_100a under oracle/_ref/naiveGPU-product) on
+    random n x n matrices of density 2^-log2_inv_density."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "naiveGPU-product")
+    if not os.path.exists(exe):
+        return {"unavailable": "oracle/_ref/naiveGPU-product not built"}
+    try:
+        p = subprocess.run([exe, str(n), str(log2_inv_density), str(reps), "7"], capture_output=True, text=True,
+                           timeout=900)
+    except subprocess.TimeoutExpired:
+        return {"error": "timed out after 900 s"}
+    if p.returncode != 0:
+        return {"error": (p.stdout + p.stderr)[-300:]}
+    return {"ms": float(p.stdout.split()[1]), "density": 2.0 ** -log2_inv_density}
+
+
+def chain_bench(pkg, ctx, torch, stream, n=65536, seed=1) -> dict:
+    """The large chain workload: N = 65536 (512 MiB per matrix), mean
+    out-degree 2, 90% of edges with |u-v| <= 64 and 10% uniform, 6 labels,
+    random CNF with 10 nonterminals and 24 binary rules; one closure with the
+    selector choosing LOP3 / Four Russians / tensor cores per term and
+    iteration (device time, CUDA events), its closure property checked on the
+    CPU on a row sample, and per-product times at this n on random matrices of
+    density 0.5 for every engine variant, the plain single-variant form and
+    the reference's naive GPU product."""
+    import numpy as np
+
+    wl = pkg.workloads.chain_query(n, seed)
+    before = ctx.selector_config()
+    ctx.selector_configure(min_tiles=1)  # a single query selects per term
+    q = pkg.query.PreparedQuery(ctx, wl.grammar, wl.graph)
+    out = {"n": n, "seed": seed, "edges": wl.graph.nedges, "nonterminals": len(wl.grammar.nonterminals),
+           "rules": len(wl.grammar.rules)}
+    try:
+        q.load()
+        ctx.synchronize()
+        ms, st = _event_ms(torch, stream, lambda: ctx.closure(wl.grammar.rules, q.mats, variant="auto"))
+        out.update({"closure_s": ms / 1e3, "iterations": st["iterations"], "products": st["products"],
+                    "tile_triples": st["tile_triples"],
+                    "executed_tbitmac_per_s": st["tile_triples"] * 64 ** 3 / (ms / 1e3) / 1e12,
+                    "dense_equiv_tbitmac_per_s": st["dense_bitops"] / (ms / 1e3) / 1e12,
+                    "variant_items": {"lop3": st["variant_items"][2], "m4r": st["variant_items"][3],
+                                      "tc": st["variant_items"][4]},
+                    "result": {k: list(v) for k, v in zip(wl.grammar.nonterminals, ctx.hash_count_many(q.mats))}})
+        out["parity"] = chain_cpu_check(wl, q)
+    finally:
+        q.close()
+        ctx.selector_configure(**{k: before[k] for k in ("mode", "min_tiles", "tc_min_tiles")})
+    # per-product times on random density-0.5 operands
+    rng = np.random.default_rng(seed)
+    wpr = n // 64
+    a, b, c = ctx.matrix(n), ctx.matrix(n), ctx.matrix(n)
+    try:
+        for m in (a, b):
+            m.upload_rows(rng.integers(0, 2 ** 63, size=(n, wpr), dtype=np.uint64)
+                          | (rng.integers(0, 2, size=(n, wpr), dtype=np.uint64) << np.uint64(63)))
+        per = {}
+        ref_hash = None
+        for variant in ("tc", "m4r", "lop3", "plain"):
+            c.clear()
+            ctx.synchronize()
+            t, _ = _event_ms(torch, stream, lambda: ctx.add_mul(c, a, b, variant))
+            h = c.hash_count()
+            ref_hash = ref_hash or h
+            per[variant] = {"ms": t, "tbitmac_per_s": n ** 3 / (t / 1e3) / 1e12, "same_result": h == ref_hash}
+        out["per_product_random_d05"] = per
+    finally:
+        for m in (a, b, c):
+            m.destroy()
+    out["per_product_random_d05"]["reference_naiveGPU"] = reference_naive_product_ms(n)
+    ref_ms = out["per_product_random_d05"]["reference_naiveGPU"].get("ms")
+    best = min(v["ms"] for k, v in out["per_product_random_d05"].items() if k in ("tc", "m4r", "lop3"))
+    out["per_product_speedup"] = {"vs_plain_form": per["plain"]["ms"] / best,
+                                  "vs_reference_naiveGPU": ref_ms / best if ref_ms else None}
+    return out
 
 
 def brackets_small(pkg, ctx, torch, stream, reps=20) -> dict:
@@ -555,20 +739,35 @@ def ours_arm(args, world, rank, local):
     h2d = 3 * 4 * graph.nedges + 4 * (q.off.size + q.lm.size)
     d2h = 16 * len(q.mats)
 
-    # per-kernel device times (instrumented pass: every launch bracketed by events)
-    # roofline of the dominant kernel: the persistent closure kernel (one
-    # launch per step; its duration is the library's event pair around it)
+    # roofline of the dominant kernel, the persistent closure kernel (one
+    # launch per step, its duration the library's event pair around it):
+    # bound by the logic-instruction issue rate (32 bit-MACs per LOP3 on a
+    # 32-bit lane), measured on the executed tile triples (64^3 bit-MACs
+    # each); HBM beside it with the tile model's algorithmic bytes
     peaks = measured_peaks()
+    cal = ctx.calibrate()
     dev_ms = statistics.mean(device_ms) if device_ms else 0.0
-    alg_bytes = st["bytes_staged"] + 16 * st["out_words"] + 8 * st["new_words"]
-    achieved = alg_bytes / (dev_ms / 1e3) / 1e9 if dev_ms > 0 else 0.0
+    executed = st["tile_triples"] * 64 ** 3
+    achieved = executed / (dev_ms / 1e3) / 1e12 if dev_ms > 0 else 0.0
+    peak = cal["bitmac_per_s"] / 1e12
     tr = committed_traffic().get("k_closure_persistent", {}).get("dram_bytes_per_launch")
-    roofline = {"kernel": "k_closure_persistent" if len(phases) else "closure iteration kernels", "bound": "hbm",
-                "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                "frac": achieved / peaks["hbm_gbs"], "traffic": tr, "peak_source": peaks["source"],
-                "avg_launch_ms": dev_ms, "algorithmic_bytes_per_launch": alg_bytes,
-                "algorithmic_bytes": "operand tiles staged global->shared + 16 B per merged output word "
-                                     "(read + atomic) + 8 B per delta word written",
+    model = tile_model_bytes(ctx, q, grammar, st["iterations"])
+    hbm_achieved = model["bytes"] / (dev_ms / 1e3) / 1e9 if dev_ms > 0 else 0.0
+    roofline = {"kernel": "k_closure_persistent" if len(phases) else "closure iteration kernels",
+                "bound": "lop3_issue", "achieved": achieved, "peak": peak, "unit": "Tbit-MAC/s",
+                "frac": achieved / peak if peak else None, "traffic": tr,
+                "peak_source": f"calibrated on this GPU (cfpq_calibrate: register-only 3-input logic chains, "
+                               f"{cal['logic_ops_per_clk_sm']:.1f} ops/clk/SM x 32 bit-MACs per op)",
+                "avg_launch_ms": dev_ms, "executed_bitmac_per_launch": executed,
+                "executed": "tile_triples x 64^3 (tile pairs skipped as empty are not counted)",
+                "hbm": {"bound": "hbm", "algorithmic_bytes_per_launch": model["bytes"], "achieved": hbm_achieved,
+                        "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": hbm_achieved / peaks["hbm_gbs"],
+                        "traffic": tr, "peak_source": peaks["source"],
+                        "algorithmic_bytes": "per product term: (occupied P tiles + occupied Q tiles in the "
+                                             "rows P's columns select + 2 x output tiles reached) x 512 B",
+                        "tile_model": model},
+                "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch "
+                                "(profiles/traffic.json); the operands stay in L2 across iterations",
                 "note": "latency-bound: a few hundred short work items per iteration; see phase_us_per_iteration "
                         "and the dense_product_kernels rooflines"}
     if not args.no_profile:
@@ -629,6 +828,8 @@ def ours_arm(args, world, rank, local):
             out["batch_512"] = batch
         if args.selector_eval:
             out["selector_eval"] = selector_eval(pkg, ctx, torch, stream)
+        if world == 1 and not args.no_extras and not args.no_chain:
+            out["chain_65536"] = chain_bench(pkg, ctx, torch, stream)
         print(json.dumps(out))
     q.close()
     ctx.close()

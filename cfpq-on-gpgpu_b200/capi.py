@@ -18,8 +18,8 @@ LIB_PATH = os.path.join(PKG_DIR, "lib", "libcfpq_b200.so")
 OK = 0
 ERR_INVALID, ERR_CUDA, ERR_OOM, ERR_UNSUPPORTED, ERR_TIMEOUT, ERR_IO = 1, 2, 3, 4, 5, 6
 
-VARIANT_AUTO, VARIANT_PLAIN, VARIANT_LOP3, VARIANT_M4R, VARIANT_TC = 0, 1, 2, 3, 4
-VARIANTS = {"auto": 0, "plain": 1, "lop3": 2, "m4r": 3, "tc": 4}
+VARIANT_AUTO, VARIANT_PLAIN, VARIANT_LOP3, VARIANT_M4R, VARIANT_TC, VARIANT_NTSET = 0, 1, 2, 3, 4, 5
+VARIANTS = {"auto": 0, "plain": 1, "lop3": 2, "m4r": 3, "tc": 4, "ntset": 5}
 LOOPS = {"host": 0, "device": 1, "graph": 2}
 DRIVER_ENGINE, DRIVER_WORKLIST = 0, 1
 
@@ -35,7 +35,9 @@ EXPORTED = (
     "cfpq_matrix_create_ordered", "cfpq_hash_count_rows_noalloc", "cfpq_noalloc_last_error", "cfpq_calibrate",
     "cfpq_last_phase_log", "cfpq_matrices_clear", "cfpq_selector_configure", "cfpq_selector_get_config",
     "cfpq_selector_weight_count", "cfpq_selector_set_weights", "cfpq_selector_get_weights", "cfpq_selector_train",
-    "cfpq_selector_loss_grad", "cfpq_selector_predict", "cfpq_autotune", "cfpq_item_log",
+    "cfpq_selector_loss_grad", "cfpq_selector_predict", "cfpq_autotune", "cfpq_item_log", "cfpq_add_mul_rows",
+    "cfpq_matrix_block_bytes", "cfpq_matrix_export_block", "cfpq_matrix_import_block", "cfpq_matrix_delta",
+    "cfpq_graph_load", "cfpq_edge_list_free",
 )
 
 
@@ -56,7 +58,11 @@ class Rule(ctypes.Structure):
 
 class ClosureOpts(ctypes.Structure):
     _fields_ = [("driver", ctypes.c_int32), ("variant", ctypes.c_int32), ("max_iterations", ctypes.c_int32),
-                ("use_graph", ctypes.c_int32), ("log_products", ctypes.c_int32), ("reserved", ctypes.c_int32 * 3)]
+                ("use_graph", ctypes.c_int32), ("log_products", ctypes.c_int32), ("wait_limit", ctypes.c_int32),
+                ("test_flags", ctypes.c_int32), ("reserved", ctypes.c_int32 * 1)]
+
+
+TEST_STALL_BARRIER = 1
 
 
 class ClosureStats(ctypes.Structure):
@@ -140,6 +146,13 @@ class TrainReport(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class EdgeList(ctypes.Structure):
+    _fields_ = [("from_", ctypes.POINTER(ctypes.c_uint32)), ("label", ctypes.POINTER(ctypes.c_uint32)),
+                ("to", ctypes.POINTER(ctypes.c_uint32)), ("nedges", ctypes.c_size_t),
+                ("nvertices", ctypes.c_uint32), ("nlabels", ctypes.c_uint32),
+                ("labels", ctypes.POINTER(ctypes.c_char_p))]
+
+
 class AutotuneOpts(ctypes.Structure):
     _fields_ = [("sizes", ctypes.POINTER(ctypes.c_uint32)), ("nsizes", ctypes.c_size_t),
                 ("densities", ctypes.POINTER(ctypes.c_float)), ("ndensities", ctypes.c_size_t),
@@ -207,6 +220,13 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "cfpq_selector_loss_grad": ([vp, vp, vp, vp, vp, sz, P(ctypes.c_float), vp], i32),
         "cfpq_selector_predict": ([vp, vp, sz, vp], i32),
         "cfpq_autotune": ([vp, P(AutotuneOpts), P(SelectorConfig), vp], i32),
+        "cfpq_add_mul_rows": ([vp, vp, vp, vp, i32, u32, u32, P(i32)], i32),
+        "cfpq_matrix_block_bytes": ([vp, u32, u32], sz),
+        "cfpq_matrix_export_block": ([vp, vp, u32, u32, vp], i32),
+        "cfpq_matrix_import_block": ([vp, vp, u32, u32, vp], i32),
+        "cfpq_matrix_delta": ([vp, vp, vp, vp], i32),
+        "cfpq_graph_load": ([ctypes.c_char_p, i32, P(P(EdgeList))], i32),
+        "cfpq_edge_list_free": ([P(EdgeList)], None),
     }
     for name, (args, res) in sigs.items():
         f = getattr(lib, name)
@@ -224,6 +244,23 @@ def _check(lib, rc: int) -> None:
 
 def _ptr(a: np.ndarray) -> ctypes.c_void_p:
     return ctypes.c_void_p(a.ctypes.data)
+
+
+def load_graph_file(path: str, threads: int = 0, lib=None):
+    """(src, label, dst, labels, n) of a graph file parsed by the library's
+    parallel loader (cfpq_graph_load); arrays are uint32 copies."""
+    lib = lib or load_library()
+    out = ctypes.POINTER(EdgeList)()
+    _check(lib, lib.cfpq_graph_load(os.fsencode(path), int(threads), ctypes.byref(out)))
+    try:
+        e = out.contents
+        m = int(e.nedges)
+        arrs = [np.ctypeslib.as_array(ptr, shape=(m,)).copy() if m else np.zeros(0, dtype=np.uint32)
+                for ptr in (e.from_, e.label, e.to)]
+        labels = [e.labels[i].decode() for i in range(e.nlabels)]
+        return arrs[0], arrs[1], arrs[2], labels, int(e.nvertices)
+    finally:
+        lib.cfpq_edge_list_free(out)
 
 
 def suggest_order(n: int, src: np.ndarray, label: np.ndarray, dst: np.ndarray, lib=None) -> np.ndarray:
@@ -296,6 +333,20 @@ class Matrix:
             _check(self.ctx.lib, self.ctx.lib.cfpq_matrix_download_rows(self.ctx.handle, self.handle, _ptr(a)))
         return a
 
+    def block_bytes(self, row_begin: int, row_end: int) -> int:
+        """Bytes of the packed row block [row_begin, row_end) (0 if the range is invalid)."""
+        return int(self.ctx.lib.cfpq_matrix_block_bytes(self.handle, int(row_begin), int(row_end)))
+
+    def export_block(self, row_begin: int, row_end: int, dst_ptr: int) -> None:
+        """Copy the packed row block to dst_ptr (device or host address; asynchronous)."""
+        _check(self.ctx.lib, self.ctx.lib.cfpq_matrix_export_block(self.ctx.handle, self.handle, int(row_begin),
+                                                                   int(row_end), ctypes.c_void_p(dst_ptr)))
+
+    def import_block(self, row_begin: int, row_end: int, src_ptr: int) -> None:
+        """Overwrite the rows [row_begin, row_end) from a packed block at src_ptr (asynchronous)."""
+        _check(self.ctx.lib, self.ctx.lib.cfpq_matrix_import_block(self.ctx.handle, self.handle, int(row_begin),
+                                                                   int(row_end), ctypes.c_void_p(src_ptr)))
+
     def tile_stats(self) -> tuple[np.ndarray, np.ndarray]:
         """(occupancy bitmap [T, ceil(T/32)] uint32, tile populations [T, T] uint32)."""
         T = (self.n + 63) // 64
@@ -359,8 +410,21 @@ class Context:
         _check(self.lib, self.lib.cfpq_add_mul(self.handle, c.handle, a.handle, b.handle, v, ctypes.byref(ch)))
         return bool(ch.value)
 
+    def add_mul_rows(self, c: Matrix, a: Matrix, b: Matrix, row_begin: int, row_end: int,
+                     variant: int | str = VARIANT_LOP3) -> bool:
+        """c[rows] |= a[rows] * b for the rows [row_begin, row_end); True if c changed."""
+        v = VARIANTS[variant] if isinstance(variant, str) else int(variant)
+        ch = ctypes.c_int(0)
+        _check(self.lib, self.lib.cfpq_add_mul_rows(self.handle, c.handle, a.handle, b.handle, v, int(row_begin),
+                                                    int(row_end), ctypes.byref(ch)))
+        return bool(ch.value)
+
+    def delta(self, delta: Matrix, cur: Matrix, prev: Matrix) -> None:
+        """delta = cur & ~prev, then prev = cur (asynchronous)."""
+        _check(self.lib, self.lib.cfpq_matrix_delta(self.handle, delta.handle, cur.handle, prev.handle))
+
     @staticmethod
-    def _opts(driver, variant, use_graph, max_iterations, log_products) -> ClosureOpts:
+    def _opts(driver, variant, use_graph, max_iterations, log_products, wait_limit=0, test_flags=0) -> ClosureOpts:
         o = ClosureOpts()
         o.driver = {"engine": DRIVER_ENGINE, "worklist": DRIVER_WORKLIST}.get(driver, driver)
         o.variant = VARIANTS[variant] if isinstance(variant, str) else int(variant)
@@ -369,19 +433,22 @@ class Context:
         o.use_graph = LOOPS[use_graph] if isinstance(use_graph, str) else int(bool(use_graph))
         o.max_iterations = int(max_iterations)
         o.log_products = int(log_products)
+        o.wait_limit = int(wait_limit)
+        o.test_flags = int(test_flags)
         return o
 
     def closure(self, rules: Sequence[tuple[int, int, int]], mats: Sequence[Matrix], driver="engine",
-                variant="auto", use_graph: bool = True, max_iterations: int = 0, log_products: bool = False) -> dict:
+                variant="auto", use_graph: bool = True, max_iterations: int = 0, log_products: bool = False,
+                wait_limit: int = 0, test_flags: int = 0) -> dict:
         # the ctypes arguments of the last call are kept: a prepared query
         # closed again (the serving loop) pays no argument marshalling
         key = (tuple(map(tuple, rules)), tuple(m.handle for m in mats), driver, variant, use_graph,
-               max_iterations, log_products)
+               max_iterations, log_products, wait_limit, test_flags)
         args = self._closure_args if self._closure_args and self._closure_args[0] == key else None
         if args is None:
             rs = (Rule * max(len(rules), 1))(*[Rule(*map(int, r)) for r in rules])
             hs = (ctypes.c_void_p * max(len(mats), 1))(*[m.handle for m in mats])
-            o = self._opts(driver, variant, use_graph, max_iterations, log_products)
+            o = self._opts(driver, variant, use_graph, max_iterations, log_products, wait_limit, test_flags)
             args = self._closure_args = (key, rs, hs, o, ClosureStats())
         _, rs, hs, o, st = args
         _check(self.lib, self.lib.cfpq_closure(self.handle, rs, len(rules), hs, len(mats), ctypes.byref(o),

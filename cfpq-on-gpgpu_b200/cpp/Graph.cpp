@@ -2,22 +2,23 @@
 #include "cfpq/Graph.h"
 
 #include <algorithm>
-#include <fstream>
 #include <stdexcept>
 
 #include "cfpq/Matrix.h"
+#include "cfpq_b200.h"
 
 // Reads "from label to" triples until the first malformed one, like the
-// reference's `while (in >> from >> label >> to)` loop (cfpq-cpp/Graph.cpp:15).
+// reference's `while (in >> from >> label >> to)` loop (cfpq-cpp/Graph.cpp:15),
+// with the library's parallel loader (cfpq_graph_load).
 Graph::Graph(const std::string &graph_filename) {
-    std::ifstream in(graph_filename);
-    if (!in) throw std::runtime_error("cannot open graph file " + graph_filename);
-    unsigned int from = 0, to = 0;
-    std::string label;
-    while (in >> from >> label >> to) {
-        edges.push_back({label, {from, to}});
-        vertices_count = std::max(vertices_count, std::max(from, to) + 1);
-    }
+    cfpq_edge_list *el = nullptr;
+    if (cfpq_graph_load(graph_filename.c_str(), 0, &el) != CFPQ_OK)
+        throw std::runtime_error(std::string("cannot read graph file ") + graph_filename + ": " + cfpq_last_error());
+    std::vector<std::string> names(el->labels, el->labels + el->nlabels);
+    edges.reserve(el->nedges);
+    for (size_t i = 0; i < el->nedges; ++i) edges.push_back({names[el->label[i]], {el->from[i], el->to[i]}});
+    vertices_count = el->nvertices;
+    cfpq_edge_list_free(el);
 }
 
 template <class W, class F>

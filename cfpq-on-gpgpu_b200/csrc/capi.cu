@@ -285,7 +285,8 @@ extern "C" int cfpq_ctx_destroy(cfpq_ctx *ctx) {
                       &ctx->mats_desc, &ctx->edge_buf, &ctx->xbuf, &ctx->phase_log, &ctx->clear_desc,
                       &ctx->d_sel, &ctx->cnts, &ctx->choice, &ctx->tc_ok, &ctx->sel_log, &ctx->mlp_w, &ctx->mlp_x,
                       &ctx->mlp_y, &ctx->mlp_m, &ctx->mlp_grad, &ctx->mlp_m1, &ctx->mlp_v2, &ctx->mlp_loss,
-                      &ctx->mlp_out, &ctx->qranges, &ctx->item_trace})
+                      &ctx->mlp_out, &ctx->qranges, &ctx->item_trace, &ctx->nt_cells, &ctx->nt_mats,
+                      &ctx->nt_rules, &ctx->nt_ctr})
         b->release();
     cudaFree(ctx->d_st);
     cudaFree(ctx->d_flag);
@@ -668,9 +669,13 @@ static int launch_tc_product(cfpq_ctx *ctx, const TcProduct &tp, uint32_t nprods
     return CFPQ_OK;
 }
 
-// Enqueue c |= a * b with a tiled variant (operands must not alias c).
-static int enqueue_tiled_product(cfpq_ctx *ctx, const DevMat &a, const DevMat &b, const DevMat &c, int variant) {
+// Enqueue c |= a * b with a tiled variant (operands must not alias c); with
+// a tile-row range [ti0, ti1) only those output tile-rows (word-level
+// variants; tensor-core products always cover the whole matrix).
+static int enqueue_tiled_product(cfpq_ctx *ctx, const DevMat &a, const DevMat &b, const DevMat &c, int variant,
+                                 uint32_t ti0 = 0, uint32_t ti1 = 0xFFFFFFFFu) {
     const uint32_t T = a.T;
+    ti1 = std::min(ti1, T);
     const int tpb = product_lop3_tiles_per_block();
     MatSlot hs[3];
     memset(hs, 0, sizeof(hs));
@@ -704,7 +709,7 @@ static int enqueue_tiled_product(cfpq_ctx *ctx, const DevMat &a, const DevMat &b
         return launch_tc_product(ctx, TcProduct{0, T, 0, (T + 3) / 4}, 1, cap, nullptr, nullptr, nullptr, nullptr,
                                  ctx->stream);
     }
-    CUDA_TRY(launch_plan(ctx->prods.as<ProdDesc>(), 1, 0, T, ctx->slots.as<MatSlot>(), ctx->d_st,
+    CUDA_TRY(launch_plan(ctx->prods.as<ProdDesc>(), 1, ti0, ti1, ctx->slots.as<MatSlot>(), ctx->d_st,
                          ctx->items.as<uint64_t>(), cap, tpb, nullptr, 0, nullptr, ctx->stream));
     TRY(launch_products(ctx, cap, variant == CFPQ_VARIANT_LOP3, variant == CFPQ_VARIANT_M4R, nullptr, nullptr,
                         ctx->stream));
@@ -724,8 +729,33 @@ static int launch_products(cfpq_ctx *ctx, size_t list_cap, bool lop3, bool m4r, 
     return CFPQ_OK;
 }
 
+static int add_mul_impl(cfpq_ctx *ctx, cfpq_matrix *c, const cfpq_matrix *a, const cfpq_matrix *b, int variant,
+                        int *changed, uint32_t ti0, uint32_t ti1);
+
 extern "C" int cfpq_add_mul(cfpq_ctx *ctx, cfpq_matrix *c, const cfpq_matrix *a, const cfpq_matrix *b, int variant,
                             int *changed) {
+    return add_mul_impl(ctx, c, a, b, variant, changed, 0, 0xFFFFFFFFu);
+}
+
+extern "C" int cfpq_add_mul_rows(cfpq_ctx *ctx, cfpq_matrix *c, const cfpq_matrix *a, const cfpq_matrix *b,
+                                 int variant, uint32_t row_begin, uint32_t row_end, int *changed) {
+    if (!c || !a || !b || !changed) return set_error(CFPQ_ERR_INVALID, "null argument");
+    const uint32_t n = c->d.n;
+    if (row_begin > row_end || row_end > n || row_begin % 64 || (row_end % 64 && row_end != n))
+        return set_error(CFPQ_ERR_INVALID, "row range [%u, %u) of an n = %u matrix: bounds must be multiples of 64 "
+                         "(the end may be n)", row_begin, row_end, n);
+    if (variant == CFPQ_VARIANT_AUTO) variant = CFPQ_VARIANT_LOP3;
+    if (variant != CFPQ_VARIANT_LOP3 && variant != CFPQ_VARIANT_M4R)
+        return set_error(CFPQ_ERR_UNSUPPORTED, "row-range products run the LOP3 or Four Russians variant");
+    if (c->order || a->order || b->order)
+        return set_error(CFPQ_ERR_UNSUPPORTED, "row-range products need matrices without a vertex order");
+    *changed = 0;
+    if (row_begin == row_end) return CFPQ_OK;
+    return add_mul_impl(ctx, c, a, b, variant, changed, row_begin / 64, (row_end + 63) / 64);
+}
+
+static int add_mul_impl(cfpq_ctx *ctx, cfpq_matrix *c, const cfpq_matrix *a, const cfpq_matrix *b, int variant,
+                        int *changed, uint32_t ti0, uint32_t ti1) {
     TRY(use_device(ctx));
     if (!c || !a || !b || !changed) return set_error(CFPQ_ERR_INVALID, "null argument");
     if (a->d.n != c->d.n || b->d.n != c->d.n)
@@ -770,13 +800,81 @@ extern "C" int cfpq_add_mul(cfpq_ctx *ctx, cfpq_matrix *c, const cfpq_matrix *a,
             db = cb->d;
         }
     }
-    TRY(enqueue_tiled_product(ctx, da, db, c->d, variant));
+    TRY(enqueue_tiled_product(ctx, da, db, c->d, variant, ti0, ti1));
     CUDA_TRY(cudaMemcpyAsync(ctx->h_st, ctx->d_st, sizeof(IterState), cudaMemcpyDeviceToHost, ctx->stream));
     CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     if (ca) TRY(pool_give(ctx, ca, true));
     if (cb) TRY(pool_give(ctx, cb, true));
     if (ctx->h_st->error) return set_error(CFPQ_ERR_TIMEOUT, "a bounded device wait gave up (product kernel)");
     *changed = ctx->h_st->changed != 0;
+    return CFPQ_OK;
+}
+
+// ---------------------------------------------------------------------------
+// row blocks (multi-GPU row-block closure)
+
+// Tile-rows [ti0, ti1) of a row range; false if the bounds are invalid.
+static bool block_tiles(const cfpq_matrix *m, uint32_t row_begin, uint32_t row_end, uint32_t *ti0, uint32_t *ti1) {
+    const uint32_t n = m->d.n;
+    if (row_begin > row_end || row_end > n || row_begin % 64 || (row_end % 64 && row_end != n)) return false;
+    *ti0 = row_begin / 64;
+    *ti1 = (row_end + 63) / 64;
+    return true;
+}
+
+extern "C" size_t cfpq_matrix_block_bytes(const cfpq_matrix *m, uint32_t row_begin, uint32_t row_end) {
+    uint32_t ti0, ti1;
+    if (!m || !block_tiles(m, row_begin, row_end, &ti0, &ti1)) return 0;
+    const size_t tr = ti1 - ti0, T = m->d.T;
+    return tr * T * 512 + tr * m->d.ow * 4 + tr * T * 4;
+}
+
+// Copies of the three contiguous ranges of a block (bits, occupancy words,
+// tile populations) between a matrix and a packed buffer (device or host:
+// cudaMemcpyDefault).
+static int block_copy(cfpq_ctx *ctx, cfpq_matrix *m, uint32_t row_begin, uint32_t row_end, void *buf, bool to_buf) {
+    TRY(use_device(ctx));
+    uint32_t ti0, ti1;
+    if (!m || !buf) return set_error(CFPQ_ERR_INVALID, "null argument");
+    if (!block_tiles(m, row_begin, row_end, &ti0, &ti1))
+        return set_error(CFPQ_ERR_INVALID, "row range [%u, %u) of an n = %u matrix: bounds must be multiples of 64 "
+                         "(the end may be n)", row_begin, row_end, m->d.n);
+    if (m->order) return set_error(CFPQ_ERR_UNSUPPORTED, "row blocks of matrices with a vertex order");
+    const size_t tr = ti1 - ti0, T = m->d.T, ow = m->d.ow;
+    if (!tr) return CFPQ_OK;
+    char *p = static_cast<char *>(buf);
+    void *dev[3] = {m->d.bits + (size_t)ti0 * T * 64, m->d.occ + (size_t)ti0 * ow, m->d.nnz + (size_t)ti0 * T};
+    const size_t bytes[3] = {tr * T * 512, tr * ow * 4, tr * T * 4};
+    for (int k = 0; k < 3; ++k) {
+        if (to_buf)
+            CUDA_TRY(cudaMemcpyAsync(p, dev[k], bytes[k], cudaMemcpyDefault, ctx->stream));
+        else
+            CUDA_TRY(cudaMemcpyAsync(dev[k], p, bytes[k], cudaMemcpyDefault, ctx->stream));
+        p += bytes[k];
+    }
+    return CFPQ_OK;
+}
+
+extern "C" int cfpq_matrix_export_block(cfpq_ctx *ctx, const cfpq_matrix *m, uint32_t row_begin, uint32_t row_end,
+                                        void *dst) {
+    return block_copy(ctx, const_cast<cfpq_matrix *>(m), row_begin, row_end, dst, true);
+}
+
+extern "C" int cfpq_matrix_import_block(cfpq_ctx *ctx, cfpq_matrix *m, uint32_t row_begin, uint32_t row_end,
+                                        const void *src) {
+    return block_copy(ctx, m, row_begin, row_end, const_cast<void *>(src), false);
+}
+
+extern "C" int cfpq_matrix_delta(cfpq_ctx *ctx, cfpq_matrix *delta, const cfpq_matrix *cur, cfpq_matrix *prev) {
+    TRY(use_device(ctx));
+    if (!delta || !cur || !prev) return set_error(CFPQ_ERR_INVALID, "null argument");
+    if (delta->d.n != cur->d.n || prev->d.n != cur->d.n)
+        return set_error(CFPQ_ERR_INVALID, "size mismatch (%u, %u, %u)", delta->d.n, cur->d.n, prev->d.n);
+    if (delta == cur || delta == prev || prev == cur)
+        return set_error(CFPQ_ERR_INVALID, "delta, current and previous must be three different matrices");
+    if (delta->order != cur->order || prev->order != cur->order)
+        return set_error(CFPQ_ERR_INVALID, "matrices with different vertex orders");
+    CUDA_TRY(launch_delta_snapshot(delta->d, cur->d, prev->d, ctx->stream));
     return CFPQ_OK;
 }
 
@@ -1398,7 +1496,8 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
                                                  : nullptr,
                                            // one small closure: latency-bound, merge without the read of C
                                            nq == 1 && pl.prods[0].T <= kDirectMergeMaxTiles ? 1 : 0,
-                                           nq > 1 ? 1 : 0, ctx->stream));
+                                           nq > 1 ? 1 : 0, (uint32_t)std::max(o.wait_limit, 0),
+                                           (o.test_flags & CFPQ_TEST_STALL_BARRIER) != 0, ctx->stream));
     } else if (exec) {
         CUDA_TRY(cudaGraphLaunch(exec, ctx->stream));
     } else {
@@ -1524,6 +1623,70 @@ static int run_worklist(cfpq_ctx *ctx, const QueryIn &q, const cfpq_closure_opts
     return CFPQ_OK;
 }
 
+// Variant NTSET: pack the query's matrices into one matrix of nonterminal
+// sets, square it on the device until a pass changes nothing (the changed
+// flag read back after each pass: the number of passes grows with the
+// logarithm of the longest derivation), unpack into the matrices.
+static int run_ntset(cfpq_ctx *ctx, const QueryIn &q, const cfpq_closure_opts &o, cfpq_closure_stats *stats) {
+    TRY(validate_query(q, 0));
+    if (stats) memset(stats, 0, sizeof(*stats));
+    if (q.nmats > 32)
+        return set_error(CFPQ_ERR_UNSUPPORTED, "nonterminal-set variant: %zu nonterminals (at most 32)", q.nmats);
+    const uint32_t nm = (uint32_t)q.nmats;
+    const uint32_t n = nm ? q.mats[0]->d.n : 0;
+    if (n > ntset_max_n(nm))
+        return set_error(CFPQ_ERR_UNSUPPORTED, "nonterminal-set variant: n = %u above %zu for %u nonterminals", n,
+                         ntset_max_n(nm), nm);
+    if (!n || !q.nrules) return CFPQ_OK;
+    const uint32_t stride = q.mats[0]->d.T * 64;
+    const size_t cb = ntset_cell_bytes(nm);
+    TRY(ctx->nt_cells.ensure((size_t)stride * stride * cb));
+    TRY(ctx->nt_mats.ensure(nm * sizeof(DevMat)));
+    TRY(ctx->nt_rules.ensure(q.nrules * 4));
+    TRY(ctx->nt_ctr.ensure(8));
+    std::vector<DevMat> dm(nm);
+    for (uint32_t i = 0; i < nm; ++i) dm[i] = q.mats[i]->d;
+    std::vector<uint8_t> rules(q.nrules * 4);
+    uint32_t ymask = 0;
+    for (size_t r = 0; r < q.nrules; ++r) {
+        rules[4 * r] = (uint8_t)q.rules[r].head;
+        rules[4 * r + 1] = (uint8_t)q.rules[r].body1;
+        rules[4 * r + 2] = (uint8_t)q.rules[r].body2;
+        rules[4 * r + 3] = 0;
+        ymask |= 1u << q.rules[r].body1;
+    }
+    ctx->tables_owner = 0;
+    CUDA_TRY(cudaMemcpyAsync(ctx->nt_mats.p, dm.data(), nm * sizeof(DevMat), cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(cudaMemcpyAsync(ctx->nt_rules.p, rules.data(), rules.size(), cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(cudaEventRecord(ctx->ev0, ctx->stream));
+    CUDA_TRY(launch_ntset_pack(ctx->nt_cells.p, stride, nm, ctx->nt_mats.as<DevMat>(), ctx->num_sms, ctx->stream));
+    uint32_t passes = 0;
+    for (;;) {
+        CUDA_TRY(cudaMemsetAsync(ctx->nt_ctr.p, 0, 8, ctx->stream));
+        CUDA_TRY(launch_ntset_square(ctx->nt_cells.p, n, stride, nm, ctx->nt_rules.p, (uint32_t)q.nrules, ymask,
+                                     ctx->nt_ctr.as<uint32_t>(), ctx->num_sms, ctx->stream));
+        ++passes;
+        CUDA_TRY(cudaMemcpyAsync(ctx->h_flag, ctx->nt_ctr.as<uint32_t>() + 1, 4, cudaMemcpyDeviceToHost, ctx->stream));
+        CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        if (!ctx->h_flag[0]) break;
+        if (o.max_iterations > 0 && passes >= (uint32_t)o.max_iterations) break;
+    }
+    CUDA_TRY(launch_ntset_unpack(ctx->nt_cells.p, stride, nm, ctx->nt_mats.as<DevMat>(), ctx->num_sms, ctx->stream));
+    for (uint32_t i = 0; i < nm; ++i) CUDA_TRY(launch_occ_rebuild(q.mats[i]->d, ctx->stream));
+    CUDA_TRY(cudaEventRecord(ctx->ev1, ctx->stream));
+    CUDA_TRY(cudaEventSynchronize(ctx->ev1));
+    float ms = 0;
+    CUDA_TRY(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    if (stats) {
+        stats->iterations = passes;
+        stats->products = passes;
+        stats->dense_bitops = (uint64_t)passes * n * n * n;
+        stats->device_ms = ms;
+        stats->kernel_launches = 2 + (uint64_t)passes + nm;
+    }
+    return CFPQ_OK;
+}
+
 static cfpq_closure_opts default_opts() {
     cfpq_closure_opts o;
     memset(&o, 0, sizeof(o));
@@ -1540,6 +1703,7 @@ extern "C" int cfpq_closure(cfpq_ctx *ctx, const cfpq_rule *rules, size_t nrules
     QueryIn q{rules, nrules, mats, nmats};
     if (o.driver == CFPQ_DRIVER_WORKLIST) return run_worklist(ctx, q, o, stats);
     if (o.driver != CFPQ_DRIVER_ENGINE) return set_error(CFPQ_ERR_INVALID, "unknown driver %d", o.driver);
+    if (o.variant == CFPQ_VARIANT_NTSET) return run_ntset(ctx, q, o, stats);
     if (o.variant == CFPQ_VARIANT_TC && !ctx->tc_grid)
         return set_error(CFPQ_ERR_UNSUPPORTED, "tensor-core variant unavailable (needs one CTA per SM)");
     if (o.variant != CFPQ_VARIANT_AUTO && o.variant != CFPQ_VARIANT_LOP3 && o.variant != CFPQ_VARIANT_M4R &&

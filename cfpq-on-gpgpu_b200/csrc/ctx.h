@@ -153,6 +153,8 @@ struct cfpq_ctx {
     bool cnts_on = false;          // the current closure keeps buffer counters
     std::vector<cudaEvent_t> tev;  // product timing events (CFPQ_LOG_PRODUCTS)
     DevBuf mlp_w, mlp_x, mlp_y, mlp_m, mlp_grad, mlp_m1, mlp_v2, mlp_loss, mlp_out;
+    // nonterminal-set variant: cell matrix, matrix descriptors, rules, counters
+    DevBuf nt_cells, nt_mats, nt_rules, nt_ctr;
 };
 
 // Selector defaults (before cfpq_autotune or cfpq_selector_configure).

@@ -58,7 +58,7 @@ using tiled::ItemCounters;
 constexpr int kPW = 8;
 constexpr uint32_t kThreads = 32 * kPW;
 
-constexpr uint32_t kBarrierSpinLimit = 1u << 25;  // ~1 s of polling
+constexpr uint32_t kBarrierSpinLimit = 1u << 25;  // default limit of the waits below: ~1 s of polling
 constexpr uint32_t kNoIndex = 0xFFFFFFFFu;
 
 // Word-level products only: output blocks of 16 tiles, at most 128 per
@@ -124,6 +124,9 @@ struct PersistArgs {
     int direct_merge;               // items merge without reading C first (small single closures)
     int prefetch;                   // take the next item index while processing one (batches)
     uint32_t *trace_count;
+    uint32_t spin_limit;            // polls of the item wait and of the grid barrier before they give up
+    uint32_t stall_barrier;         // test hook: the first grid barrier waits for one arrival more than
+                                    // there are CTAs, so that its bounded wait runs out
 };
 
 // Records one processed item (thread 0 of the CTA); sub: the item's
@@ -201,7 +204,8 @@ __device__ __forceinline__ uint32_t active_find(const ActiveList &L, uint32_t u)
 // word until the count reaches `target`; the high half, final by then, comes
 // with the same load.  Returns false when the wait gave up; *flags receives
 // the high half.
-__device__ __forceinline__ bool grid_barrier(unsigned long long *w, uint32_t target, bool abort, uint32_t *flags) {
+__device__ __forceinline__ bool grid_barrier(unsigned long long *w, uint32_t target, bool abort, uint32_t *flags,
+                                             uint32_t spin_limit) {
     __shared__ uint32_t s_ok, s_flags;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -212,7 +216,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned long long *w, uint32_t tar
         unsigned long long v = atom_add_acq_rel_u64(w, 1ull) + 1ull;
         uint32_t i = 0;
         while ((uint32_t)v < target) {
-            if (++i > kBarrierSpinLimit) {
+            if (++i > spin_limit) {
                 ok = 0;
                 break;
             }
@@ -360,7 +364,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_closure_persistent(PersistArgs 
                             break;
                         }
                     }
-                    if (++spins > kBarrierSpinLimit) {
+                    if (++spins > a.spin_limit) {
                         stop = 2;
                         break;
                     }
@@ -402,7 +406,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_closure_persistent(PersistArgs 
             if (a.trace && tid == 0) trace_item(a, item, t, (uint32_t)(v & 1ull), t0, sub);
         }
         uint32_t flags = 0;
-        if (!grid_barrier(&st->pbar[par], ++bar_uses[par] * gridDim.x, timed_out, &flags)) timed_out = true;
+        const uint32_t target = ++bar_uses[par] * gridDim.x + (a.stall_barrier && t == iter0 ? 1u : 0u);
+        if (!grid_barrier(&st->pbar[par], target, timed_out, &flags, a.spin_limit)) timed_out = true;
         if (flags & kBarAbort) timed_out = true;
         if (timed_out) break;
 
@@ -500,7 +505,8 @@ cudaError_t launch_closure_persistent(int has_m4r, int grid, const ProdDesc *pro
                                       uint32_t phase_log_iters, BufCounters *cnts, uint8_t *choice,
                                       const SelectorParams *sel, SelLogRow *sel_log, uint32_t sel_log_iters,
                                       const QueryRange *qr, ItemTrace *trace, uint32_t *trace_count,
-                                      int direct_merge, int prefetch, cudaStream_t s) {
+                                      int direct_merge, int prefetch, uint32_t spin_limit, int stall_barrier,
+                                      cudaStream_t s) {
     PersistArgs a;
     a.prods = prods;
     a.nprods = nprods;
@@ -526,6 +532,8 @@ cudaError_t launch_closure_persistent(int has_m4r, int grid, const ProdDesc *pro
     a.trace_count = trace_count;
     a.direct_merge = direct_merge;
     a.prefetch = prefetch;
+    a.spin_limit = spin_limit ? spin_limit : kBarrierSpinLimit;
+    a.stall_barrier = stall_barrier ? 1u : 0u;
     void *args[] = {&a};
     if (has_m4r)
         return cudaLaunchCooperativeKernel((const void *)k_closure_persistent<true>, dim3(grid), dim3(kThreads), args,

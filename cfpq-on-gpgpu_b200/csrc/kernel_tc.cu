@@ -223,15 +223,25 @@ __global__ void __launch_bounds__(kThreads, 1)
                     bulk_g2s(S.a[s] + g * 4096, xp + tile_offset(T, ti0 + g, tk) * 64, 4096u, &S.ready_bar[s]);
                 bulk_g2s(S.b[s], xq + tile_offset(T, tk, tj0) * 64, nq * 4096u, &S.ready_bar[s]);
             };
+            // k-tiles [0, issued) have their copies issued, [0, ready_seen)
+            // their arrival waited for, [0, committed) their MMAs committed
+            // and [0, mma_seen) those MMAs' completion waited for: every
+            // stage has at most one copy and one commit outstanding
+            uint32_t issued = 0, ready_seen = 0, committed = 0, mma_seen = 0;
+            // a wait that gives up leaves the stage's parity as it was, so the
+            // drain below waits for the same phase again
             auto wait_phase = [&](uint64_t *bars, uint32_t &phases, uint32_t s) {
-                if (!timed_out && !mbar_wait_bounded(&bars[s], (phases >> s) & 1u)) timed_out = true;
-                phases ^= 1u << s;
+                if (!timed_out && mbar_wait_bounded(&bars[s], (phases >> s) & 1u))
+                    phases ^= 1u << s;
+                else
+                    timed_out = true;
             };
-            for (uint32_t e = 0; e < nk && e < kStages; ++e) issue_copies(e);
+            for (uint32_t e = 0; e < nk && e < kStages; ++e, ++issued) issue_copies(e);
             for (uint32_t e = 0; e < nk; ++e) {
                 const uint32_t s = e % kStages;
                 wait_phase(S.ready_bar, ready_phase, s);
                 if (timed_out) break;
+                ++ready_seen;
                 tc_fence_after();
                 const uint32_t abase = smem_addr(S.a[s]), bbase = smem_addr(S.b[s]);
 #pragma unroll
@@ -244,18 +254,31 @@ __global__ void __launch_bounds__(kThreads, 1)
                     }
                 }
                 mma_commit(&S.mma_bar[s]);
+                ++committed;
                 // refill the stage of k-tile e-1 once its MMAs completed (the
                 // tensor pipe keeps working on k-tile e meanwhile)
                 if (e >= 1 && e - 1 + kStages < nk) {
                     const uint32_t s1 = (e - 1) % kStages;
                     wait_phase(S.mma_bar, mma_phase, s1);
                     if (timed_out) break;
+                    ++mma_seen;
                     issue_copies(e - 1 + kStages);
+                    ++issued;
                 }
             }
-            // drain: every commit not waited for above (the last kStages k-tiles)
-            const uint32_t first_unwaited = nk > kStages ? nk - kStages : 0;
-            for (uint32_t e = first_unwaited; e < nk; ++e) wait_phase(S.mma_bar, mma_phase, e % kStages);
+            // drain, also after a wait gave up: every copy whose arrival and
+            // every commit whose completion was not waited for above, so that
+            // no copy or MMA is in flight when the CTA moves on, frees TMEM or
+            // exits (each wait bounded on its own)
+            bool drained = true;
+            auto drain = [&](uint64_t *bars, uint32_t &phases, uint32_t e) {
+                const uint32_t s = e % kStages;
+                if (!mbar_wait_bounded(&bars[s], (phases >> s) & 1u)) drained = false;
+                phases ^= 1u << s;
+            };
+            for (uint32_t e = ready_seen; e < issued; ++e) drain(S.ready_bar, ready_phase, e);
+            for (uint32_t e = mma_seen; e < committed; ++e) drain(S.mma_bar, mma_phase, e);
+            if (!drained) timed_out = true;
         }
         tc_fence_before();
         timed_out = __syncthreads_or(timed_out) != 0;

@@ -471,6 +471,27 @@ cudaError_t launch_tiles_to_rows(const DevMat &m, uint64_t *d_rows, cudaStream_t
     return cudaGetLastError();
 }
 
+// delta = cur & ~prev, then prev = cur (whole matrices, word by word); the
+// tile statistics of delta and prev are rebuilt afterwards.
+__global__ void k_delta_snapshot(DevMat delta, DevMat cur, DevMat prev) {
+    const size_t words = (size_t)cur.T * cur.T * 64;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < words; i += (size_t)gridDim.x * blockDim.x) {
+        const uint64_t c = cur.bits[i];
+        delta.bits[i] = c & ~prev.bits[i];
+        prev.bits[i] = c;
+    }
+}
+
+cudaError_t launch_delta_snapshot(const DevMat &delta, const DevMat &cur, const DevMat &prev, cudaStream_t s) {
+    if (cur.T == 0) return cudaSuccess;
+    if (delta.T != cur.T || prev.T != cur.T) return cudaErrorInvalidValue;
+    k_delta_snapshot<<<capped_grid((size_t)cur.T * cur.T * 64, 256, 1u << 16), 256, 0, s>>>(delta, cur, prev);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    if ((e = launch_occ_rebuild(delta, s)) != cudaSuccess) return e;
+    return launch_occ_rebuild(prev, s);
+}
+
 cudaError_t launch_copy_matrix(const DevMat &dst, const DevMat &src, cudaStream_t s) {
     if (dst.T != src.T) return cudaErrorInvalidValue;
     if (dst.T == 0) return cudaSuccess;

@@ -16,6 +16,22 @@ cudaError_t launch_load_edges(const DevMat *d_mats, const uint32_t *d_from, cons
                               uint32_t nlabels, uint32_t *d_bad, cudaStream_t s);
 cudaError_t launch_set_diag(const DevMat &m, cudaStream_t s);
 cudaError_t launch_occ_rebuild(const DevMat &m, cudaStream_t s);
+// delta = cur & ~prev, then prev = cur; tile statistics of both rebuilt.
+cudaError_t launch_delta_snapshot(const DevMat &delta, const DevMat &cur, const DevMat &prev, cudaStream_t s);
+
+// Nonterminal-set closure (kernel_ntset.cu): one n x n matrix of cells holding
+// sets of nonterminals (1-byte cells for <= 8 nonterminals, 4-byte for <= 32),
+// row stride `stride` cells (n rounded up to 64).  d_rules: nrules records of
+// 4 bytes (head, body1, body2, 0); counters: [0] row counter, [1] changed
+// flag, zero before each squaring pass.
+size_t ntset_cell_bytes(uint32_t nmats);
+size_t ntset_max_n(uint32_t nmats);
+cudaError_t launch_ntset_pack(void *cells, uint32_t stride, uint32_t nmats, const DevMat *d_mats, int num_sms,
+                              cudaStream_t s);
+cudaError_t launch_ntset_unpack(const void *cells, uint32_t stride, uint32_t nmats, const DevMat *d_mats, int num_sms,
+                                cudaStream_t s);
+cudaError_t launch_ntset_square(void *cells, uint32_t n, uint32_t stride, uint32_t nmats, const void *d_rules,
+                                uint32_t nrules, uint32_t ymask, uint32_t *counters, int num_sms, cudaStream_t s);
 cudaError_t launch_rows_to_tiles(const DevMat &m, const uint64_t *d_rows, cudaStream_t s);
 cudaError_t launch_tiles_to_rows(const DevMat &m, uint64_t *d_rows, cudaStream_t s);
 cudaError_t launch_copy_matrix(const DevMat &dst, const DevMat &src, cudaStream_t s);
@@ -100,8 +116,10 @@ cudaError_t launch_closure_persistent(int has_m4r, int grid, const ProdDesc *pro
                                       uint32_t phase_log_iters, BufCounters *cnts, uint8_t *choice,
                                       const SelectorParams *sel, SelLogRow *sel_log, uint32_t sel_log_iters,
                                       const QueryRange *qr, ItemTrace *trace, uint32_t *trace_count,
-                                      int direct_merge, int prefetch, cudaStream_t s);
-// (trace non-null: one ItemTrace per processed item, counted in *trace_count)
+                                      int direct_merge, int prefetch, uint32_t spin_limit, int stall_barrier,
+                                      cudaStream_t s);
+// (spin_limit 0: the default of about a second of polling per wait;
+// trace non-null: one ItemTrace per processed item, counted in *trace_count)
 // (direct_merge: result words go to their atomic OR without reading C first)
 // (prefetch: a CTA takes its next item index while it processes one)
 // (qr non-null: per-query ranges of a batch of 2..kMaxActiveQueries queries,

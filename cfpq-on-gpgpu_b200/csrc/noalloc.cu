@@ -16,7 +16,11 @@
 // exits.  All calls on one device share it and it keeps the last call's
 // contents: every call rebuilds the power tables and clears the accumulators
 // before use, and calls whose work overlaps on the GPU (for example on two
-// streams without ordering) race on the array and give wrong results.
+// streams without ordering) race on the array and give wrong results.  The
+// array's address is looked up per device and CUDA context: a first call in
+// a new context (after cudaDeviceReset, or under a caller's own driver
+// context) repeats the set-up, so it too should come before any stream
+// capture.
 #include <cstdio>
 #include <mutex>
 
@@ -111,7 +115,16 @@ __global__ void k_noalloc_finish(void *scratch, unsigned long long *out) {
 }
 
 std::mutex g_setup_mutex;
-void *g_scratch_ptr[kMaxDevices] = {};
+
+// The array's device address belongs to the CUDA context that loaded the
+// module: it is looked up again whenever the current context of the device
+// is another one (a caller's own driver context, or the primary context
+// created anew after cudaDeviceReset), identified by its unique context id.
+struct ScratchAddr {
+    void *ptr;
+    unsigned long long ctx_id;
+};
+ScratchAddr g_scratch[kMaxDevices] = {};
 
 thread_local char g_noalloc_error[256];
 
@@ -123,18 +136,51 @@ int fail(int code, const char *msg, cudaError_t e = cudaSuccess) {
     return code;
 }
 
+// Unique id of the current CUDA context (the driver's cuCtxGetCurrent and
+// cuCtxGetId, reached through the runtime's entry-point query so that the
+// library needs no link-time dependency on the driver library); 0 when the
+// driver does not provide it, in which case the address is looked up on
+// every call.
+unsigned long long current_context_id() {
+    using GetCurrent = int (*)(void **);
+    using GetId = int (*)(void *, unsigned long long *);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static bool resolved = false;
+    if (!resolved) {
+        void *f = nullptr, *g = nullptr;
+        cudaDriverEntryPointQueryResult r1, r2;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &r1) == cudaSuccess &&
+            r1 == cudaDriverEntryPointSuccess &&
+            cudaGetDriverEntryPoint("cuCtxGetId", &g, cudaEnableDefault, &r2) == cudaSuccess &&
+            r2 == cudaDriverEntryPointSuccess) {
+            get_current = reinterpret_cast<GetCurrent>(f);
+            get_id = reinterpret_cast<GetId>(g);
+        }
+        resolved = true;
+    }
+    void *c = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || !get_id || get_current(&c) != 0 || !c || get_id(c, &id) != 0) return 0;
+    return id;
+}
+
 // Device address of the scratch array on `device` (which must be current).
-// Looked up once per device with cudaGetSymbolAddress; host code never uses
-// the array's name as a device address.
+// Looked up with cudaGetSymbolAddress at set-up, once per device and context;
+// host code never uses the array's name as a device address.
 int scratch_for(int device, void **out) {
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_ptr[device]) {
+    // 0 before the runtime made any context current: looked up again next call
+    const unsigned long long id = current_context_id();
+    ScratchAddr &sa = g_scratch[device];
+    if (!sa.ptr || id == 0 || sa.ctx_id != id) {
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || !p) return fail(CFPQ_ERR_CUDA, "cudaGetSymbolAddress(g_noalloc_scratch)", e);
-        g_scratch_ptr[device] = p;
+        sa.ptr = p;
+        sa.ctx_id = id;
     }
-    *out = g_scratch_ptr[device];
+    *out = sa.ptr;
     return CFPQ_OK;
 }
 

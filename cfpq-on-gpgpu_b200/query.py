@@ -75,28 +75,10 @@ class EdgeGraph:
         return int(self.src.size)
 
     @classmethod
-    def from_file(cls, path: str) -> "EdgeGraph":
-        src, dst, lab = [], [], []
-        lid: dict[str, int] = {}
-        with open(path) as f:
-            toks = f.read().split()
-        for i in range(0, len(toks) - 2, 3):
-            try:
-                a, b = int(toks[i]), int(toks[i + 2])
-            except ValueError:
-                break
-            if a < 0 or b < 0:
-                break
-            src.append(a)
-            dst.append(b)
-            lab.append(lid.setdefault(toks[i + 1], len(lid)))
-        labels = [None] * len(lid)
-        for k, v in lid.items():
-            labels[v] = k
-        s = np.asarray(src, dtype=np.uint32)
-        d = np.asarray(dst, dtype=np.uint32)
-        n = int(max(s.max(initial=0), d.max(initial=0)) + 1) if s.size else 0
-        return cls(s, np.asarray(lab, dtype=np.uint32), d, labels, n)
+    def from_file(cls, path: str, threads: int = 0) -> "EdgeGraph":
+        """Parse with the library's parallel loader (cfpq_graph_load)."""
+        src, lab, dst, labels, n = capi.load_graph_file(path, threads)
+        return cls(src, lab, dst, labels, n)
 
     def write(self, path: str) -> None:
         lab = np.asarray(self.labels, dtype=object)[self.label] if self.nedges else []

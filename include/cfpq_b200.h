@@ -50,7 +50,13 @@ typedef enum cfpq_variant {
     CFPQ_VARIANT_PLAIN = 1,  /* dense word-level kernel, no tiles, no skipping */
     CFPQ_VARIANT_LOP3 = 2,   /* tiled word-level AND/OR kernel with bulk-copy staged panels */
     CFPQ_VARIANT_M4R = 3,    /* Four Russians with 8-bit lookup tables in shared memory */
-    CFPQ_VARIANT_TC = 4      /* exact tensor-core product (0/1 operands, int accumulators > 0) */
+    CFPQ_VARIANT_TC = 4,     /* exact tensor-core product (0/1 operands, int accumulators > 0) */
+    CFPQ_VARIANT_NTSET = 5   /* cfpq_closure only: the whole closure as one n x n matrix of
+                                nonterminal sets squared until it stops changing (the
+                                formulation of the reference's single-matrix CUTLASS backend,
+                                cuda/cutlass/CutlassMatrix.cu:290-316, rule encoding
+                                cfpq-cpp/Grammar.cpp:63-75); at most 32 nonterminals (one
+                                byte per cell up to 8) and n <= 16384 (<= 8192 above 8) */
 } cfpq_variant;
 
 /* Closure drivers. */
@@ -88,8 +94,19 @@ typedef struct cfpq_closure_opts {
                                 2 (CFPQ_LOOP_GRAPH)  one CUDA graph with a device-side
                                    while condition, one node per kernel */
     int32_t log_products;    /* CFPQ_LOG_* flags (cfpq_last_kernel_profile, cfpq_product_log) */
-    int32_t reserved[3];
+    int32_t wait_limit;      /* persistent kernel: polls of each bounded device wait (work-item
+                                wait, grid barrier) before it gives up and the closure returns
+                                CFPQ_ERR_TIMEOUT; 0 = default (about one second) */
+    int32_t test_flags;      /* CFPQ_TEST_* hooks for testing the failure paths; 0 in normal use */
+    int32_t reserved[1];
 } cfpq_closure_opts;
+
+/* Test hook: the persistent kernel's first grid barrier waits for one arrival
+ * more than there are CTAs, so its bounded wait runs out.  The closure then
+ * returns CFPQ_ERR_TIMEOUT with the matrices holding a subset of the fixpoint
+ * (every bit set is a true result) and the context stays usable.  Nothing
+ * faults: the wait is a bounded poll. */
+#define CFPQ_TEST_STALL_BARRIER 1
 
 typedef struct cfpq_closure_stats {
     uint32_t iterations;        /* ENGINE: device iterations run; WORKLIST: 0 */
@@ -172,6 +189,32 @@ int cfpq_order_destroy(cfpq_ctx *ctx, cfpq_order *order);
 int cfpq_order_suggest(uint32_t n, const uint32_t *from, const uint32_t *label, const uint32_t *to,
                        size_t nedges, uint32_t *perm_out);
 
+/* ---- graph files ----------------------------------------------------------- */
+
+/* Edge list of a graph file in the reference's format: "from label to"
+ * triples separated by whitespace, read until the first triple whose vertex
+ * tokens are not decimal numbers of at most 4294967295 (the stream extraction
+ * loop of cfpq-cpp/Graph.cpp:15 stops there too; a vertex token with a sign
+ * or with trailing non-digits, such as "-2" or "2.0", ends the list here,
+ * while the stream would still take its leading part); nvertices = max id + 1.
+ * Labels are numbered by first appearance in the file. */
+typedef struct cfpq_edge_list {
+    uint32_t *from;       /* nedges source vertices */
+    uint32_t *label;      /* nedges label ids, indices into labels */
+    uint32_t *to;         /* nedges target vertices */
+    size_t nedges;
+    uint32_t nvertices;
+    uint32_t nlabels;
+    const char **labels;  /* nlabels NUL-terminated names (then a NULL) */
+} cfpq_edge_list;
+/* Parses a graph file with `threads` host threads (0 = all cores): the file is
+ * cut at line starts and the chunks parsed in parallel (a layout with triples
+ * across lines falls back to one sequential pass).  Replaces the iostream
+ * loop of Graph::Graph (cfpq-cpp/Graph.cpp:11-20).  *out is freed with
+ * cfpq_edge_list_free.  No GPU needed. */
+int cfpq_graph_load(const char *path, int threads, cfpq_edge_list **out);
+void cfpq_edge_list_free(cfpq_edge_list *e);
+
 /* ---- matrices ----------------------------------------------------------- */
 
 /* Allocates a zero n x n matrix on the device.  Replaces
@@ -249,8 +292,9 @@ int cfpq_matrix_count(cfpq_ctx *ctx, const cfpq_matrix *m, uint64_t *count);
  * that receives (hash, count).  Asynchronous on `stream` (a cudaStream_t, NULL
  * = the default stream) of `device`.  Scratch memory is a fixed device array
  * in the library sized for n <= CFPQ_NOALLOC_MAX_N; larger n is rejected with
- * CFPQ_ERR_UNSUPPORTED.  The first call on a device looks that array up, so
- * make it before any stream capture.  All calls on a device share the array:
+ * CFPQ_ERR_UNSUPPORTED.  The first call on a device looks that array up (and
+ * so does the first call in another CUDA context of the device, e.g. after
+ * cudaDeviceReset), so make it before any stream capture.  All calls on a device share the array:
  * calls that overlap on the GPU race and must be ordered by the caller.
  * Errors are described by cfpq_noalloc_last_error(). */
 #define CFPQ_NOALLOC_MAX_N 65536u
@@ -277,6 +321,37 @@ int cfpq_hash_count_many(cfpq_ctx *ctx, cfpq_matrix *const *mats, size_t nmats, 
  * Synchronous: returns after the product is done and the flag is read. */
 int cfpq_add_mul(cfpq_ctx *ctx, cfpq_matrix *c, const cfpq_matrix *a, const cfpq_matrix *b,
                  int variant, int *changed);
+
+/* ---- row blocks: the multi-GPU row-block closure ---------------------------
+ * A single large query can be closed by several processes (one per GPU), each
+ * owning a contiguous block of rows of every matrix and holding full copies of
+ * all matrices: per iteration every rank runs the products of its rows, and
+ * the changed row blocks are exchanged (all-gather) between iterations.  The
+ * exchange itself is the caller's (the package's rowblock.py uses
+ * torch.distributed).  Row ranges [row_begin, row_end) start and end on
+ * multiples of 64 (the end may be n).  None of these has a reference
+ * counterpart: the reference runs one query on one GPU per process
+ * (cuda/naive-gpu/main.cpp:9-10). */
+
+/* c[rows] |= a[rows] * b over the Boolean semiring for the rows in
+ * [row_begin, row_end) only (the other rows of c are untouched); *changed = 1
+ * if a bit of c changed.  Variant LOP3, M4R or AUTO (= LOP3); matrices without
+ * a vertex order.  Aliasing as in cfpq_add_mul.  Synchronous. */
+int cfpq_add_mul_rows(cfpq_ctx *ctx, cfpq_matrix *c, const cfpq_matrix *a, const cfpq_matrix *b, int variant,
+                      uint32_t row_begin, uint32_t row_end, int *changed);
+/* Bytes of the packed form of a row block: the 64x64-bit tiles of its
+ * tile-rows, then their occupancy words, then their tile populations (0 for
+ * an invalid range). */
+size_t cfpq_matrix_block_bytes(const cfpq_matrix *m, uint32_t row_begin, uint32_t row_end);
+/* Copies a row block into (export) or out of (import: overwrites those rows)
+ * a packed buffer of cfpq_matrix_block_bytes bytes, device or host memory.
+ * Asynchronous on the context's stream. */
+int cfpq_matrix_export_block(cfpq_ctx *ctx, const cfpq_matrix *m, uint32_t row_begin, uint32_t row_end, void *dst);
+int cfpq_matrix_import_block(cfpq_ctx *ctx, cfpq_matrix *m, uint32_t row_begin, uint32_t row_end, const void *src);
+/* delta = cur AND NOT prev, then prev = cur (three different matrices of the
+ * same n): the bits an iteration added, for semi-naive products.
+ * Asynchronous. */
+int cfpq_matrix_delta(cfpq_ctx *ctx, cfpq_matrix *delta, const cfpq_matrix *cur, cfpq_matrix *prev);
 
 /* Runs the whole fixpoint "mats[head] |= mats[body1] * mats[body2] for every
  * rule until nothing changes" on the device.  Replaces the worklist loop of

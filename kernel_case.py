@@ -1,10 +1,10 @@
 #!/usr/bin/env python
 """Single-kernel cases for profiling the product variants in isolation.
 
-  python cfpq-on-gpgpu_b200/kernel_case.py dense --variant tc --n 8192 --density 0.3 --reps 3
-  python cfpq-on-gpgpu_b200/kernel_case.py closure --n 8192 --reps 3
-  python cfpq-on-gpgpu_b200/kernel_case.py batch --queries 64 --reps 2
-  python cfpq-on-gpgpu_b200/kernel_case.py chain --n 16384 --reps 1
+  python kernel_case.py dense --variant tc --n 8192 --density 0.3 --reps 3
+  python kernel_case.py closure --n 8192 --reps 3
+  python kernel_case.py batch --queries 64 --reps 2
+  python kernel_case.py chain --n 16384 --reps 1
 
 `dense` runs C |= A * B on two seeded random n x n bit matrices (every tile
 populated) `reps` times with one variant; `closure` runs the same-generation
@@ -24,7 +24,7 @@ import json
 import os
 import sys
 
-sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
 
 
 def main():

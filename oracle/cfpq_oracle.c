@@ -39,6 +39,7 @@
 #include "m4ri_restated.h"
 
 #include <stdio.h>
+#include <omp.h>
 #include <stdlib.h>
 #include <string.h>
 #include <ctype.h>
@@ -252,6 +253,34 @@ int orc_add_mul(int n, uint64_t *c, const uint64_t *a, const uint64_t *b, int me
     }
     free(t);
     return changed;
+}
+
+/* Rows rows[0..nrows-1] of C | A*B (the same semantics as orc_add_mul,
+ * restricted to a sample of rows): out receives nrows rows of wpr words, row
+ * i = C[rows[i]] | OR of B[k] over the set bits k of A[rows[i]].  For checking
+ * products whose full CPU evaluation would take hours (n = 65536); rows run
+ * in parallel. */
+void orc_add_mul_rows(int n, uint64_t *out, const uint64_t *c, const uint64_t *a, const uint64_t *b,
+                      const uint32_t *rows, int nrows, int threads) {
+    const int wpr = (n + 63) / 64;
+    if (threads > 0) omp_set_num_threads(threads);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int i = 0; i < nrows; ++i) {
+        const size_t r = rows[i];
+        uint64_t *acc = out + (size_t)i * wpr;
+        memcpy(acc, c + r * wpr, (size_t)wpr * sizeof(uint64_t));
+        const uint64_t *ar = a + r * wpr;
+        for (int w = 0; w < wpr; ++w) {
+            uint64_t bits = ar[w];
+            while (bits) {
+                const int k = w * 64 + __builtin_ctzll(bits);
+                bits &= bits - 1;
+                if (k >= n) break;
+                const uint64_t *br = b + (size_t)k * wpr;
+                for (int j = 0; j < wpr; ++j) acc[j] |= br[j];
+            }
+        }
+    }
 }
 
 /* The reference's per-bit loop (Grammar.cpp:84-97). */

@@ -48,6 +48,7 @@ def lib() -> ctypes.CDLL:
         L.orc_write_results.argtypes, L.orc_write_results.restype = [vp, ctypes.c_char_p], i32
         L.orc_add_mul.argtypes, L.orc_add_mul.restype = [i32, vp, vp, vp, i32, i32], i32
         L.orc_hash_count.argtypes, L.orc_hash_count.restype = [i32, vp, P(ctypes.c_uint64), P(ctypes.c_uint64)], None
+        L.orc_add_mul_rows.argtypes, L.orc_add_mul_rows.restype = [i32, vp, vp, vp, vp, vp, i32, i32], None
         _lib = L
     return _lib
 
@@ -61,6 +62,20 @@ def add_mul(c: np.ndarray, a: np.ndarray, b: np.ndarray, n: int, method: int = N
     for x in (a, b, c):
         assert x.dtype == np.uint64 and x.flags["C_CONTIGUOUS"] and x.size == n * ((n + 63) // 64)
     return bool(lib().orc_add_mul(n, _p(c), _p(a), _p(b), method, threads))
+
+
+def add_mul_rows(c: np.ndarray, a: np.ndarray, b: np.ndarray, n: int, rows: np.ndarray,
+                 threads: int = 0) -> np.ndarray:
+    """Rows `rows` of c | a * b (row-bit arrays, n x ceil(n/64) uint64): the
+    product checked on a row sample where the whole product is too costly."""
+    wpr = (n + 63) // 64
+    for x in (a, b, c):
+        assert x.dtype == np.uint64 and x.flags["C_CONTIGUOUS"] and x.size == n * wpr
+    r = np.ascontiguousarray(rows, dtype=np.uint32)
+    assert r.size == 0 or int(r.max()) < n
+    out = np.zeros((r.size, wpr), dtype=np.uint64)
+    lib().orc_add_mul_rows(n, _p(out), _p(c), _p(a), _p(b), _p(r), int(r.size), threads)
+    return out
 
 
 def hash_count(m: np.ndarray, n: int) -> tuple[int, int]:

@@ -73,27 +73,49 @@ def test_order_suggest_rejects_out_of_range(pkg):
     assert rc == pkg.capi.ERR_INVALID
 
 
+# ctypes mirror -> C struct of include/cfpq_b200.h
+CTYPES_STRUCTS = {
+    "Calibration": "cfpq_calibration", "Rule": "cfpq_rule", "ClosureOpts": "cfpq_closure_opts",
+    "ClosureStats": "cfpq_closure_stats", "KernelProfile": "cfpq_kernel_profile", "Query": "cfpq_query",
+    "ProductRecord": "cfpq_product_record", "SelectorConfig": "cfpq_selector_config", "TrainOpts": "cfpq_train_opts",
+    "TrainReport": "cfpq_train_report", "AutotuneOpts": "cfpq_autotune_opts",
+}
+
+
 def test_python_record_layouts_match_the_header(pkg, tmp_path):
     """The numpy / ctypes views of the C records have the header's sizes and
     field offsets (compiled with the host C compiler, no GPU)."""
     import subprocess
 
+    capi = pkg.capi
+    lines = []
+    for py, c in CTYPES_STRUCTS.items():
+        cls = getattr(capi, py)
+        lines.append(f'  printf("{py} %zu\\n", sizeof({c}));')
+        for name, _ in cls._fields_:
+            lines.append(f'  printf("{py}.{name} %zu\\n", offsetof({c}, {name}));')
+    for name in ITEM_FIELDS:
+        lines.append(f'  printf("item.{name} %zu\\n", offsetof(cfpq_item_record, {name}));')
+    lines.append('  printf("item %zu\\n", sizeof(cfpq_item_record));')
     src = tmp_path / "sizes.c"
-    src.write_text(
-        '#include <stddef.h>\n#include <stdio.h>\n#include "cfpq_b200.h"\n'
-        "int main(void) {\n"
-        '  printf("%zu %zu %zu %zu %zu %zu\\n", sizeof(cfpq_item_record), offsetof(cfpq_item_record, start_ns),\n'
-        "         offsetof(cfpq_item_record, klist_ns), sizeof(cfpq_product_record),\n"
-        "         offsetof(cfpq_product_record, features), offsetof(cfpq_product_record, usec));\n"
-        "  return 0;\n}\n")
+    src.write_text('#include <stddef.h>\n#include <stdio.h>\n#include "cfpq_b200.h"\nint main(void) {\n'
+                   + "\n".join(lines) + "\n  return 0;\n}\n")
     exe = tmp_path / "sizes"
     subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), "-o", str(exe), str(src)], check=True)
-    item, item_start, item_klist, prod, prod_feat, prod_usec = map(int, subprocess.run(
-        [str(exe)], check=True, capture_output=True, text=True).stdout.split())
-    capi = pkg.capi
-    assert capi.ITEM_RECORD_DTYPE.itemsize == item
-    assert capi.ITEM_RECORD_DTYPE.fields["start_ns"][1] == item_start
-    assert capi.ITEM_RECORD_DTYPE.fields["klist_ns"][1] == item_klist
-    assert capi.PRODUCT_RECORD_DTYPE.itemsize == prod == ctypes.sizeof(capi.ProductRecord)
-    assert capi.PRODUCT_RECORD_DTYPE.fields["features"][1] == prod_feat
-    assert capi.PRODUCT_RECORD_DTYPE.fields["usec"][1] == prod_usec
+    got = dict(ln.split() for ln in subprocess.run([str(exe)], check=True, capture_output=True,
+                                                   text=True).stdout.splitlines())
+    for py in CTYPES_STRUCTS:
+        cls = getattr(capi, py)
+        assert ctypes.sizeof(cls) == int(got[py]), py
+        for name, _ in cls._fields_:
+            assert getattr(cls, name).offset == int(got[f"{py}.{name}"]), f"{py}.{name}"
+    assert capi.ITEM_RECORD_DTYPE.itemsize == int(got["item"])
+    for name in ITEM_FIELDS:
+        assert capi.ITEM_RECORD_DTYPE.fields[name][1] == int(got[f"item.{name}"]), name
+    assert capi.PRODUCT_RECORD_DTYPE.itemsize == ctypes.sizeof(capi.ProductRecord)
+    for name, _ in capi.ProductRecord._fields_:
+        assert capi.PRODUCT_RECORD_DTYPE.fields[name][1] == capi.ProductRecord.__dict__[name].offset, name
+
+
+ITEM_FIELDS = ("item", "iteration", "cta", "list", "start_ns", "end_ns", "klist_ns", "staged_ns", "computed_ns",
+               "gate_ns")

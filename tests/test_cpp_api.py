@@ -18,11 +18,16 @@ def cpu_backend(tmp_path_factory):
     cxx = shutil.which("g++")
     if cxx is None:
         pytest.skip("no C++ compiler")
+    lib = os.path.join(PKG, "lib", "libcfpq_b200.so")
+    if not os.path.exists(lib):
+        pytest.skip("library not built")
     exe = str(tmp_path_factory.mktemp("cpp") / "cpu_backend_main")
+    # the graph loader is the library's (cfpq_graph_load, host code: no GPU needed)
     subprocess.run([cxx, "-O2", "-std=c++17", "-Wall", "-I", os.path.join(PKG, "cpp"),
                     "-I", os.path.join(ROOT, "include"), "-o", exe,
                     os.path.join(ROOT, "tests", "cpp", "cpu_backend_main.cpp"),
-                    os.path.join(PKG, "cpp", "Grammar.cpp"), os.path.join(PKG, "cpp", "Graph.cpp")], check=True)
+                    os.path.join(PKG, "cpp", "Grammar.cpp"), os.path.join(PKG, "cpp", "Graph.cpp"),
+                    "-L", os.path.dirname(lib), "-lcfpq_b200", f"-Wl,-rpath,{os.path.dirname(lib)}"], check=True)
     return exe
 
 
