@@ -52,8 +52,9 @@ def parse_args():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-profile", action="store_true")
-    ap.add_argument("--selector-eval", action="store_true",
-                    help="train the cost model on logged product timings and report its regret (about a minute)")
+    ap.add_argument("--no-selector-eval", action="store_true",
+                    help="skip the learned-selector evaluation (trains the cost model on logged product timings "
+                         "and reports its regret and batch closure time on fresh queries; about a minute)")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the plain-GPU-form, reference-GPU, brackets and 512-query batch measurements")
     ap.add_argument("--no-chain", action="store_true",
@@ -297,7 +298,10 @@ def plain_gpu_form(ctx, q, grammar, torch, stream, reps=2) -> dict:
 
 def reference_gpu_forms(wl, lines_expected) -> dict:
     """The reference's own GPU executables (naiveGPU, m4riGPU built from its
-    sources for sm_100a): algorithm time printed by their main."""
+    sources for sm_100a) and this repository's drop-in executable b200GPU
+    (cfpq-cpp Grammar/Graph driver with the B200Matrix backend, the plugin
+    boundary) on the same files: "total algo" milliseconds printed by each
+    main (the harness contract), median of 3 runs for b200GPU."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
 
@@ -305,6 +309,17 @@ def reference_gpu_forms(wl, lines_expected) -> dict:
     with tempfile.TemporaryDirectory() as d:
         gp, rp = os.path.join(d, "grammar.txt"), os.path.join(d, "graph.txt")
         wl.write(gp, rp)
+        ours = os.path.join(ROOT, "cfpq-on-gpgpu_b200", "bin", "b200GPU")
+        if os.path.exists(ours):
+            runs = []
+            for _ in range(3):
+                answer, (total, algo) = oracle.run_executable(ours, gp, rp, timeout=600)
+                runs.append((total, algo, answer == lines_expected))
+            runs.sort()
+            total, algo, _ = runs[1]
+            out["b200GPU"] = {"algo_ms": algo, "total_ms": total, "matches_ours": all(r[2] for r in runs),
+                              "note": "this repository's drop-in executable: the reference's harness contract "
+                                      "(process start, file parsing, device init and upload included in total)"}
         for name in ("naiveGPU", "m4riGPU"):
             exe = oracle.ref_executable(name)
             if exe is None:
@@ -579,20 +594,25 @@ def selector_eval(pkg, ctx, torch, stream, n_train=32, n_eval=32) -> dict:
         # batch closure time of the fresh queries with each selector (the
         # default tensor-core size limit, n >= 16384, keeps these terms on the
         # word-level kernels: the choice is LOP3 or M4R per term and iteration)
-        times = {}
+        # in the persistent loop (8-warp kernel, the default) and in the CUDA-
+        # graph loop (the plan + product kernels whose timings the model was
+        # trained on)
+        times, times_graph = {}, {}
         for label, kw in (("fixed_lop3", dict(mode="fixed")),
                           ("heuristic", dict(mode="heuristic", min_tiles=1, tc_min_tiles=256)),
                           ("mlp", dict(mode="mlp", min_tiles=1, tc_min_tiles=256, conf_margin=0.0))):
             ctx.selector_configure(**kw)
-            ms = []
-            for _ in range(3):
-                for q in ev_qs:
-                    q.load()
-                ctx.synchronize()
-                ms.append(_event_ms(torch, stream, lambda: ctx.closure_batch(
-                    [(q.grammar.rules, q.mats) for q in ev_qs]))[0])
-            times[label] = min(ms)
+            for loop, dest in (("device", times), ("graph", times_graph)):
+                ms = []
+                for _ in range(3):
+                    for q in ev_qs:
+                        q.load()
+                    ctx.synchronize()
+                    ms.append(_event_ms(torch, stream, lambda: ctx.closure_batch(
+                        [(q.grammar.rules, q.mats) for q in ev_qs], use_graph=loop))[0])
+                dest[label] = min(ms)
         out["batch_closure_ms"] = times
+        out["batch_closure_ms_graph_loop"] = times_graph
     finally:
         for q in ev_qs:
             q.close()
@@ -683,8 +703,8 @@ def ours_arm(args, world, rank, local):
         ctx.load_edges(q.mats, h_src, h_lab, h_dst, q.off, q.lm)
         for e in grammar.epsilon:
             q.mats[e].set_diagonal()
-        st = ctx.closure(grammar.rules, q.mats, use_graph=not args.no_graph)
-        return st, ctx.hash_count_many(q.mats)
+        # closure and result lines with one synchronisation (cfpq_closure_hash)
+        return ctx.closure_hash(grammar.rules, q.mats, use_graph=not args.no_graph)
 
     def timed(fn, k):
         times, last = [], None
@@ -826,7 +846,7 @@ def ours_arm(args, world, rank, local):
             out["closure"]["parity_vs_cpu"] = answer == {k: tuple(v) for k, v in zip(grammar.nonterminals, lines)}
         if batch is not None:
             out["batch_512"] = batch
-        if args.selector_eval:
+        if world == 1 and not args.no_extras and not args.no_selector_eval:
             out["selector_eval"] = selector_eval(pkg, ctx, torch, stream)
         if world == 1 and not args.no_extras and not args.no_chain:
             out["chain_65536"] = chain_bench(pkg, ctx, torch, stream)

@@ -37,7 +37,7 @@ EXPORTED = (
     "cfpq_selector_weight_count", "cfpq_selector_set_weights", "cfpq_selector_get_weights", "cfpq_selector_train",
     "cfpq_selector_loss_grad", "cfpq_selector_predict", "cfpq_autotune", "cfpq_item_log", "cfpq_add_mul_rows",
     "cfpq_matrix_block_bytes", "cfpq_matrix_export_block", "cfpq_matrix_import_block", "cfpq_matrix_delta",
-    "cfpq_graph_load", "cfpq_edge_list_free",
+    "cfpq_graph_load", "cfpq_edge_list_free", "cfpq_closure_hash",
 )
 
 
@@ -226,6 +226,7 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "cfpq_matrix_import_block": ([vp, vp, u32, u32, vp], i32),
         "cfpq_matrix_delta": ([vp, vp, vp, vp], i32),
         "cfpq_graph_load": ([ctypes.c_char_p, i32, P(P(EdgeList))], i32),
+        "cfpq_closure_hash": ([vp, P(Rule), sz, P(vp), sz, P(ClosureOpts), P(ClosureStats), P(u64), P(u64)], i32),
         "cfpq_edge_list_free": ([P(EdgeList)], None),
     }
     for name, (args, res) in sigs.items():
@@ -454,6 +455,25 @@ class Context:
         _check(self.lib, self.lib.cfpq_closure(self.handle, rs, len(rules), hs, len(mats), ctypes.byref(o),
                                                ctypes.byref(st)))
         return st.as_dict()
+
+    def closure_hash(self, rules: Sequence[tuple[int, int, int]], mats: Sequence[Matrix], variant="auto",
+                     use_graph: bool = True) -> tuple[dict, list[tuple[int, int]]]:
+        """Closure, then the result line (hash, count) of every matrix, with one
+        synchronisation (cfpq_closure_hash).  The ctypes arguments of the last
+        call are kept, like closure()."""
+        key = (tuple(map(tuple, rules)), tuple(m.handle for m in mats), variant, use_graph)
+        args = self._hash_args if getattr(self, "_hash_args", None) and self._hash_args[0] == key else None
+        if args is None:
+            rs = (Rule * max(len(rules), 1))(*[Rule(*map(int, r)) for r in rules])
+            hs = (ctypes.c_void_p * max(len(mats), 1))(*[m.handle for m in mats])
+            o = self._opts("engine", variant, use_graph, 0, 0)
+            hh = (ctypes.c_uint64 * max(len(mats), 1))()
+            cc = (ctypes.c_uint64 * max(len(mats), 1))()
+            args = self._hash_args = (key, rs, hs, o, ClosureStats(), hh, cc)
+        _, rs, hs, o, st, hh, cc = args
+        _check(self.lib, self.lib.cfpq_closure_hash(self.handle, rs, len(rules), hs, len(mats), ctypes.byref(o),
+                                                    ctypes.byref(st), hh, cc))
+        return st.as_dict(), [(int(hh[i]), int(cc[i])) for i in range(len(mats))]
 
     def closure_batch(self, queries: Sequence[tuple[Sequence[tuple[int, int, int]], Sequence[Matrix]]],
                       variant="auto", use_graph: bool = True, max_iterations: int = 0, log_products: int = 0):

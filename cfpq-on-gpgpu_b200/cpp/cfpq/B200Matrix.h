@@ -60,6 +60,7 @@ inline int variant_from_env() {
     if (!std::strcmp(v, "lop3")) return CFPQ_VARIANT_LOP3;
     if (!std::strcmp(v, "m4r")) return CFPQ_VARIANT_M4R;
     if (!std::strcmp(v, "tc")) return CFPQ_VARIANT_TC;
+    if (!std::strcmp(v, "ntset")) return CFPQ_VARIANT_NTSET;
     throw std::runtime_error(std::string("unknown CFPQ_VARIANT ") + v);
 }
 

@@ -282,7 +282,7 @@ extern "C" int cfpq_ctx_destroy(cfpq_ctx *ctx) {
         cudaFree(kv.second.d_pow13);
     }
     for (DevBuf *b : {&ctx->stage, &ctx->items, &ctx->prods, &ctx->slots, &ctx->qtrack, &ctx->prod_seen,
-                      &ctx->mats_desc, &ctx->edge_buf, &ctx->xbuf, &ctx->phase_log, &ctx->clear_desc,
+                      &ctx->mats_desc, &ctx->edge_buf, &ctx->phase_log, &ctx->clear_desc,
                       &ctx->d_sel, &ctx->cnts, &ctx->choice, &ctx->tc_ok, &ctx->sel_log, &ctx->mlp_w, &ctx->mlp_x,
                       &ctx->mlp_y, &ctx->mlp_m, &ctx->mlp_grad, &ctx->mlp_m1, &ctx->mlp_v2, &ctx->mlp_loss,
                       &ctx->mlp_out, &ctx->qranges, &ctx->item_trace, &ctx->nt_cells, &ctx->nt_mats,
@@ -591,20 +591,37 @@ static int ensure_hash_buffers(cfpq_ctx *ctx, size_t nm) {
     return CFPQ_OK;
 }
 
+// Hash launches of several matrices (one kernel per kHashBatch matrices) and
+// the copy of their (hash terms, count) pairs into the pinned h_hash.
+static int enqueue_hash_many(cfpq_ctx *ctx, cfpq_matrix *const *mats, size_t nmats) {
+    TRY(ensure_hash_buffers(ctx, nmats));
+    for (size_t i0 = 0; i0 < nmats; i0 += kHashBatch) {
+        HashBatch hb;
+        memset(&hb, 0, sizeof(hb));
+        for (size_t i = i0; i < nmats && i < i0 + kHashBatch; ++i) {
+            if (!mats[i]) return set_error(CFPQ_ERR_INVALID, "null matrix %zu", i);
+            PowTables pt;
+            TRY(get_pow_tables(ctx, mats[i], &pt));
+            const uint32_t k = hb.count++;
+            hb.m[k] = mats[i]->d;
+            hb.pow11[k] = pt.d_pow11;
+            hb.pow13[k] = pt.d_pow13;
+            const size_t tiles = (size_t)mats[i]->d.T * mats[i]->d.T;
+            hb.start[k + 1] = hb.start[k] + (uint32_t)((tiles + 3) / 4);
+        }
+        CUDA_TRY(launch_hash_count_many(hb, ctx->d_hash + 2 * i0, ctx->stream));
+    }
+    CUDA_TRY(cudaMemcpyAsync(ctx->h_hash, ctx->d_hash, nmats * 2 * sizeof(unsigned long long),
+                             cudaMemcpyDeviceToHost, ctx->stream));
+    return CFPQ_OK;
+}
+
 extern "C" int cfpq_hash_count_many(cfpq_ctx *ctx, cfpq_matrix *const *mats, size_t nmats, uint64_t *hashes,
                                     uint64_t *counts) {
     TRY(use_device(ctx));
     if (nmats && (!mats || !hashes || !counts)) return set_error(CFPQ_ERR_INVALID, "null argument");
     if (nmats == 0) return CFPQ_OK;
-    TRY(ensure_hash_buffers(ctx, nmats));
-    for (size_t i = 0; i < nmats; ++i) {
-        if (!mats[i]) return set_error(CFPQ_ERR_INVALID, "null matrix %zu", i);
-        PowTables pt;
-        TRY(get_pow_tables(ctx, mats[i], &pt));
-        CUDA_TRY(launch_hash_count(mats[i]->d, pt.d_pow11, pt.d_pow13, ctx->d_hash + 2 * i, ctx->stream));
-    }
-    CUDA_TRY(cudaMemcpyAsync(ctx->h_hash, ctx->d_hash, nmats * 2 * sizeof(unsigned long long),
-                             cudaMemcpyDeviceToHost, ctx->stream));
+    TRY(enqueue_hash_many(ctx, mats, nmats));
     TRY(sync_and_check(ctx));
     for (size_t i = 0; i < nmats; ++i) {
         hashes[i] = ctx->h_hash[2 * i] % 1000000007ULL;
@@ -642,29 +659,18 @@ struct TcProduct {
     uint32_t index, T, row_start, rows;
 };
 
-// Expanded-operand scratch for tensor-core products of up to T tiles per side
-// (P by rows and Q transposed, 4 KiB per tile each).  Allocated before any
-// graph capture.
-static int ensure_expand_scratch(cfpq_ctx *ctx, uint32_t T) {
-    return ctx->xbuf.ensure(2 * (size_t)T * T * 4096);
-}
-
-// One tensor-core product: expand its operands, plan its items, run the
-// tensor-core kernel, close the item list.  With a choice array every step is
-// a no-op unless this iteration's variant of the product is TC.
+// One tensor-core product: plan its items, run the tensor-core kernel, close
+// the item list.  With a choice array the plan emits nothing (and the kernel
+// finds no items) unless this iteration's variant of the product is TC.
 static int launch_tc_product(cfpq_ctx *ctx, const TcProduct &tp, uint32_t nprods, size_t list_cap,
                              uint32_t *prod_seen, uint32_t *qchanged, const uint8_t *choice, BufCounters *cnts,
                              cudaStream_t s) {
-    uint8_t *xp = ctx->xbuf.as<uint8_t>();
-    uint8_t *xq = xp + (size_t)tp.T * tp.T * 4096;
     const ProdDesc *pr = ctx->prods.as<ProdDesc>();
     const MatSlot *sl = ctx->slots.as<MatSlot>();
-    CUDA_TRY(launch_expand_operand(pr, tp.index, tp.T, sl, ctx->d_st, 0, xp, ctx->num_sms, choice, s));
-    CUDA_TRY(launch_expand_operand(pr, tp.index, tp.T, sl, ctx->d_st, 1, xq, ctx->num_sms, choice, s));
     CUDA_TRY(launch_plan(pr, nprods, tp.row_start, tp.row_start + tp.rows, sl, ctx->d_st, ctx->items.as<uint64_t>(),
                          list_cap, product_lop3_tiles_per_block(), prod_seen, 1, choice, s));
-    CUDA_TRY(launch_product_tc(pr, sl, ctx->d_st, ctx->items.as<uint64_t>(), list_cap, qchanged, ctx->tc_grid, xp, xq,
-                               cnts, s));
+    CUDA_TRY(launch_product_tc(pr, sl, ctx->d_st, ctx->items.as<uint64_t>(), list_cap, qchanged, ctx->tc_grid, cnts,
+                               s));
     CUDA_TRY(launch_reset_list(ctx->d_st, 2, s));
     return CFPQ_OK;
 }
@@ -705,7 +711,6 @@ static int enqueue_tiled_product(cfpq_ctx *ctx, const DevMat &a, const DevMat &b
     CUDA_TRY(cudaMemcpyAsync(ctx->prods.p, &pd, sizeof(pd), cudaMemcpyHostToDevice, ctx->stream));
     CUDA_TRY(cudaMemcpyAsync(ctx->d_st, ctx->h_st, sizeof(IterState), cudaMemcpyHostToDevice, ctx->stream));
     if (variant == CFPQ_VARIANT_TC) {
-        TRY(ensure_expand_scratch(ctx, T));
         return launch_tc_product(ctx, TcProduct{0, T, 0, (T + 3) / 4}, 1, cap, nullptr, nullptr, nullptr, nullptr,
                                  ctx->stream);
     }
@@ -1176,7 +1181,7 @@ static int get_loop_graph(cfpq_ctx *ctx, const ClosurePlan &pl, const QueryTrack
                                  (uint64_t)(uintptr_t)qt.changed,     (uint64_t)(uintptr_t)qt.last_iter,
                                  (uint64_t)(uintptr_t)qt.done_ns,     (uint64_t)ctx->lop3_grid,
                                  (uint64_t)pl.item_cap,               (uint64_t)(pl.uses_lop3 + 2 * pl.uses_m4r + 4 * pl.uses_tc),
-                                 (uint64_t)(uintptr_t)ctx->xbuf.p,    (uint64_t)(uintptr_t)ctx->choice.p,
+                                 (uint64_t)(uintptr_t)ctx->choice.p,
                                  (uint64_t)(uintptr_t)ctx->cnts.p,    (uint64_t)(uintptr_t)ctx->d_sel.p,
                                  (uint64_t)(uintptr_t)ctx->tc_ok.p,   (uint64_t)(uintptr_t)ctx->sel_log.p,
                                  (uint64_t)ctx->sel_log_iters,        (uint64_t)pl.auto_select};
@@ -1350,8 +1355,24 @@ static int run_logged_iterations(cfpq_ctx *ctx, const ClosurePlan &pl, const Que
     return CFPQ_OK;
 }
 
+// Result lines wanted with a closure (cfpq_closure_hash): hashed on the
+// device right after the closure, read back with the same synchronisation.
+struct HashOut {
+    cfpq_matrix *const *mats;
+    size_t n;
+    uint64_t *hashes, *counts;
+};
+
+static void fill_hash_out(const cfpq_ctx *ctx, const HashOut *ho) {
+    for (size_t i = 0; ho && i < ho->n; ++i) {
+        ho->hashes[i] = ctx->h_hash[2 * i] % 1000000007ULL;
+        ho->counts[i] = ctx->h_hash[2 * i + 1];
+    }
+}
+
 static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_closure_opts &o,
-                      cfpq_closure_stats *stats, uint32_t *iters_out, double *done_ms_out) {
+                      cfpq_closure_stats *stats, uint32_t *iters_out, double *done_ms_out,
+                      const HashOut *ho = nullptr) {
     for (size_t qi = 0; qi < qs.size(); ++qi) TRY(validate_query(qs[qi], qi));
     std::vector<uint64_t> key;
     plan_key(ctx, qs, o.variant, &key);
@@ -1375,6 +1396,11 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
         for (size_t q = 0; q < nq; ++q) {
             if (iters_out) iters_out[q] = 0;
             if (done_ms_out) done_ms_out[q] = 0;
+        }
+        if (ho && ho->n) {
+            TRY(enqueue_hash_many(ctx, ho->mats, ho->n));
+            TRY(sync_and_check(ctx));
+            fill_hash_out(ctx, ho);
         }
         return CFPQ_OK;
     }
@@ -1408,7 +1434,6 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
     if (ctx->sel_log_iters) TRY(ctx->sel_log.ensure((size_t)kSelLogIters * nprods * sizeof(SelLogRow)));
     ctx->log.clear();
     TRY(ctx->prod_seen.ensure(pl.prods.size() * 4));
-    if (pl.tc_max_T) TRY(ensure_expand_scratch(ctx, pl.tc_max_T));
     if (persistent) TRY(ctx->phase_log.ensure(kPhaseLogIters * 3 * 8));
     static_assert(sizeof(ItemTrace) == sizeof(cfpq_item_record), "item trace layout");
     const bool trace = persistent && (o.log_products & CFPQ_LOG_ITEMS) != 0;
@@ -1537,6 +1562,7 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
         CUDA_TRY(cudaMemcpyAsync(h_done, qt.done_ns, nq * 8, cudaMemcpyDeviceToHost, ctx->stream));
         CUDA_TRY(cudaMemcpyAsync(h_last, qt.last_iter, nq * 4, cudaMemcpyDeviceToHost, ctx->stream));
     }
+    if (ho && ho->n) TRY(enqueue_hash_many(ctx, ho->mats, ho->n));
     CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     float ms = 0;
     CUDA_TRY(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
@@ -1574,6 +1600,7 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
         if (done_ms_out) done_ms_out[q] = h_last[q] ? (double)(h_done[q] - hs.t_start_ns) / 1e6 : 0.0;
     }
     if (ctx->sel_log_iters && !log_products) TRY(collect_selection_log(ctx, pl, hs.iter));
+    fill_hash_out(ctx, ho);
     return CFPQ_OK;
 }
 
@@ -1711,6 +1738,26 @@ extern "C" int cfpq_closure(cfpq_ctx *ctx, const cfpq_rule *rules, size_t nrules
         return set_error(CFPQ_ERR_UNSUPPORTED, "variant %d is not available in the engine driver", o.variant);
     std::vector<QueryIn> qs{q};
     return run_engine(ctx, qs, o, stats, nullptr, nullptr);
+}
+
+extern "C" int cfpq_closure_hash(cfpq_ctx *ctx, const cfpq_rule *rules, size_t nrules, cfpq_matrix *const *mats,
+                                 size_t nmats, const cfpq_closure_opts *opts, cfpq_closure_stats *stats,
+                                 uint64_t *hashes, uint64_t *counts) {
+    TRY(use_device(ctx));
+    if (nmats && (!hashes || !counts)) return set_error(CFPQ_ERR_INVALID, "null result array");
+    const cfpq_closure_opts o = opts ? *opts : default_opts();
+    if (o.driver != CFPQ_DRIVER_ENGINE || o.variant == CFPQ_VARIANT_NTSET) {
+        TRY(cfpq_closure(ctx, rules, nrules, mats, nmats, opts, stats));
+        return cfpq_hash_count_many(ctx, mats, nmats, hashes, counts);
+    }
+    if (o.variant == CFPQ_VARIANT_TC && !ctx->tc_grid)
+        return set_error(CFPQ_ERR_UNSUPPORTED, "tensor-core variant unavailable (needs one CTA per SM)");
+    if (o.variant != CFPQ_VARIANT_AUTO && o.variant != CFPQ_VARIANT_LOP3 && o.variant != CFPQ_VARIANT_M4R &&
+        o.variant != CFPQ_VARIANT_TC)
+        return set_error(CFPQ_ERR_UNSUPPORTED, "variant %d is not available in the engine driver", o.variant);
+    std::vector<QueryIn> qs{QueryIn{rules, nrules, mats, nmats}};
+    HashOut ho{mats, nmats, hashes, counts};
+    return run_engine(ctx, qs, o, stats, nullptr, nullptr, &ho);
 }
 
 extern "C" int cfpq_closure_batch(cfpq_ctx *ctx, const cfpq_query *queries, size_t nqueries,

@@ -120,7 +120,7 @@ struct cfpq_ctx {
     unsigned long long *h_hash = nullptr;
     size_t h_hash_cap = 0;
     // growable device scratch
-    DevBuf stage, items, prods, slots, qtrack, prod_seen, mats_desc, edge_buf, xbuf, clear_desc;
+    DevBuf stage, items, prods, slots, qtrack, prod_seen, mats_desc, edge_buf, clear_desc;
     std::unordered_map<uint32_t, PowTables> pow;
     std::vector<cfpq_matrix *> pool;  // zeroed spare matrices (deltas, alias copies)
     GraphCache gcache;

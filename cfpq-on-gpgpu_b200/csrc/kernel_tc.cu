@@ -2,52 +2,69 @@
 // cores (tcgen05.mma kind::i8, 0/1 operands, int32 accumulators in TMEM,
 // result bit = accumulator > 0).
 //
-// Operands come pre-expanded (kernel_expand.cu): P as 0/1 bytes by rows and Q
-// transposed, both in the canonical no-swizzle K-major layout (8-row x 16-byte
-// core matrices, K-adjacent core matrices 128 B apart, M/N-adjacent 512 B
-// apart), one 4 KiB block per 64 x 64 tile.  The main loop does no ALU work on
-// operands: a single thread drives
-//   bulk copies (TMA engine) of the 4 P blocks (ti0..ti0+3, tk) and the 4 Q
-//   blocks (tk, tj0..tj0+3) of k-tile tk into one of kStages operand stages
-//   (32 KiB each, completion on the stage's mbarrier), and
-//   4 tcgen05.mma per k-tile (2 accumulators of M=128 x N=256, 2 K-halves of
-//   32), committed to the stage's mbarrier; a stage is refilled once its MMAs
-//   completed.
+// Operands travel as packed bits and are expanded on chip.  Per k-tile tk of
+// a work item the copy warp stages the 4 P tiles (ti0..ti0+3, tk) and the Q
+// block (tk, tj0..tj0+3) -- 4 KiB of bits, bulk copies completing on the
+// stage's mbarrier -- into one of kPkStages packed stages.  Eight expander
+// warps turn a packed stage into the MMA operands in one of kOpStages operand
+// stages: warp w < 4 writes P tile w as 0/1 bytes by rows (64 rows x 64 k),
+// warp w >= 4 transposes Q tile w-4 in registers and writes it the same way
+// (operand row = output column), both in the canonical no-swizzle K-major
+// layout (8-row x 16-byte core matrices, K-adjacent core matrices 128 B
+// apart, 8-row groups 512 B apart), then fence the writes for the async proxy
+// and arrive on the operand stage's "full" barrier.  The MMA warp issues 4
+// tcgen05.mma per k-tile (2 accumulators of M=128 x N=256, 2 K-halves of 32)
+// and commits them to the operand stage's "empty" barrier, which the
+// expanders wait on before reusing it; after the item's last k-tile a commit
+// to the accumulator barrier releases the epilogue.  Global memory only ever
+// supplies packed bits (512 B per 64x64 tile): the operands of a dense
+// n = 8192 product are 16 MiB and stay in L2.
+//
 // Work item (item list 2) = (product, group of 4 output tile-rows, block of 4
 // output tiles): a 256 x 256-bit output block over the whole inner dimension,
 // accumulated in TMEM as two 128 x 256 int32 matrices (all 512 TMEM columns;
-// one CTA per SM).
-// Epilogue (all 8 warps): tcgen05.ld 32x32b.x64 (warp w reads accumulator
-// w/4, TMEM lanes 32*(w%4)..), threshold > 0, pack 64 columns into a word,
-// then the atomic-OR epilogue of the word-level kernels (C, next delta D,
-// occupancy, populations).
+// one CTA per SM).  Epilogue (the 8 expander warps): tcgen05.ld 32x32b.x64
+// (warp w reads accumulator w/4, TMEM lanes 32*(w%4)..), threshold > 0, pack
+// 64 columns into a word, then the atomic-OR epilogue of the word-level
+// kernels (C, next delta D, occupancy, populations).
 //
 // Arithmetic: 256*256*64 MACs per k-tile; bound = the tensor pipe's dense int8
-// rate.  All waits are bounded and report CFPQ_ERR_TIMEOUT.
+// rate.  Every wait is bounded; a wait that gives up raises the CTA's abort
+// flag (which ends every other role's waits), the CTA then waits (bounded) for
+// each bulk copy and MMA still in flight, frees TMEM and reports
+// CFPQ_ERR_TIMEOUT.
 #include "launch.h"
 
 namespace cfpq {
 
 namespace {
 
-constexpr int kThreads = 256;
+constexpr int kExpWarps = 8;             // expanders, then the epilogue
+constexpr int kCopyWarp = kExpWarps;     // lane 0 issues the bulk copies
+constexpr int kMmaWarp = kExpWarps + 1;  // lane 0 issues the MMAs
+constexpr int kThreads = 32 * (kExpWarps + 2);
 constexpr int kMaxTiles = 2048;
 constexpr uint32_t kTmemCols = 512;
 constexpr unsigned kFull = 0xffffffffu;
 constexpr uint32_t kOperandBytes = 256 * 64;  // one operand, one stage: 256 rows x 64 bytes
-constexpr uint32_t kStages = 6;               // operand stages in flight
+constexpr uint32_t kPkStages = 8;             // packed k-tiles in flight (4 KiB each)
+constexpr uint32_t kOpStages = 3;             // expanded operand stages (32 KiB each)
 
 // Instruction descriptor, kind::i8: D = S32 (bits 4-5 = 2), A = B = U8 (0),
 // both K-major, N = 256 (bits 17-22 = N/8), M = 128 (bits 24-28 = M/16).
 constexpr uint32_t kIdesc = (2u << 4) | ((256u / 8) << 17) | ((128u / 16) << 24);
 
 struct __align__(1024) TcSmem {
-    uint8_t a[kStages][kOperandBytes];  // P blocks of 4 tile-rows, 4 x 4 KiB per stage
-    uint8_t b[kStages][kOperandBytes];  // Q^T blocks of 4 tiles, 4 x 4 KiB per stage
-    uint64_t ready_bar[kStages];
-    uint64_t mma_bar[kStages];
+    uint8_t a[kOpStages][kOperandBytes];  // P rows of 4 tile-rows, 4 x 4 KiB per stage
+    uint8_t b[kOpStages][kOperandBytes];  // Q^T of 4 tiles, 4 x 4 KiB per stage
+    uint64_t pk[kPkStages][8][64];        // packed: P tiles 0..3, then Q tiles 0..3
+    uint64_t pk_full[kPkStages], pk_empty[kPkStages];
+    uint64_t op_full[kOpStages], op_empty[kOpStages];
+    uint64_t acc_full;
     uint32_t tmem_base;
     uint32_t item;
+    uint32_t abort;    // a role's wait gave up: every other wait ends too
+    uint32_t pk_seen;  // packed stages expander warp 0 saw land (sequence count)
     uint16_t cand[kMaxTiles];
     uint16_t cmask[kMaxTiles];
     uint16_t ktile[kMaxTiles];
@@ -79,6 +96,10 @@ __device__ __forceinline__ void mma_commit(uint64_t *bar) {
                  : "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
@@ -102,14 +123,69 @@ __device__ __forceinline__ void tmem_ld64(uint32_t taddr, uint32_t (&r)[64]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// 16 bits -> 16 bytes of 0/1 (nibble * 0x00204081 & 0x01010101 spreads 4 bits
+// to 4 bytes).
+__device__ __forceinline__ uint4 expand16(uint32_t x) {
+    uint4 v;
+    v.x = ((x & 15u) * 0x00204081u) & 0x01010101u;
+    v.y = (((x >> 4) & 15u) * 0x00204081u) & 0x01010101u;
+    v.z = (((x >> 8) & 15u) * 0x00204081u) & 0x01010101u;
+    v.w = (((x >> 12) & 15u) * 0x00204081u) & 0x01010101u;
+    return v;
+}
+
+// Operand row r (0..63) of a 4 KiB block: its 64 k-bytes as 4 16-byte chunks
+// at ((r/8)*4 + kg)*128 + (r%8)*16.
+__device__ __forceinline__ void store_row(uint8_t *block, uint32_t r, uint64_t bits) {
+    uint8_t *base = block + (r >> 3) * 512 + (r & 7) * 16;
+#pragma unroll
+    for (int kg = 0; kg < 4; ++kg)
+        *reinterpret_cast<uint4 *>(base + kg * 128) = expand16((uint32_t)(bits >> (16 * kg)) & 0xFFFFu);
+}
+
+// Lane l holds rows l (lo) and l+32 (hi) of a 64 x 64 bit tile; afterwards it
+// holds columns l and l+32 as bit rows (bit r = original row r).  Exchange
+// stages j = 32 .. 1: rows k (bit j clear) and k|j swap the off-diagonal
+// j x j blocks, t = ((A[k] >> j) ^ A[k|j]) & m_j.
+__device__ __forceinline__ void transpose64(uint64_t &lo, uint64_t &hi, uint32_t lane) {
+    {
+        const uint64_t t = ((lo >> 32) ^ hi) & 0x00000000FFFFFFFFULL;
+        lo ^= t << 32;
+        hi ^= t;
+    }
+#pragma unroll
+    for (int j = 16; j >= 1; j >>= 1) {
+        const uint64_t m = j == 16 ? 0x0000FFFF0000FFFFULL
+                         : j == 8  ? 0x00FF00FF00FF00FFULL
+                         : j == 4  ? 0x0F0F0F0F0F0F0F0FULL
+                         : j == 2  ? 0x3333333333333333ULL
+                                   : 0x5555555555555555ULL;
+        const bool low = (lane & j) == 0;
+        const uint64_t plo = __shfl_xor_sync(kFull, lo, j), phi = __shfl_xor_sync(kFull, hi, j);
+        const uint64_t tlo = low ? (((lo >> j) ^ plo) & m) : (((plo >> j) ^ lo) & m);
+        const uint64_t thi = low ? (((hi >> j) ^ phi) & m) : (((phi >> j) ^ hi) & m);
+        lo ^= low ? (tlo << j) : tlo;
+        hi ^= low ? (thi << j) : thi;
+    }
+}
+
+// Bounded wait that also ends when another role raised the abort flag.
+__device__ __forceinline__ bool wait_or_abort(uint64_t *bar, uint32_t parity, const volatile uint32_t *abort) {
+    for (uint32_t i = 0; i < kWaitLimit; ++i) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((i & 63u) == 63u && *abort) return false;
+    }
+    return false;
+}
+
 __global__ void __launch_bounds__(kThreads, 1)
     k_product_tc(const ProdDesc *__restrict__ prods, const MatSlot *__restrict__ slots, IterState *st,
-                 const uint64_t *__restrict__ items_all, size_t list_cap, uint32_t *qchanged,
-                 const uint8_t *__restrict__ xp, const uint8_t *__restrict__ xq, BufCounters *cnts) {
+                 const uint64_t *__restrict__ items_all, size_t list_cap, uint32_t *qchanged, BufCounters *cnts) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     TcSmem &S = *reinterpret_cast<TcSmem *>(smem_raw);
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint64_t *items = items_all + 2 * list_cap;
+    volatile uint32_t *abort = &S.abort;
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&S.tmem_base)),
@@ -118,27 +194,39 @@ __global__ void __launch_bounds__(kThreads, 1)
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 0) {
-        for (uint32_t s = 0; s < kStages; ++s) {
-            mbar_init(&S.ready_bar[s], 1);
-            mbar_init(&S.mma_bar[s], 1);
+        for (uint32_t s = 0; s < kPkStages; ++s) {
+            mbar_init(&S.pk_full[s], 1);
+            mbar_init(&S.pk_empty[s], kExpWarps);
         }
+        for (uint32_t s = 0; s < kOpStages; ++s) {
+            mbar_init(&S.op_full[s], kExpWarps);
+            mbar_init(&S.op_empty[s], 1);
+        }
+        mbar_init(&S.acc_full, 1);
+        S.abort = 0;
+        S.pk_seen = 0;
         fence_mbar_init();
     }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = S.tmem_base;
-    uint32_t ready_phase = 0, mma_phase = 0;  // thread 0's per-stage parities
     const uint32_t iter = st->iter;
     const uint32_t nitems = st->item_count[2];
     unsigned long long triples = 0, outw = 0, neww = 0;
-    bool timed_out = false;
+    // k-tile sequence numbers across the CTA's items: stage = seq % stages,
+    // use = seq / stages; a "full" barrier is waited with parity use & 1, an
+    // "empty" one with (use & 1) ^ 1 (a fresh barrier counts its previous
+    // phase as complete, so the first use of every stage passes)
+    uint32_t seq = 0, items_done = 0;
+    uint32_t pk_issued = 0;      // copy warp: packed stages issued (sequence count)
+    uint32_t mma_committed = 0;  // MMA warp: k-tiles committed (sequence count)
 
     for (;;) {
         if (tid == 0) S.item = atomicAdd(&st->item_next[2], 1u);
         __syncthreads();
         const uint32_t idx = S.item;
-        if (idx >= nitems) break;
+        if (idx >= nitems || *abort) break;
         const uint64_t it = items[idx];
         const ProdDesc pd = prods[item_prod(it)];
         const uint32_t tig = item_ti(it), tjb = item_tjb(it), klo = item_klo(it), khi = item_khi(it);
@@ -149,6 +237,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         const uint32_t T = pd.T, ow = P.ow;
         const uint32_t ti0 = tig * 4, tj0 = tjb * 4;
         const uint32_t qword = tj0 >> 5, qshift = tj0 & 31;
+        const uint32_t np = min(4u, T - ti0), nq = min(4u, T - tj0);  // existing P tile-rows / Q tiles
 
         // ---- k-list: tk with an occupied P tile in the 4 tile-rows and a
         // non-empty Q block, increasing tk, within the item's range ----
@@ -157,7 +246,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             for (uint32_t base = 0; base < ow; base += 32) {
                 uint32_t bits = 0;
                 if (base + lane < ow) {
-                    for (uint32_t g = 0; g < 4 && ti0 + g < T; ++g) bits |= P.occ[(size_t)(ti0 + g) * ow + base + lane];
+                    for (uint32_t g = 0; g < np; ++g) bits |= P.occ[(size_t)(ti0 + g) * ow + base + lane];
                     bits &= range_word_mask(base + lane, klo, khi);
                 }
                 const uint32_t cnt = __popc(bits);
@@ -213,120 +302,136 @@ __global__ void __launch_bounds__(kThreads, 1)
         __syncthreads();
         const uint32_t nk = S.nk;
 
-        // ---- main loop: one thread drives copies and MMAs ----
-        if (tid == 0 && nk > 0) {
-            const uint32_t np = min(4u, T - ti0), nq = min(4u, T - tj0);  // existing P tile-rows / Q tiles
-            auto issue_copies = [&](uint32_t e) {
-                const uint32_t s = e % kStages, tk = S.ktile[e];
-                mbar_arrive_expect_tx(&S.ready_bar[s], (np + nq) * 4096u);
-                for (uint32_t g = 0; g < np; ++g)
-                    bulk_g2s(S.a[s] + g * 4096, xp + tile_offset(T, ti0 + g, tk) * 64, 4096u, &S.ready_bar[s]);
-                bulk_g2s(S.b[s], xq + tile_offset(T, tk, tj0) * 64, nq * 4096u, &S.ready_bar[s]);
-            };
-            // k-tiles [0, issued) have their copies issued, [0, ready_seen)
-            // their arrival waited for, [0, committed) their MMAs committed
-            // and [0, mma_seen) those MMAs' completion waited for: every
-            // stage has at most one copy and one commit outstanding
-            uint32_t issued = 0, ready_seen = 0, committed = 0, mma_seen = 0;
-            // a wait that gives up leaves the stage's parity as it was, so the
-            // drain below waits for the same phase again
-            auto wait_phase = [&](uint64_t *bars, uint32_t &phases, uint32_t s) {
-                if (!timed_out && mbar_wait_bounded(&bars[s], (phases >> s) & 1u))
-                    phases ^= 1u << s;
-                else
-                    timed_out = true;
-            };
-            for (uint32_t e = 0; e < nk && e < kStages; ++e, ++issued) issue_copies(e);
-            for (uint32_t e = 0; e < nk; ++e) {
-                const uint32_t s = e % kStages;
-                wait_phase(S.ready_bar, ready_phase, s);
-                if (timed_out) break;
-                ++ready_seen;
-                tc_fence_after();
-                const uint32_t abase = smem_addr(S.a[s]), bbase = smem_addr(S.b[s]);
-#pragma unroll
-                for (uint32_t h = 0; h < 2; ++h) {      // accumulator h: operand rows 128h .. 128h+127
-#pragma unroll
-                    for (uint32_t kh = 0; kh < 2; ++kh) {  // K halves of 32 bytes
-                        const uint64_t ad = smem_desc(abase + h * 8192 + kh * 256, 128, 512);
-                        const uint64_t bd = smem_desc(bbase + kh * 256, 128, 512);
-                        mma_i8(tmem + h * 256, ad, bd, (e > 0 || kh > 0) ? 1u : 0u);
+        // ---- pipeline over the item's k-tiles ----
+        if (warp == kCopyWarp) {
+            if (lane == 0) {
+                for (uint32_t e = 0; e < nk; ++e) {
+                    const uint32_t q = seq + e, s = q % kPkStages, use = q / kPkStages;
+                    if (!wait_or_abort(&S.pk_empty[s], (use & 1u) ^ 1u, abort)) {
+                        *abort = 1;
+                        break;
                     }
-                }
-                mma_commit(&S.mma_bar[s]);
-                ++committed;
-                // refill the stage of k-tile e-1 once its MMAs completed (the
-                // tensor pipe keeps working on k-tile e meanwhile)
-                if (e >= 1 && e - 1 + kStages < nk) {
-                    const uint32_t s1 = (e - 1) % kStages;
-                    wait_phase(S.mma_bar, mma_phase, s1);
-                    if (timed_out) break;
-                    ++mma_seen;
-                    issue_copies(e - 1 + kStages);
-                    ++issued;
+                    const uint32_t tk = S.ktile[e];
+                    mbar_arrive_expect_tx(&S.pk_full[s], (np + nq) * 512u);
+                    for (uint32_t g = 0; g < np; ++g)
+                        bulk_g2s(S.pk[s][g], P.bits + tile_offset(T, ti0 + g, tk), 512u, &S.pk_full[s]);
+                    bulk_g2s(S.pk[s][4], Q.bits + tile_offset(T, tk, tj0), nq * 512u, &S.pk_full[s]);
+                    ++pk_issued;
                 }
             }
-            // drain, also after a wait gave up: every copy whose arrival and
-            // every commit whose completion was not waited for above, so that
-            // no copy or MMA is in flight when the CTA moves on, frees TMEM or
-            // exits (each wait bounded on its own)
-            bool drained = true;
-            auto drain = [&](uint64_t *bars, uint32_t &phases, uint32_t e) {
-                const uint32_t s = e % kStages;
-                if (!mbar_wait_bounded(&bars[s], (phases >> s) & 1u)) drained = false;
-                phases ^= 1u << s;
-            };
-            for (uint32_t e = ready_seen; e < issued; ++e) drain(S.ready_bar, ready_phase, e);
-            for (uint32_t e = mma_seen; e < committed; ++e) drain(S.mma_bar, mma_phase, e);
-            if (!drained) timed_out = true;
-        }
-        tc_fence_before();
-        timed_out = __syncthreads_or(timed_out) != 0;
-        tc_fence_after();
-        if (timed_out) break;  // uniform: the error status is set below
-
-        // ---- epilogue ----
-        bool any_new = false;
-        if (nk > 0) {
-            uint32_t tile_new[4] = {0, 0, 0, 0};
-            const uint32_t h = warp >> 2, q = warp & 3;
-            const uint32_t m = 128 * h + 32 * q + lane;  // output row within the 256-row block
-            const uint32_t ti = ti0 + (m >> 6), r = m & 63;
-#pragma unroll 1
-            for (uint32_t jt = 0; jt < 4; ++jt) {
-                uint32_t v[64];
-                tmem_ld64(tmem + ((32 * q) << 16) + h * 256 + jt * 64, v);
-                uint64_t a = 0;
+        } else if (warp == kMmaWarp) {
+            if (lane == 0) {
+                for (uint32_t e = 0; e < nk; ++e) {
+                    const uint32_t q = seq + e, o = q % kOpStages, use = q / kOpStages;
+                    if (!wait_or_abort(&S.op_full[o], use & 1u, abort)) {
+                        *abort = 1;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t abase = smem_addr(S.a[o]), bbase = smem_addr(S.b[o]);
 #pragma unroll
-                for (int c = 0; c < 64; ++c) a |= (uint64_t)(v[c] != 0) << c;
-                const uint32_t tj = tj0 + jt;
-                uint32_t newcnt = 0;
-                if (a && ti < T && tj < T) {
-                    ++outw;
-                    const size_t off = tile_offset(T, ti, tj) + r;
-                    unsigned long long *cw = reinterpret_cast<unsigned long long *>(C.bits + off);
-                    const uint64_t seen = __ldcg(cw);
-                    if (a & ~seen) {
-                        const uint64_t prev = atomicOr(cw, (unsigned long long)a);
-                        const uint64_t nw = a & ~prev;
-                        if (nw) {
-                            ++neww;
-                            newcnt = __popcll(nw);
-                            if (D.bits)
-                                atomicOr(reinterpret_cast<unsigned long long *>(D.bits + off), (unsigned long long)nw);
+                    for (uint32_t h = 0; h < 2; ++h) {      // accumulator h: operand rows 128h .. 128h+127
+#pragma unroll
+                        for (uint32_t kh = 0; kh < 2; ++kh) {  // K halves of 32 bytes
+                            const uint64_t ad = smem_desc(abase + h * 8192 + kh * 256, 128, 512);
+                            const uint64_t bd = smem_desc(bbase + kh * 256, 128, 512);
+                            mma_i8(tmem + h * 256, ad, bd, (e > 0 || kh > 0) ? 1u : 0u);
                         }
                     }
+                    mma_commit(&S.op_empty[o]);
+                    ++mma_committed;
                 }
-                tile_new[jt] = __reduce_add_sync(kFull, newcnt);  // the warp's 32 rows share (ti, tj)
+                if (nk && !*abort) mma_commit(&S.acc_full);  // completes after every MMA of the item
             }
-            any_new = (tile_new[0] | tile_new[1] | tile_new[2] | tile_new[3]) != 0;
-            if (any_new && ti < T) {  // lane j: tile tj0 + j (populations, occupancy, buffer counters)
-                const uint32_t mine = lane == 0 ? tile_new[0] : lane == 1 ? tile_new[1] : lane == 2 ? tile_new[2]
-                                    : lane == 3 ? tile_new[3] : 0u;
-                tiles_gain(C, ti, tj0, mine, cnts ? cnts + 3 * pd.head : nullptr);
-                if (D.bits) tiles_gain(D, ti, tj0, mine, cnts ? cnts + 3 * pd.head + 1 + ((iter & 1) ^ 1) : nullptr);
+        } else {
+            // expander warp w: P tile w (w < 4) or Q tile w - 4
+            const bool is_p = warp < 4;
+            const uint32_t g = is_p ? warp : warp - 4;
+            const bool present = g < (is_p ? np : nq);
+            for (uint32_t e = 0; e < nk; ++e) {
+                const uint32_t q = seq + e, s = q % kPkStages, o = q % kOpStages;
+                // waits are warp-uniform: one lane giving up ends the whole warp's loop
+                if (!__all_sync(kFull, wait_or_abort(&S.pk_full[s], (q / kPkStages) & 1u, abort))) {
+                    if (lane == 0) *abort = 1;
+                    break;
+                }
+                if (warp == 0 && lane == 0) S.pk_seen = q + 1;
+                uint64_t lo = 0, hi = 0;
+                if (present) {
+                    lo = S.pk[s][is_p ? g : 4 + g][lane];
+                    hi = S.pk[s][is_p ? g : 4 + g][lane + 32];
+                }
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&S.pk_empty[s]);  // the packed stage may be refilled
+                if (!__all_sync(kFull, wait_or_abort(&S.op_empty[o], ((q / kOpStages) & 1u) ^ 1u, abort))) {
+                    if (lane == 0) *abort = 1;
+                    break;
+                }
+                if (present) {
+                    if (!is_p) transpose64(lo, hi, lane);
+                    uint8_t *block = (is_p ? S.a[o] : S.b[o]) + g * 4096;
+                    store_row(block, lane, lo);
+                    store_row(block, lane + 32, hi);
+                }
+                fence_proxy_async_smem();  // generic-proxy writes before the tensor core reads them
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&S.op_full[o]);
             }
         }
+        seq += nk;
+        __syncthreads();
+        if (*abort) break;
+
+        // ---- epilogue (expander warps) ----
+        bool any_new = false;
+        if (nk > 0 && warp < kExpWarps) {
+            const bool acc_ok = __all_sync(kFull, wait_or_abort(&S.acc_full, items_done & 1u, abort));
+            if (!acc_ok && lane == 0) *abort = 1;
+            tc_fence_after();
+            if (acc_ok) {
+                uint32_t tile_new[4] = {0, 0, 0, 0};
+                const uint32_t h = warp >> 2, qq = warp & 3;
+                const uint32_t m = 128 * h + 32 * qq + lane;  // output row within the 256-row block
+                const uint32_t ti = ti0 + (m >> 6), r = m & 63;
+#pragma unroll 1
+                for (uint32_t jt = 0; jt < 4; ++jt) {
+                    uint32_t v[64];
+                    tmem_ld64(tmem + ((32 * qq) << 16) + h * 256 + jt * 64, v);
+                    uint64_t a = 0;
+#pragma unroll
+                    for (int c = 0; c < 64; ++c) a |= (uint64_t)(v[c] != 0) << c;
+                    const uint32_t tj = tj0 + jt;
+                    uint32_t newcnt = 0;
+                    if (a && ti < T && tj < T) {
+                        ++outw;
+                        const size_t off = tile_offset(T, ti, tj) + r;
+                        unsigned long long *cw = reinterpret_cast<unsigned long long *>(C.bits + off);
+                        const uint64_t seen = __ldcg(cw);
+                        if (a & ~seen) {
+                            const uint64_t prev = atomicOr(cw, (unsigned long long)a);
+                            const uint64_t nw = a & ~prev;
+                            if (nw) {
+                                ++neww;
+                                newcnt = __popcll(nw);
+                                if (D.bits)
+                                    atomicOr(reinterpret_cast<unsigned long long *>(D.bits + off),
+                                             (unsigned long long)nw);
+                            }
+                        }
+                    }
+                    tile_new[jt] = __reduce_add_sync(kFull, newcnt);  // the warp's 32 rows share (ti, tj)
+                }
+                any_new = (tile_new[0] | tile_new[1] | tile_new[2] | tile_new[3]) != 0;
+                if (any_new && ti < T) {  // lane j: tile tj0 + j (populations, occupancy, buffer counters)
+                    const uint32_t mine = lane == 0 ? tile_new[0] : lane == 1 ? tile_new[1] : lane == 2 ? tile_new[2]
+                                        : lane == 3 ? tile_new[3] : 0u;
+                    tiles_gain(C, ti, tj0, mine, cnts ? cnts + 3 * pd.head : nullptr);
+                    if (D.bits)
+                        tiles_gain(D, ti, tj0, mine, cnts ? cnts + 3 * pd.head + 1 + ((iter & 1) ^ 1) : nullptr);
+                }
+            }
+        }
+        if (nk > 0) ++items_done;
         if (any_new && lane == 0) {
             st->changed = 1u;
             if (qchanged) qchanged[pd.query] = 1u;
@@ -334,6 +439,24 @@ __global__ void __launch_bounds__(kThreads, 1)
         tc_fence_before();
         __syncthreads();  // TMEM reads done before the next item's first MMA overwrites it
         tc_fence_after();
+        if (*abort) break;
+    }
+
+    // ---- exit: after a wait gave up, wait (bounded) for every bulk copy and
+    // MMA still in flight before TMEM is freed and the CTA ends ----
+    __syncthreads();
+    const bool aborted = *abort != 0;
+    if (aborted) {
+        if (warp == kCopyWarp && lane == 0) {
+            // copies of the stages [pk_seen, pk_issued) may still be landing
+            for (uint32_t q = S.pk_seen; q < pk_issued; ++q)
+                mbar_wait_bounded(&S.pk_full[q % kPkStages], (q / kPkStages) & 1u);
+        }
+        if (warp == kMmaWarp && lane == 0 && mma_committed) {
+            // the last commit completes after every MMA issued before it
+            const uint32_t q = mma_committed - 1;
+            mbar_wait_bounded(&S.op_empty[q % kOpStages], (q / kOpStages) & 1u);
+        }
     }
     for (int o = 16; o > 0; o >>= 1) {
         triples += __shfl_down_sync(kFull, triples, o);
@@ -345,7 +468,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (outw) atomicAdd(&st->out_words, outw);
         if (neww) atomicAdd(&st->new_words, neww);
     }
-    if (timed_out && tid == 0) atomicExch(&st->error, 5u);
+    if (aborted && tid == 0) atomicExch(&st->error, 5u);
     tc_fence_before();
     __syncthreads();
     if (warp == 0)
@@ -363,9 +486,8 @@ int product_tc_blocks_per_sm() {
 
 cudaError_t launch_product_tc(const ProdDesc *d_prods, const MatSlot *d_slots, IterState *d_st,
                               const uint64_t *d_items, size_t list_cap, uint32_t *d_qchanged, int grid,
-                              const uint8_t *xp, const uint8_t *xq, BufCounters *cnts, cudaStream_t s) {
-    k_product_tc<<<grid, kThreads, sizeof(TcSmem), s>>>(d_prods, d_slots, d_st, d_items, list_cap, d_qchanged, xp,
-                                                        xq, cnts);
+                              BufCounters *cnts, cudaStream_t s) {
+    k_product_tc<<<grid, kThreads, sizeof(TcSmem), s>>>(d_prods, d_slots, d_st, d_items, list_cap, d_qchanged, cnts);
     return cudaGetLastError();
 }
 

@@ -185,9 +185,10 @@ __global__ void k_rows_scatter(DevMat m, const uint64_t *__restrict__ rows) {
 // Block = 4 tiles x 64 rows; thread = one row word of one tile.  Unoccupied
 // tiles exit at once.  out[0] accumulates terms < 2^30 (no overflow below
 // 2^34 terms), out[1] the bit count.
-__global__ void __launch_bounds__(256) k_hash_count(DevMat m, const uint32_t *__restrict__ pow11,
-                                                    const uint32_t *__restrict__ pow13, unsigned long long *out) {
-    const size_t tile = (size_t)blockIdx.x * 4 + (threadIdx.x >> 6);
+__device__ __forceinline__ void hash_count_block(const DevMat &m, const uint32_t *__restrict__ pow11,
+                                                 const uint32_t *__restrict__ pow13, unsigned long long *out,
+                                                 size_t block) {
+    const size_t tile = block * 4 + (threadIdx.x >> 6);
     const uint32_t r = threadIdx.x & 63;
     unsigned long long h = 0, cnt = 0;
     if (tile < (size_t)m.T * m.T) {
@@ -226,6 +227,19 @@ __global__ void __launch_bounds__(256) k_hash_count(DevMat m, const uint32_t *__
         if (H) atomicAdd(out, H);
         if (C) atomicAdd(out + 1, C);
     }
+}
+
+__global__ void __launch_bounds__(256) k_hash_count(DevMat m, const uint32_t *__restrict__ pow11,
+                                                    const uint32_t *__restrict__ pow13, unsigned long long *out) {
+    hash_count_block(m, pow11, pow13, out, blockIdx.x);
+}
+
+// Several matrices in one launch: blocks [start[i], start[i+1]) hash matrix i
+// into out[2i], out[2i+1] (zeroed by the launcher).
+__global__ void __launch_bounds__(256) k_hash_count_many(HashBatch hb, unsigned long long *out) {
+    uint32_t i = 0;
+    while (i + 1 < hb.count && blockIdx.x >= hb.start[i + 1]) ++i;
+    hash_count_block(hb.m[i], hb.pow11[i], hb.pow13[i], out + 2 * i, blockIdx.x - hb.start[i]);
 }
 
 // ---- plain dense product (variant PLAIN) ------------------------------------
@@ -517,6 +531,14 @@ cudaError_t launch_hash_count(const DevMat &m, const uint32_t *d_pow11, const ui
     if (e != cudaSuccess || m.T == 0) return e;
     const size_t tiles = (size_t)m.T * m.T;
     k_hash_count<<<(unsigned)((tiles + 3) / 4), 256, 0, s>>>(m, d_pow11, d_pow13, d_out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_hash_count_many(const HashBatch &hb, unsigned long long *d_out, cudaStream_t s) {
+    if (hb.count == 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(d_out, 0, 2 * sizeof(unsigned long long) * hb.count, s);
+    if (e != cudaSuccess || hb.start[hb.count] == 0) return e;
+    k_hash_count_many<<<hb.start[hb.count], 256, 0, s>>>(hb, d_out);
     return cudaGetLastError();
 }
 

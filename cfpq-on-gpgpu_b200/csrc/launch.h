@@ -44,6 +44,18 @@ cudaError_t launch_clear_rows(const MatRows *d_tab, uint32_t nmats, uint32_t tot
 // Result hash / count (cfpq-cpp/Grammar.cpp:81-100 on the device)
 cudaError_t launch_hash_count(const DevMat &m, const uint32_t *d_pow11, const uint32_t *d_pow13,
                               unsigned long long *d_out, cudaStream_t s);
+// Result lines of up to kHashBatch matrices in one launch (blocks of 4 tiles;
+// matrix i owns blocks [start[i], start[i+1])): out[2i] = hash terms,
+// out[2i+1] = bit count.
+constexpr uint32_t kHashBatch = 16;
+struct HashBatch {
+    DevMat m[kHashBatch];
+    const uint32_t *pow11[kHashBatch];
+    const uint32_t *pow13[kHashBatch];
+    uint32_t start[kHashBatch + 1];
+    uint32_t count;
+};
+cudaError_t launch_hash_count_many(const HashBatch &hb, unsigned long long *d_out, cudaStream_t s);
 
 // Plain dense product (variant PLAIN): mode 0 ORs into c and sets *d_flag on
 // change; mode 1 writes the product into c (c must not alias a or b).
@@ -65,19 +77,13 @@ cudaError_t launch_plan(const ProdDesc *d_prods, uint32_t nprods, uint32_t row_b
 cudaError_t launch_product_tiled(int m4r, const ProdDesc *d_prods, const MatSlot *d_slots, IterState *d_st,
                                  const uint64_t *d_items, size_t list_cap, uint32_t *d_qchanged, int grid,
                                  BufCounters *d_cnts, cudaStream_t s);
-// Tensor-core product over item list 2 (d_items + 2 * list_cap) of one
-// product whose operands were expanded into xp (P by rows) and xq (Q
-// transposed); one CTA per SM (it owns all 512 TMEM columns).
+// Tensor-core product over item list 2 (d_items + 2 * list_cap): packed
+// operand tiles staged by bulk copies and expanded to 0/1 bytes in shared
+// memory; one CTA per SM (it owns all 512 TMEM columns).
 cudaError_t launch_product_tc(const ProdDesc *d_prods, const MatSlot *d_slots, IterState *d_st,
                               const uint64_t *d_items, size_t list_cap, uint32_t *d_qchanged, int grid,
-                              const uint8_t *xp, const uint8_t *xq, BufCounters *d_cnts, cudaStream_t s);
+                              BufCounters *d_cnts, cudaStream_t s);
 int product_tc_blocks_per_sm();
-// Operand expansion for the tensor-core product (4 KiB of 0/1 bytes per tile,
-// canonical layout): side 0 = P of product p by rows, side 1 = Q transposed.
-cudaError_t launch_expand_operand(const ProdDesc *d_prods, uint32_t p, uint32_t T, const MatSlot *d_slots,
-                                  const IterState *d_st, int side, uint8_t *out, int num_sms,
-                                  const uint8_t *d_choice, cudaStream_t s);
-// (does nothing when d_choice is given and d_choice[p] is not the tensor-core variant)
 // Closes a tensor-core product's item list (counts it, resets the counters).
 cudaError_t launch_reset_list(IterState *st, int list, cudaStream_t s);
 int product_lop3_tiles_per_block();

@@ -116,11 +116,16 @@ def closure(engine, rules: Sequence[tuple[int, int, int]], dist=None, group=None
     blocks = row_blocks(engine.n, world)
     r0, r1 = blocks[rank]
     chunk = max((engine.block_bytes(a, b) for a, b in blocks), default=0)
-    dev = engine.device
     nccl = dist is not None and dist.get_backend(group) == "nccl"
-    pinned = dev == "cpu" and torch.cuda.is_available()  # host buffers a GPU engine copies into
+    # exchange buffers: device memory only for NCCL (a device engine's blocks
+    # then never leave the GPUs); otherwise host memory, pinned when a device
+    # engine copies into it.  The collective runs on torch's stream, the
+    # engine's copies on its own: every hand-over below is synchronised.
+    dev = "cuda" if nccl and engine.device == "cuda" else "cpu"
+    pinned = dev == "cpu" and engine.device == "cuda"
     send = torch.zeros(max(chunk, 1), dtype=torch.uint8, device=dev, pin_memory=pinned)
-    recv = torch.zeros(max(chunk, 1) * world, dtype=torch.uint8, device=dev) if world > 1 else None
+    recv = (torch.zeros(max(chunk, 1) * world, dtype=torch.uint8, device=dev, pin_memory=pinned)
+            if world > 1 else None)
     flags = torch.zeros(max(engine.nmats, 1), dtype=torch.int32, device="cuda" if nccl else "cpu")
     st = RowBlockStats()
     while True:
@@ -141,11 +146,11 @@ def closure(engine, rules: Sequence[tuple[int, int, int]], dist=None, group=None
             break
         if world > 1:
             for m in any_changed:
-                send.zero_()
+                # (bytes of send past this rank's block are never imported)
                 if r1 > r0:
                     engine.export(m, r0, r1, send)
                 engine.sync()
-                if nccl:
+                if dev == "cuda":
                     dist.all_gather_into_tensor(recv, send, group=group)
                     torch.cuda.current_stream().synchronize()
                 else:

@@ -360,6 +360,16 @@ int cfpq_matrix_delta(cfpq_ctx *ctx, cfpq_matrix *delta, const cfpq_matrix *cur,
 int cfpq_closure(cfpq_ctx *ctx, const cfpq_rule *rules, size_t nrules, cfpq_matrix *const *mats,
                  size_t nmats, const cfpq_closure_opts *opts, cfpq_closure_stats *stats);
 
+/* cfpq_closure followed by the result line (hash, count) of every matrix,
+ * as cfpq_hash_count_many gives them, with one host synchronisation for both
+ * (the hashes are computed on the device right after the closure).  Replaces
+ * the worklist loop plus the print_results pass of the reference
+ * (cfpq-cpp/Grammar.h:58-69, cfpq-cpp/Grammar.cpp:81-100) for callers that
+ * want the answer lines of a query. */
+int cfpq_closure_hash(cfpq_ctx *ctx, const cfpq_rule *rules, size_t nrules, cfpq_matrix *const *mats,
+                      size_t nmats, const cfpq_closure_opts *opts, cfpq_closure_stats *stats, uint64_t *hashes,
+                      uint64_t *counts);
+
 /* One independent query of a batch: its rules index into its own matrices. */
 typedef struct cfpq_query {
     const cfpq_rule *rules;
