@@ -7,12 +7,15 @@
 // block (tk, tj0..tj0+3) -- 4 KiB of bits, bulk copies completing on the
 // stage's mbarrier -- into one of kPkStages packed stages.  Eight expander
 // warps turn a packed stage into the MMA operands in one of kOpStages operand
-// stages: warp w < 4 writes P tile w as 0/1 bytes by rows (64 rows x 64 k),
-// warp w >= 4 transposes Q tile w-4 in registers and writes it the same way
-// (operand row = output column), both in the canonical no-swizzle K-major
-// layout (8-row x 16-byte core matrices, K-adjacent core matrices 128 B
-// apart, 8-row groups 512 B apart), then fence the writes for the async proxy
-// and arrive on the operand stage's "full" barrier.  The MMA warp issues 4
+// stages: warp w < 4 writes P tile w as 0/1 bytes by rows (64 rows x 64 k)
+// in the canonical no-swizzle K-major layout (8-row x 16-byte core matrices,
+// K-adjacent core matrices 128 B apart, 8-row groups 512 B apart), warp
+// w >= 4 writes Q tile w-4 by its rows (k) in the MN-major layout (16 output
+// columns x 8 k-rows per 128-byte core matrix, column groups 128 B apart,
+// 8-row k groups 2048 B apart), so neither operand is transposed; each
+// nibble of bits becomes 4 bytes of 0/1 by one multiply and one mask.
+// The warps then fence the writes for the async proxy and arrive on the
+// operand stage's "full" barrier.  The MMA warp issues 4
 // tcgen05.mma per k-tile (2 accumulators of M=128 x N=256, 2 K-halves of 32)
 // and commits them to the operand stage's "empty" barrier, which the
 // expanders wait on before reusing it; after the item's last k-tile a commit
@@ -51,8 +54,12 @@ constexpr uint32_t kPkStages = 8;             // packed k-tiles in flight (4 KiB
 constexpr uint32_t kOpStages = 3;             // expanded operand stages (32 KiB each)
 
 // Instruction descriptor, kind::i8: D = S32 (bits 4-5 = 2), A = B = U8 (0),
-// both K-major, N = 256 (bits 17-22 = N/8), M = 128 (bits 24-28 = M/16).
-constexpr uint32_t kIdesc = (2u << 4) | ((256u / 8) << 17) | ((128u / 16) << 24);
+// A K-major (bit 15 = 0), B MN-major (bit 16 = 1), N = 256 (bits 17-22 =
+// N/8), M = 128 (bits 24-28 = M/16).
+constexpr uint32_t kIdesc = (2u << 4) | (1u << 16) | ((256u / 8) << 17) | ((128u / 16) << 24);
+// B operand (MN-major, no swizzle): 16-column groups 128 B apart (SBO),
+// 8-row k groups 2048 B apart (LBO).
+constexpr uint32_t kBSbo = 128, kBLbo = 2048;
 
 struct __align__(1024) TcSmem {
     uint8_t a[kOpStages][kOperandBytes];  // P rows of 4 tile-rows, 4 x 4 KiB per stage
@@ -123,9 +130,11 @@ __device__ __forceinline__ void tmem_ld64(uint32_t taddr, uint32_t (&r)[64]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-// 16 bits -> 16 bytes of 0/1 (nibble * 0x00204081 & 0x01010101 spreads 4 bits
-// to 4 bytes).
-__device__ __forceinline__ uint4 expand16(uint32_t x) {
+// 16 bits of `bits` starting at bit 16*c -> 16 bytes of 0/1 (bit i -> byte
+// i): each nibble times 0x00204081 puts its bits at 0, 8, 16, 24 without
+// overlapping sums; the mask keeps them.
+__device__ __forceinline__ uint4 expand16(uint64_t bits, int c) {
+    const uint32_t x = (uint32_t)(bits >> (16 * c));
     uint4 v;
     v.x = ((x & 15u) * 0x00204081u) & 0x01010101u;
     v.y = (((x >> 4) & 15u) * 0x00204081u) & 0x01010101u;
@@ -134,39 +143,21 @@ __device__ __forceinline__ uint4 expand16(uint32_t x) {
     return v;
 }
 
-// Operand row r (0..63) of a 4 KiB block: its 64 k-bytes as 4 16-byte chunks
-// at ((r/8)*4 + kg)*128 + (r%8)*16.
-__device__ __forceinline__ void store_row(uint8_t *block, uint32_t r, uint64_t bits) {
+// A operand (K-major), operand row r (0..63) of a 4 KiB block: its 64 k-bytes
+// as 4 16-byte chunks at ((r/8)*4 + kg)*128 + (r%8)*16.
+__device__ __forceinline__ void store_row_k(uint8_t *block, uint32_t r, uint64_t bits) {
     uint8_t *base = block + (r >> 3) * 512 + (r & 7) * 16;
 #pragma unroll
-    for (int kg = 0; kg < 4; ++kg)
-        *reinterpret_cast<uint4 *>(base + kg * 128) = expand16((uint32_t)(bits >> (16 * kg)) & 0xFFFFu);
+    for (int kg = 0; kg < 4; ++kg) *reinterpret_cast<uint4 *>(base + kg * 128) = expand16(bits, kg);
 }
 
-// Lane l holds rows l (lo) and l+32 (hi) of a 64 x 64 bit tile; afterwards it
-// holds columns l and l+32 as bit rows (bit r = original row r).  Exchange
-// stages j = 32 .. 1: rows k (bit j clear) and k|j swap the off-diagonal
-// j x j blocks, t = ((A[k] >> j) ^ A[k|j]) & m_j.
-__device__ __forceinline__ void transpose64(uint64_t &lo, uint64_t &hi, uint32_t lane) {
-    {
-        const uint64_t t = ((lo >> 32) ^ hi) & 0x00000000FFFFFFFFULL;
-        lo ^= t << 32;
-        hi ^= t;
-    }
+// B operand (MN-major), k-row k (0..63) of Q tile j (output columns
+// 64j .. 64j+63): 16-column chunk c of the row at
+// (4j + c)*kBSbo + (k/8)*kBLbo + (k%8)*16.
+__device__ __forceinline__ void store_row_mn(uint8_t *b, uint32_t j, uint32_t k, uint64_t bits) {
+    uint8_t *base = b + (k >> 3) * kBLbo + (k & 7) * 16 + 4 * j * kBSbo;
 #pragma unroll
-    for (int j = 16; j >= 1; j >>= 1) {
-        const uint64_t m = j == 16 ? 0x0000FFFF0000FFFFULL
-                         : j == 8  ? 0x00FF00FF00FF00FFULL
-                         : j == 4  ? 0x0F0F0F0F0F0F0F0FULL
-                         : j == 2  ? 0x3333333333333333ULL
-                                   : 0x5555555555555555ULL;
-        const bool low = (lane & j) == 0;
-        const uint64_t plo = __shfl_xor_sync(kFull, lo, j), phi = __shfl_xor_sync(kFull, hi, j);
-        const uint64_t tlo = low ? (((lo >> j) ^ plo) & m) : (((plo >> j) ^ lo) & m);
-        const uint64_t thi = low ? (((hi >> j) ^ phi) & m) : (((phi >> j) ^ hi) & m);
-        lo ^= low ? (tlo << j) : tlo;
-        hi ^= low ? (thi << j) : thi;
-    }
+    for (int c = 0; c < 4; ++c) *reinterpret_cast<uint4 *>(base + c * kBSbo) = expand16(bits, c);
 }
 
 // Bounded wait that also ends when another role raised the abort flag.
@@ -334,7 +325,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
                         for (uint32_t kh = 0; kh < 2; ++kh) {  // K halves of 32 bytes
                             const uint64_t ad = smem_desc(abase + h * 8192 + kh * 256, 128, 512);
-                            const uint64_t bd = smem_desc(bbase + kh * 256, 128, 512);
+                            const uint64_t bd = smem_desc(bbase + kh * 4 * kBLbo, kBLbo, kBSbo);
                             mma_i8(tmem + h * 256, ad, bd, (e > 0 || kh > 0) ? 1u : 0u);
                         }
                     }
@@ -344,7 +335,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 if (nk && !*abort) mma_commit(&S.acc_full);  // completes after every MMA of the item
             }
         } else {
-            // expander warp w: P tile w (w < 4) or Q tile w - 4
+            // expander warp w: P tile w (w < 4) or Q tile w - 4 (by rows, no transpose)
             const bool is_p = warp < 4;
             const uint32_t g = is_p ? warp : warp - 4;
             const bool present = g < (is_p ? np : nq);
@@ -368,10 +359,13 @@ __global__ void __launch_bounds__(kThreads, 1)
                     break;
                 }
                 if (present) {
-                    if (!is_p) transpose64(lo, hi, lane);
-                    uint8_t *block = (is_p ? S.a[o] : S.b[o]) + g * 4096;
-                    store_row(block, lane, lo);
-                    store_row(block, lane + 32, hi);
+                    if (is_p) {
+                        store_row_k(S.a[o] + g * 4096, lane, lo);
+                        store_row_k(S.a[o] + g * 4096, lane + 32, hi);
+                    } else {
+                        store_row_mn(S.b[o], g, lane, lo);
+                        store_row_mn(S.b[o], g, lane + 32, hi);
+                    }
                 }
                 fence_proxy_async_smem();  // generic-proxy writes before the tensor core reads them
                 __syncwarp();
