@@ -5,9 +5,11 @@
 // Operands travel as packed bits and are expanded on chip.  Per k-tile tk of
 // a work item the copy warp stages the 4 P tiles (ti0..ti0+3, tk) and the Q
 // block (tk, tj0..tj0+3) -- 4 KiB of bits, bulk copies completing on the
-// stage's mbarrier -- into one of kPkStages packed stages.  Eight expander
-// warps turn a packed stage into the MMA operands in one of kOpStages operand
-// stages: warp w < 4 writes P tile w as 0/1 bytes by rows (64 rows x 64 k)
+// stage's mbarrier -- into one of kPkStages packed stages.  Sixteen expander
+// warps in two groups of eight (group g takes the k-tiles of parity g, so a
+// warp has two k-tiles' time for each of its expansions) turn a packed stage
+// into the MMA operands in one of kOpStages operand stages: warp w < 4 of a
+// group writes P tile w as 0/1 bytes by rows (64 rows x 64 k)
 // in the canonical no-swizzle K-major layout (8-row x 16-byte core matrices,
 // K-adjacent core matrices 128 B apart, 8-row groups 512 B apart), warp
 // w >= 4 writes Q tile w-4 by its rows (k) in the MN-major layout (16 output
@@ -26,10 +28,11 @@
 // Work item (item list 2) = (product, group of 4 output tile-rows, block of 4
 // output tiles): a 256 x 256-bit output block over the whole inner dimension,
 // accumulated in TMEM as two 128 x 256 int32 matrices (all 512 TMEM columns;
-// one CTA per SM).  Epilogue (the 8 expander warps): tcgen05.ld 32x32b.x64
-// (warp w reads accumulator w/4, TMEM lanes 32*(w%4)..), threshold > 0, pack
-// 64 columns into a word, then the atomic-OR epilogue of the word-level
-// kernels (C, next delta D, occupancy, populations).
+// one CTA per SM).  Epilogue (the 16 expander warps): tcgen05.ld 32x32b.x32
+// (warp w reads accumulator (w/4)%2, TMEM lanes 32*(w%4).., output tiles
+// 2*(w/8) and 2*(w/8)+1 of the block), threshold > 0, pack 64 columns into a
+// word, then the atomic-OR epilogue of the word-level kernels (C, next delta
+// D, occupancy, populations).
 //
 // Arithmetic: 256*256*64 MACs per k-tile; bound = the tensor pipe's dense int8
 // rate.  Every wait is bounded; a wait that gives up raises the CTA's abort
@@ -42,7 +45,8 @@ namespace cfpq {
 
 namespace {
 
-constexpr int kExpWarps = 8;             // expanders, then the epilogue
+constexpr int kGroupWarps = 8;           // expanders of one k-tile: 4 P tiles, 4 Q tiles
+constexpr int kExpWarps = 2 * kGroupWarps;  // two groups (k-tile parity), then the epilogue
 constexpr int kCopyWarp = kExpWarps;     // lane 0 issues the bulk copies
 constexpr int kMmaWarp = kExpWarps + 1;  // lane 0 issues the MMAs
 constexpr int kThreads = 32 * (kExpWarps + 2);
@@ -71,7 +75,7 @@ struct __align__(1024) TcSmem {
     uint32_t tmem_base;
     uint32_t item;
     uint32_t abort;    // a role's wait gave up: every other wait ends too
-    uint32_t pk_seen;  // packed stages expander warp 0 saw land (sequence count)
+    uint32_t pk_seen[2];  // group g: 1 + the last packed stage its warp 0 saw land (sequence number)
     uint16_t cand[kMaxTiles];
     uint16_t cmask[kMaxTiles];
     uint16_t ktile[kMaxTiles];
@@ -110,22 +114,16 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-// 32 lanes x 64 consecutive 32-bit TMEM columns -> 64 registers.
-__device__ __forceinline__ void tmem_ld64(uint32_t taddr, uint32_t (&r)[64]) {
+// 32 lanes x 32 consecutive 32-bit TMEM columns -> 32 registers.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
     asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x64.b32 "
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
         "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,"
-        "%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47,"
-        "%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, [%64];"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
           "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
           "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]),
-          "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]),
-          "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]),
-          "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]),
-          "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
         : "r"(taddr));
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
@@ -187,15 +185,15 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (tid == 0) {
         for (uint32_t s = 0; s < kPkStages; ++s) {
             mbar_init(&S.pk_full[s], 1);
-            mbar_init(&S.pk_empty[s], kExpWarps);
+            mbar_init(&S.pk_empty[s], kGroupWarps);
         }
         for (uint32_t s = 0; s < kOpStages; ++s) {
-            mbar_init(&S.op_full[s], kExpWarps);
+            mbar_init(&S.op_full[s], kGroupWarps);
             mbar_init(&S.op_empty[s], 1);
         }
         mbar_init(&S.acc_full, 1);
         S.abort = 0;
-        S.pk_seen = 0;
+        S.pk_seen[0] = S.pk_seen[1] = 0;
         fence_mbar_init();
     }
     tc_fence_before();
@@ -335,18 +333,20 @@ __global__ void __launch_bounds__(kThreads, 1)
                 if (nk && !*abort) mma_commit(&S.acc_full);  // completes after every MMA of the item
             }
         } else {
-            // expander warp w: P tile w (w < 4) or Q tile w - 4 (by rows, no transpose)
-            const bool is_p = warp < 4;
-            const uint32_t g = is_p ? warp : warp - 4;
+            // expander warp w of group gp (k-tiles e with e % 2 == gp): P tile
+            // w (w < 4) or Q tile w - 4 (by rows, no transpose)
+            const uint32_t gp = warp / kGroupWarps, wr = warp % kGroupWarps;
+            const bool is_p = wr < 4;
+            const uint32_t g = is_p ? wr : wr - 4;
             const bool present = g < (is_p ? np : nq);
-            for (uint32_t e = 0; e < nk; ++e) {
+            for (uint32_t e = gp; e < nk; e += 2) {
                 const uint32_t q = seq + e, s = q % kPkStages, o = q % kOpStages;
                 // waits are warp-uniform: one lane giving up ends the whole warp's loop
                 if (!__all_sync(kFull, wait_or_abort(&S.pk_full[s], (q / kPkStages) & 1u, abort))) {
                     if (lane == 0) *abort = 1;
                     break;
                 }
-                if (warp == 0 && lane == 0) S.pk_seen = q + 1;
+                if (wr == 0 && lane == 0) S.pk_seen[q & 1u] = q + 1;
                 uint64_t lo = 0, hi = 0;
                 if (present) {
                     lo = S.pk[s][is_p ? g : 4 + g][lane];
@@ -383,17 +383,24 @@ __global__ void __launch_bounds__(kThreads, 1)
             if (!acc_ok && lane == 0) *abort = 1;
             tc_fence_after();
             if (acc_ok) {
-                uint32_t tile_new[4] = {0, 0, 0, 0};
-                const uint32_t h = warp >> 2, qq = warp & 3;
+                uint32_t tile_new[2] = {0, 0};
+                const uint32_t h = (warp >> 2) & 1u, qq = warp & 3, half = warp >> 3;
                 const uint32_t m = 128 * h + 32 * qq + lane;  // output row within the 256-row block
                 const uint32_t ti = ti0 + (m >> 6), r = m & 63;
 #pragma unroll 1
-                for (uint32_t jt = 0; jt < 4; ++jt) {
-                    uint32_t v[64];
-                    tmem_ld64(tmem + ((32 * qq) << 16) + h * 256 + jt * 64, v);
-                    uint64_t a = 0;
+                for (uint32_t jh = 0; jh < 2; ++jh) {
+                    const uint32_t jt = 2 * half + jh;
+                    uint32_t a32[2];
 #pragma unroll
-                    for (int c = 0; c < 64; ++c) a |= (uint64_t)(v[c] != 0) << c;
+                    for (int x = 0; x < 2; ++x) {
+                        uint32_t v[32];
+                        tmem_ld32(tmem + ((32 * qq) << 16) + h * 256 + jt * 64 + x * 32, v);
+                        uint32_t w = 0;
+#pragma unroll
+                        for (int c = 0; c < 32; ++c) w |= (uint32_t)(v[c] != 0) << c;
+                        a32[x] = w;
+                    }
+                    const uint64_t a = (uint64_t)a32[0] | ((uint64_t)a32[1] << 32);
                     const uint32_t tj = tj0 + jt;
                     uint32_t newcnt = 0;
                     if (a && ti < T && tj < T) {
@@ -413,15 +420,15 @@ __global__ void __launch_bounds__(kThreads, 1)
                             }
                         }
                     }
-                    tile_new[jt] = __reduce_add_sync(kFull, newcnt);  // the warp's 32 rows share (ti, tj)
+                    tile_new[jh] = __reduce_add_sync(kFull, newcnt);  // the warp's 32 rows share (ti, tj)
                 }
-                any_new = (tile_new[0] | tile_new[1] | tile_new[2] | tile_new[3]) != 0;
-                if (any_new && ti < T) {  // lane j: tile tj0 + j (populations, occupancy, buffer counters)
-                    const uint32_t mine = lane == 0 ? tile_new[0] : lane == 1 ? tile_new[1] : lane == 2 ? tile_new[2]
-                                        : lane == 3 ? tile_new[3] : 0u;
-                    tiles_gain(C, ti, tj0, mine, cnts ? cnts + 3 * pd.head : nullptr);
+                any_new = (tile_new[0] | tile_new[1]) != 0;
+                if (any_new && ti < T) {  // lane j: tile tj0 + 2 * half + j (populations, occupancy, counters)
+                    const uint32_t mine = lane == 0 ? tile_new[0] : lane == 1 ? tile_new[1] : 0u;
+                    tiles_gain(C, ti, tj0 + 2 * half, mine, cnts ? cnts + 3 * pd.head : nullptr);
                     if (D.bits)
-                        tiles_gain(D, ti, tj0, mine, cnts ? cnts + 3 * pd.head + 1 + ((iter & 1) ^ 1) : nullptr);
+                        tiles_gain(D, ti, tj0 + 2 * half, mine,
+                                   cnts ? cnts + 3 * pd.head + 1 + ((iter & 1) ^ 1) : nullptr);
                 }
             }
         }
@@ -442,9 +449,11 @@ __global__ void __launch_bounds__(kThreads, 1)
     const bool aborted = *abort != 0;
     if (aborted) {
         if (warp == kCopyWarp && lane == 0) {
-            // copies of the stages [pk_seen, pk_issued) may still be landing
-            for (uint32_t q = S.pk_seen; q < pk_issued; ++q)
-                mbar_wait_bounded(&S.pk_full[q % kPkStages], (q / kPkStages) & 1u);
+            // copies of the stages not seen by their group may still be
+            // landing (a stage is refilled only after its group saw it)
+            const uint32_t seen0 = S.pk_seen[0], seen1 = S.pk_seen[1];
+            for (uint32_t q = min(seen0, seen1); q < pk_issued; ++q)
+                if (q >= ((q & 1u) ? seen1 : seen0)) mbar_wait_bounded(&S.pk_full[q % kPkStages], (q / kPkStages) & 1u);
         }
         if (warp == kMmaWarp && lane == 0 && mma_committed) {
             // the last commit completes after every MMA issued before it
