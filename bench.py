@@ -687,24 +687,21 @@ def ours_arm(args, world, rank, local):
     launches = {"n": 0}
     device_ms: list[float] = []
 
+    dev_edges = (d_src.data_ptr(), d_lab.data_ptr(), d_dst.data_ptr())
+
     def step_value():
-        ctx.clear_many(q.mats)
-        ctx.load_edges_device(q.mats, d_src.data_ptr(), d_lab.data_ptr(), d_dst.data_ptr(), graph.nedges,
-                              q.off, q.lm)
-        for e in grammar.epsilon:
-            q.mats[e].set_diagonal()
-        st = ctx.closure(grammar.rules, q.mats, use_graph=not args.no_graph)
+        # cfpq_intersection: clear + edge scatter + epsilon diagonals +
+        # closure, enqueued back to back, one synchronisation
+        st, _ = ctx.intersection(grammar.rules, q.mats, *dev_edges, q.off, q.lm, epsilon=grammar.epsilon,
+                                 nedges=graph.nedges, use_graph=not args.no_graph, lines=False)
         launches["n"] += 2 + len(grammar.epsilon) + st["kernel_launches"]  # clear + edge scatter + closure
         device_ms.append(st["device_ms"])
         return st
 
     def step_e2e():
-        ctx.clear_many(q.mats)
-        ctx.load_edges(q.mats, h_src, h_lab, h_dst, q.off, q.lm)
-        for e in grammar.epsilon:
-            q.mats[e].set_diagonal()
-        # closure and result lines with one synchronisation (cfpq_closure_hash)
-        return ctx.closure_hash(grammar.rules, q.mats, use_graph=not args.no_graph)
+        # the same from pinned host edges, with the result lines copied back
+        return ctx.intersection(grammar.rules, q.mats, h_src, h_lab, h_dst, q.off, q.lm, epsilon=grammar.epsilon,
+                                use_graph=not args.no_graph, lines=True)
 
     def timed(fn, k):
         times, last = [], None

@@ -37,7 +37,7 @@ EXPORTED = (
     "cfpq_selector_weight_count", "cfpq_selector_set_weights", "cfpq_selector_get_weights", "cfpq_selector_train",
     "cfpq_selector_loss_grad", "cfpq_selector_predict", "cfpq_autotune", "cfpq_item_log", "cfpq_add_mul_rows",
     "cfpq_matrix_block_bytes", "cfpq_matrix_export_block", "cfpq_matrix_import_block", "cfpq_matrix_delta",
-    "cfpq_graph_load", "cfpq_edge_list_free", "cfpq_closure_hash",
+    "cfpq_graph_load", "cfpq_edge_list_free", "cfpq_closure_hash", "cfpq_intersection",
 )
 
 
@@ -54,6 +54,13 @@ class CfpqError(RuntimeError):
 
 class Rule(ctypes.Structure):
     _fields_ = [("head", ctypes.c_uint32), ("body1", ctypes.c_uint32), ("body2", ctypes.c_uint32)]
+
+
+class Edges(ctypes.Structure):
+    """cfpq_edges: a labelled graph for cfpq_intersection."""
+    _fields_ = [("from", ctypes.c_void_p), ("label", ctypes.c_void_p), ("to", ctypes.c_void_p),
+                ("count", ctypes.c_size_t), ("label_offsets", ctypes.c_void_p), ("label_mats", ctypes.c_void_p),
+                ("nlabels", ctypes.c_uint32), ("on_device", ctypes.c_int32)]
 
 
 class ClosureOpts(ctypes.Structure):
@@ -126,7 +133,7 @@ PRODUCT_RECORD_DTYPE = np.dtype([("iteration", np.uint32), ("query", np.uint32),
 
 class SelectorConfig(ctypes.Structure):
     _fields_ = [("mode", ctypes.c_int32), ("allowed", ctypes.c_uint32), ("tc_min_tiles", ctypes.c_uint32),
-                ("tc_min_occ", ctypes.c_float), ("tc_min_pop", ctypes.c_float), ("m4r_min_dense", ctypes.c_float),
+                ("tc_min_occ", ctypes.c_float), ("tc_min_dense", ctypes.c_float), ("m4r_min_dense", ctypes.c_float),
                 ("conf_margin", ctypes.c_float), ("range_margin", ctypes.c_float), ("min_tiles", ctypes.c_uint32)]
 
     def as_dict(self) -> dict:
@@ -228,6 +235,8 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "cfpq_graph_load": ([ctypes.c_char_p, i32, P(P(EdgeList))], i32),
         "cfpq_closure_hash": ([vp, P(Rule), sz, P(vp), sz, P(ClosureOpts), P(ClosureStats), P(u64), P(u64)], i32),
         "cfpq_edge_list_free": ([P(EdgeList)], None),
+        "cfpq_intersection": ([vp, P(Rule), sz, P(vp), sz, P(Edges), P(u32), sz, P(ClosureOpts), P(ClosureStats),
+                               P(u64), P(u64)], i32),
     }
     for name, (args, res) in sigs.items():
         f = getattr(lib, name)
@@ -474,6 +483,46 @@ class Context:
         _check(self.lib, self.lib.cfpq_closure_hash(self.handle, rs, len(rules), hs, len(mats), ctypes.byref(o),
                                                     ctypes.byref(st), hh, cc))
         return st.as_dict(), [(int(hh[i]), int(cc[i])) for i in range(len(mats))]
+
+    def intersection(self, rules: Sequence[tuple[int, int, int]], mats: Sequence[Matrix], src, label, dst,
+                     label_offsets: np.ndarray, label_mats: np.ndarray, epsilon: Sequence[int] = (),
+                     nedges: int | None = None, variant="auto", use_graph: bool = True, lines: bool = True):
+        """One whole query with one synchronisation (cfpq_intersection): clear
+        mats, scatter the edges, set the epsilon diagonals, close, and (lines)
+        the result line (hash, count) of every matrix.  src/label/dst: uint32
+        host arrays, or device pointers as ints (nedges then required).
+        Returns (stats, lines or None).  The ctypes arguments of the last call
+        are kept (keyed on the arrays' addresses), like closure()."""
+        on_device = isinstance(src, int)
+        if on_device:
+            if nedges is None:
+                raise ValueError("nedges is required with device pointers")
+            ptrs, keep = (src, label, dst), ()
+        else:
+            keep = tuple(np.ascontiguousarray(a, dtype=np.uint32) for a in (src, label, dst))
+            ptrs, nedges = tuple(a.ctypes.data for a in keep), keep[0].size
+        key = (tuple(map(tuple, rules)), tuple(m.handle for m in mats), ptrs, int(nedges),
+               tuple(np.asarray(label_offsets).tolist()), tuple(np.asarray(label_mats).tolist()), tuple(epsilon),
+               variant, use_graph, lines)
+        args = self._isect_args if getattr(self, "_isect_args", None) and self._isect_args[0] == key else None
+        if args is None:
+            rs = (Rule * max(len(rules), 1))(*[Rule(*map(int, r)) for r in rules])
+            hs = (ctypes.c_void_p * max(len(mats), 1))(*[m.handle for m in mats])
+            off = np.ascontiguousarray(label_offsets, dtype=np.uint32)
+            lm = np.ascontiguousarray(label_mats, dtype=np.uint32)
+            if lm.size == 0:
+                lm = np.zeros(1, dtype=np.uint32)
+            e = Edges(ptrs[0], ptrs[1], ptrs[2], int(nedges), off.ctypes.data, lm.ctypes.data, off.size - 1,
+                      1 if on_device else 0)
+            eps = (ctypes.c_uint32 * max(len(epsilon), 1))(*[int(x) for x in epsilon])
+            o = self._opts("engine", variant, use_graph, 0, 0)
+            hh = (ctypes.c_uint64 * max(len(mats), 1))() if lines else None
+            cc = (ctypes.c_uint64 * max(len(mats), 1))() if lines else None
+            args = self._isect_args = (key, rs, hs, e, eps, o, ClosureStats(), hh, cc, (keep, off, lm))
+        _, rs, hs, e, eps, o, st, hh, cc, _ = args
+        _check(self.lib, self.lib.cfpq_intersection(self.handle, rs, len(rules), hs, len(mats), ctypes.byref(e),
+                                                    eps, len(epsilon), ctypes.byref(o), ctypes.byref(st), hh, cc))
+        return st.as_dict(), ([(int(hh[i]), int(cc[i])) for i in range(len(mats))] if lines else None)
 
     def closure_batch(self, queries: Sequence[tuple[Sequence[tuple[int, int, int]], Sequence[Matrix]]],
                       variant="auto", use_graph: bool = True, max_iterations: int = 0, log_products: int = 0):

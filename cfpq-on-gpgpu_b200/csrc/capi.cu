@@ -487,7 +487,8 @@ static int load_edges_impl(cfpq_ctx *ctx, cfpq_matrix *const *mats, size_t nmats
         CUDA_TRY(cudaMemcpyAsync(d_to, to, be, cudaMemcpyHostToDevice, ctx->stream));
     }
     CUDA_TRY(cudaMemsetAsync(ctx->d_bad, 0, 4, ctx->stream));
-    CUDA_TRY(launch_load_edges(d_desc, d_from, d_label, d_to, nedges, d_off, d_lm, nlabels, ctx->d_bad, ctx->stream));
+    CUDA_TRY(launch_load_edges(d_desc, (uint32_t)nmats, d_from, d_label, d_to, nedges, d_off, d_lm, nlabels, nlm,
+                               ctx->d_bad, ctx->stream));
     return CFPQ_OK;
 }
 
@@ -1285,14 +1286,13 @@ static int run_logged_iterations(cfpq_ctx *ctx, const ClosurePlan &pl, const Que
                                ctx->d_sel.as<SelectorParams>(), ctx->choice.as<uint8_t>(), ctx->tc_ok.as<uint8_t>(),
                                ctx->sel_log.as<SelLogRow>(), ctx->sel_log_iters, s));
         if (!pl.auto_select) CUDA_TRY(launch_fill_choice(ctx->choice.as<uint8_t>(), np, pl.fixed_variant, s));
-        // the real work
-        CUDA_TRY(launch_plan(ctx->prods.as<ProdDesc>(), np, 0, pl.prod_rows, ctx->slots.as<MatSlot>(), ctx->d_st,
-                             ctx->items.as<uint64_t>(), pl.item_cap, tpb, ctx->prod_seen.as<uint32_t>(), 0,
-                             ctx->choice.as<uint8_t>(), s));
-        TRY(enqueue_products(ctx, pl, qt, s));
-        CUDA_TRY(launch_reset_list(ctx->d_st, 0, s));
-        CUDA_TRY(launch_reset_list(ctx->d_st, 1, s));
-        // every term alone with every candidate variant
+        uint8_t *const kept = ctx->choice.as<uint8_t>() + np;
+        CUDA_TRY(cudaMemcpyAsync(kept, ctx->choice.p, np, cudaMemcpyDeviceToDevice, s));
+        // every term alone with every candidate variant, first, so that the
+        // timings see the operands the selection saw (plus what the terms
+        // timed before them added, as in a sequential pass); the candidates
+        // are real products of this iteration: their new bits go to the
+        // heads and the deltas like any other
         std::vector<std::pair<uint32_t, int>> timed;  // (product, variant)
         size_t ev = 0;
         for (uint32_t p = 0; p < np; ++p) {
@@ -1318,6 +1318,15 @@ static int run_logged_iterations(cfpq_ctx *ctx, const ClosurePlan &pl, const Que
                 timed.push_back({p, v});
             }
         }
+        // then the iteration with the selector's choices (it finds little
+        // new: the candidates did the same products)
+        CUDA_TRY(cudaMemcpyAsync(ctx->choice.p, kept, np, cudaMemcpyDeviceToDevice, s));
+        CUDA_TRY(launch_plan(ctx->prods.as<ProdDesc>(), np, 0, pl.prod_rows, ctx->slots.as<MatSlot>(), ctx->d_st,
+                             ctx->items.as<uint64_t>(), pl.item_cap, tpb, ctx->prod_seen.as<uint32_t>(), 0,
+                             ctx->choice.as<uint8_t>(), s));
+        TRY(enqueue_products(ctx, pl, qt, s));
+        CUDA_TRY(launch_reset_list(ctx->d_st, 0, s));
+        CUDA_TRY(launch_reset_list(ctx->d_st, 1, s));
         CUDA_TRY(launch_advance_end(ctx->slots.as<MatSlot>(), (uint32_t)pl.slots.size(), pl.slot_rows, ctx->d_st, qt, 0,
                                     0, ctx->cnts.as<BufCounters>(), s));
         CUDA_TRY(cudaMemcpyAsync(ctx->h_st, ctx->d_st, sizeof(IterState), cudaMemcpyDeviceToHost, s));
@@ -1361,6 +1370,8 @@ struct HashOut {
     cfpq_matrix *const *mats;
     size_t n;
     uint64_t *hashes, *counts;
+    const uint32_t *flag_src;  // non-null: one device word read back with the same synchronisation
+    uint32_t *flag_dst;        // (pinned host)
 };
 
 static void fill_hash_out(const cfpq_ctx *ctx, const HashOut *ho) {
@@ -1397,8 +1408,10 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
             if (iters_out) iters_out[q] = 0;
             if (done_ms_out) done_ms_out[q] = 0;
         }
-        if (ho && ho->n) {
-            TRY(enqueue_hash_many(ctx, ho->mats, ho->n));
+        if (ho && ho->n) TRY(enqueue_hash_many(ctx, ho->mats, ho->n));
+        if (ho && ho->flag_src)
+            CUDA_TRY(cudaMemcpyAsync(ho->flag_dst, ho->flag_src, 4, cudaMemcpyDeviceToHost, ctx->stream));
+        if (ho) {
             TRY(sync_and_check(ctx));
             fill_hash_out(ctx, ho);
         }
@@ -1424,7 +1437,7 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
     const size_t list_words = 3 * pl.item_cap * 2;
     const bool lists_clean = ctx->items_clean_ptr == ctx->items.p && ctx->items_clean_words >= list_words;
     ctx->items_clean_words = 0;
-    TRY(ctx->choice.ensure(nprods));
+    TRY(ctx->choice.ensure(2 * (size_t)nprods));  // choices, then a copy kept by the product log
     TRY(ctx->tc_ok.ensure(nprods));
     TRY(ctx->cnts.ensure((size_t)nslots * 3 * sizeof(BufCounters)));
     ctx->cnts_on = pl.auto_select || log_products;
@@ -1563,6 +1576,8 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
         CUDA_TRY(cudaMemcpyAsync(h_last, qt.last_iter, nq * 4, cudaMemcpyDeviceToHost, ctx->stream));
     }
     if (ho && ho->n) TRY(enqueue_hash_many(ctx, ho->mats, ho->n));
+    if (ho && ho->flag_src)
+        CUDA_TRY(cudaMemcpyAsync(ho->flag_dst, ho->flag_src, 4, cudaMemcpyDeviceToHost, ctx->stream));
     CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     float ms = 0;
     CUDA_TRY(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
@@ -1756,8 +1771,56 @@ extern "C" int cfpq_closure_hash(cfpq_ctx *ctx, const cfpq_rule *rules, size_t n
         o.variant != CFPQ_VARIANT_TC)
         return set_error(CFPQ_ERR_UNSUPPORTED, "variant %d is not available in the engine driver", o.variant);
     std::vector<QueryIn> qs{QueryIn{rules, nrules, mats, nmats}};
-    HashOut ho{mats, nmats, hashes, counts};
+    HashOut ho{mats, nmats, hashes, counts, nullptr, nullptr};
     return run_engine(ctx, qs, o, stats, nullptr, nullptr, &ho);
+}
+
+// Slot of the context's pinned flag block that receives the edge scatter's
+// out-of-range count in cfpq_intersection (slot 0 belongs to the
+// synchronous flag reads).
+constexpr int kIntersectBadSlot = 8;
+
+extern "C" int cfpq_intersection(cfpq_ctx *ctx, const cfpq_rule *rules, size_t nrules, cfpq_matrix *const *mats,
+                                 size_t nmats, const cfpq_edges *edges, const uint32_t *epsilon, size_t nepsilon,
+                                 const cfpq_closure_opts *opts, cfpq_closure_stats *stats, uint64_t *hashes,
+                                 uint64_t *counts) {
+    TRY(use_device(ctx));
+    if (!edges) return set_error(CFPQ_ERR_INVALID, "null edge list");
+    if (nepsilon && !epsilon) return set_error(CFPQ_ERR_INVALID, "null epsilon list");
+    if (nmats && !mats) return set_error(CFPQ_ERR_INVALID, "null matrix list");
+    const bool want_lines = hashes != nullptr || counts != nullptr;
+    if (want_lines && (!hashes || !counts)) return set_error(CFPQ_ERR_INVALID, "hashes and counts go together");
+    for (size_t i = 0; i < nepsilon; ++i)
+        if (epsilon[i] >= nmats || !mats[epsilon[i]])
+            return set_error(CFPQ_ERR_INVALID, "epsilon[%zu] = %u is not a matrix of the query", i, epsilon[i]);
+    const cfpq_closure_opts o = opts ? *opts : default_opts();
+    // input: clear, scatter, diagonals (asynchronous); the scatter's
+    // out-of-range count travels back with the closure's own read-back
+    TRY(cfpq_matrices_clear(ctx, mats, nmats));
+    uint32_t *const h_bad = ctx->h_flag + kIntersectBadSlot;
+    *h_bad = 0;
+    const bool scatter = edges->count && edges->nlabels;
+    if (scatter)
+        TRY(load_edges_impl(ctx, mats, nmats, edges->from, edges->label, edges->to, edges->count,
+                            edges->label_offsets, edges->label_mats, edges->nlabels, edges->on_device != 0));
+    for (size_t i = 0; i < nepsilon; ++i) CUDA_TRY(launch_set_diag(mats[epsilon[i]]->d, ctx->stream));
+    // closure (+ result lines); the engine reads the scatter's count back
+    // with its own final read-back, the other drivers synchronise on the way
+    const bool engine = o.driver == CFPQ_DRIVER_ENGINE &&
+                        (o.variant == CFPQ_VARIANT_AUTO || o.variant == CFPQ_VARIANT_LOP3 ||
+                         o.variant == CFPQ_VARIANT_M4R || (o.variant == CFPQ_VARIANT_TC && ctx->tc_grid));
+    if (engine) {
+        std::vector<QueryIn> qs{QueryIn{rules, nrules, mats, nmats}};
+        HashOut ho{mats, want_lines ? nmats : 0, hashes, counts, scatter ? ctx->d_bad : nullptr, h_bad};
+        TRY(run_engine(ctx, qs, o, stats, nullptr, nullptr, &ho));
+    } else {
+        if (scatter) CUDA_TRY(cudaMemcpyAsync(h_bad, ctx->d_bad, 4, cudaMemcpyDeviceToHost, ctx->stream));
+        TRY(cfpq_closure(ctx, rules, nrules, mats, nmats, &o, stats));
+        if (want_lines) TRY(cfpq_hash_count_many(ctx, mats, nmats, hashes, counts));
+        else TRY(sync_and_check(ctx));
+    }
+    if (*h_bad) return set_error(CFPQ_ERR_INVALID, "cfpq_intersection: %u edge coordinates out of range", *h_bad);
+    return CFPQ_OK;
 }
 
 extern "C" int cfpq_closure_batch(cfpq_ctx *ctx, const cfpq_query *queries, size_t nqueries,

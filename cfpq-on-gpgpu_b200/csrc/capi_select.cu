@@ -10,12 +10,13 @@ void selector_defaults(SelectorParams *sp) {
     memset(sp, 0, sizeof(*sp));
     sp->mode = CFPQ_SELECT_HEURISTIC;
     sp->allowed = (1u << CFPQ_VARIANT_LOP3) | (1u << CFPQ_VARIANT_M4R) | (1u << CFPQ_VARIANT_TC);
-    // Until cfpq_autotune runs: tensor cores for n >= 16384 with most tiles
-    // occupied and populated above a quarter; Four Russians when most P tiles
-    // are dense.
+    // Until cfpq_autotune runs: tensor cores for n >= 16384 when a fifth of
+    // the P tiles are occupied and 30% of them dense (fit to the exhaustive
+    // per-term timings of a chain closure at n = 32768); Four Russians when
+    // a quarter of the P tiles are dense.
     sp->tc_min_tiles = 256;
-    sp->tc_min_occ = 0.5f;
-    sp->tc_min_pop = 0.25f;
+    sp->tc_min_occ = 0.2f;
+    sp->tc_min_dense = 0.3f;
     sp->m4r_min_dense = 0.25f;
     sp->conf_margin = 0.05f;
     sp->range_margin = 0.1f;
@@ -56,7 +57,7 @@ extern "C" int cfpq_selector_configure(cfpq_ctx *ctx, const cfpq_selector_config
     sp.allowed = cfg->allowed & (ctx->tc_grid ? ~0u : ~(1u << CFPQ_VARIANT_TC));
     sp.tc_min_tiles = std::max<uint32_t>(cfg->tc_min_tiles, 1);
     sp.tc_min_occ = cfg->tc_min_occ;
-    sp.tc_min_pop = cfg->tc_min_pop;
+    sp.tc_min_dense = cfg->tc_min_dense;
     sp.m4r_min_dense = cfg->m4r_min_dense;
     sp.conf_margin = cfg->conf_margin;
     sp.range_margin = cfg->range_margin;
@@ -72,7 +73,7 @@ extern "C" int cfpq_selector_get_config(cfpq_ctx *ctx, cfpq_selector_config *cfg
     cfg->allowed = sp.allowed;
     cfg->tc_min_tiles = sp.tc_min_tiles;
     cfg->tc_min_occ = sp.tc_min_occ;
-    cfg->tc_min_pop = sp.tc_min_pop;
+    cfg->tc_min_dense = sp.tc_min_dense;
     cfg->m4r_min_dense = sp.m4r_min_dense;
     cfg->conf_margin = sp.conf_margin;
     cfg->range_margin = sp.range_margin;
@@ -354,25 +355,26 @@ extern "C" int cfpq_autotune(cfpq_ctx *ctx, const cfpq_autotune_opts *opts, cfpq
                 m4r_wins = m4r_wins && T(si, di, 1) > 0 && T(si, di, 1) < T(si, di, 0);
             }
     sp.m4r_min_dense = (any_dense && m4r_wins) ? 0.25f : 1.5f;
-    // tensor cores: the smallest density from which TC beats both word-level
-    // variants at every larger density, per size; the smallest such size sets
-    // tc_min_tiles, its crossover tc_min_pop
-    sp.tc_min_pop = 2.f;  // never, unless a size shows a crossover
+    // tensor cores: the smallest size at which TC beats both word-level
+    // variants at every density whose tiles are dense sets tc_min_tiles (the
+    // rule then takes TC where most P tiles are dense); no such size: never
+    sp.tc_min_dense = 2.f;
     bool found = false;
     for (size_t si = 0; si < o.nsizes && ctx->tc_grid; ++si) {
-        int from = -1;
-        for (int di = (int)o.ndensities - 1; di >= 0; --di) {
+        bool wins = false;
+        for (size_t di = 0; di < o.ndensities; ++di) {
+            if (o.densities[di] * 4096.f <= (float)kDenseTilePop) continue;
             const float tc = T(si, di, 2), w = std::min(T(si, di, 0), T(si, di, 1) > 0 ? T(si, di, 1) : 1e30f);
-            if (tc > 0 && tc < w) from = di;
-            else break;
+            wins = tc > 0 && tc < w;
+            if (!wins) break;
         }
-        if (from >= 0 && (!found || o.sizes[si] / 64 < sp.tc_min_tiles)) {
+        if (wins && (!found || (o.sizes[si] + 63) / 64 < sp.tc_min_tiles)) {
             sp.tc_min_tiles = std::max<uint32_t>(1, (o.sizes[si] + 63) / 64);
-            sp.tc_min_pop = o.densities[from];
+            sp.tc_min_dense = 0.3f;
             found = true;
         }
     }
-    sp.tc_min_occ = 0.5f;
+    sp.tc_min_occ = 0.2f;
     if (sp.mode == CFPQ_SELECT_FIXED) sp.mode = CFPQ_SELECT_HEURISTIC;
     ctx->sel_dirty = true;
     if (result) TRY(cfpq_selector_get_config(ctx, result));

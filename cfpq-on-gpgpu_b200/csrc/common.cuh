@@ -74,10 +74,12 @@ struct IterState {
     uint32_t nqueries;
     uint32_t blocks_done;   // blocks of the advance kernel that finished (the last one ends the iteration)
     // persistent closure kernel: per-parity iteration counters
-    uint32_t pitem_count[2][2];  // [iteration parity][list]
-    uint32_t pitem_m4r[2];       // Four Russians items among pitem_count[.][0]
+    uint32_t pitem_m4r[2];       // Four Russians items among the items counted in pplan[.]
     // polled by every CTA of the persistent kernel: own cache lines
-    alignas(128) uint32_t plan_done[2];  // CTAs done with the plan/clear units of the iteration (per parity)
+    // plan word of the iterations of parity p: the low 32 bits count the work
+    // items written (the planners' item_count[0]), the high 32 bits the CTAs
+    // done with their plan/clear units; one load returns both
+    alignas(128) unsigned long long pplan[2];
     alignas(128) uint32_t pitem_next[2][2];
     // grid barrier of the iterations of parity p: low 32 bits count the CTAs'
     // arrivals (cumulative over the closure), high 32 bits are the
@@ -125,7 +127,7 @@ struct SelectorParams {
     int32_t mode;           // 0 fixed, 1 heuristic, 2 MLP with heuristic fallback
     uint32_t allowed;       // bit v: variant v may be chosen
     uint32_t tc_min_tiles;  // tensor cores only for products with T >= tc_min_tiles
-    float tc_min_occ, tc_min_pop, m4r_min_dense;
+    float tc_min_occ, tc_min_dense, m4r_min_dense;
     float conf_margin, range_margin;
     uint32_t min_tiles;     // closures whose largest term has fewer tile-rows run LOP3 throughout
     int32_t has_weights;
@@ -356,22 +358,30 @@ __device__ __forceinline__ void tiles_gain(const DevMat &m, uint32_t ti, uint32_
 
 // One warp: clear tile-row ti of D -- zero every occupied tile and its
 // population, then the occupancy row (tiles without an occupancy bit hold no
-// bit and have population 0).
+// bit and have population 0).  The occupancy words come 32 at a time, one per
+// lane, so a row costs one load round trip; the zeroing stores are not
+// waited for.
 __device__ __forceinline__ void clear_tile_row(const DevMat &D, uint32_t ti) {
     const uint32_t lane = threadIdx.x & 31;
     uint32_t *orow = D.occ + (size_t)ti * D.ow;
-    for (uint32_t w = 0; w < D.ow; ++w) {
-        uint32_t bits = orow[w];
-        while (bits) {
-            const uint32_t tj = w * 32 + (__ffs(bits) - 1);
-            bits &= bits - 1;
-            uint4 *tile = reinterpret_cast<uint4 *>(D.bits + tile_offset(D.T, ti, tj));
-            tile[lane] = make_uint4(0, 0, 0, 0);
-            if (lane == 0) D.nnz[(size_t)ti * D.T + tj] = 0;
+    for (uint32_t base = 0; base < D.ow; base += 32) {
+        const uint32_t mine = base + lane < D.ow ? orow[base + lane] : 0u;
+        unsigned todo = __ballot_sync(0xffffffffu, mine != 0);
+        while (todo) {
+            const uint32_t src = __ffs(todo) - 1;
+            todo &= todo - 1;
+            uint32_t bits = __shfl_sync(0xffffffffu, mine, src);
+            while (bits) {
+                const uint32_t tj = (base + src) * 32 + (__ffs(bits) - 1);
+                bits &= bits - 1;
+                uint4 *tile = reinterpret_cast<uint4 *>(D.bits + tile_offset(D.T, ti, tj));
+                tile[lane] = make_uint4(0, 0, 0, 0);
+                if (lane == 0) D.nnz[(size_t)ti * D.T + tj] = 0;
+            }
         }
+        __syncwarp();
+        if (mine) orow[base + lane] = 0;
     }
-    __syncwarp();
-    for (uint32_t w = lane; w < D.ow; w += 32) orow[w] = 0;
 }
 
 // One warp: clear tile-row `row` (over all slots, slot tile-rows in order) of

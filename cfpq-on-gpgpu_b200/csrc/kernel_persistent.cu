@@ -17,11 +17,12 @@
 //            deltas of the others are empty): every CTA compacts the
 //            per-query changed flags into its own active lists first, so
 //            converged queries cost nothing in the tail of a batch.  The CTA
-//            then counts itself in plan_done[par].
+//            then counts itself in the plan word pplan[par] (high half;
+//            the low half counts the items written).
 //   products the CTA takes items from the list as soon as they are written
 //            (no barrier after the plan) and runs tiled::process_item; an
 //            item merges its results only once every CTA is done planning
-//            and clearing (plan_done[par] == grid).  New bits set
+//            and clearing (plan-done half == grid).  New bits set
 //            changed[par] and the query's flag in qt.changed[t % 3] (three
 //            rotating flag arrays: iteration t reads those of t-1 and t-2;
 //            CTA 0 zeroes those of t+1 after the barrier of t).
@@ -276,16 +277,19 @@ __global__ void __launch_bounds__(kThreads, 2) k_closure_persistent(PersistArgs 
             if (t > iter0 + 1) reinterpret_cast<uint32_t *>(&st->pbar[par])[1] = 0;
             if (t > iter0) {  // counters of iteration t-1 -> statistics, then reset for iteration t+1
                 const uint32_t q = par ^ 1;
-                const uint32_t c0 = st->pitem_count[q][0], m4r = st->pitem_m4r[q];
+                const uint32_t c0 = (uint32_t)st->pplan[q], m4r = st->pitem_m4r[q];
                 st->items_total += c0;
                 st->items_by_variant[2] += c0 - m4r;
                 st->items_by_variant[3] += m4r;
-                st->pitem_count[q][0] = st->pitem_count[q][1] = 0;
+                st->pplan[q] = 0;
                 st->pitem_next[q][0] = st->pitem_next[q][1] = 0;
-                st->plan_done[q] = 0;
                 st->pitem_m4r[q] = 0;
             }
         }
+        // plan word halves: the planners' item count (list 0: every
+        // word-level item, Four Russians ones marked) and the plan-done count
+        uint32_t *const item_count = reinterpret_cast<uint32_t *>(&st->pplan[par]);
+        uint32_t *const plan_done = item_count + 1;
         // ---- plan of iteration t + clear of the delta read in t-1 ----
         const unsigned long long plan_t0 = a.trace && tid == 0 ? globaltimer_ns() : 0ull;
         if (a.cnts && blockIdx.x == 0 && t > 0)  // that delta's counters restart at zero
@@ -304,7 +308,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_closure_persistent(PersistArgs 
                     const uint32_t i = active_find(X.act_plan, u);
                     const QueryRange qr = a.qr[X.act_plan.q[i]];
                     plan::plan_row(qr.prow0 + (u - X.act_plan.pref[i]), prods, a.nprods, slots, t, st,
-                                   st->pitem_count[par], items, a.list_cap, a.tpb, a.prod_seen, 0, psel,
+                                   item_count, items, a.list_cap, a.tpb, a.prod_seen, 0, psel,
                                    X.plan[warp].cnt, X.plan[warp].bnd, qr.prod0, qr.prod0 + qr.nprod,
                                    &st->pitem_m4r[par]);
                 } else {
@@ -320,7 +324,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_closure_persistent(PersistArgs 
             const uint32_t units = a.prod_rows + clear_rows;
             for (uint32_t u = gwarp; u < units; u += nwarps) {
                 if (u < a.prod_rows) {
-                    plan::plan_row(u, prods, a.nprods, slots, t, st, st->pitem_count[par], items, a.list_cap, a.tpb,
+                    plan::plan_row(u, prods, a.nprods, slots, t, st, item_count, items, a.list_cap, a.tpb,
                                    a.prod_seen, 0, psel, X.plan[warp].cnt, X.plan[warp].bnd, 0u, 0xFFFFFFFFu,
                                    &st->pitem_m4r[par]);
                 } else {
@@ -332,7 +336,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_closure_persistent(PersistArgs 
         fence_proxy_async_smem();  // the scratch writes come before the next bulk copies into the same bytes
         __syncthreads();
         if (tid == 0) {  // this CTA's items, clears and counter resets are all published
-            red_add_release_u32(&st->plan_done[par], 1u);
+            red_add_release_u32(plan_done, 1u);
             if (blockIdx.x == 0 && a.phase_log && t - iter0 < a.phase_log_iters)
                 a.phase_log[3 * (t - iter0) + 1] = globaltimer_ns();
             if (a.trace) trace_item(a, 0, t, 2, plan_t0);
@@ -347,7 +351,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_closure_persistent(PersistArgs 
         // CTA's delta clear (the gate before the epilogue).
         uint32_t *const qchanged = a.qt.changed ? a.qt.changed + (t % 3) * st->nqueries : nullptr;
         uint32_t *const changed = reinterpret_cast<uint32_t *>(&st->pbar[par]) + 1;  // kBarChanged
-        const uint32_t *gate = &st->plan_done[par];  // cleared by the first item that passes it
+        const uint32_t *gate = plan_done;  // cleared by the first item that passes it
         uint32_t next_idx = kNoIndex;  // (thread 0) list index taken ahead
         while (!timed_out) {
             if (tid == 0) {
@@ -357,12 +361,19 @@ __global__ void __launch_bounds__(kThreads, 2) k_closure_persistent(PersistArgs 
                 unsigned long long v = 0;
                 uint32_t stop = 0, spins = 0;
                 for (;;) {
-                    if (idx < a.list_cap && (v = *slot) != 0) break;
-                    if (ld_acquire_u32(&st->plan_done[par]) == gridDim.x) {
-                        if (idx >= *reinterpret_cast<volatile uint32_t *>(&st->pitem_count[par][0])) {
+                    // the slot and the plan word load together (one round
+                    // trip); a slot read empty is read again once the plan
+                    // word (acquire) says that every planner is done and the
+                    // item exists
+                    v = idx < a.list_cap ? *slot : 0ull;
+                    const unsigned long long pw = ld_acquire_u64(&st->pplan[par]);
+                    if (v) break;
+                    if ((uint32_t)(pw >> 32) == gridDim.x) {
+                        if (idx >= (uint32_t)pw) {
                             stop = 1;
                             break;
                         }
+                        if (idx < a.list_cap && (v = *slot) != 0) break;
                     }
                     if (++spins > a.spin_limit) {
                         stop = 2;
@@ -469,7 +480,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_closure_persistent(PersistArgs 
     if (tid == 0 && timed_out) atomicExch(&st->error, (uint32_t)5);
     if (blockIdx.x == 0 && tid == 0 && !timed_out) {
         const uint32_t par = t & 1;
-        const uint32_t c0 = st->pitem_count[par][0], m4r = st->pitem_m4r[par];
+        const uint32_t c0 = (uint32_t)st->pplan[par], m4r = st->pitem_m4r[par];
         st->items_total += c0;
         st->items_by_variant[2] += c0 - m4r;
         st->items_by_variant[3] += m4r;

@@ -64,21 +64,52 @@ __global__ void k_set_bits(DevMat m, const uint32_t *__restrict__ rows, const ui
 
 // Edge scatter: edge e sets (from, to) in every matrix its label derives
 // (cfpq-cpp/Grammar.h:41-45).
-__global__ void k_load_edges(const DevMat *__restrict__ mats, const uint32_t *__restrict__ from,
+// Edge scatter.  The label -> matrices tables and the matrix descriptors
+// (kLoadTableBytes at most) are copied into shared memory while the block's
+// first edges load, so an edge waits only for its vertex order entries and
+// its bit's atomic; larger tables are read from global memory.
+constexpr uint32_t kLoadTableBytes = 12288;
+
+template <bool kSmem>
+__global__ void k_load_edges(const DevMat *__restrict__ mats, uint32_t nmats, const uint32_t *__restrict__ from,
                              const uint32_t *__restrict__ label, const uint32_t *__restrict__ to, size_t ne,
                              const uint32_t *__restrict__ off, const uint32_t *__restrict__ lm, uint32_t nlabels,
-                             uint32_t *bad) {
-    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < ne; e += (size_t)gridDim.x * blockDim.x) {
-        const uint32_t l = label[e];
-        if (l >= nlabels) continue;
-        const uint32_t r = from[e], c = to[e];
-        for (uint32_t j = off[l]; j < off[l + 1]; ++j) {
-            const DevMat m = mats[lm[j]];
-            if (r >= m.n || c >= m.n) {
-                atomicAdd(bad, 1u);
-                continue;
+                             uint32_t nlm, uint32_t *bad) {
+    extern __shared__ __align__(16) unsigned char load_smem[];
+    if constexpr (kSmem) {
+        DevMat *sm = reinterpret_cast<DevMat *>(load_smem);
+        uint32_t *so = reinterpret_cast<uint32_t *>(sm + nmats), *sl = so + nlabels + 1;
+        for (uint32_t i = threadIdx.x; i < nmats; i += blockDim.x) sm[i] = mats[i];
+        for (uint32_t i = threadIdx.x; i <= nlabels; i += blockDim.x) so[i] = off[i];
+        for (uint32_t i = threadIdx.x; i < nlm; i += blockDim.x) sl[i] = lm[i];
+        mats = sm;
+        off = so;
+        lm = sl;
+    }
+    size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    uint32_t l = 0, r = 0, c = 0;
+    if (e < ne) {  // the first edge's loads overlap the table copies
+        l = label[e];
+        r = from[e];
+        c = to[e];
+    }
+    if constexpr (kSmem) __syncthreads();
+    for (; e < ne; e += (size_t)gridDim.x * blockDim.x) {
+        if (l < nlabels) {
+            for (uint32_t j = off[l]; j < off[l + 1]; ++j) {
+                const DevMat m = mats[lm[j]];
+                if (r >= m.n || c >= m.n) {
+                    atomicAdd(bad, 1u);
+                    continue;
+                }
+                set_one_bit(m, r, c);
             }
-            set_one_bit(m, r, c);
+        }
+        const size_t e2 = e + (size_t)gridDim.x * blockDim.x;
+        if (e2 < ne) {
+            l = label[e2];
+            r = from[e2];
+            c = to[e2];
         }
     }
 }
@@ -431,12 +462,17 @@ cudaError_t launch_set_bits(const DevMat &m, const uint32_t *d_rows, const uint3
     return cudaGetLastError();
 }
 
-cudaError_t launch_load_edges(const DevMat *d_mats, const uint32_t *d_from, const uint32_t *d_label,
+cudaError_t launch_load_edges(const DevMat *d_mats, uint32_t nmats, const uint32_t *d_from, const uint32_t *d_label,
                               const uint32_t *d_to, size_t ne, const uint32_t *d_off, const uint32_t *d_lm,
-                              uint32_t nlabels, uint32_t *d_bad, cudaStream_t s) {
+                              uint32_t nlabels, uint32_t nlm, uint32_t *d_bad, cudaStream_t s) {
     if (ne == 0) return cudaSuccess;
-    k_load_edges<<<capped_grid(ne, 256, 65535u * 16), 256, 0, s>>>(d_mats, d_from, d_label, d_to, ne, d_off, d_lm,
-                                                                   nlabels, d_bad);
+    const size_t tb = (size_t)nmats * sizeof(DevMat) + ((size_t)nlabels + 1 + nlm) * 4;
+    if (tb <= kLoadTableBytes)
+        k_load_edges<true><<<capped_grid(ne, 256, 65535u * 16), 256, tb, s>>>(d_mats, nmats, d_from, d_label, d_to, ne,
+                                                                            d_off, d_lm, nlabels, nlm, d_bad);
+    else
+        k_load_edges<false><<<capped_grid(ne, 256, 65535u * 16), 256, 0, s>>>(d_mats, nmats, d_from, d_label, d_to,
+                                                                            ne, d_off, d_lm, nlabels, nlm, d_bad);
     return cudaGetLastError();
 }
 

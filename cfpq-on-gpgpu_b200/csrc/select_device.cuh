@@ -46,8 +46,11 @@ __device__ __forceinline__ void product_features(const ProdDesc &pd, const BufCo
 
 __device__ __forceinline__ uint32_t heuristic_choice(const SelectorParams &sp, const float *f, uint32_t T, bool tc_ok) {
     const uint32_t allowed = sp.allowed;
-    if (tc_ok && (allowed & (1u << 4)) && T >= sp.tc_min_tiles && f[2] >= sp.tc_min_occ && f[4] >= sp.tc_min_pop &&
-        f[5] >= sp.tc_min_pop)
+    // tensor cores: a k-tile costs them the same whatever the tiles hold, so
+    // they win where the word-level kernels pay full tiles too -- dense P
+    // tiles, whose cost does not depend on Q's population or occupancy --
+    // and the product is not tiny
+    if (tc_ok && (allowed & (1u << 4)) && T >= sp.tc_min_tiles && f[2] >= sp.tc_min_occ && f[6] >= sp.tc_min_dense)
         return 4;
     if ((allowed & (1u << 3)) && f[6] >= sp.m4r_min_dense) return 3;
     if (allowed & (1u << 2)) return 2;

@@ -370,6 +370,37 @@ int cfpq_closure_hash(cfpq_ctx *ctx, const cfpq_rule *rules, size_t nrules, cfpq
                       size_t nmats, const cfpq_closure_opts *opts, cfpq_closure_stats *stats, uint64_t *hashes,
                       uint64_t *counts);
 
+/* A labelled graph for cfpq_intersection: edge e goes from[e] -> to[e] with
+ * terminal label[e], and label l sets its bit in the matrices
+ * label_mats[label_offsets[l] .. label_offsets[l+1]) (the terminal's
+ * nonterminals, cfpq-cpp/Grammar.h:41-45).  from/label/to are device
+ * pointers when on_device is nonzero; label_offsets and label_mats are host
+ * arrays. */
+typedef struct cfpq_edges {
+    const uint32_t *from;
+    const uint32_t *label;
+    const uint32_t *to;
+    size_t count;
+    const uint32_t *label_offsets;  /* nlabels + 1 entries */
+    const uint32_t *label_mats;
+    uint32_t nlabels;
+    int32_t on_device;
+} cfpq_edges;
+
+/* One whole query, the work of Grammar::intersection_with_graph
+ * (cfpq-cpp/Grammar.h:24-69): clears mats, scatters the edges, sets the
+ * diagonal of the `nepsilon` matrices listed in `epsilon` (indices into
+ * mats; Grammar.h:47-51), runs the closure and, when hashes and counts are
+ * non-NULL, computes every matrix's result line -- all enqueued back to back
+ * with ONE synchronisation at the end (the separate calls cost one host
+ * round trip each).  An edge whose vertex id is >= a matrix's n makes the
+ * call return CFPQ_ERR_INVALID after the closure; the matrices then hold the
+ * closure of the in-range edges. */
+int cfpq_intersection(cfpq_ctx *ctx, const cfpq_rule *rules, size_t nrules, cfpq_matrix *const *mats,
+                      size_t nmats, const cfpq_edges *edges, const uint32_t *epsilon, size_t nepsilon,
+                      const cfpq_closure_opts *opts, cfpq_closure_stats *stats, uint64_t *hashes,
+                      uint64_t *counts);
+
 /* One independent query of a batch: its rules index into its own matrices. */
 typedef struct cfpq_query {
     const cfpq_rule *rules;
@@ -391,11 +422,13 @@ int cfpq_closure_batch(cfpq_ctx *ctx, const cfpq_query *queries, size_t nqueries
 /* Per-product log of the last cfpq_closure / cfpq_closure_batch call run with
  * opts->log_products & CFPQ_LOG_PRODUCTS (engine driver): one record per
  * (iteration, product term).  In that mode the iterations run from the host;
- * each term first runs once with the selected variant (the real work), then
- * is timed again with every candidate variant on the same state (bits only
- * ever get added, so the re-runs change nothing): usec[v] is the device time
- * of variant v (CUDA events around its plan and product launches, tensor
- * cores including operand expansion), or < 0 where v was not timed.  These
+ * after the selection, every term runs alone with every candidate variant,
+ * term after term, so each timing sees the operands the selection saw plus
+ * what the terms timed before it added (as in a sequential pass; the
+ * candidates are real products, bits only ever get added), then the
+ * iteration runs with the selected variants: usec[v] is the device time of
+ * variant v (CUDA events around its plan and product launches), or < 0 where
+ * v was not timed.  These
  * records are the cost model's training data and the ground truth of its
  * regret.  Returns the number of records available; copies at most cap.
  * No reference counterpart (the reference only times the whole closure,
@@ -431,7 +464,9 @@ typedef struct cfpq_selector_config {
     uint32_t allowed;       /* bit v set: variant v may be chosen (bits 2, 3, 4) */
     uint32_t tc_min_tiles;  /* tensor cores only for n >= 64 * tc_min_tiles */
     float tc_min_occ;       /* TC: minimum occupied-tile fraction of P */
-    float tc_min_pop;       /* TC: minimum mean tile population / 4096 of P and Q */
+    float tc_min_dense;     /* TC: minimum fraction of dense P tiles (population > 96): the
+                               word-level kernels pay a dense tile's full cost whatever its
+                               population, the tensor cores pay it for every tile */
     float m4r_min_dense;    /* M4R: minimum fraction of dense P tiles (population > 96) */
     float conf_margin;      /* MLP: best prediction ahead of the second by this (log us) */
     float range_margin;     /* MLP: features within the training range widened by this fraction */

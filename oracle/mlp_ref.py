@@ -61,7 +61,7 @@ def heuristic_choice(cfg: dict, f: np.ndarray, T: int, tc_ok: bool) -> int:
     """The selector's threshold rule (variants 2 LOP3, 3 M4R, 4 TC)."""
     allowed = cfg["allowed"]
     if (tc_ok and allowed & (1 << 4) and T >= cfg["tc_min_tiles"] and f[2] >= cfg["tc_min_occ"]
-            and f[4] >= cfg["tc_min_pop"] and f[5] >= cfg["tc_min_pop"]):
+            and f[6] >= cfg["tc_min_dense"]):
         return 4
     if allowed & (1 << 3) and f[6] >= cfg["m4r_min_dense"]:
         return 3

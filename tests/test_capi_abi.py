@@ -78,7 +78,7 @@ CTYPES_STRUCTS = {
     "Calibration": "cfpq_calibration", "Rule": "cfpq_rule", "ClosureOpts": "cfpq_closure_opts",
     "ClosureStats": "cfpq_closure_stats", "KernelProfile": "cfpq_kernel_profile", "Query": "cfpq_query",
     "ProductRecord": "cfpq_product_record", "SelectorConfig": "cfpq_selector_config", "TrainOpts": "cfpq_train_opts",
-    "TrainReport": "cfpq_train_report", "AutotuneOpts": "cfpq_autotune_opts",
+    "TrainReport": "cfpq_train_report", "AutotuneOpts": "cfpq_autotune_opts", "Edges": "cfpq_edges",
 }
 
 

@@ -105,7 +105,7 @@ def test_auto_closure_with_tensor_core_terms(pkg, oracle, sctx, tmp_path, loop):
     word-level and tensor-core launch sequences."""
     wl = pkg.workloads.ontology_query(1024, 3)
     exp = _expected(oracle, wl, tmp_path)
-    sctx.selector_configure(mode="heuristic", tc_min_tiles=1, tc_min_occ=0.0, tc_min_pop=0.001, min_tiles=1)
+    sctx.selector_configure(mode="heuristic", tc_min_tiles=1, tc_min_occ=0.0, tc_min_dense=0.0, min_tiles=1)
     q = pkg.query.PreparedQuery(sctx, wl.grammar, wl.graph)
     try:
         res = q.run(variant="auto", use_graph=loop)
