@@ -253,6 +253,14 @@ extern "C" int cfpq_ctx_create(int device, cfpq_ctx **out) {
     CUDA_TRY(cudaMalloc(&c->d_bad, 64));
     CUDA_TRY(cudaMallocHost(&c->h_st, sizeof(IterState)));
     CUDA_TRY(cudaMallocHost(&c->h_flag, 64));
+    // the persistent kernel writes its final state straight into these
+    // (device views of the pinned blocks; without them it is copied back)
+    if (cudaHostGetDevicePointer(reinterpret_cast<void **>(&c->h_st_dev), c->h_st, 0) != cudaSuccess ||
+        cudaHostGetDevicePointer(reinterpret_cast<void **>(&c->h_flag_dev), c->h_flag, 0) != cudaSuccess) {
+        c->h_st_dev = nullptr;
+        c->h_flag_dev = nullptr;
+        (void)cudaGetLastError();
+    }
     c->lop3_grid = c->num_sms * product_tiled_blocks_per_sm(0);
     c->m4r_grid = c->num_sms * product_tiled_blocks_per_sm(1);
     // The tensor-core kernel allocates all 512 TMEM columns of its SM, so it
@@ -282,7 +290,7 @@ extern "C" int cfpq_ctx_destroy(cfpq_ctx *ctx) {
         cudaFree(kv.second.d_pow13);
     }
     for (DevBuf *b : {&ctx->stage, &ctx->items, &ctx->prods, &ctx->slots, &ctx->qtrack, &ctx->prod_seen,
-                      &ctx->mats_desc, &ctx->edge_buf, &ctx->phase_log, &ctx->clear_desc,
+                      &ctx->mats_desc, &ctx->edge_buf, &ctx->phase_log, &ctx->clear_desc, &ctx->diag_desc,
                       &ctx->d_sel, &ctx->cnts, &ctx->choice, &ctx->tc_ok, &ctx->sel_log, &ctx->mlp_w, &ctx->mlp_x,
                       &ctx->mlp_y, &ctx->mlp_m, &ctx->mlp_grad, &ctx->mlp_m1, &ctx->mlp_v2, &ctx->mlp_loss,
                       &ctx->mlp_out, &ctx->qranges, &ctx->item_trace, &ctx->nt_cells, &ctx->nt_mats,
@@ -409,10 +417,14 @@ extern "C" int cfpq_load_edges_device(cfpq_ctx *ctx, cfpq_matrix *const *mats, s
 
 extern "C" void *cfpq_ctx_stream(const cfpq_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
 
-static int load_edges_impl(cfpq_ctx *ctx, cfpq_matrix *const *mats, size_t nmats, const uint32_t *from,
-                           const uint32_t *label, const uint32_t *to, size_t nedges, const uint32_t *label_offsets,
-                           const uint32_t *label_mats, uint32_t nlabels, bool on_device) {
-    TRY(use_device(ctx));
+// Validates an edge list and stages it for the scatter: the small tables
+// (matrix descriptors, label offsets, label -> matrices) on the device, host
+// edge arrays copied (asynchronously) into the context's staging block.
+// Fills the edge fields of *in; launches nothing.  Nothing to scatter: in->nedges = 0.
+static int prepare_edges(cfpq_ctx *ctx, cfpq_matrix *const *mats, size_t nmats, const uint32_t *from,
+                         const uint32_t *label, const uint32_t *to, size_t nedges, const uint32_t *label_offsets,
+                         const uint32_t *label_mats, uint32_t nlabels, bool on_device, ClosureInput *in) {
+    in->nedges = 0;
     if ((nmats && !mats) || (nedges && (!from || !label || !to)) || (nlabels && (!label_offsets)))
         return set_error(CFPQ_ERR_INVALID, "null argument");
     if (nedges == 0 || nlabels == 0) return CFPQ_OK;
@@ -486,9 +498,31 @@ static int load_edges_impl(cfpq_ctx *ctx, cfpq_matrix *const *mats, size_t nmats
         CUDA_TRY(cudaMemcpyAsync(d_label, label, be, cudaMemcpyHostToDevice, ctx->stream));
         CUDA_TRY(cudaMemcpyAsync(d_to, to, be, cudaMemcpyHostToDevice, ctx->stream));
     }
+    in->mats = d_desc;
+    in->nmats = (uint32_t)nmats;
+    in->nlabels = nlabels;
+    in->from = d_from;
+    in->label = d_label;
+    in->to = d_to;
+    in->nedges = nedges;
+    in->off = d_off;
+    in->lm = d_lm;
+    in->nlm = nlm;
+    in->bad = ctx->d_bad;
+    return CFPQ_OK;
+}
+
+static int load_edges_impl(cfpq_ctx *ctx, cfpq_matrix *const *mats, size_t nmats, const uint32_t *from,
+                           const uint32_t *label, const uint32_t *to, size_t nedges, const uint32_t *label_offsets,
+                           const uint32_t *label_mats, uint32_t nlabels, bool on_device) {
+    TRY(use_device(ctx));
+    ClosureInput in;
+    memset(&in, 0, sizeof(in));
+    TRY(prepare_edges(ctx, mats, nmats, from, label, to, nedges, label_offsets, label_mats, nlabels, on_device, &in));
+    if (!in.nedges) return CFPQ_OK;
     CUDA_TRY(cudaMemsetAsync(ctx->d_bad, 0, 4, ctx->stream));
-    CUDA_TRY(launch_load_edges(d_desc, (uint32_t)nmats, d_from, d_label, d_to, nedges, d_off, d_lm, nlabels, nlm,
-                               ctx->d_bad, ctx->stream));
+    CUDA_TRY(launch_load_edges(in.mats, in.nmats, in.from, in.label, in.to, in.nedges, in.off, in.lm, in.nlabels,
+                               in.nlm, ctx->d_bad, ctx->stream));
     return CFPQ_OK;
 }
 
@@ -506,8 +540,10 @@ extern "C" int cfpq_matrix_clear(cfpq_ctx *ctx, cfpq_matrix *m) {
     return CFPQ_OK;
 }
 
-extern "C" int cfpq_matrices_clear(cfpq_ctx *ctx, cfpq_matrix *const *mats, size_t count) {
-    TRY(use_device(ctx));
+// The clear list of `count` matrices on the device (one unit per tile-row,
+// MatRows prefix sums), re-sent only when it differs from the last one.
+static int prepare_clear(cfpq_ctx *ctx, cfpq_matrix *const *mats, size_t count, ClosureInput *in) {
+    in->clear_rows = 0;
     if (count == 0) return CFPQ_OK;
     if (!mats) return set_error(CFPQ_ERR_INVALID, "null matrix list");
     std::vector<MatRows> tab(count);
@@ -531,7 +567,18 @@ extern "C" int cfpq_matrices_clear(cfpq_ctx *ctx, cfpq_matrix *const *mats, size
                                  ctx->stream));
         ctx->clear_desc_key = std::move(key);
     }
-    CUDA_TRY(launch_clear_rows(ctx->clear_desc.as<MatRows>(), (uint32_t)count, rows, ctx->stream));
+    in->clear = ctx->clear_desc.as<MatRows>();
+    in->nclear = (uint32_t)count;
+    in->clear_rows = rows;
+    return CFPQ_OK;
+}
+
+extern "C" int cfpq_matrices_clear(cfpq_ctx *ctx, cfpq_matrix *const *mats, size_t count) {
+    TRY(use_device(ctx));
+    ClosureInput in;
+    memset(&in, 0, sizeof(in));
+    TRY(prepare_clear(ctx, mats, count, &in));
+    if (in.clear_rows) CUDA_TRY(launch_clear_rows(in.clear, in.nclear, in.clear_rows, ctx->stream));
     return CFPQ_OK;
 }
 
@@ -1383,7 +1430,7 @@ static void fill_hash_out(const cfpq_ctx *ctx, const HashOut *ho) {
 
 static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_closure_opts &o,
                       cfpq_closure_stats *stats, uint32_t *iters_out, double *done_ms_out,
-                      const HashOut *ho = nullptr) {
+                      const HashOut *ho = nullptr, const ClosureInput *input = nullptr) {
     for (size_t qi = 0; qi < qs.size(); ++qi) TRY(validate_query(qs[qi], qi));
     std::vector<uint64_t> key;
     plan_key(ctx, qs, o.variant, &key);
@@ -1403,6 +1450,10 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
     ClosurePlan &pl = pc.pl;
     const size_t nq = qs.size();
     if (pl.prods.empty()) {
+        if (input) {
+            if (input->bad) CUDA_TRY(cudaMemsetAsync(input->bad, 0, 4, ctx->stream));
+            CUDA_TRY(launch_closure_input(*input, ctx->num_sms, ctx->stream));
+        }
         if (stats) memset(stats, 0, sizeof(*stats));
         for (size_t q = 0; q < nq; ++q) {
             if (iters_out) iters_out[q] = 0;
@@ -1473,6 +1524,18 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
                                  cudaMemcpyHostToDevice, ctx->stream));
         ctx->tables_owner = pc.id;
     }
+    // the persistent kernel hands its final state (and the caller's flag
+    // word, which lives in the pinned flag block) to the host itself
+    const bool st_mapped = persistent && ctx->h_st_dev != nullptr;
+    const bool flag_mapped = st_mapped && ho && ho->flag_src && ho->flag_dst >= ctx->h_flag &&
+                             ho->flag_dst < ctx->h_flag + 16;
+    // the query's input phase, enqueued right before the closure's own
+    // launches (stand-alone kernels: as a prologue of the persistent kernel,
+    // between two grid barriers, it measured ~10 us slower per query)
+    if (input) {
+        if (input->bad) CUDA_TRY(cudaMemsetAsync(input->bad, 0, 4, ctx->stream));
+        CUDA_TRY(launch_closure_input(*input, ctx->num_sms, ctx->stream));
+    }
     if (ctx->cnts_on) CUDA_TRY(launch_counters_init(ctx->slots.as<MatSlot>(), nslots, ctx->cnts.as<BufCounters>(),
                                                     ctx->stream));
     if (ctx->sel_log_iters)
@@ -1535,7 +1598,11 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
                                            // one small closure: latency-bound, merge without the read of C
                                            nq == 1 && pl.prods[0].T <= kDirectMergeMaxTiles ? 1 : 0,
                                            nq > 1 ? 1 : 0, (uint32_t)std::max(o.wait_limit, 0),
-                                           (o.test_flags & CFPQ_TEST_STALL_BARRIER) != 0, ctx->stream));
+                                           (o.test_flags & CFPQ_TEST_STALL_BARRIER) != 0,
+                                           st_mapped ? ctx->h_st_dev : nullptr,
+                                           flag_mapped ? ho->flag_src : nullptr,
+                                           flag_mapped ? ctx->h_flag_dev + (ho->flag_dst - ctx->h_flag) : nullptr,
+                                           ctx->stream));
     } else if (exec) {
         CUDA_TRY(cudaGraphLaunch(exec, ctx->stream));
     } else {
@@ -1553,7 +1620,8 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
         }
     }
     CUDA_TRY(cudaEventRecord(ctx->ev1, ctx->stream));
-    CUDA_TRY(cudaMemcpyAsync(ctx->h_st, ctx->d_st, sizeof(IterState), cudaMemcpyDeviceToHost, ctx->stream));
+    if (!st_mapped)
+        CUDA_TRY(cudaMemcpyAsync(ctx->h_st, ctx->d_st, sizeof(IterState), cudaMemcpyDeviceToHost, ctx->stream));
     if (trace)
         CUDA_TRY(cudaMemcpyAsync(&ctx->item_trace_n, static_cast<char *>(ctx->item_trace.p) + trace_bytes, 4,
                                  cudaMemcpyDeviceToHost, ctx->stream));
@@ -1576,7 +1644,7 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
         CUDA_TRY(cudaMemcpyAsync(h_last, qt.last_iter, nq * 4, cudaMemcpyDeviceToHost, ctx->stream));
     }
     if (ho && ho->n) TRY(enqueue_hash_many(ctx, ho->mats, ho->n));
-    if (ho && ho->flag_src)
+    if (ho && ho->flag_src && !flag_mapped)
         CUDA_TRY(cudaMemcpyAsync(ho->flag_dst, ho->flag_src, 4, cudaMemcpyDeviceToHost, ctx->stream));
     CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     float ms = 0;
@@ -1775,6 +1843,29 @@ extern "C" int cfpq_closure_hash(cfpq_ctx *ctx, const cfpq_rule *rules, size_t n
     return run_engine(ctx, qs, o, stats, nullptr, nullptr, &ho);
 }
 
+// The epsilon matrices' descriptors on the device, re-sent only when they
+// differ from the last call's.
+static int prepare_diag(cfpq_ctx *ctx, cfpq_matrix *const *mats, const uint32_t *epsilon, size_t nepsilon,
+                        ClosureInput *in) {
+    in->ndiag = 0;
+    if (!nepsilon) return CFPQ_OK;
+    std::vector<DevMat> tab(nepsilon);
+    for (size_t i = 0; i < nepsilon; ++i) tab[i] = mats[epsilon[i]]->d;
+    void *const before = ctx->diag_desc.p;
+    TRY(ctx->diag_desc.ensure(nepsilon * sizeof(DevMat)));
+    const unsigned char *tb = reinterpret_cast<const unsigned char *>(tab.data());
+    std::vector<unsigned char> key(tb, tb + nepsilon * sizeof(DevMat));
+    if (ctx->diag_desc.p != before || key != ctx->diag_desc_key) {
+        ctx->diag_desc_key.clear();
+        // synchronous: the descriptors are small and change only with the query
+        CUDA_TRY(cudaMemcpy(ctx->diag_desc.p, tab.data(), nepsilon * sizeof(DevMat), cudaMemcpyHostToDevice));
+        ctx->diag_desc_key = std::move(key);
+    }
+    in->diag = ctx->diag_desc.as<DevMat>();
+    in->ndiag = (uint32_t)nepsilon;
+    return CFPQ_OK;
+}
+
 // Slot of the context's pinned flag block that receives the edge scatter's
 // out-of-range count in cfpq_intersection (slot 0 belongs to the
 // synchronous flag reads).
@@ -1788,33 +1879,38 @@ extern "C" int cfpq_intersection(cfpq_ctx *ctx, const cfpq_rule *rules, size_t n
     if (!edges) return set_error(CFPQ_ERR_INVALID, "null edge list");
     if (nepsilon && !epsilon) return set_error(CFPQ_ERR_INVALID, "null epsilon list");
     if (nmats && !mats) return set_error(CFPQ_ERR_INVALID, "null matrix list");
+    for (size_t i = 0; i < nmats; ++i)
+        if (!mats[i]) return set_error(CFPQ_ERR_INVALID, "matrix %zu is null", i);
     const bool want_lines = hashes != nullptr || counts != nullptr;
     if (want_lines && (!hashes || !counts)) return set_error(CFPQ_ERR_INVALID, "hashes and counts go together");
     for (size_t i = 0; i < nepsilon; ++i)
-        if (epsilon[i] >= nmats || !mats[epsilon[i]])
+        if (epsilon[i] >= nmats)
             return set_error(CFPQ_ERR_INVALID, "epsilon[%zu] = %u is not a matrix of the query", i, epsilon[i]);
     const cfpq_closure_opts o = opts ? *opts : default_opts();
-    // input: clear, scatter, diagonals (asynchronous); the scatter's
-    // out-of-range count travels back with the closure's own read-back
-    TRY(cfpq_matrices_clear(ctx, mats, nmats));
+    // the input phase: clear, scatter, diagonals
+    ClosureInput in;
+    memset(&in, 0, sizeof(in));
+    TRY(prepare_clear(ctx, mats, nmats, &in));
+    TRY(prepare_edges(ctx, mats, nmats, edges->from, edges->label, edges->to, edges->count, edges->label_offsets,
+                      edges->label_mats, edges->nlabels, edges->on_device != 0, &in));
+    TRY(prepare_diag(ctx, mats, epsilon, nepsilon, &in));
+    in.bad = in.nedges ? ctx->d_bad : nullptr;
     uint32_t *const h_bad = ctx->h_flag + kIntersectBadSlot;
     *h_bad = 0;
-    const bool scatter = edges->count && edges->nlabels;
-    if (scatter)
-        TRY(load_edges_impl(ctx, mats, nmats, edges->from, edges->label, edges->to, edges->count,
-                            edges->label_offsets, edges->label_mats, edges->nlabels, edges->on_device != 0));
-    for (size_t i = 0; i < nepsilon; ++i) CUDA_TRY(launch_set_diag(mats[epsilon[i]]->d, ctx->stream));
-    // closure (+ result lines); the engine reads the scatter's count back
-    // with its own final read-back, the other drivers synchronise on the way
     const bool engine = o.driver == CFPQ_DRIVER_ENGINE &&
                         (o.variant == CFPQ_VARIANT_AUTO || o.variant == CFPQ_VARIANT_LOP3 ||
                          o.variant == CFPQ_VARIANT_M4R || (o.variant == CFPQ_VARIANT_TC && ctx->tc_grid));
     if (engine) {
+        // the engine runs the input phase itself (in the persistent kernel's
+        // prologue when it can) and reads the scatter's count back with its
+        // own final read-back: one synchronisation in all
         std::vector<QueryIn> qs{QueryIn{rules, nrules, mats, nmats}};
-        HashOut ho{mats, want_lines ? nmats : 0, hashes, counts, scatter ? ctx->d_bad : nullptr, h_bad};
-        TRY(run_engine(ctx, qs, o, stats, nullptr, nullptr, &ho));
+        HashOut ho{mats, want_lines ? nmats : 0, hashes, counts, in.bad, h_bad};
+        TRY(run_engine(ctx, qs, o, stats, nullptr, nullptr, &ho, &in));
     } else {
-        if (scatter) CUDA_TRY(cudaMemcpyAsync(h_bad, ctx->d_bad, 4, cudaMemcpyDeviceToHost, ctx->stream));
+        if (in.bad) CUDA_TRY(cudaMemsetAsync(in.bad, 0, 4, ctx->stream));
+        CUDA_TRY(launch_closure_input(in, ctx->num_sms, ctx->stream));
+        if (in.bad) CUDA_TRY(cudaMemcpyAsync(h_bad, in.bad, 4, cudaMemcpyDeviceToHost, ctx->stream));
         TRY(cfpq_closure(ctx, rules, nrules, mats, nmats, &o, stats));
         if (want_lines) TRY(cfpq_hash_count_many(ctx, mats, nmats, hashes, counts));
         else TRY(sync_and_check(ctx));

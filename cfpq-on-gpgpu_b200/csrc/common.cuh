@@ -94,6 +94,7 @@ struct IterState {
     unsigned long long bytes_staged;  // operand bytes copied global -> shared by product kernels
     unsigned long long out_words;     // non-zero accumulator words merged into heads
     unsigned long long new_words;     // words that received new bits
+    uint32_t exit_count;              // persistent kernel: CTAs past their exit statistics
 };
 
 // A matrix and the prefix sum of tile-rows over a list of matrices (kernels

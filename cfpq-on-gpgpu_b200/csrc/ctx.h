@@ -116,11 +116,13 @@ struct cfpq_ctx {
     uint32_t *d_bad = nullptr;
     // pinned host scratch
     IterState *h_st = nullptr;
+    IterState *h_st_dev = nullptr;  // h_st as the device sees it (pinned, mapped)
+    uint32_t *h_flag_dev = nullptr; // h_flag as the device sees it
     uint32_t *h_flag = nullptr;
     unsigned long long *h_hash = nullptr;
     size_t h_hash_cap = 0;
     // growable device scratch
-    DevBuf stage, items, prods, slots, qtrack, prod_seen, mats_desc, edge_buf, clear_desc;
+    DevBuf stage, items, prods, slots, qtrack, prod_seen, mats_desc, edge_buf, clear_desc, diag_desc;
     std::unordered_map<uint32_t, PowTables> pow;
     std::vector<cfpq_matrix *> pool;  // zeroed spare matrices (deltas, alias copies)
     GraphCache gcache;
@@ -141,6 +143,7 @@ struct cfpq_ctx {
     size_t h_small_cap = 0;
     std::vector<unsigned char> edge_tables_key;  // small tables of the last edge load still in edge_buf
     std::vector<unsigned char> clear_desc_key;   // matrix list of the last cfpq_matrices_clear in clear_desc
+    std::vector<unsigned char> diag_desc_key;    // epsilon matrices of the last cfpq_intersection in diag_desc
     void *items_clean_ptr = nullptr;  // items buffer whose first items_clean_words words are zero
     size_t items_clean_words = 0;
     void *h_query = nullptr;  // pinned: per-query results of a closure (done_ns, last_iter)

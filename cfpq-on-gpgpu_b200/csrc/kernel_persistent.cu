@@ -128,6 +128,9 @@ struct PersistArgs {
     uint32_t spin_limit;            // polls of the item wait and of the grid barrier before they give up
     uint32_t stall_barrier;         // test hook: the first grid barrier waits for one arrival more than
                                     // there are CTAs, so that its bounded wait runs out
+    IterState *host_st;             // non-null: the last CTA to exit writes the final state here
+    const uint32_t *flag_src;       // and (non-null) this word to *flag_dst (both mapped host memory)
+    uint32_t *flag_dst;
 };
 
 // Records one processed item (thread 0 of the CTA); sub: the item's
@@ -488,6 +491,25 @@ __global__ void __launch_bounds__(kThreads, 2) k_closure_persistent(PersistArgs 
         st->iter = t + 1;
         st->active = 0;
     }
+    // the final state to the host without a copy after the kernel: the last
+    // CTA past this point (every other CTA's statistics and block 0's final
+    // writes are then performed) writes it into mapped host memory
+    if (a.host_st) {
+        __shared__ uint32_t s_last;
+        __syncthreads();
+        if (tid == 0) {
+            __threadfence();
+            s_last = atomicAdd(&st->exit_count, 1u) == gridDim.x - 1 ? 1u : 0u;
+        }
+        __syncthreads();
+        if (s_last) {
+            __threadfence();
+            const uint32_t *src = reinterpret_cast<const uint32_t *>(st);
+            uint32_t *dst = reinterpret_cast<uint32_t *>(a.host_st);
+            for (uint32_t i = tid; i < sizeof(IterState) / 4; i += kThreads) dst[i] = __ldcg(src + i);
+            if (tid == 0 && a.flag_src) *a.flag_dst = __ldcg(a.flag_src);
+        }
+    }
 }
 
 template <bool kHasM4R>
@@ -517,6 +539,7 @@ cudaError_t launch_closure_persistent(int has_m4r, int grid, const ProdDesc *pro
                                       const SelectorParams *sel, SelLogRow *sel_log, uint32_t sel_log_iters,
                                       const QueryRange *qr, ItemTrace *trace, uint32_t *trace_count,
                                       int direct_merge, int prefetch, uint32_t spin_limit, int stall_barrier,
+                                      IterState *host_st, const uint32_t *flag_src, uint32_t *flag_dst,
                                       cudaStream_t s) {
     PersistArgs a;
     a.prods = prods;
@@ -545,6 +568,9 @@ cudaError_t launch_closure_persistent(int has_m4r, int grid, const ProdDesc *pro
     a.prefetch = prefetch;
     a.spin_limit = spin_limit ? spin_limit : kBarrierSpinLimit;
     a.stall_barrier = stall_barrier ? 1u : 0u;
+    a.host_st = host_st;
+    a.flag_src = flag_src;
+    a.flag_dst = flag_dst;
     void *args[] = {&a};
     if (has_m4r)
         return cudaLaunchCooperativeKernel((const void *)k_closure_persistent<true>, dim3(grid), dim3(kThreads), args,

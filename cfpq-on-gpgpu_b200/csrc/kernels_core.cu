@@ -3,6 +3,7 @@
 // steps of the device-resident closure iteration.
 #include <algorithm>
 
+#include "input_device.cuh"
 #include "launch.h"
 #include "plan_device.cuh"
 
@@ -21,27 +22,6 @@ inline unsigned grid_for(size_t n, unsigned block) {
 inline unsigned capped_grid(size_t n, unsigned block, unsigned cap) {
     const unsigned g = grid_for(n, block);
     return g > cap ? cap : g;
-}
-
-__device__ __forceinline__ void set_occ_bit(const DevMat &m, uint32_t ti, uint32_t tj) {
-    atomicOr(m.occ + (size_t)ti * m.ow + (tj >> 5), 1u << (tj & 31));
-}
-
-// Set bit (r, c) given in vertex ids (mapped through the matrix's vertex
-// order); keep occupancy and population exact.
-__device__ __forceinline__ void set_one_bit(const DevMat &m, uint32_t r, uint32_t c) {
-    if (m.perm) {
-        r = m.perm[r];
-        c = m.perm[c];
-    }
-    unsigned long long *w =
-        reinterpret_cast<unsigned long long *>(m.bits + tile_offset(m.T, r >> 6, c >> 6) + (r & 63));
-    const unsigned long long bit = 1ULL << (c & 63);
-    const unsigned long long old = atomicOr(w, bit);
-    if (!(old & bit)) {
-        atomicAdd(m.nnz + (size_t)(r >> 6) * m.T + (c >> 6), 1u);
-        set_occ_bit(m, r >> 6, c >> 6);
-    }
 }
 
 __device__ __forceinline__ uint32_t warp_sum(uint32_t v) {
@@ -95,16 +75,7 @@ __global__ void k_load_edges(const DevMat *__restrict__ mats, uint32_t nmats, co
     }
     if constexpr (kSmem) __syncthreads();
     for (; e < ne; e += (size_t)gridDim.x * blockDim.x) {
-        if (l < nlabels) {
-            for (uint32_t j = off[l]; j < off[l + 1]; ++j) {
-                const DevMat m = mats[lm[j]];
-                if (r >= m.n || c >= m.n) {
-                    atomicAdd(bad, 1u);
-                    continue;
-                }
-                set_one_bit(m, r, c);
-            }
-        }
+        scatter_edge(mats, off, lm, nlabels, l, r, c, bad);
         const size_t e2 = e + (size_t)gridDim.x * blockDim.x;
         if (e2 < ne) {
             l = label[e2];
@@ -442,13 +413,16 @@ __global__ void k_closure_begin(ClosureBegin a) {
 // Clear a list of matrices: one warp per (matrix, tile-row), occupied tiles only.
 __global__ void k_clear_rows(const MatRows *__restrict__ tab, uint32_t nmats, uint32_t total_rows) {
     const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (gw >= total_rows) return;
-    uint32_t lo = 0, hi = nmats;
-    while (hi - lo > 1) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (tab[mid].row_start <= gw) lo = mid; else hi = mid;
+    if (gw < total_rows) clear_unit(tab, nmats, gw);
+}
+
+// Diagonals of a list of matrices (epsilon nonterminals).
+__global__ void k_set_diags(const DevMat *__restrict__ diag, uint32_t ndiag) {
+    const size_t tid = blockIdx.x * (size_t)blockDim.x + threadIdx.x, nt = (size_t)gridDim.x * blockDim.x;
+    for (uint32_t d = 0; d < ndiag; ++d) {
+        const DevMat m = diag[d];
+        for (size_t i = tid; i < m.n; i += nt) set_one_bit(m, (uint32_t)i, (uint32_t)i);
     }
-    clear_tile_row(tab[lo].m, gw - tab[lo].row_start);
 }
 
 }  // namespace
@@ -615,6 +589,23 @@ cudaError_t launch_clear_rows(const MatRows *d_tab, uint32_t nmats, uint32_t tot
     if (total_rows == 0 || nmats == 0) return cudaSuccess;
     k_clear_rows<<<grid_for((size_t)total_rows * 32, 256), 256, 0, s>>>(d_tab, nmats, total_rows);
     return cudaGetLastError();
+}
+
+cudaError_t launch_closure_input(const ClosureInput &in, int num_sms, cudaStream_t s) {
+    if (in.clear_rows) {
+        cudaError_t e = launch_clear_rows(in.clear, in.nclear, in.clear_rows, s);
+        if (e != cudaSuccess) return e;
+    }
+    if (in.nedges) {
+        cudaError_t e = launch_load_edges(in.mats, in.nmats, in.from, in.label, in.to, in.nedges, in.off, in.lm,
+                                          in.nlabels, in.nlm, in.bad, s);
+        if (e != cudaSuccess) return e;
+    }
+    if (in.ndiag) {
+        k_set_diags<<<num_sms * 4, 256, 0, s>>>(in.diag, in.ndiag);
+        return cudaGetLastError();
+    }
+    return cudaSuccess;
 }
 
 cudaError_t launch_closure_begin(const ClosureBegin &a, int num_sms, cudaStream_t s) {

@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include "common.cuh"
+#include "input_device.cuh"
 
 namespace cfpq {
 
@@ -111,6 +112,8 @@ struct ClosureBegin {
     uint32_t max_iter, nqueries;
 };
 cudaError_t launch_closure_begin(const ClosureBegin &a, int num_sms, cudaStream_t s);
+// A query's input phase as stand-alone kernels: clear, edge scatter, diagonals.
+cudaError_t launch_closure_input(const ClosureInput &in, int num_sms, cudaStream_t s);
 // Persistent closure (word-level variants only): the whole fixpoint in one
 // cooperative launch of `grid` CTAs (at most persistent_blocks_per_sm() per
 // SM); items: 4 lists of list_cap; phase_log: 3 timestamps per iteration.
@@ -123,6 +126,7 @@ cudaError_t launch_closure_persistent(int has_m4r, int grid, const ProdDesc *pro
                                       const SelectorParams *sel, SelLogRow *sel_log, uint32_t sel_log_iters,
                                       const QueryRange *qr, ItemTrace *trace, uint32_t *trace_count,
                                       int direct_merge, int prefetch, uint32_t spin_limit, int stall_barrier,
+                                      IterState *host_st, const uint32_t *flag_src, uint32_t *flag_dst,
                                       cudaStream_t s);
 // (spin_limit 0: the default of about a second of polling per wait;
 // trace non-null: one ItemTrace per processed item, counted in *trace_count)

@@ -16,11 +16,6 @@ constexpr uint32_t kLaneBits = 4;    // sparse loop: bits per row a lane walks b
 constexpr int kThreads = 128;        // 4 warps (product kernels; the persistent kernel runs 8)
 constexpr int kMaxTiles = 2048;      // k-list capacity (n <= 131072)
 constexpr uint32_t kSparseMax = 96;  // P-tile population up to which the sparse loop runs
-// A P tile above kSparseMax whose bits sit in at most this many rows with
-// more than kLaneBits bits still takes the sparse loop: its cost is about
-// 100 warp instructions plus 95 per such row, the dense loop's about 830
-// whatever the rows hold (hub vertices make dense-by-count tiles of few rows).
-constexpr uint32_t kHubRowsMax = 6;
 constexpr int kTabRow = 17;          // padded table row (uint64 words): 16 keys, or kBJ tiles
 constexpr unsigned kFull = 0xffffffffu;
 constexpr uint32_t kGateSpinLimit = 1u << 24;  // ~1 s of polling
@@ -268,16 +263,7 @@ __device__ __forceinline__ void process_item(Smem &S, uint64_t it, const ProdDes
         }
         const uint32_t wmask = ((uint32_t)S.kmask[e] >> (kTPW * warp)) & kWMask;
         const uint4 pp = *reinterpret_cast<const uint4 *>(&S.p[stage][2 * lane]);
-        bool dense = (S.ktile[e] & 0x8000u) != 0;
-        if (!(kM4R && kTPW > 2) && dense) {
-            // every warp reads the same 64 rows, so the choice is the same in
-            // all of them (the CTA-wide table build of the 4-warp Four
-            // Russians loop keeps the population rule: it has a barrier)
-            const uint32_t heavy =
-                __popc(__ballot_sync(kFull, (uint32_t)(__popc(pp.x) + __popc(pp.y)) > kLaneBits)) +
-                __popc(__ballot_sync(kFull, (uint32_t)(__popc(pp.z) + __popc(pp.w)) > kLaneBits));
-            dense = heavy > kHubRowsMax;
-        }
+        const bool dense = (S.ktile[e] & 0x8000u) != 0;
         if (!dense) {
             // sparse P tile, only the occupied Q tiles staged.  Each lane
             // first walks up to kLaneBits set bits of its rows 2l and 2l+1;
