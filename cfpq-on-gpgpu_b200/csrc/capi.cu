@@ -291,7 +291,7 @@ extern "C" int cfpq_ctx_destroy(cfpq_ctx *ctx) {
     }
     for (DevBuf *b : {&ctx->stage, &ctx->items, &ctx->prods, &ctx->slots, &ctx->qtrack, &ctx->prod_seen,
                       &ctx->mats_desc, &ctx->edge_buf, &ctx->phase_log, &ctx->clear_desc, &ctx->diag_desc,
-                      &ctx->d_sel, &ctx->cnts, &ctx->choice, &ctx->tc_ok, &ctx->sel_log, &ctx->mlp_w, &ctx->mlp_x,
+                      &ctx->d_sel, &ctx->cnts, &ctx->choice, &ctx->tc_ok, &ctx->sel_log, &ctx->tc_rows, &ctx->mlp_w, &ctx->mlp_x,
                       &ctx->mlp_y, &ctx->mlp_m, &ctx->mlp_grad, &ctx->mlp_m1, &ctx->mlp_v2, &ctx->mlp_loss,
                       &ctx->mlp_out, &ctx->qranges, &ctx->item_trace, &ctx->nt_cells, &ctx->nt_mats,
                       &ctx->nt_rules, &ctx->nt_ctr})
@@ -951,6 +951,8 @@ struct ClosurePlan {
     size_t item_cap = 0;  // per item list
     bool uses_lop3 = false, uses_m4r = false, uses_tc = false;
     std::vector<TcProduct> tc_prods;
+    std::vector<TcRows> tc_rows;  // the same for the grouped tensor-core plan (k_plan_tc)
+    uint32_t tc_groups = 0;       // groups of 4 tile-rows over all tensor-core-capable products
     uint32_t tc_max_T = 0;
     bool auto_select = false;     // variants chosen on the device every iteration
     uint8_t fixed_variant = 0;    // otherwise: every product's variant
@@ -1095,6 +1097,10 @@ static int build_plan(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, int variant
     }
     pl->item_cap = std::max<size_t>(pl->item_cap, 1);
     pl->uses_tc = !pl->tc_prods.empty();
+    for (const TcProduct &tp : pl->tc_prods) {
+        pl->tc_rows.push_back(TcRows{tp.index, tp.row_start, pl->tc_groups, 0});
+        pl->tc_groups += tp.rows;
+    }
     if (pl->prods.size() > kMaxItemProducts)
         return set_error(CFPQ_ERR_INVALID, "%zu rule products in one closure (at most %u)", pl->prods.size(),
                          kMaxItemProducts);
@@ -1157,9 +1163,19 @@ static int enqueue_select_plan(cfpq_ctx *ctx, const ClosurePlan &pl, cudaStream_
 static int enqueue_products(cfpq_ctx *ctx, const ClosurePlan &pl, const QueryTrack &qt, cudaStream_t s) {
     BufCounters *cnts = closure_counters(ctx, pl);
     TRY(launch_products(ctx, pl.item_cap, pl.uses_lop3, pl.uses_m4r, qt.changed, cnts, s));
-    for (const TcProduct &tp : pl.tc_prods)
-        TRY(launch_tc_product(ctx, tp, (uint32_t)pl.prods.size(), pl.item_cap, ctx->prod_seen.as<uint32_t>(),
-                              qt.changed, ctx->choice.as<uint8_t>(), cnts, s));
+    if (!pl.tc_prods.empty()) {
+        // every tensor-core product of the iteration together: one plan
+        // launch, one tensor-core launch over all their items, one list reset
+        const ProdDesc *pr = ctx->prods.as<ProdDesc>();
+        const MatSlot *sl = ctx->slots.as<MatSlot>();
+        CUDA_TRY(launch_plan_tc(pr, (uint32_t)pl.prods.size(), ctx->tc_rows.as<TcRows>(),
+                                (uint32_t)pl.tc_rows.size(), pl.tc_groups, sl, ctx->d_st, ctx->items.as<uint64_t>(),
+                                pl.item_cap, product_lop3_tiles_per_block(), ctx->prod_seen.as<uint32_t>(),
+                                ctx->choice.as<uint8_t>(), s));
+        CUDA_TRY(launch_product_tc(pr, sl, ctx->d_st, ctx->items.as<uint64_t>(), pl.item_cap, qt.changed,
+                                   ctx->tc_grid, cnts, s));
+        CUDA_TRY(launch_reset_list(ctx->d_st, 2, s));
+    }
     return CFPQ_OK;
 }
 
@@ -1233,10 +1249,8 @@ static int get_loop_graph(cfpq_ctx *ctx, const ClosurePlan &pl, const QueryTrack
                                  (uint64_t)(uintptr_t)ctx->cnts.p,    (uint64_t)(uintptr_t)ctx->d_sel.p,
                                  (uint64_t)(uintptr_t)ctx->tc_ok.p,   (uint64_t)(uintptr_t)ctx->sel_log.p,
                                  (uint64_t)ctx->sel_log_iters,        (uint64_t)pl.auto_select};
-    for (const TcProduct &tp : pl.tc_prods) {  // kernel arguments of the tensor-core launches
-        key.push_back(((uint64_t)tp.index << 32) | tp.T);
-        key.push_back(((uint64_t)tp.row_start << 32) | tp.rows);
-    }
+    key.push_back((uint64_t)(uintptr_t)ctx->tc_rows.p);  // the grouped tensor-core launches
+    key.push_back(((uint64_t)pl.tc_rows.size() << 32) | pl.tc_groups);
     if (ctx->gcache.exec && ctx->gcache.key == key) {
         *out = ctx->gcache.exec;
         return CFPQ_OK;
@@ -1470,11 +1484,15 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
     }
     // device tables
     void *const slots_before = ctx->slots.p, *const prods_before = ctx->prods.p, *const qr_before = ctx->qranges.p;
+    void *const tcok_before = ctx->tc_ok.p, *const tcr_before = ctx->tc_rows.p;
     TRY(ctx->slots.ensure(pl.slots.size() * sizeof(MatSlot)));
     TRY(ctx->prods.ensure(pl.prods.size() * sizeof(ProdDesc)));
     TRY(ctx->qranges.ensure(pl.qranges.size() * sizeof(QueryRange)));
+    TRY(ctx->tc_ok.ensure(pl.prods.size()));
+    TRY(ctx->tc_rows.ensure(pl.tc_rows.size() * sizeof(TcRows)));
     const bool tables_current = ctx->tables_owner == pc.id && ctx->slots.p == slots_before &&
-                                ctx->prods.p == prods_before && ctx->qranges.p == qr_before;
+                                ctx->prods.p == prods_before && ctx->qranges.p == qr_before &&
+                                ctx->tc_ok.p == tcok_before && ctx->tc_rows.p == tcr_before;
     const bool timed = (o.log_products & CFPQ_LOG_KERNELS) != 0;
     const bool log_products = (o.log_products & CFPQ_LOG_PRODUCTS) != 0;
     const int persist_grid = ctx->persist_grid[pl.uses_m4r ? 1 : 0];
@@ -1489,7 +1507,6 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
     const bool lists_clean = ctx->items_clean_ptr == ctx->items.p && ctx->items_clean_words >= list_words;
     ctx->items_clean_words = 0;
     TRY(ctx->choice.ensure(2 * (size_t)nprods));  // choices, then a copy kept by the product log
-    TRY(ctx->tc_ok.ensure(nprods));
     TRY(ctx->cnts.ensure((size_t)nslots * 3 * sizeof(BufCounters)));
     ctx->cnts_on = pl.auto_select || log_products;
     if (ctx->cnts_on) TRY(selector_sync(ctx));
@@ -1522,6 +1539,9 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
         CUDA_TRY(cudaMemcpyAsync(ctx->tc_ok.p, pl.tc_ok.data(), nprods, cudaMemcpyHostToDevice, ctx->stream));
         CUDA_TRY(cudaMemcpyAsync(ctx->qranges.p, pl.qranges.data(), pl.qranges.size() * sizeof(QueryRange),
                                  cudaMemcpyHostToDevice, ctx->stream));
+        if (!pl.tc_rows.empty())
+            CUDA_TRY(cudaMemcpyAsync(ctx->tc_rows.p, pl.tc_rows.data(), pl.tc_rows.size() * sizeof(TcRows),
+                                     cudaMemcpyHostToDevice, ctx->stream));
         ctx->tables_owner = pc.id;
     }
     // the persistent kernel hands its final state (and the caller's flag

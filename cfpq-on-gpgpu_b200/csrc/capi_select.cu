@@ -10,11 +10,15 @@ void selector_defaults(SelectorParams *sp) {
     memset(sp, 0, sizeof(*sp));
     sp->mode = CFPQ_SELECT_HEURISTIC;
     sp->allowed = (1u << CFPQ_VARIANT_LOP3) | (1u << CFPQ_VARIANT_M4R) | (1u << CFPQ_VARIANT_TC);
-    // Until cfpq_autotune runs: tensor cores for n >= 16384 when a fifth of
+    // Until cfpq_autotune runs: tensor cores for n >= 2048 when a fifth of
     // the P tiles are occupied and 30% of them dense (fit to the exhaustive
-    // per-term timings of a chain closure at n = 32768); Four Russians when
-    // a quarter of the P tiles are dense.
-    sp->tc_min_tiles = 256;
+    // per-term timings of a chain closure at n = 32768; n >= 2048 from the
+    // 512-query batch, whose tensor-core terms of all queries share one plan
+    // and one product launch per iteration: 1.59 s without them, 1.18 s from
+    // n = 4096, 1.13 s from n = 2048); Four Russians when a quarter of the P
+    // tiles are dense.  (A single query selects only from n >= 64 *
+    // min_tiles.)
+    sp->tc_min_tiles = 32;
     sp->tc_min_occ = 0.2f;
     sp->tc_min_dense = 0.3f;
     sp->m4r_min_dense = 0.25f;

@@ -151,7 +151,7 @@ struct cfpq_ctx {
     // variant selector
     SelectorParams sel;            // host copy of the device parameters
     bool sel_dirty = true;         // host copy changed since the last upload
-    DevBuf d_sel, cnts, choice, tc_ok, sel_log;
+    DevBuf d_sel, cnts, choice, tc_ok, sel_log, tc_rows;
     uint32_t sel_log_iters = 0, sel_log_prods = 0;
     bool cnts_on = false;          // the current closure keeps buffer counters
     std::vector<cudaEvent_t> tev;  // product timing events (CFPQ_LOG_PRODUCTS)

@@ -327,6 +327,28 @@ __global__ void __launch_bounds__(kPlanThreads)
                    tc_mode, ps, areas[threadIdx.x >> 5].cnt, areas[threadIdx.x >> 5].bnd);
 }
 
+// Tensor-core plan of every tensor-core-capable product of a closure in one
+// launch: the products' groups of 4 tile-rows laid end to end, one warp per
+// group (tc[i].pref groups come before product tc[i].prod).  A product whose
+// variant is not TC this iteration plans nothing.
+__global__ void __launch_bounds__(kPlanThreads)
+    k_plan_tc(const ProdDesc *__restrict__ prods, uint32_t nprods, const TcRows *__restrict__ tc, uint32_t ntc,
+              uint32_t total, const MatSlot *__restrict__ slots, IterState *st, uint64_t *__restrict__ items_all,
+              size_t list_cap, int tpb, uint32_t *prod_seen, PlanSelect ps) {
+    __shared__ plan::WarpArea<plan::kPlanMaxBlocks> areas[kPlanThreads / 32];
+    const uint32_t r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (r >= total || !st->active) return;
+    uint32_t lo = 0, hi = ntc;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (tc[mid].pref <= r) lo = mid; else hi = mid;
+    }
+    const TcRows t = tc[lo];
+    plan::plan_row(t.row_start + (r - t.pref), prods, nprods, slots, st->iter, st, st->item_count, items_all,
+                   list_cap, tpb, prod_seen, 1, ps, areas[threadIdx.x >> 5].cnt, areas[threadIdx.x >> 5].bnd, t.prod,
+                   t.prod + 1);
+}
+
 // ---- closure iteration: advance + end ----------------------------------------
 // Clears the delta buffer that was read in this iteration (it receives the next
 // iteration's new bits): zero every occupied tile and its population, then the
@@ -574,6 +596,17 @@ cudaError_t launch_plan(const ProdDesc *d_prods, uint32_t nprods, uint32_t row_b
     k_plan<<<grid_for((size_t)(row_end - row_begin) * 32, kPlanThreads), kPlanThreads, 0, s>>>(
         d_prods, nprods, row_begin, row_end, d_slots, d_st, d_items, list_cap, tiles_per_block, d_prod_seen, tc_mode,
         ps);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_plan_tc(const ProdDesc *d_prods, uint32_t nprods, const TcRows *d_tc, uint32_t ntc,
+                           uint32_t total_groups, const MatSlot *d_slots, IterState *d_st, uint64_t *d_items,
+                           size_t list_cap, int tiles_per_block, uint32_t *d_prod_seen, const uint8_t *d_choice,
+                           cudaStream_t s) {
+    if (ntc == 0 || total_groups == 0) return cudaSuccess;
+    const PlanSelect ps{nullptr, nullptr, nullptr, const_cast<uint8_t *>(d_choice), nullptr, 0};
+    k_plan_tc<<<grid_for((size_t)total_groups * 32, kPlanThreads), kPlanThreads, 0, s>>>(
+        d_prods, nprods, d_tc, ntc, total_groups, d_slots, d_st, d_items, list_cap, tiles_per_block, d_prod_seen, ps);
     return cudaGetLastError();
 }
 

@@ -66,6 +66,15 @@ cudaError_t launch_plain_product(const DevMat &a, const DevMat &b, const DevMat 
 cudaError_t launch_merge_or(const DevMat &dst, const DevMat &src, uint32_t *d_flag, cudaStream_t s);
 
 // Closure iteration
+// A tensor-core-capable product of a closure and where its groups of 4
+// tile-rows start in the grouped tensor-core plan (k_plan_tc).
+struct TcRows {
+    uint32_t prod, row_start, pref, pad;
+};
+cudaError_t launch_plan_tc(const ProdDesc *d_prods, uint32_t nprods, const TcRows *d_tc, uint32_t ntc,
+                           uint32_t total_groups, const MatSlot *d_slots, IterState *d_st, uint64_t *d_items,
+                           size_t list_cap, int tiles_per_block, uint32_t *d_prod_seen, const uint8_t *d_choice,
+                           cudaStream_t s);
 cudaError_t launch_plan(const ProdDesc *d_prods, uint32_t nprods, uint32_t row_begin, uint32_t row_end,
                         const MatSlot *d_slots, IterState *d_st, uint64_t *d_items, size_t list_cap,
                         int tiles_per_block, uint32_t *d_prod_seen, int tc_mode, const uint8_t *d_choice,

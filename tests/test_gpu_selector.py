@@ -115,6 +115,32 @@ def test_auto_closure_with_tensor_core_terms(pkg, oracle, sctx, tmp_path, loop):
         q.close()
 
 
+@pytest.mark.parametrize("loop", ["graph", "host"])
+def test_batch_with_grouped_tensor_core_launches(pkg, oracle, sctx, tmp_path, loop):
+    """A batch whose terms go to the tensor cores from the first iteration:
+    every iteration plans all tensor-core terms of all queries (different n,
+    grammars and matrices) in one launch and runs their items in one
+    tensor-core launch; every query's lines equal the oracle's, and so do
+    those of the fixed-variant TC batch."""
+    wls = [pkg.workloads.ontology_query(700, 5), pkg.workloads.brackets_query(300, 1500, 2),
+           _random_cnf(pkg, 520, 1400, 4), pkg.workloads.ontology_query(1100, 6), _random_cnf(pkg, 257, 900, 8)]
+    exp = [_expected(oracle, w, tmp_path) for w in wls]
+    sctx.selector_configure(mode="heuristic", tc_min_tiles=1, tc_min_occ=0.0, tc_min_dense=0.0, min_tiles=1)
+    qs = [pkg.query.PreparedQuery(sctx, w.grammar, w.graph) for w in wls]
+    try:
+        for variant in ("auto", "tc"):
+            for q in qs:
+                q.load()
+            st, iters, _ = sctx.closure_batch([(q.grammar.rules, q.mats) for q in qs], variant=variant,
+                                              use_graph=loop)
+            for q, e in zip(qs, exp):
+                assert dict(zip(q.grammar.nonterminals, sctx.hash_count_many(q.mats))) == e
+            assert st["variant_items"][pkg.capi.VARIANT_TC] > 0
+    finally:
+        for q in qs:
+            q.close()
+
+
 def test_product_log_times_every_candidate(pkg, oracle, sctx, tmp_path):
     wl = pkg.workloads.ontology_query(1024, 4)
     exp = _expected(oracle, wl, tmp_path)
