@@ -639,8 +639,9 @@ static int ensure_hash_buffers(cfpq_ctx *ctx, size_t nm) {
     return CFPQ_OK;
 }
 
-// Hash launches of several matrices (one kernel per kHashBatch matrices) and
-// the copy of their (hash terms, count) pairs into the pinned h_hash.
+// Hash launches of several matrices (one kernel per kHashBatch matrices, one
+// block per occupancy word) and the copy of their (hash terms, count) pairs into the
+// pinned h_hash.
 static int enqueue_hash_many(cfpq_ctx *ctx, cfpq_matrix *const *mats, size_t nmats) {
     TRY(ensure_hash_buffers(ctx, nmats));
     for (size_t i0 = 0; i0 < nmats; i0 += kHashBatch) {
@@ -654,8 +655,7 @@ static int enqueue_hash_many(cfpq_ctx *ctx, cfpq_matrix *const *mats, size_t nma
             hb.m[k] = mats[i]->d;
             hb.pow11[k] = pt.d_pow11;
             hb.pow13[k] = pt.d_pow13;
-            const size_t tiles = (size_t)mats[i]->d.T * mats[i]->d.T;
-            hb.start[k + 1] = hb.start[k] + (uint32_t)((tiles + 3) / 4);
+            hb.start[k + 1] = hb.start[k] + mats[i]->d.T * mats[i]->d.ow;  // one block per occupancy word
         }
         CUDA_TRY(launch_hash_count_many(hb, ctx->d_hash + 2 * i0, ctx->stream));
     }

@@ -187,42 +187,68 @@ __global__ void k_rows_scatter(DevMat m, const uint64_t *__restrict__ rows) {
 // Block = 4 tiles x 64 rows; thread = one row word of one tile.  Unoccupied
 // tiles exit at once.  out[0] accumulates terms < 2^30 (no overflow below
 // 2^34 terms), out[1] the bit count.
-__device__ __forceinline__ void hash_count_block(const DevMat &m, const uint32_t *__restrict__ pow11,
-                                                 const uint32_t *__restrict__ pow13, unsigned long long *out,
-                                                 size_t block) {
-    const size_t tile = block * 4 + (threadIdx.x >> 6);
-    const uint32_t r = threadIdx.x & 63;
-    unsigned long long h = 0, cnt = 0;
-    if (tile < (size_t)m.T * m.T) {
-        const uint32_t ti = (uint32_t)(tile / m.T), tj = (uint32_t)(tile % m.T);
-        if ((m.occ[(size_t)ti * m.ow + (tj >> 5)] >> (tj & 31)) & 1u) {
-            uint64_t v = m.bits[tile * 64 + r];
-            if (v) {
-                cnt = __popcll(v);
-                const uint32_t *p = pow11 + tj * 64;
-                unsigned long long line = 0;
-                while (v) {
-                    const int b = __ffsll((long long)v) - 1;
-                    v &= v - 1;
-                    line += p[b];
-                }
-                h = ((line % kHashMod) * pow13[ti * 64 + r]) % kHashMod;
-            }
+// Result line terms of one occupied tile (ti, tj) (one warp), with no loads
+// inside the bit loops: Sum over set bits (r, c) of 11^(n-1-c) 13^(n-1-r)
+// regrouped by column -- lane l sums the row powers of the rows whose bit l
+// (and bit l + 32) is set, broadcast row by row with shuffles, then
+// multiplies once by its columns' powers.  The power tables are indexed by
+// internal vertex index; every addend is below 2^30 (row sums below 2^36
+// before their reduction), so the 64-bit sums cannot overflow.
+__device__ __forceinline__ void hash_tile(const DevMat &m, const uint32_t *__restrict__ pow11,
+                                          const uint32_t *__restrict__ pow13, uint32_t ti, uint32_t tj,
+                                          unsigned long long &h, unsigned long long &cnt) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t *tile = m.bits + tile_offset(m.T, ti, tj);
+    const uint64_t w0 = tile[lane], w1 = tile[lane + 32];  // rows lane, lane + 32
+    const uint32_t q0 = pow13[(size_t)ti * 64 + lane], q1 = pow13[(size_t)ti * 64 + lane + 32];
+    const uint32_t pa = pow11[(size_t)tj * 64 + lane], pb = pow11[(size_t)tj * 64 + lane + 32];
+    cnt += __popcll(w0) + __popcll(w1);
+    unsigned long long acc_a = 0, acc_b = 0;  // columns lane, lane + 32
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+        const uint64_t w = half ? w1 : w0;
+        const uint32_t q = half ? q1 : q0;
+        unsigned rows = __ballot_sync(kFull, w != 0);
+        while (rows) {
+            const uint32_t r = __ffs(rows) - 1;
+            rows &= rows - 1;
+            const uint64_t v = __shfl_sync(kFull, w, r);
+            const uint32_t qr = __shfl_sync(kFull, q, r);
+            if ((v >> lane) & 1u) acc_a += qr;
+            if ((v >> (lane + 32)) & 1u) acc_b += qr;
         }
+    }
+    h += ((acc_a % kHashMod) * pa) % kHashMod + ((acc_b % kHashMod) * pb) % kHashMod;
+}
+
+// Result line of occupancy word wi of m (one block of 8 warps: the word's
+// occupied tiles dealt round-robin to the warps), then one atomic pair per
+// block.
+__device__ __forceinline__ void hash_count_word(const DevMat &m, const uint32_t *__restrict__ pow11,
+                                                const uint32_t *__restrict__ pow13, unsigned long long *out,
+                                                uint32_t wi) {
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const uint32_t ti = wi / m.ow, word = wi % m.ow;
+    uint32_t bits = m.occ[wi];
+    unsigned long long h = 0, cnt = 0;
+    for (uint32_t k = 0; bits; ++k) {
+        const uint32_t tj = word * 32 + (__ffs(bits) - 1);
+        bits &= bits - 1;
+        if (k % nw == warp) hash_tile(m, pow11, pow13, ti, tj, h, cnt);
     }
     for (int o = 16; o > 0; o >>= 1) {
         h += __shfl_down_sync(kFull, h, o);
         cnt += __shfl_down_sync(kFull, cnt, o);
     }
     __shared__ unsigned long long sh[8], sc[8];
-    if ((threadIdx.x & 31) == 0) {
-        sh[threadIdx.x >> 5] = h;
-        sc[threadIdx.x >> 5] = cnt;
+    if (lane == 0) {
+        sh[warp] = h;
+        sc[warp] = cnt;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
         unsigned long long H = 0, C = 0;
-        for (int i = 0; i < 8; ++i) {
+        for (uint32_t i = 0; i < nw; ++i) {
             H += sh[i];
             C += sc[i];
         }
@@ -233,15 +259,16 @@ __device__ __forceinline__ void hash_count_block(const DevMat &m, const uint32_t
 
 __global__ void __launch_bounds__(256) k_hash_count(DevMat m, const uint32_t *__restrict__ pow11,
                                                     const uint32_t *__restrict__ pow13, unsigned long long *out) {
-    hash_count_block(m, pow11, pow13, out, blockIdx.x);
+    hash_count_word(m, pow11, pow13, out, blockIdx.x);
 }
 
-// Several matrices in one launch: blocks [start[i], start[i+1]) hash matrix i
-// into out[2i], out[2i+1] (zeroed by the launcher).
+// Several matrices in one launch: blocks [start[i], start[i+1]) hash the
+// occupancy words of matrix i into out[2i], out[2i+1] (zeroed by the
+// launcher).
 __global__ void __launch_bounds__(256) k_hash_count_many(HashBatch hb, unsigned long long *out) {
     uint32_t i = 0;
     while (i + 1 < hb.count && blockIdx.x >= hb.start[i + 1]) ++i;
-    hash_count_block(hb.m[i], hb.pow11[i], hb.pow13[i], out + 2 * i, blockIdx.x - hb.start[i]);
+    hash_count_word(hb.m[i], hb.pow11[i], hb.pow13[i], out + 2 * i, blockIdx.x - hb.start[i]);
 }
 
 // ---- plain dense product (variant PLAIN) ------------------------------------
@@ -561,8 +588,7 @@ cudaError_t launch_hash_count(const DevMat &m, const uint32_t *d_pow11, const ui
                               unsigned long long *d_out, cudaStream_t s) {
     cudaError_t e = cudaMemsetAsync(d_out, 0, 2 * sizeof(unsigned long long), s);
     if (e != cudaSuccess || m.T == 0) return e;
-    const size_t tiles = (size_t)m.T * m.T;
-    k_hash_count<<<(unsigned)((tiles + 3) / 4), 256, 0, s>>>(m, d_pow11, d_pow13, d_out);
+    k_hash_count<<<m.T * m.ow, 256, 0, s>>>(m, d_pow11, d_pow13, d_out);
     return cudaGetLastError();
 }
 

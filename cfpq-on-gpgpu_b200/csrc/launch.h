@@ -53,7 +53,7 @@ struct HashBatch {
     DevMat m[kHashBatch];
     const uint32_t *pow11[kHashBatch];
     const uint32_t *pow13[kHashBatch];
-    uint32_t start[kHashBatch + 1];
+    uint32_t start[kHashBatch + 1];  // prefix sums of the matrices' occupancy words (one block each)
     uint32_t count;
 };
 cudaError_t launch_hash_count_many(const HashBatch &hb, unsigned long long *d_out, cudaStream_t s);
