@@ -97,6 +97,29 @@ def test_hash_count(ctx, oracle, n):
         m.destroy()
 
 
+def test_hash_count_large_ragged(ctx, oracle):
+    """The result-line hash (one block per occupancy word, column sums of
+    row powers per tile) on a ragged n = 20000 (313 tile-rows, 10 occupancy
+    words per row): scattered bits plus some dense blocks, and the
+    single-matrix and batched entry points against the oracle."""
+    n = 20000
+    rng = np.random.default_rng(20000)
+    wpr = (n + 63) // 64
+    rows = np.zeros((n, wpr), dtype=np.uint64)
+    r = rng.integers(0, n, 300000)
+    c = rng.integers(0, n, 300000)
+    np.bitwise_or.at(rows, (r, c // 64), np.left_shift(np.uint64(1), (c % 64).astype(np.uint64)))
+    rows[4000:4200, 30:40] = np.uint64(0xFFFFFFFFFFFFFFFF)   # dense blocks, a full tile-row stripe
+    rows[19990:20000, wpr - 1] = np.uint64((1 << (n % 64)) - 1)  # last columns of the last rows
+    m = upload(ctx, n, rows)
+    try:
+        exp = oracle.hash_count(rows, n)
+        assert m.hash_count() == exp
+        assert ctx.hash_count_many([m, m]) == [exp, exp]
+    finally:
+        m.destroy()
+
+
 def test_upload_download_roundtrip(ctx):
     rng = np.random.default_rng(3)
     for n in (1, 64, 77, 1000):
