@@ -36,7 +36,9 @@ def main():
     ap.add_argument("--density", type=float, default=0.3)
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--seed", type=int, default=1)
-    ap.add_argument("--no-graph", action="store_true", help="closure, chain: host-launched iterations, no CUDA graph")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="closure, chain, batch: host-launched iterations, no CUDA graph or persistent kernel "
+                         "(every kernel a separate launch, as a profiler needs)")
     args = ap.parse_args()
 
     import numpy as np
@@ -80,7 +82,8 @@ def main():
             ctx.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            st, iters, _ = ctx.closure_batch([(q.grammar.rules, q.mats) for q in qs])
+            st, iters, _ = ctx.closure_batch([(q.grammar.rules, q.mats) for q in qs],
+                                             use_graph="host" if args.no_graph else True)
             e1.record(stream)
             e1.synchronize()
             times.append(e0.elapsed_time(e1))
