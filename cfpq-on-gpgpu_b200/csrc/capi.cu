@@ -1147,14 +1147,14 @@ static BufCounters *closure_counters(cfpq_ctx *ctx, const ClosurePlan &) {
 
 // Plan of one iteration; in AUTO closures the planner also chooses every
 // term's variant (PlanSelect).
-static int enqueue_select_plan(cfpq_ctx *ctx, const ClosurePlan &pl, cudaStream_t s) {
+static int enqueue_select_plan(cfpq_ctx *ctx, const ClosurePlan &pl, const QueryTrack &qt, cudaStream_t s) {
     const PlanSelect ps = {ctx->d_sel.as<SelectorParams>(), ctx->cnts.as<BufCounters>(), ctx->tc_ok.as<uint8_t>(),
                            ctx->choice.as<uint8_t>(), ctx->sel_log_iters ? ctx->sel_log.as<SelLogRow>() : nullptr,
                            ctx->sel_log_iters};
     CUDA_TRY(launch_plan(ctx->prods.as<ProdDesc>(), (uint32_t)pl.prods.size(), 0, pl.prod_rows,
                          ctx->slots.as<MatSlot>(), ctx->d_st, ctx->items.as<uint64_t>(), pl.item_cap,
                          product_lop3_tiles_per_block(), ctx->prod_seen.as<uint32_t>(), 0, ctx->choice.as<uint8_t>(),
-                         s, pl.auto_select ? &ps : nullptr));
+                         s, pl.auto_select ? &ps : nullptr, qt.last_iter));
     return CFPQ_OK;
 }
 
@@ -1171,7 +1171,7 @@ static int enqueue_products(cfpq_ctx *ctx, const ClosurePlan &pl, const QueryTra
         CUDA_TRY(launch_plan_tc(pr, (uint32_t)pl.prods.size(), ctx->tc_rows.as<TcRows>(),
                                 (uint32_t)pl.tc_rows.size(), pl.tc_groups, sl, ctx->d_st, ctx->items.as<uint64_t>(),
                                 pl.item_cap, product_lop3_tiles_per_block(), ctx->prod_seen.as<uint32_t>(),
-                                ctx->choice.as<uint8_t>(), s));
+                                ctx->choice.as<uint8_t>(), s, qt.last_iter));
         CUDA_TRY(launch_product_tc(pr, sl, ctx->d_st, ctx->items.as<uint64_t>(), pl.item_cap, qt.changed,
                                    ctx->tc_grid, cnts, s));
         CUDA_TRY(launch_reset_list(ctx->d_st, 2, s));
@@ -1181,7 +1181,7 @@ static int enqueue_products(cfpq_ctx *ctx, const ClosurePlan &pl, const QueryTra
 
 static int enqueue_iteration(cfpq_ctx *ctx, const ClosurePlan &pl, const QueryTrack &qt,
                              cudaGraphConditionalHandle handle, int use_handle) {
-    TRY(enqueue_select_plan(ctx, pl, ctx->stream));
+    TRY(enqueue_select_plan(ctx, pl, qt, ctx->stream));
     TRY(enqueue_products(ctx, pl, qt, ctx->stream));
     CUDA_TRY(launch_advance_end(ctx->slots.as<MatSlot>(), (uint32_t)pl.slots.size(), pl.slot_rows, ctx->d_st, qt,
                                 handle, use_handle, closure_counters(ctx, pl), ctx->stream));
@@ -1192,7 +1192,7 @@ static int enqueue_iteration(cfpq_ctx *ctx, const ClosurePlan &pl, const QueryTr
 static int enqueue_iteration_timed(cfpq_ctx *ctx, const ClosurePlan &pl, const QueryTrack &qt) {
     cudaStream_t s = ctx->stream;
     CUDA_TRY(cudaEventRecord(ctx->kev[0], s));
-    TRY(enqueue_select_plan(ctx, pl, s));
+    TRY(enqueue_select_plan(ctx, pl, qt, s));
     CUDA_TRY(cudaEventRecord(ctx->kev[1], s));
     TRY(enqueue_products(ctx, pl, qt, s));
     CUDA_TRY(cudaEventRecord(ctx->kev[2], s));

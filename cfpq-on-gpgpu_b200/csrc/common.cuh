@@ -157,6 +157,10 @@ struct PlanSelect {
     uint8_t *choice;
     SelLogRow *log;
     uint32_t log_iters;
+    // non-null (multi-kernel iterations): per query the last iteration
+    // (1-based) in which it changed; a query that did not change in the
+    // previous iteration has empty deltas and is not planned
+    const uint32_t *q_last;
 };
 
 constexpr uint32_t kBarChanged = 1u;  // some product set a new bit

@@ -616,9 +616,11 @@ cudaError_t launch_merge_or(const DevMat &dst, const DevMat &src, uint32_t *d_fl
 cudaError_t launch_plan(const ProdDesc *d_prods, uint32_t nprods, uint32_t row_begin, uint32_t row_end,
                         const MatSlot *d_slots, IterState *d_st, uint64_t *d_items, size_t list_cap,
                         int tiles_per_block, uint32_t *d_prod_seen, int tc_mode, const uint8_t *d_choice,
-                        cudaStream_t s, const PlanSelect *sel) {
+                        cudaStream_t s, const PlanSelect *sel, const uint32_t *d_q_last) {
     if (row_end <= row_begin || nprods == 0) return cudaSuccess;
-    PlanSelect ps = sel ? *sel : PlanSelect{nullptr, nullptr, nullptr, const_cast<uint8_t *>(d_choice), nullptr, 0};
+    PlanSelect ps = sel ? *sel
+                        : PlanSelect{nullptr, nullptr, nullptr, const_cast<uint8_t *>(d_choice), nullptr, 0, nullptr};
+    ps.q_last = d_q_last;
     k_plan<<<grid_for((size_t)(row_end - row_begin) * 32, kPlanThreads), kPlanThreads, 0, s>>>(
         d_prods, nprods, row_begin, row_end, d_slots, d_st, d_items, list_cap, tiles_per_block, d_prod_seen, tc_mode,
         ps);
@@ -628,9 +630,9 @@ cudaError_t launch_plan(const ProdDesc *d_prods, uint32_t nprods, uint32_t row_b
 cudaError_t launch_plan_tc(const ProdDesc *d_prods, uint32_t nprods, const TcRows *d_tc, uint32_t ntc,
                            uint32_t total_groups, const MatSlot *d_slots, IterState *d_st, uint64_t *d_items,
                            size_t list_cap, int tiles_per_block, uint32_t *d_prod_seen, const uint8_t *d_choice,
-                           cudaStream_t s) {
+                           cudaStream_t s, const uint32_t *d_q_last) {
     if (ntc == 0 || total_groups == 0) return cudaSuccess;
-    const PlanSelect ps{nullptr, nullptr, nullptr, const_cast<uint8_t *>(d_choice), nullptr, 0};
+    const PlanSelect ps{nullptr, nullptr, nullptr, const_cast<uint8_t *>(d_choice), nullptr, 0, d_q_last};
     k_plan_tc<<<grid_for((size_t)total_groups * 32, kPlanThreads), kPlanThreads, 0, s>>>(
         d_prods, nprods, d_tc, ntc, total_groups, d_slots, d_st, d_items, list_cap, tiles_per_block, d_prod_seen, ps);
     return cudaGetLastError();

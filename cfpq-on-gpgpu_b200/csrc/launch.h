@@ -74,11 +74,11 @@ struct TcRows {
 cudaError_t launch_plan_tc(const ProdDesc *d_prods, uint32_t nprods, const TcRows *d_tc, uint32_t ntc,
                            uint32_t total_groups, const MatSlot *d_slots, IterState *d_st, uint64_t *d_items,
                            size_t list_cap, int tiles_per_block, uint32_t *d_prod_seen, const uint8_t *d_choice,
-                           cudaStream_t s);
+                           cudaStream_t s, const uint32_t *d_q_last = nullptr);
 cudaError_t launch_plan(const ProdDesc *d_prods, uint32_t nprods, uint32_t row_begin, uint32_t row_end,
                         const MatSlot *d_slots, IterState *d_st, uint64_t *d_items, size_t list_cap,
                         int tiles_per_block, uint32_t *d_prod_seen, int tc_mode, const uint8_t *d_choice,
-                        cudaStream_t s, const PlanSelect *sel = nullptr);
+                        cudaStream_t s, const PlanSelect *sel = nullptr, const uint32_t *d_q_last = nullptr);
 // (tc_mode 0 plans the word-level products of the row range, 1 the tensor-core
 // ones; the variant of product p is d_choice[p], or its descriptor's when
 // null; with sel, the word-level plan decides the variants, PlanSelect.)

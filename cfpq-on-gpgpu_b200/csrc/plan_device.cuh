@@ -77,6 +77,7 @@ __device__ __forceinline__ void plan_row(uint32_t gw, const ProdDesc *__restrict
     }
     const ProdDesc pd = prods[lo];
     if (pd.term == 1 && iter == 0) return;  // first iteration: delta(A) = A, one term covers A*B
+    if (ps.q_last && iter > 0 && ps.q_last[pd.query] != iter) return;  // both terms read an empty delta
     uint32_t variant;  // this iteration's variant of the product
     if (ps.sel && !tc_mode) {
         float f[kSelFeatures], pred[kSelOutputs] = {0.f, 0.f, 0.f};
