@@ -88,3 +88,28 @@ def test_intersection_errors(ctx, pkg):
         assert lines == ctx.closure_hash(wl.grammar.rules, q.mats)[1]
     finally:
         q.close()
+
+
+def test_intersection_empty_graph(ctx, pkg, oracle, tmp_path):
+    """No edges: only the epsilon diagonal is set (S -> S S keeps it, the
+    other nonterminals stay empty), matching the oracle's line of the n x n
+    identity; a later call with the edges gives the full answer on the same
+    matrices."""
+    graph = pkg.workloads.uniform_graph(200, 600, ["a", "b"], 9)
+    wl = pkg.workloads.Workload("dyck_eps", "S\nS A S1\nS1 S B\nS S S\nA a\nB b\n", graph, {})
+    n = graph.n
+    ident = np.zeros((n, (n + 63) // 64), dtype=np.uint64)
+    for v in range(n):
+        ident[v, v // 64] |= np.uint64(1) << np.uint64(v % 64)
+    exp_empty = {name: (0, 0) for name in wl.grammar.nonterminals}
+    exp_empty["S"] = oracle.hash_count(ident, n)
+    q = pkg.query.PreparedQuery(ctx, wl.grammar, wl.graph)
+    try:
+        z = np.zeros(0, np.uint32)
+        _, lines = ctx.intersection(wl.grammar.rules, q.mats, z, z, z, q.off, q.lm, epsilon=wl.grammar.epsilon)
+        assert dict(zip(wl.grammar.nonterminals, lines)) == exp_empty
+        _, lines = ctx.intersection(wl.grammar.rules, q.mats, graph.src, graph.label, graph.dst, q.off, q.lm,
+                                    epsilon=wl.grammar.epsilon)
+        assert dict(zip(wl.grammar.nonterminals, lines)) == _oracle_lines(oracle, wl, tmp_path)
+    finally:
+        q.close()
