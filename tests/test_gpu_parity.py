@@ -501,14 +501,20 @@ def test_engine_matches_golden(ctx, pkg, oracle, case):
 
 
 def test_b200gpu_executable(pkg, oracle, tmp_path):
+    """The drop-in executable on a random graph and an ontology graph: the
+    engine with the vertex order its backend suggests at upload (default),
+    without it (CFPQ_ORDER=0), and the reference's worklist with the plain
+    product on ordered matrices; every answer equals the oracle's."""
     exe = os.path.join(os.path.dirname(pkg.capi.LIB_PATH), "..", "bin", "b200GPU")
-    wl = pkg.workloads.brackets_query(n=512, nedges=2048, seed=3)
-    gp, rp = _write(wl, tmp_path)
-    exp, _, _ = _oracle_run(oracle, gp, rp)
-    for env in ({}, {"CFPQ_DRIVER": "worklist", "CFPQ_VARIANT": "plain"}):
-        got, (total, algo) = oracle.run_executable(exe, gp, rp, env={**os.environ, **env})
-        assert got == exp
-        assert total >= algo >= 0
+    for wl in (pkg.workloads.brackets_query(n=512, nedges=2048, seed=3), pkg.workloads.ontology_query(2048, 2)):
+        d = tmp_path / wl.name
+        d.mkdir()
+        gp, rp = _write(wl, d)
+        exp, _, _ = _oracle_run(oracle, gp, rp)
+        for env in ({}, {"CFPQ_ORDER": "0"}, {"CFPQ_DRIVER": "worklist", "CFPQ_VARIANT": "plain"}):
+            got, (total, algo) = oracle.run_executable(exe, gp, rp, env={**os.environ, **env})
+            assert got == exp, (wl.name, env)
+            assert total >= algo >= 0
 
 
 @pytest.mark.parametrize("exe", ["naiveGPU", "m4riGPU"])
