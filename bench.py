@@ -190,32 +190,44 @@ def reference_arm(args, world, rank):
     print(json.dumps(line))
 
 
-def cpu_baseline(wl, budget_s=12.0) -> dict:
+def cpu_baseline(wl, budget_s=12.0, budget_1thread_s=8.0) -> dict:
+    """The reference's CPU path on this host's cores: all threads (the
+    reported value) and one thread (a bounded sample beside it)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
 
     exe = oracle.ref_executable("m4riCPU")
-    threads = os.cpu_count() or 1
+    nproc = os.cpu_count() or 1
     with tempfile.TemporaryDirectory() as d:
         gp, rp = os.path.join(d, "grammar.txt"), os.path.join(d, "graph.txt")
         wl.write(gp, rp)
-        times, answer = [], None
-        t_start = time.perf_counter()
-        while time.perf_counter() - t_start < budget_s or not times:
-            if exe:
-                answer, (_, algo) = oracle.run_executable(exe, gp, rp,
-                                                          env={**os.environ, "OMP_NUM_THREADS": str(threads)})
-                times.append(max(algo, 1) / 1e3)
-            else:
-                with oracle.Problem(gp, rp) as p:
-                    times.append(p.closure(oracle.M4RM, threads) / 1e3)
-                    answer = p.results()
-            if len(times) >= 50:
-                break
+
+        def sample(threads, budget):
+            times, answer = [], None
+            t_start = time.perf_counter()
+            while time.perf_counter() - t_start < budget or not times:
+                if exe:
+                    answer, (_, algo) = oracle.run_executable(exe, gp, rp,
+                                                              env={**os.environ, "OMP_NUM_THREADS": str(threads)})
+                    times.append(max(algo, 1) / 1e3)
+                else:
+                    with oracle.Problem(gp, rp) as p:
+                        times.append(p.closure(oracle.M4RM, threads) / 1e3)
+                        answer = p.results()
+                if len(times) >= 50:
+                    break
+            return times, answer
+
+        times, answer = sample(nproc, budget_s)
+        times1, answer1 = sample(1, budget_1thread_s) if nproc > 1 else (times, answer)
     kind = "reference" if exe else "port"
-    return {"value": len(times) / sum(times), "unit": "closures/s", "cores": threads, "kind": kind,
-            "sample": f"{len(times)} full closures of the same workload, algorithm time, "
-                      f"{'reference m4riCPU main + restated libm4ri' if exe else 'oracle M4RM port'}",
+    what = "reference m4riCPU main + restated libm4ri" if exe else "oracle M4RM port"
+    return {"value": len(times) / sum(times), "unit": "closures/s", "cores": nproc, "kind": kind,
+            "nproc": nproc,
+            "sample": f"{len(times)} full closures of the same workload, algorithm time, {what}",
+            "one_thread": {"value": len(times1) / sum(times1), "unit": "closures/s", "cores": 1,
+                           "sample": f"{len(times1)} full closures, OMP_NUM_THREADS=1",
+                           "same_answer": answer1 == answer},
             "answer": answer}
 
 
