@@ -137,8 +137,9 @@ static int pool_give(cfpq_ctx *ctx, cfpq_matrix *m, bool dirty) {
 
 // Hash power tables for vertex ids 0..n-1 stored at internal index perm[v]
 // (identity when perm is null): pow11[perm[c]] = 11^(n-1-c),
-// pow13[perm[r]] = 13^(n-1-r) modulo 1e9+7 (cfpq-cpp/Grammar.cpp:12-14).
-static int make_pow_tables(uint32_t n, const uint32_t *perm, PowTables *t) {
+// pow13[perm[r]] = 13^(n-1-r) modulo 1e9+7 (cfpq-cpp/Grammar.cpp:12-14),
+// and the subset sums of pow11 the hash kernel reads (built on stream s).
+static int make_pow_tables(uint32_t n, const uint32_t *perm, PowTables *t, cudaStream_t s) {
     const uint32_t np = tiles_for(n) * 64;
     std::vector<uint32_t> p11(np ? np : 1, 0), p13(np ? np : 1, 0);
     const uint64_t mod = 1000000007ULL;
@@ -154,6 +155,9 @@ static int make_pow_tables(uint32_t n, const uint32_t *perm, PowTables *t) {
     CUDA_TRY(cudaMalloc(&t->d_pow13, p13.size() * 4));
     CUDA_TRY(cudaMemcpy(t->d_pow11, p11.data(), p11.size() * 4, cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(t->d_pow13, p13.data(), p13.size() * 4, cudaMemcpyHostToDevice));
+    const uint32_t T = tiles_for(n);
+    CUDA_TRY(cudaMalloc(&t->d_sub11, (size_t)(T ? T : 1) * 2048 * 4));
+    if (T) CUDA_TRY(launch_pow_subsets(t->d_pow11, T, t->d_sub11, s));
     return CFPQ_OK;
 }
 
@@ -169,7 +173,7 @@ static int get_pow_tables(cfpq_ctx *ctx, const cfpq_matrix *m, PowTables *out) {
         return CFPQ_OK;
     }
     PowTables t;
-    TRY(make_pow_tables(n, nullptr, &t));
+    TRY(make_pow_tables(n, nullptr, &t, ctx->stream));
     ctx->pow[n] = t;
     *out = t;
     return CFPQ_OK;
@@ -194,7 +198,7 @@ extern "C" int cfpq_order_create(cfpq_ctx *ctx, uint32_t n, const uint32_t *perm
             return set_error(CFPQ_ERR_CUDA, "order upload: %s", cudaGetErrorString(e));
         }
     }
-    int rc = make_pow_tables(n, n ? perm : nullptr, &o->pow);
+    int rc = make_pow_tables(n, n ? perm : nullptr, &o->pow, ctx->stream);
     if (rc != CFPQ_OK) {
         if (o->d_perm) cudaFree(o->d_perm);
         delete o;
@@ -211,6 +215,7 @@ extern "C" int cfpq_order_destroy(cfpq_ctx *ctx, cfpq_order *order) {
     if (order->d_perm) cudaFree(order->d_perm);
     if (order->pow.d_pow11) cudaFree(order->pow.d_pow11);
     if (order->pow.d_pow13) cudaFree(order->pow.d_pow13);
+    if (order->pow.d_sub11) cudaFree(order->pow.d_sub11);
     delete order;
     return CFPQ_OK;
 }
@@ -288,6 +293,7 @@ extern "C" int cfpq_ctx_destroy(cfpq_ctx *ctx) {
     for (auto &kv : ctx->pow) {
         cudaFree(kv.second.d_pow11);
         cudaFree(kv.second.d_pow13);
+        cudaFree(kv.second.d_sub11);
     }
     for (DevBuf *b : {&ctx->stage, &ctx->items, &ctx->prods, &ctx->slots, &ctx->qtrack, &ctx->prod_seen,
                       &ctx->mats_desc, &ctx->edge_buf, &ctx->phase_log, &ctx->clear_desc, &ctx->diag_desc,
@@ -300,6 +306,8 @@ extern "C" int cfpq_ctx_destroy(cfpq_ctx *ctx) {
     cudaFree(ctx->d_flag);
     cudaFree(ctx->d_bad);
     if (ctx->d_hash) cudaFree(ctx->d_hash);
+    if (ctx->d_hash_part) cudaFree(ctx->d_hash_part);
+    if (ctx->d_hash_ticket) cudaFree(ctx->d_hash_ticket);
     cudaFreeHost(ctx->h_st);
     cudaFreeHost(ctx->h_flag);
     if (ctx->h_hash) cudaFreeHost(ctx->h_hash);
@@ -421,9 +429,32 @@ extern "C" void *cfpq_ctx_stream(const cfpq_ctx *ctx) { return ctx ? (void *)ctx
 // (matrix descriptors, label offsets, label -> matrices) on the device, host
 // edge arrays copied (asynchronously) into the context's staging block.
 // Fills the edge fields of *in; launches nothing.  Nothing to scatter: in->nedges = 0.
+// The device address of host array a[0..n) when all of it is pinned and
+// mapped into this device's address space, else null.
+static const uint32_t *mapped_host_array(const uint32_t *a, size_t n) {
+    const uint32_t *ends[2] = {a, a + n - 1};
+    const uint32_t *dev[2] = {nullptr, nullptr};
+    for (int k = 0; k < 2; ++k) {
+        cudaPointerAttributes at;
+        if (cudaPointerGetAttributes(&at, ends[k]) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        if (at.type != cudaMemoryTypeHost || !at.devicePointer) return nullptr;
+        dev[k] = static_cast<const uint32_t *>(at.devicePointer);
+    }
+    return dev[1] == dev[0] + (n - 1) ? dev[0] : nullptr;
+}
+
+// The edge scatter's input.  Host edge arrays are copied into the context's
+// staging buffer, except with read_pinned_in_place, where arrays in pinned
+// mapped host memory are read by the scatter kernel itself over the bus (the
+// caller must keep them unchanged until the stream has run the kernel).
 static int prepare_edges(cfpq_ctx *ctx, cfpq_matrix *const *mats, size_t nmats, const uint32_t *from,
                          const uint32_t *label, const uint32_t *to, size_t nedges, const uint32_t *label_offsets,
-                         const uint32_t *label_mats, uint32_t nlabels, bool on_device, ClosureInput *in) {
+                         const uint32_t *label_mats, uint32_t nlabels, bool on_device, ClosureInput *in,
+                         bool read_pinned_in_place = false, bool *read_in_place = nullptr) {
+    if (read_in_place) *read_in_place = false;
     in->nedges = 0;
     if ((nmats && !mats) || (nedges && (!from || !label || !to)) || (nlabels && (!label_offsets)))
         return set_error(CFPQ_ERR_INVALID, "null argument");
@@ -489,7 +520,14 @@ static int prepare_edges(cfpq_ctx *ctx, cfpq_matrix *const *mats, size_t nmats, 
         // host-edge loads overwrite the edge arrays only, never the tables
         ctx->edge_tables_key = std::move(key);
     }
-    if (on_device) {
+    const uint32_t *m_from = nullptr, *m_label = nullptr, *m_to = nullptr;
+    if (!on_device && read_pinned_in_place && (m_from = mapped_host_array(from, nedges)) &&
+        (m_label = mapped_host_array(label, nedges)) && (m_to = mapped_host_array(to, nedges))) {
+        d_from = const_cast<uint32_t *>(m_from);
+        d_label = const_cast<uint32_t *>(m_label);
+        d_to = const_cast<uint32_t *>(m_to);
+        if (read_in_place) *read_in_place = true;
+    } else if (on_device) {
         d_from = const_cast<uint32_t *>(from);
         d_label = const_cast<uint32_t *>(label);
         d_to = const_cast<uint32_t *>(to);
@@ -625,42 +663,76 @@ extern "C" int cfpq_matrix_tile_stats(cfpq_ctx *ctx, const cfpq_matrix *m, uint3
     return sync_and_check(ctx);
 }
 
-static int ensure_hash_buffers(cfpq_ctx *ctx, size_t nm) {
+// Result buffers for nm matrices and `blocks` hash blocks: the pinned h_hash
+// (written by the kernel through its mapping when the device can map it,
+// else copied from d_hash), the per-block partial sums and the ticket.
+static int ensure_hash_buffers(cfpq_ctx *ctx, size_t nm, size_t blocks) {
     if (ctx->d_hash_cap < nm) {
         if (ctx->d_hash) cudaFree(ctx->d_hash);
         if (ctx->h_hash) cudaFreeHost(ctx->h_hash);
         ctx->d_hash = nullptr;
-        ctx->h_hash = nullptr;
+        ctx->h_hash = ctx->h_hash_dev = nullptr;
         ctx->d_hash_cap = ctx->h_hash_cap = 0;
         CUDA_TRY(cudaMalloc(&ctx->d_hash, nm * 2 * sizeof(unsigned long long)));
         CUDA_TRY(cudaMallocHost(&ctx->h_hash, nm * 2 * sizeof(unsigned long long)));
+        if (cudaHostGetDevicePointer(reinterpret_cast<void **>(&ctx->h_hash_dev), ctx->h_hash, 0) != cudaSuccess) {
+            ctx->h_hash_dev = nullptr;
+            cudaGetLastError();
+        }
         ctx->d_hash_cap = ctx->h_hash_cap = nm;
+    }
+    if (ctx->d_hash_part_cap < blocks) {
+        if (ctx->d_hash_part) cudaFree(ctx->d_hash_part);
+        ctx->d_hash_part = nullptr;
+        ctx->d_hash_part_cap = 0;
+        CUDA_TRY(cudaMalloc(&ctx->d_hash_part, blocks * 2 * sizeof(unsigned long long)));
+        ctx->d_hash_part_cap = blocks;
+    }
+    if (!ctx->d_hash_ticket) {
+        CUDA_TRY(cudaMalloc(&ctx->d_hash_ticket, sizeof(uint32_t)));
+        CUDA_TRY(cudaMemsetAsync(ctx->d_hash_ticket, 0, sizeof(uint32_t), ctx->stream));
     }
     return CFPQ_OK;
 }
 
 // Hash launches of several matrices (one kernel per kHashBatch matrices, one
-// block per occupancy word) and the copy of their (hash terms, count) pairs into the
-// pinned h_hash.
+// block per tile-row); their (hash, count) pairs land in the pinned h_hash
+// with no copy after the kernel when h_hash is mapped.
 static int enqueue_hash_many(cfpq_ctx *ctx, cfpq_matrix *const *mats, size_t nmats) {
-    TRY(ensure_hash_buffers(ctx, nmats));
+    size_t blocks = 0;
+    for (size_t i0 = 0; i0 < nmats; i0 += kHashBatch) {
+        size_t b = 0;
+        for (size_t i = i0; i < nmats && i < i0 + kHashBatch; ++i) {
+            if (!mats[i]) return set_error(CFPQ_ERR_INVALID, "null matrix %zu", i);
+            b += mats[i]->d.T;
+        }
+        blocks = std::max(blocks, b);
+    }
+    TRY(ensure_hash_buffers(ctx, nmats, blocks));
+    unsigned long long *const out = ctx->h_hash_dev ? ctx->h_hash_dev : ctx->d_hash;
     for (size_t i0 = 0; i0 < nmats; i0 += kHashBatch) {
         HashBatch hb;
         memset(&hb, 0, sizeof(hb));
         for (size_t i = i0; i < nmats && i < i0 + kHashBatch; ++i) {
-            if (!mats[i]) return set_error(CFPQ_ERR_INVALID, "null matrix %zu", i);
             PowTables pt;
             TRY(get_pow_tables(ctx, mats[i], &pt));
             const uint32_t k = hb.count++;
             hb.m[k] = mats[i]->d;
-            hb.pow11[k] = pt.d_pow11;
+            hb.sub11[k] = pt.d_sub11;
             hb.pow13[k] = pt.d_pow13;
-            hb.start[k + 1] = hb.start[k] + mats[i]->d.T * mats[i]->d.ow;  // one block per occupancy word
+            hb.start[k + 1] = hb.start[k] + mats[i]->d.T;  // one block per tile-row
         }
-        CUDA_TRY(launch_hash_count_many(hb, ctx->d_hash + 2 * i0, ctx->stream));
+        if (hb.start[hb.count] == 0) {  // matrices of size 0 only: their lines are (0, 0)
+            if (ctx->h_hash_dev) memset(ctx->h_hash + 2 * i0, 0, 2 * sizeof(unsigned long long) * hb.count);
+            else CUDA_TRY(cudaMemsetAsync(ctx->d_hash + 2 * i0, 0, 2 * sizeof(unsigned long long) * hb.count,
+                                          ctx->stream));
+            continue;
+        }
+        CUDA_TRY(launch_hash_lines(hb, ctx->d_hash_part, ctx->d_hash_ticket, out + 2 * i0, ctx->stream));
     }
-    CUDA_TRY(cudaMemcpyAsync(ctx->h_hash, ctx->d_hash, nmats * 2 * sizeof(unsigned long long),
-                             cudaMemcpyDeviceToHost, ctx->stream));
+    if (!ctx->h_hash_dev)
+        CUDA_TRY(cudaMemcpyAsync(ctx->h_hash, ctx->d_hash, nmats * 2 * sizeof(unsigned long long),
+                                 cudaMemcpyDeviceToHost, ctx->stream));
     return CFPQ_OK;
 }
 
@@ -1464,10 +1536,7 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
     ClosurePlan &pl = pc.pl;
     const size_t nq = qs.size();
     if (pl.prods.empty()) {
-        if (input) {
-            if (input->bad) CUDA_TRY(cudaMemsetAsync(input->bad, 0, 4, ctx->stream));
-            CUDA_TRY(launch_closure_input(*input, ctx->num_sms, ctx->stream));
-        }
+        if (input) CUDA_TRY(launch_closure_input(*input, ctx->num_sms, ctx->stream));  // sets input->bad to 0 first
         if (stats) memset(stats, 0, sizeof(*stats));
         for (size_t q = 0; q < nq; ++q) {
             if (iters_out) iters_out[q] = 0;
@@ -1549,38 +1618,35 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
     const bool st_mapped = persistent && ctx->h_st_dev != nullptr;
     const bool flag_mapped = st_mapped && ho && ho->flag_src && ho->flag_dst >= ctx->h_flag &&
                              ho->flag_dst < ctx->h_flag + 16;
+    // the closure prologue: product-seen flags, query tracking, the
+    // persistent kernel's item lists (one per iteration parity, at 0 and 2 *
+    // item_cap: a zero entry means "not yet written"), the variant choices and
+    // the iteration state (zeroed, then active, limit, query count, start stamp)
+    ClosureBegin b;
+    memset(&b, 0, sizeof(b));
+    b.zero[0] = ctx->prod_seen.as<uint32_t>();
+    b.nwords[0] = pl.prods.size();
+    b.zero[1] = ctx->qtrack.as<uint32_t>();
+    b.nwords[1] = qbytes / 4;
+    b.zero[2] = ctx->items.as<uint32_t>();
+    b.nwords[2] = persistent && !lists_clean ? list_words : 0;
+    b.choice = ctx->choice.as<uint8_t>();
+    b.nchoice = nprods;
+    b.choice_value = pl.auto_select ? (uint8_t)CFPQ_VARIANT_LOP3 : pl.fixed_variant;
+    b.st = ctx->d_st;
+    b.max_iter = o.max_iterations > 0 ? (uint32_t)o.max_iterations : 0;
+    b.nqueries = (uint32_t)nq;
     // the query's input phase, enqueued right before the closure's own
     // launches (stand-alone kernels: as a prologue of the persistent kernel,
-    // between two grid barriers, it measured ~10 us slower per query)
-    if (input) {
-        if (input->bad) CUDA_TRY(cudaMemsetAsync(input->bad, 0, 4, ctx->stream));
-        CUDA_TRY(launch_closure_input(*input, ctx->num_sms, ctx->stream));
-    }
+    // between two grid barriers, it measured ~10 us slower per query); its
+    // first kernel clears the matrices and runs the closure prologue, which
+    // touches neither the matrices nor the counters
+    if (input) CUDA_TRY(launch_closure_input(*input, ctx->num_sms, ctx->stream, &b));
     if (ctx->cnts_on) CUDA_TRY(launch_counters_init(ctx->slots.as<MatSlot>(), nslots, ctx->cnts.as<BufCounters>(),
                                                     ctx->stream));
     if (ctx->sel_log_iters)
         CUDA_TRY(cudaMemsetAsync(ctx->sel_log.p, 0, (size_t)kSelLogIters * nprods * sizeof(SelLogRow), ctx->stream));
-    {
-        // one launch: product-seen flags, query tracking, the persistent
-        // kernel's item lists (one per iteration parity, at 0 and 2 * item_cap:
-        // a zero entry means "not yet written"), the variant choices and the
-        // iteration state (zeroed, then active, limit, query count, start stamp)
-        ClosureBegin b;
-        memset(&b, 0, sizeof(b));
-        b.zero[0] = ctx->prod_seen.as<uint32_t>();
-        b.nwords[0] = pl.prods.size();
-        b.zero[1] = ctx->qtrack.as<uint32_t>();
-        b.nwords[1] = qbytes / 4;
-        b.zero[2] = ctx->items.as<uint32_t>();
-        b.nwords[2] = persistent && !lists_clean ? list_words : 0;
-        b.choice = ctx->choice.as<uint8_t>();
-        b.nchoice = nprods;
-        b.choice_value = pl.auto_select ? (uint8_t)CFPQ_VARIANT_LOP3 : pl.fixed_variant;
-        b.st = ctx->d_st;
-        b.max_iter = o.max_iterations > 0 ? (uint32_t)o.max_iterations : 0;
-        b.nqueries = (uint32_t)nq;
-        CUDA_TRY(launch_closure_begin(b, ctx->num_sms, ctx->stream));
-    }
+    if (!input) CUDA_TRY(launch_closure_begin(b, ctx->num_sms, ctx->stream));
 
     cudaGraphExec_t exec = nullptr;
     if (o.use_graph && !timed && !log_products && !persistent) TRY(get_loop_graph(ctx, pl, qt, &exec));
@@ -1690,7 +1756,12 @@ static int run_engine(cfpq_ctx *ctx, const std::vector<QueryIn> &qs, const cfpq_
         stats->work_items = hs.items_total;
         stats->dense_bitops = hs.dense_bitops;
         stats->device_ms = ms;
-        stats->kernel_launches = persistent ? 2 : (uint64_t)hs.iter * 3 + 1;
+        // the input phase (first kernel with the prologue, scatter, diagonals),
+        // the counters, the prologue when it ran alone, the closure, the hash
+        const uint64_t input_launches = input ? 1 + (input->nedges ? 1 : 0) + (input->ndiag ? 1 : 0) : 0;
+        stats->kernel_launches = input_launches + (ctx->cnts_on ? 1 : 0) + (input ? 0 : 1) +
+                                 (persistent ? 1 : (uint64_t)hs.iter * 3) +
+                                 (ho && ho->n ? (ho->n + kHashBatch - 1) / kHashBatch : 0);
         stats->variant_items[CFPQ_VARIANT_LOP3] = hs.items_by_variant[2];
         stats->variant_items[CFPQ_VARIANT_M4R] = hs.items_by_variant[3];
         stats->variant_items[CFPQ_VARIANT_TC] = hs.items_by_variant[4];
@@ -1891,11 +1962,10 @@ static int prepare_diag(cfpq_ctx *ctx, cfpq_matrix *const *mats, const uint32_t 
 // synchronous flag reads).
 constexpr int kIntersectBadSlot = 8;
 
-extern "C" int cfpq_intersection(cfpq_ctx *ctx, const cfpq_rule *rules, size_t nrules, cfpq_matrix *const *mats,
-                                 size_t nmats, const cfpq_edges *edges, const uint32_t *epsilon, size_t nepsilon,
-                                 const cfpq_closure_opts *opts, cfpq_closure_stats *stats, uint64_t *hashes,
-                                 uint64_t *counts) {
-    TRY(use_device(ctx));
+static int intersection_impl(cfpq_ctx *ctx, const cfpq_rule *rules, size_t nrules, cfpq_matrix *const *mats,
+                             size_t nmats, const cfpq_edges *edges, const uint32_t *epsilon, size_t nepsilon,
+                             const cfpq_closure_opts *opts, cfpq_closure_stats *stats, uint64_t *hashes,
+                             uint64_t *counts, bool *read_in_place) {
     if (!edges) return set_error(CFPQ_ERR_INVALID, "null edge list");
     if (nepsilon && !epsilon) return set_error(CFPQ_ERR_INVALID, "null epsilon list");
     if (nmats && !mats) return set_error(CFPQ_ERR_INVALID, "null matrix list");
@@ -1911,8 +1981,10 @@ extern "C" int cfpq_intersection(cfpq_ctx *ctx, const cfpq_rule *rules, size_t n
     ClosureInput in;
     memset(&in, 0, sizeof(in));
     TRY(prepare_clear(ctx, mats, nmats, &in));
+    // the call returns only after its final synchronisation, so pinned host
+    // edges can be read in place by the scatter kernel
     TRY(prepare_edges(ctx, mats, nmats, edges->from, edges->label, edges->to, edges->count, edges->label_offsets,
-                      edges->label_mats, edges->nlabels, edges->on_device != 0, &in));
+                      edges->label_mats, edges->nlabels, edges->on_device != 0, &in, true, read_in_place));
     TRY(prepare_diag(ctx, mats, epsilon, nepsilon, &in));
     in.bad = in.nedges ? ctx->d_bad : nullptr;
     uint32_t *const h_bad = ctx->h_flag + kIntersectBadSlot;
@@ -1928,8 +2000,7 @@ extern "C" int cfpq_intersection(cfpq_ctx *ctx, const cfpq_rule *rules, size_t n
         HashOut ho{mats, want_lines ? nmats : 0, hashes, counts, in.bad, h_bad};
         TRY(run_engine(ctx, qs, o, stats, nullptr, nullptr, &ho, &in));
     } else {
-        if (in.bad) CUDA_TRY(cudaMemsetAsync(in.bad, 0, 4, ctx->stream));
-        CUDA_TRY(launch_closure_input(in, ctx->num_sms, ctx->stream));
+        CUDA_TRY(launch_closure_input(in, ctx->num_sms, ctx->stream));  // sets in.bad to 0 first
         if (in.bad) CUDA_TRY(cudaMemcpyAsync(h_bad, in.bad, 4, cudaMemcpyDeviceToHost, ctx->stream));
         TRY(cfpq_closure(ctx, rules, nrules, mats, nmats, &o, stats));
         if (want_lines) TRY(cfpq_hash_count_many(ctx, mats, nmats, hashes, counts));
@@ -1937,6 +2008,20 @@ extern "C" int cfpq_intersection(cfpq_ctx *ctx, const cfpq_rule *rules, size_t n
     }
     if (*h_bad) return set_error(CFPQ_ERR_INVALID, "cfpq_intersection: %u edge coordinates out of range", *h_bad);
     return CFPQ_OK;
+}
+
+extern "C" int cfpq_intersection(cfpq_ctx *ctx, const cfpq_rule *rules, size_t nrules, cfpq_matrix *const *mats,
+                                 size_t nmats, const cfpq_edges *edges, const uint32_t *epsilon, size_t nepsilon,
+                                 const cfpq_closure_opts *opts, cfpq_closure_stats *stats, uint64_t *hashes,
+                                 uint64_t *counts) {
+    TRY(use_device(ctx));
+    bool in_place = false;
+    const int rc = intersection_impl(ctx, rules, nrules, mats, nmats, edges, epsilon, nepsilon, opts, stats, hashes,
+                                     counts, &in_place);
+    // the scatter read the caller's pinned edges in place: never return
+    // while it may still run (the error paths skip the final synchronisation)
+    if (rc != CFPQ_OK && in_place) cudaStreamSynchronize(ctx->stream);
+    return rc;
 }
 
 extern "C" int cfpq_closure_batch(cfpq_ctx *ctx, const cfpq_query *queries, size_t nqueries,

@@ -70,6 +70,7 @@ struct DevBuf {
 struct PowTables {
     uint32_t *d_pow11 = nullptr;
     uint32_t *d_pow13 = nullptr;
+    uint32_t *d_sub11 = nullptr;  // per tile column and byte: the 256 subset sums of pow11 (launch_pow_subsets)
 };
 
 struct GraphCache {
@@ -111,8 +112,11 @@ struct cfpq_ctx {
     // small device scratch
     IterState *d_st = nullptr;
     uint32_t *d_flag = nullptr;
-    unsigned long long *d_hash = nullptr;  // 2 per matrix for hash_count_many
+    unsigned long long *d_hash = nullptr;  // 2 per matrix for hash_count_many (when h_hash is not mapped)
     size_t d_hash_cap = 0;
+    unsigned long long *d_hash_part = nullptr;  // 2 per hash block (tile-row)
+    size_t d_hash_part_cap = 0;                 // in blocks
+    uint32_t *d_hash_ticket = nullptr;          // blocks done of the running hash launch (0 between launches)
     uint32_t *d_bad = nullptr;
     // pinned host scratch
     IterState *h_st = nullptr;
@@ -120,6 +124,7 @@ struct cfpq_ctx {
     uint32_t *h_flag_dev = nullptr; // h_flag as the device sees it
     uint32_t *h_flag = nullptr;
     unsigned long long *h_hash = nullptr;
+    unsigned long long *h_hash_dev = nullptr;  // h_hash as the device sees it (null: not mapped)
     size_t h_hash_cap = 0;
     // growable device scratch
     DevBuf stage, items, prods, slots, qtrack, prod_seen, mats_desc, edge_buf, clear_desc, diag_desc;

@@ -33,7 +33,10 @@ __device__ __forceinline__ void set_occ_bit(const DevMat &m, uint32_t ti, uint32
 }
 
 // Set bit (r, c) given in vertex ids (mapped through the matrix's vertex
-// order); keep occupancy and population exact.
+// order); keep occupancy and population exact.  Only the bit that takes its
+// tile's population from 0 sets the occupancy bit (a population above 0
+// always has its occupancy bit set): a hub vertex's tile-row gets thousands
+// of new bits, and one atomic on its occupancy word per bit serialised them.
 __device__ __forceinline__ void set_one_bit(const DevMat &m, uint32_t r, uint32_t c) {
     if (m.perm) {
         r = m.perm[r];
@@ -43,10 +46,8 @@ __device__ __forceinline__ void set_one_bit(const DevMat &m, uint32_t r, uint32_
         reinterpret_cast<unsigned long long *>(m.bits + tile_offset(m.T, r >> 6, c >> 6) + (r & 63));
     const unsigned long long bit = 1ULL << (c & 63);
     const unsigned long long old = atomicOr(w, bit);
-    if (!(old & bit)) {
-        atomicAdd(m.nnz + (size_t)(r >> 6) * m.T + (c >> 6), 1u);
+    if (!(old & bit) && atomicAdd(m.nnz + (size_t)(r >> 6) * m.T + (c >> 6), 1u) == 0u)
         set_occ_bit(m, r >> 6, c >> 6);
-    }
 }
 
 // One edge (label l, r -> c) into every matrix of its label; ids out of a

@@ -183,92 +183,135 @@ __global__ void k_rows_scatter(DevMat m, const uint64_t *__restrict__ rows) {
 // ---- result hash ------------------------------------------------------------
 // The reference's Horner loop (cfpq-cpp/Grammar.cpp:86-97) equals
 //   hash = sum over set bits (r, c) of 11^(n-1-c) * 13^(n-1-r)   (mod p),
-// a sum that is linear in the bits, so every word is reduced independently.
-// Block = 4 tiles x 64 rows; thread = one row word of one tile.  Unoccupied
-// tiles exit at once.  out[0] accumulates terms < 2^30 (no overflow below
-// 2^34 terms), out[1] the bit count.
-// Result line terms of one occupied tile (ti, tj) (one warp), with no loads
-// inside the bit loops: Sum over set bits (r, c) of 11^(n-1-c) 13^(n-1-r)
-// regrouped by column -- lane l sums the row powers of the rows whose bit l
-// (and bit l + 32) is set, broadcast row by row with shuffles, then
-// multiplies once by its columns' powers.  The power tables are indexed by
-// internal vertex index; every addend is below 2^30 (row sums below 2^36
-// before their reduction), so the 64-bit sums cannot overflow.
-__device__ __forceinline__ void hash_tile(const DevMat &m, const uint32_t *__restrict__ pow11,
-                                          const uint32_t *__restrict__ pow13, uint32_t ti, uint32_t tj,
-                                          unsigned long long &h, unsigned long long &cnt) {
+// a sum that is linear in the bits, so every tile is reduced independently
+// and only occupied tiles are read.
+//
+// Column terms of one occupied tile (ti, tj) (one warp): lane l takes rows
+// l and l + 32.  A row's column term, Sum over its set bits c of
+// 11^(n-1-c), is the sum of 8 entries of the subset-sum table, one per byte
+// of the row's tile word (k_pow_subsets): one round of independent loads
+// after the tile words.  The row power 13^(n-1-r) is the same for every
+// tile of the row, so the column terms are only added here (acc0 / acc1,
+// rows l and l + 32) and multiplied once per row by the caller.  Entries
+// are below p < 2^30, so a tile adds less than 2^33 to acc0 and acc1.
+__device__ __forceinline__ void hash_tile(const DevMat &m, const uint32_t *__restrict__ sub11, uint32_t ti,
+                                          uint32_t tj, unsigned long long &acc0, unsigned long long &acc1,
+                                          unsigned long long &cnt) {
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t *tile = m.bits + tile_offset(m.T, ti, tj);
-    const uint64_t w0 = tile[lane], w1 = tile[lane + 32];  // rows lane, lane + 32
-    const uint32_t q0 = pow13[(size_t)ti * 64 + lane], q1 = pow13[(size_t)ti * 64 + lane + 32];
-    const uint32_t pa = pow11[(size_t)tj * 64 + lane], pb = pow11[(size_t)tj * 64 + lane + 32];
+    const uint64_t w0 = tile[lane], w1 = tile[lane + 32];
+    const uint32_t *sub = sub11 + (size_t)tj * 2048;
     cnt += __popcll(w0) + __popcll(w1);
-    unsigned long long acc_a = 0, acc_b = 0;  // columns lane, lane + 32
 #pragma unroll
-    for (int half = 0; half < 2; ++half) {
-        const uint64_t w = half ? w1 : w0;
-        const uint32_t q = half ? q1 : q0;
-        unsigned rows = __ballot_sync(kFull, w != 0);
-        while (rows) {
-            const uint32_t r = __ffs(rows) - 1;
-            rows &= rows - 1;
-            const uint64_t v = __shfl_sync(kFull, w, r);
-            const uint32_t qr = __shfl_sync(kFull, q, r);
-            if ((v >> lane) & 1u) acc_a += qr;
-            if ((v >> (lane + 32)) & 1u) acc_b += qr;
-        }
+    for (int j = 0; j < 8; ++j) {
+        acc0 += sub[j * 256 + (uint32_t)((w0 >> (8 * j)) & 255u)];
+        acc1 += sub[j * 256 + (uint32_t)((w1 >> (8 * j)) & 255u)];
     }
-    h += ((acc_a % kHashMod) * pa) % kHashMod + ((acc_b % kHashMod) * pb) % kHashMod;
 }
 
-// Result line of occupancy word wi of m (one block of 8 warps: the word's
-// occupied tiles dealt round-robin to the warps), then one atomic pair per
-// block.
-__device__ __forceinline__ void hash_count_word(const DevMat &m, const uint32_t *__restrict__ pow11,
-                                                const uint32_t *__restrict__ pow13, unsigned long long *out,
-                                                uint32_t wi) {
-    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const uint32_t ti = wi / m.ow, word = wi % m.ow;
-    uint32_t bits = m.occ[wi];
-    unsigned long long h = 0, cnt = 0;
-    for (uint32_t k = 0; bits; ++k) {
-        const uint32_t tj = word * 32 + (__ffs(bits) - 1);
-        bits &= bits - 1;
-        if (k % nw == warp) hash_tile(m, pow11, pow13, ti, tj, h, cnt);
+// Subset sums of the column powers (one entry per thread):
+// sub[(tj * 8 + j) * 256 + v] = Sum over the set bits b of v of
+// pow11[64 tj + 8 j + b] mod p.
+__global__ void k_pow_subsets(const uint32_t *__restrict__ pow11, uint32_t T, uint32_t *__restrict__ sub) {
+    const size_t total = (size_t)T * 2048;
+    for (size_t x = blockIdx.x * (size_t)blockDim.x + threadIdx.x; x < total; x += (size_t)gridDim.x * blockDim.x) {
+        const uint32_t v = (uint32_t)(x & 255u);
+        const size_t col0 = (x >> 8) * 8;  // first column of byte j of tile column tj
+        unsigned long long acc = 0;
+#pragma unroll
+        for (uint32_t b = 0; b < 8; ++b)
+            if ((v >> b) & 1u) acc += pow11[col0 + b];
+        sub[x] = (uint32_t)(acc % kHashMod);
     }
+}
+
+// Sum of (h, cnt) over the block (8 warps); the totals are valid in thread 0.
+__device__ __forceinline__ void block_sum2(unsigned long long &h, unsigned long long &cnt) {
+    __shared__ unsigned long long sh[8], sc[8];
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     for (int o = 16; o > 0; o >>= 1) {
         h += __shfl_down_sync(kFull, h, o);
         cnt += __shfl_down_sync(kFull, cnt, o);
     }
-    __shared__ unsigned long long sh[8], sc[8];
     if (lane == 0) {
         sh[warp] = h;
         sc[warp] = cnt;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        unsigned long long H = 0, C = 0;
-        for (uint32_t i = 0; i < nw; ++i) {
-            H += sh[i];
-            C += sc[i];
+    if (threadIdx.x == 0)
+        for (uint32_t i = 1; i < nw; ++i) {
+            h += sh[i];
+            cnt += sc[i];
         }
-        if (H) atomicAdd(out, H);
-        if (C) atomicAdd(out + 1, C);
-    }
+    __syncthreads();  // sh / sc free for the next call
 }
 
-__global__ void __launch_bounds__(256) k_hash_count(DevMat m, const uint32_t *__restrict__ pow11,
-                                                    const uint32_t *__restrict__ pow13, unsigned long long *out) {
-    hash_count_word(m, pow11, pow13, out, blockIdx.x);
-}
-
-// Several matrices in one launch: blocks [start[i], start[i+1]) hash the
-// occupancy words of matrix i into out[2i], out[2i+1] (zeroed by the
-// launcher).
-__global__ void __launch_bounds__(256) k_hash_count_many(HashBatch hb, unsigned long long *out) {
+// Result lines of several matrices in one launch.  Block b hashes tile-row
+// b - start[i] of matrix i (its occupied tiles dealt round-robin to the 8
+// warps) into partial[b]; the last block to finish (ticket, which it resets
+// to 0 for the next launch) adds every matrix's partials and writes out[2i]
+// = hash mod p and out[2i+1] = bit count, so the output needs no zeroing
+// and may live in mapped host memory.  No sum can overflow: a tile adds
+// less than 2^33 to a lane's row sums (below 2^59 over fewer than 2^26
+// tiles), every thread's term and every row's partial are reduced mod p
+// (< 2^30) before they are added up, and a matrix has fewer than 2^26
+// tile-rows.
+__global__ void __launch_bounds__(256, 8) k_hash_lines(HashBatch hb, unsigned long long *__restrict__ partial,
+                                                       uint32_t *ticket, unsigned long long *out) {
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     uint32_t i = 0;
     while (i + 1 < hb.count && blockIdx.x >= hb.start[i + 1]) ++i;
-    hash_count_word(hb.m[i], hb.pow11[i], hb.pow13[i], out + 2 * i, blockIdx.x - hb.start[i]);
+    const DevMat &m = hb.m[i];
+    const uint32_t ti = blockIdx.x - hb.start[i];
+    const uint32_t *orow = m.occ + (size_t)ti * m.ow;
+    const uint32_t *sub11 = hb.sub11[i];
+    const uint32_t q0 = hb.pow13[i][(size_t)ti * 64 + lane], q1 = hb.pow13[i][(size_t)ti * 64 + lane + 32];
+    unsigned long long acc0 = 0, acc1 = 0, cnt = 0;
+    uint32_t k = 0;  // occupied tiles of the row seen so far (the deal order)
+    for (uint32_t base = 0; base < m.ow; base += 32) {
+        const uint32_t mine = base + lane < m.ow ? orow[base + lane] : 0u;
+        unsigned todo = __ballot_sync(kFull, mine != 0);
+        while (todo) {
+            const uint32_t src = __ffs(todo) - 1;
+            todo &= todo - 1;
+            uint32_t bits = __shfl_sync(kFull, mine, src);
+            while (bits) {
+                const uint32_t tj = (base + src) * 32 + (__ffs(bits) - 1);
+                bits &= bits - 1;
+                if (k++ % nw == warp) hash_tile(m, sub11, ti, tj, acc0, acc1, cnt);
+            }
+        }
+    }
+    unsigned long long h = (acc0 % kHashMod) * q0 % kHashMod + (acc1 % kHashMod) * q1 % kHashMod;
+    block_sum2(h, cnt);
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+        partial[2 * blockIdx.x] = h % kHashMod;
+        partial[2 * blockIdx.x + 1] = cnt;
+        __threadfence();
+        last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    // warp j adds the partials of matrices j, j + 8, ...: independent loads, no block barrier
+    for (uint32_t j = warp; j < hb.count; j += nw) {
+        unsigned long long H = 0, C = 0;
+#pragma unroll 4
+        for (uint32_t b = hb.start[j] + lane; b < hb.start[j + 1]; b += 32) {
+            H += __ldcg(partial + 2 * b);
+            C += __ldcg(partial + 2 * b + 1);
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            H += __shfl_xor_sync(kFull, H, o);
+            C += __shfl_xor_sync(kFull, C, o);
+        }
+        if (lane == 0) {
+            out[2 * j] = H % kHashMod;
+            out[2 * j + 1] = C;
+        }
+    }
+    if (threadIdx.x == 0) *ticket = 0;
 }
 
 // ---- plain dense product (variant PLAIN) ------------------------------------
@@ -441,7 +484,9 @@ __global__ void k_advance_end(const MatSlot *__restrict__ slots, uint32_t nslots
 
 // Closure prologue in one launch: zero the given word ranges, fill the
 // variant choices, initialise the iteration state and stamp its start.
-__global__ void k_closure_begin(ClosureBegin a) {
+// The closure prologue's work, spread over the whole grid (block 0 also
+// initialises the iteration state; every thread of block 0 must call it).
+__device__ __forceinline__ void closure_begin_body(const ClosureBegin &a) {
     const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x, nt = (size_t)gridDim.x * blockDim.x;
     for (int r = 0; r < ClosureBegin::kRanges; ++r)
         for (size_t i = tid; i < a.nwords[r]; i += nt) a.zero[r][i] = 0u;
@@ -459,10 +504,23 @@ __global__ void k_closure_begin(ClosureBegin a) {
     }
 }
 
+__global__ void k_closure_begin(ClosureBegin a) { closure_begin_body(a); }
+
 // Clear a list of matrices: one warp per (matrix, tile-row), occupied tiles only.
 __global__ void k_clear_rows(const MatRows *__restrict__ tab, uint32_t nmats, uint32_t total_rows) {
     const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (gw < total_rows) clear_unit(tab, nmats, gw);
+}
+
+// First kernel of a query's input phase: the clear of its matrices, the
+// scatter's out-of-range counter set to 0 and (with_begin) the closure
+// prologue, in one launch ahead of the scatter.
+__global__ void k_input_first(const MatRows *__restrict__ tab, uint32_t nmats, uint32_t total_rows, uint32_t *bad,
+                              ClosureBegin begin, int with_begin) {
+    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (gw < total_rows) clear_unit(tab, nmats, gw);
+    if (bad && blockIdx.x == 0 && threadIdx.x == 0) *bad = 0u;
+    if (with_begin) closure_begin_body(begin);
 }
 
 // Diagonals of a list of matrices (epsilon nonterminals).
@@ -584,19 +642,16 @@ cudaError_t launch_clear_matrix(const DevMat &m, cudaStream_t s) {
     return cudaMemsetAsync(m.occ, 0, (size_t)m.T * m.ow * 4, s);
 }
 
-cudaError_t launch_hash_count(const DevMat &m, const uint32_t *d_pow11, const uint32_t *d_pow13,
-                              unsigned long long *d_out, cudaStream_t s) {
-    cudaError_t e = cudaMemsetAsync(d_out, 0, 2 * sizeof(unsigned long long), s);
-    if (e != cudaSuccess || m.T == 0) return e;
-    k_hash_count<<<m.T * m.ow, 256, 0, s>>>(m, d_pow11, d_pow13, d_out);
+cudaError_t launch_pow_subsets(const uint32_t *d_pow11, uint32_t T, uint32_t *d_sub, cudaStream_t s) {
+    if (T == 0) return cudaSuccess;
+    k_pow_subsets<<<capped_grid((size_t)T * 2048, 256, 65535u), 256, 0, s>>>(d_pow11, T, d_sub);
     return cudaGetLastError();
 }
 
-cudaError_t launch_hash_count_many(const HashBatch &hb, unsigned long long *d_out, cudaStream_t s) {
-    if (hb.count == 0) return cudaSuccess;
-    cudaError_t e = cudaMemsetAsync(d_out, 0, 2 * sizeof(unsigned long long) * hb.count, s);
-    if (e != cudaSuccess || hb.start[hb.count] == 0) return e;
-    k_hash_count_many<<<hb.start[hb.count], 256, 0, s>>>(hb, d_out);
+cudaError_t launch_hash_lines(const HashBatch &hb, unsigned long long *d_partial, uint32_t *d_ticket,
+                              unsigned long long *out, cudaStream_t s) {
+    if (hb.count == 0 || hb.start[hb.count] == 0) return cudaErrorInvalidValue;
+    k_hash_lines<<<hb.start[hb.count], 256, 0, s>>>(hb, d_partial, d_ticket, out);
     return cudaGetLastError();
 }
 
@@ -652,9 +707,21 @@ cudaError_t launch_clear_rows(const MatRows *d_tab, uint32_t nmats, uint32_t tot
     return cudaGetLastError();
 }
 
-cudaError_t launch_closure_input(const ClosureInput &in, int num_sms, cudaStream_t s) {
-    if (in.clear_rows) {
-        cudaError_t e = launch_clear_rows(in.clear, in.nclear, in.clear_rows, s);
+static unsigned closure_begin_blocks(const ClosureBegin &a, int num_sms) {
+    size_t words = a.nchoice;
+    for (int r = 0; r < ClosureBegin::kRanges; ++r) words = words > a.nwords[r] ? words : a.nwords[r];
+    return (unsigned)std::max<size_t>(1, std::min<size_t>((words + 255) / 256, (size_t)num_sms * 4));
+}
+
+cudaError_t launch_closure_input(const ClosureInput &in, int num_sms, cudaStream_t s, const ClosureBegin *begin) {
+    if (in.clear_rows || in.bad || begin) {
+        const unsigned clear_blocks = in.clear_rows && in.nclear ? grid_for((size_t)in.clear_rows * 32, 256) : 1;
+        const unsigned blocks = begin ? std::max(clear_blocks, closure_begin_blocks(*begin, num_sms)) : clear_blocks;
+        ClosureBegin none;
+        memset(&none, 0, sizeof(none));
+        k_input_first<<<blocks, 256, 0, s>>>(in.clear, in.nclear, in.nclear ? in.clear_rows : 0, in.bad,
+                                             begin ? *begin : none, begin ? 1 : 0);
+        cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
     if (in.nedges) {
@@ -670,10 +737,7 @@ cudaError_t launch_closure_input(const ClosureInput &in, int num_sms, cudaStream
 }
 
 cudaError_t launch_closure_begin(const ClosureBegin &a, int num_sms, cudaStream_t s) {
-    size_t words = a.nchoice;
-    for (int r = 0; r < ClosureBegin::kRanges; ++r) words = words > a.nwords[r] ? words : a.nwords[r];
-    const unsigned blocks = (unsigned)std::max<size_t>(1, std::min<size_t>((words + 255) / 256, (size_t)num_sms * 4));
-    k_closure_begin<<<blocks, 256, 0, s>>>(a);
+    k_closure_begin<<<closure_begin_blocks(a, num_sms), 256, 0, s>>>(a);
     return cudaGetLastError();
 }
 

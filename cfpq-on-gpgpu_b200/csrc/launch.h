@@ -42,21 +42,26 @@ cudaError_t launch_random_fill(const DevMat &m, double density, uint64_t seed, c
 // Clear the matrices of d_tab (occupied tiles only; relies on the occupancy invariant).
 cudaError_t launch_clear_rows(const MatRows *d_tab, uint32_t nmats, uint32_t total_rows, cudaStream_t s);
 
-// Result hash / count (cfpq-cpp/Grammar.cpp:81-100 on the device)
-cudaError_t launch_hash_count(const DevMat &m, const uint32_t *d_pow11, const uint32_t *d_pow13,
-                              unsigned long long *d_out, cudaStream_t s);
-// Result lines of up to kHashBatch matrices in one launch (blocks of 4 tiles;
-// matrix i owns blocks [start[i], start[i+1])): out[2i] = hash terms,
-// out[2i+1] = bit count.
+// Result hash / count (cfpq-cpp/Grammar.cpp:81-100 on the device) of up to
+// kHashBatch matrices in one launch: one block per tile-row (matrix i owns
+// blocks [start[i], start[i+1])), partial sums in d_partial (2 words per
+// block), and the last block writes out[2i] = hash, out[2i+1] = bit count.
+// d_ticket must be 0 before the first launch (every launch leaves it 0);
+// out may be mapped host memory.  start[count] must be > 0.
 constexpr uint32_t kHashBatch = 16;
 struct HashBatch {
     DevMat m[kHashBatch];
-    const uint32_t *pow11[kHashBatch];
+    const uint32_t *sub11[kHashBatch];  // subset sums of the column powers (launch_pow_subsets)
     const uint32_t *pow13[kHashBatch];
-    uint32_t start[kHashBatch + 1];  // prefix sums of the matrices' occupancy words (one block each)
+    uint32_t start[kHashBatch + 1];  // prefix sums of the matrices' tile-rows (one block each)
     uint32_t count;
 };
-cudaError_t launch_hash_count_many(const HashBatch &hb, unsigned long long *d_out, cudaStream_t s);
+cudaError_t launch_hash_lines(const HashBatch &hb, unsigned long long *d_partial, uint32_t *d_ticket,
+                              unsigned long long *out, cudaStream_t s);
+// sub[(tj * 8 + j) * 256 + v] = sum over the set bits b of v of pow11[64 tj + 8 j + b]
+// (mod 1e9+7) for the T tile columns: a row's column term is the sum of 8
+// entries, one per byte of its tile word.
+cudaError_t launch_pow_subsets(const uint32_t *d_pow11, uint32_t T, uint32_t *d_sub, cudaStream_t s);
 
 // Plain dense product (variant PLAIN): mode 0 ORs into c and sets *d_flag on
 // change; mode 1 writes the product into c (c must not alias a or b).
@@ -121,8 +126,11 @@ struct ClosureBegin {
     uint32_t max_iter, nqueries;
 };
 cudaError_t launch_closure_begin(const ClosureBegin &a, int num_sms, cudaStream_t s);
-// A query's input phase as stand-alone kernels: clear, edge scatter, diagonals.
-cudaError_t launch_closure_input(const ClosureInput &in, int num_sms, cudaStream_t s);
+// A query's input phase as stand-alone kernels: clear (with in.bad set to 0
+// and, when begin is given, the closure prologue in the same launch), edge
+// scatter, diagonals.
+cudaError_t launch_closure_input(const ClosureInput &in, int num_sms, cudaStream_t s,
+                                 const ClosureBegin *begin = nullptr);
 // Persistent closure (word-level variants only): the whole fixpoint in one
 // cooperative launch of `grid` CTAs (at most persistent_blocks_per_sm() per
 // SM); items: 4 lists of list_cap; phase_log: 3 timestamps per iteration.

@@ -393,9 +393,12 @@ typedef struct cfpq_edges {
  * mats; Grammar.h:47-51), runs the closure and, when hashes and counts are
  * non-NULL, computes every matrix's result line -- all enqueued back to back
  * with ONE synchronisation at the end (the separate calls cost one host
- * round trip each).  An edge whose vertex id is >= a matrix's n makes the
- * call return CFPQ_ERR_INVALID after the closure; the matrices then hold the
- * closure of the in-range edges. */
+ * round trip each).  Host edge arrays in pinned memory that the device can
+ * map (cudaMallocHost / cudaHostAlloc, or registered) are read in place by
+ * the scatter kernel, with no copy; other host arrays are copied first.  An
+ * edge whose vertex id is >= a matrix's n makes the call return
+ * CFPQ_ERR_INVALID after the closure; the matrices then hold the closure of
+ * the in-range edges. */
 int cfpq_intersection(cfpq_ctx *ctx, const cfpq_rule *rules, size_t nrules, cfpq_matrix *const *mats,
                       size_t nmats, const cfpq_edges *edges, const uint32_t *epsilon, size_t nepsilon,
                       const cfpq_closure_opts *opts, cfpq_closure_stats *stats, uint64_t *hashes,

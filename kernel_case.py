@@ -5,6 +5,7 @@
   python kernel_case.py closure --n 8192 --reps 3
   python kernel_case.py batch --queries 64 --reps 2
   python kernel_case.py chain --n 16384 --reps 1
+  python kernel_case.py lines --n 8192 --reps 20
 
 `dense` runs C |= A * B on two seeded random n x n bit matrices (every tile
 populated) `reps` times with one variant; `closure` runs the same-generation
@@ -12,7 +13,10 @@ ontology query (seeded, n vertices) `reps` times; `batch` closes a seeded
 mixed batch of `queries` queries (N log-uniform in [256, 8192]) with one
 cfpq_closure_batch per repetition; `chain` closes the chain workload (mean
 out-degree 2, 90% local edges, random CNF with 10 nonterminals and 24 rules)
-at n vertices with the selector (variant AUTO, every size selects).  Each prints one JSON line
+at n vertices with the selector (variant AUTO, every size selects); `lines`
+closes the same-generation query once and then computes the result lines of
+its matrices (cfpq_hash_count_many: one hash launch, one synchronisation)
+`reps` times.  Each prints one JSON line
 with the device time of every repetition (CUDA events on the library's
 stream), so the same command can run with and without a profiler.
 """
@@ -29,7 +33,7 @@ sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["dense", "closure", "batch", "chain"])
+    ap.add_argument("case", choices=["dense", "closure", "batch", "chain", "lines"])
     ap.add_argument("--queries", type=int, default=64)
     ap.add_argument("--variant", default="lop3", choices=["plain", "lop3", "m4r", "tc"])
     ap.add_argument("--n", type=int, default=8192)
@@ -106,6 +110,19 @@ def main():
             times.append(e0.elapsed_time(e1))
         out.update(iterations=st["iterations"], tile_triples=st["tile_triples"], variant_items=st["variant_items"],
                    lines={k: list(v) for k, v in zip(wl.grammar.nonterminals, ctx.hash_count_many(q.mats))})
+        q.close()
+    elif args.case == "lines":
+        wl = pkg.workloads.ontology_query(args.n, args.seed)
+        q = pkg.query.PreparedQuery(ctx, wl.grammar, wl.graph)
+        q.run()
+        for _ in range(args.reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            lines = ctx.hash_count_many(q.mats)
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        out.update(lines={k: list(v) for k, v in zip(wl.grammar.nonterminals, lines)})
         q.close()
     else:
         wl = pkg.workloads.ontology_query(args.n, args.seed)

@@ -45,3 +45,24 @@ def test_closure_hash_matches_oracle(ctx, pkg, oracle, tmp_path, loop):
                 assert st["iterations"] > 1
         finally:
             q.close()
+
+
+def test_hash_count_many_empty_launch(ctx):
+    """A launch whose matrices are all of size 0 (the 17th matrix, alone in
+    the second launch) gives (0, 0) without a kernel; the first launch's
+    lines are unaffected."""
+    rng = np.random.default_rng(9)
+    mats = []
+    try:
+        for i in range(16):
+            m = ctx.matrix(100 + 37 * i)
+            m.set_bits(rng.integers(0, m.n, 300).astype(np.uint32), rng.integers(0, m.n, 300).astype(np.uint32))
+            mats.append(m)
+        mats.append(ctx.matrix(0))
+        many = ctx.hash_count_many(mats)
+        assert many[16] == (0, 0)
+        assert many[:16] == [m.hash_count() for m in mats[:16]]
+    finally:
+        for m in mats:
+            m.destroy()
+

@@ -17,8 +17,10 @@ def _oracle_lines(oracle, wl, tmp_path):
         return p.results()
 
 
-@pytest.mark.parametrize("where", ["host", "device"])
+@pytest.mark.parametrize("where", ["host", "pinned", "device"])
 def test_intersection_matches_oracle(ctx, pkg, oracle, tmp_path, where):
+    """host: pageable arrays (copied by the call); pinned: page-locked
+    arrays, which the scatter kernel reads in place; device: device arrays."""
     import torch
 
     for wl in (pkg.workloads.ontology_query(1500, 4), pkg.workloads.brackets_query()):
@@ -28,6 +30,10 @@ def test_intersection_matches_oracle(ctx, pkg, oracle, tmp_path, where):
         try:
             if where == "host":
                 arrays = (g.src, g.label, g.dst)
+                kw = {}
+            elif where == "pinned":
+                pinned = [torch.from_numpy(a.view(np.int32)).pin_memory() for a in (g.src, g.label, g.dst)]
+                arrays = tuple(t.numpy().view(np.uint32) for t in pinned)
                 kw = {}
             else:
                 dev = [torch.from_numpy(a.view(np.int32)).cuda() for a in (g.src, g.label, g.dst)]
@@ -113,3 +119,50 @@ def test_intersection_empty_graph(ctx, pkg, oracle, tmp_path):
         assert dict(zip(wl.grammar.nonterminals, lines)) == _oracle_lines(oracle, wl, tmp_path)
     finally:
         q.close()
+
+
+def test_scatter_hub_vertices_exact_tile_stats(ctx):
+    """Edge scatter with hub vertices (one vertex with an edge to every
+    other, every vertex with an edge to another hub, duplicates): thousands
+    of new bits share a tile-row and tiles, so the population counts and the
+    occupancy bits (set once, by the tile's first bit) are checked exactly,
+    through cfpq_load_edges and through cfpq_intersection's pinned path."""
+    import torch
+
+    n = 3000
+    rng = np.random.default_rng(77)
+    others = np.arange(n, dtype=np.uint32)
+    src = np.concatenate([np.full(n, 5, np.uint32), others, rng.integers(0, n, 4000).astype(np.uint32)])
+    dst = np.concatenate([others, np.full(n, 2900, np.uint32), rng.integers(0, n, 4000).astype(np.uint32)])
+    src = np.concatenate([src, src[:500]])  # duplicate edges add no bits
+    dst = np.concatenate([dst, dst[:500]])
+    lab = np.zeros(src.size, np.uint32)
+    wpr = (n + 63) // 64
+    rows = np.zeros((n, wpr), dtype=np.uint64)
+    np.bitwise_or.at(rows, (src, dst // 64), np.left_shift(np.uint64(1), (dst % 64).astype(np.uint64)))
+    T = wpr
+    padded = np.zeros((T * 64, T), dtype=np.uint64)
+    padded[:n] = rows
+    exp_nnz = np.bitwise_count(padded).reshape(T, 64, T).sum(axis=1).astype(np.uint32)
+    off, lm = np.array([0, 1], np.uint32), np.array([0], np.uint32)
+
+    def check(m):
+        assert np.array_equal(m.download_rows(), rows)
+        occ, nnz = m.tile_stats()
+        assert np.array_equal(nnz, exp_nnz)
+        occ_bits = np.unpackbits(occ.view(np.uint8), axis=1, bitorder="little")[:, :T].astype(bool)
+        assert np.array_equal(occ_bits, exp_nnz > 0)
+
+    m = ctx.matrix(n)
+    try:
+        ctx.load_edges([m], src, lab, dst, off, lm)
+        check(m)
+        ctx.load_edges([m], src, lab, dst, off, lm)  # again on top: nothing new
+        check(m)
+        pinned = [torch.from_numpy(a.view(np.int32)).pin_memory().numpy().view(np.uint32) for a in (src, lab, dst)]
+        st, lines = ctx.intersection([], [m], *pinned, off, lm)
+        check(m)
+        assert lines == [m.hash_count()]
+    finally:
+        m.destroy()
+

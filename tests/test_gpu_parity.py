@@ -98,9 +98,9 @@ def test_hash_count(ctx, oracle, n):
 
 
 def test_hash_count_large_ragged(ctx, oracle):
-    """The result-line hash (one block per occupancy word, column sums of
-    row powers per tile) on a ragged n = 20000 (313 tile-rows, 10 occupancy
-    words per row): scattered bits plus some dense blocks, and the
+    """The result-line hash (one block per tile-row, subset-sum lookups of
+    the column powers per row byte) on a ragged n = 20000 (313 tile-rows, 10
+    occupancy words per row): scattered bits plus some dense blocks, and the
     single-matrix and batched entry points against the oracle."""
     n = 20000
     rng = np.random.default_rng(20000)
