@@ -16,7 +16,8 @@ out-degree 2, 90% local edges, random CNF with 10 nonterminals and 24 rules)
 at n vertices with the selector (variant AUTO, every size selects); `lines`
 closes the same-generation query once and then computes the result lines of
 its matrices (cfpq_hash_count_many: one hash launch, one synchronisation)
-`reps` times.  Each prints one JSON line
+`reps` times (`--empty`: of the same matrices cleared after the closure,
+so every block finds no tile).  Each prints one JSON line
 with the device time of every repetition (CUDA events on the library's
 stream), so the same command can run with and without a profiler.
 """
@@ -40,6 +41,7 @@ def main():
     ap.add_argument("--density", type=float, default=0.3)
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--empty", action="store_true", help="lines: hash the query's matrices after clearing them")
     ap.add_argument("--no-graph", action="store_true",
                     help="closure, chain, batch: host-launched iterations, no CUDA graph or persistent kernel "
                          "(every kernel a separate launch, as a profiler needs)")
@@ -115,6 +117,8 @@ def main():
         wl = pkg.workloads.ontology_query(args.n, args.seed)
         q = pkg.query.PreparedQuery(ctx, wl.grammar, wl.graph)
         q.run()
+        if args.empty:
+            ctx.clear_many(q.mats)
         for _ in range(args.reps):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
