@@ -28,6 +28,13 @@ __device__ __forceinline__ uint32_t warp_sum(uint32_t v) {
     return __reduce_add_sync(kFull, v);
 }
 
+// Programmatic dependent launch: let the stream's next kernel (launched with
+// the programmatic-serialization attribute) start before this one ends /
+// wait until the stream's previous kernel has completed and its writes are
+// visible (returns at once for a kernel launched without the attribute).
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // ---- initialisation ---------------------------------------------------------
 
 __global__ void k_set_bits(DevMat m, const uint32_t *__restrict__ rows, const uint32_t *__restrict__ cols,
@@ -43,11 +50,14 @@ __global__ void k_set_bits(DevMat m, const uint32_t *__restrict__ rows, const ui
 }
 
 // Edge scatter: edge e sets (from, to) in every matrix its label derives
-// (cfpq-cpp/Grammar.h:41-45).
-// Edge scatter.  The label -> matrices tables and the matrix descriptors
-// (kLoadTableBytes at most) are copied into shared memory while the block's
-// first edges load, so an edge waits only for its vertex order entries and
-// its bit's atomic; larger tables are read from global memory.
+// (cfpq-cpp/Grammar.h:41-45).  The label -> matrices tables and the matrix
+// descriptors (kLoadTableBytes at most) are copied into shared memory while
+// the block's first edges load, so an edge waits only for its vertex order
+// entries and its bit's atomic; larger tables are read from global memory.
+// After the input phase's first kernel (programmatic dependent launch) the
+// block starts while that kernel still clears the matrices: the edge and
+// table loads, which do not depend on it, go first, and pdl_wait() keeps
+// every write to the matrices and the counter after its end.
 constexpr uint32_t kLoadTableBytes = 12288;
 
 template <bool kSmem>
@@ -74,6 +84,7 @@ __global__ void k_load_edges(const DevMat *__restrict__ mats, uint32_t nmats, co
         c = to[e];
     }
     if constexpr (kSmem) __syncthreads();
+    pdl_wait();
     for (; e < ne; e += (size_t)gridDim.x * blockDim.x) {
         scatter_edge(mats, off, lm, nlabels, l, r, c, bad);
         const size_t e2 = e + (size_t)gridDim.x * blockDim.x;
@@ -517,6 +528,7 @@ __global__ void k_clear_rows(const MatRows *__restrict__ tab, uint32_t nmats, ui
 // prologue, in one launch ahead of the scatter.
 __global__ void k_input_first(const MatRows *__restrict__ tab, uint32_t nmats, uint32_t total_rows, uint32_t *bad,
                               ClosureBegin begin, int with_begin) {
+    pdl_launch_dependents();  // the scatter may start its loads now
     const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (gw < total_rows) clear_unit(tab, nmats, gw);
     if (bad && blockIdx.x == 0 && threadIdx.x == 0) *bad = 0u;
@@ -545,16 +557,24 @@ cudaError_t launch_set_bits(const DevMat &m, const uint32_t *d_rows, const uint3
 
 cudaError_t launch_load_edges(const DevMat *d_mats, uint32_t nmats, const uint32_t *d_from, const uint32_t *d_label,
                               const uint32_t *d_to, size_t ne, const uint32_t *d_off, const uint32_t *d_lm,
-                              uint32_t nlabels, uint32_t nlm, uint32_t *d_bad, cudaStream_t s) {
+                              uint32_t nlabels, uint32_t nlm, uint32_t *d_bad, cudaStream_t s, bool dependent) {
     if (ne == 0) return cudaSuccess;
     const size_t tb = (size_t)nmats * sizeof(DevMat) + ((size_t)nlabels + 1 + nlm) * 4;
-    if (tb <= kLoadTableBytes)
-        k_load_edges<true><<<capped_grid(ne, 256, 65535u * 16), 256, tb, s>>>(d_mats, nmats, d_from, d_label, d_to, ne,
-                                                                            d_off, d_lm, nlabels, nlm, d_bad);
-    else
-        k_load_edges<false><<<capped_grid(ne, 256, 65535u * 16), 256, 0, s>>>(d_mats, nmats, d_from, d_label, d_to,
-                                                                            ne, d_off, d_lm, nlabels, nlm, d_bad);
-    return cudaGetLastError();
+    const bool smem = tb <= kLoadTableBytes;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(capped_grid(ne, 256, 65535u * 16));
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = smem ? tb : 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = dependent ? 1 : 0;
+    return smem ? cudaLaunchKernelEx(&cfg, k_load_edges<true>, d_mats, nmats, d_from, d_label, d_to, ne, d_off, d_lm,
+                                     nlabels, nlm, d_bad)
+                : cudaLaunchKernelEx(&cfg, k_load_edges<false>, d_mats, nmats, d_from, d_label, d_to, ne, d_off,
+                                     d_lm, nlabels, nlm, d_bad);
 }
 
 cudaError_t launch_set_diag(const DevMat &m, cudaStream_t s) {
@@ -724,9 +744,10 @@ cudaError_t launch_closure_input(const ClosureInput &in, int num_sms, cudaStream
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
+    const bool first_launched = in.clear_rows || in.bad || begin;
     if (in.nedges) {
         cudaError_t e = launch_load_edges(in.mats, in.nmats, in.from, in.label, in.to, in.nedges, in.off, in.lm,
-                                          in.nlabels, in.nlm, in.bad, s);
+                                          in.nlabels, in.nlm, in.bad, s, first_launched);
         if (e != cudaSuccess) return e;
     }
     if (in.ndiag) {

@@ -12,9 +12,11 @@ namespace cfpq {
 // Layout / initialisation
 cudaError_t launch_set_bits(const DevMat &m, const uint32_t *d_rows, const uint32_t *d_cols, size_t count,
                             uint32_t *d_bad, cudaStream_t s);
+// dependent: launched right after k_input_first as a programmatic dependent
+// launch (its loads of edges and tables overlap that kernel).
 cudaError_t launch_load_edges(const DevMat *d_mats, uint32_t nmats, const uint32_t *d_from, const uint32_t *d_label,
                               const uint32_t *d_to, size_t ne, const uint32_t *d_off, const uint32_t *d_lm,
-                              uint32_t nlabels, uint32_t nlm, uint32_t *d_bad, cudaStream_t s);
+                              uint32_t nlabels, uint32_t nlm, uint32_t *d_bad, cudaStream_t s, bool dependent = false);
 cudaError_t launch_set_diag(const DevMat &m, cudaStream_t s);
 cudaError_t launch_occ_rebuild(const DevMat &m, cudaStream_t s);
 // delta = cur & ~prev, then prev = cur; tile statistics of both rebuilt.
