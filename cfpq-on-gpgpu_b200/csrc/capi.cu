@@ -138,7 +138,7 @@ static int pool_give(cfpq_ctx *ctx, cfpq_matrix *m, bool dirty) {
 // Hash power tables for vertex ids 0..n-1 stored at internal index perm[v]
 // (identity when perm is null): pow11[perm[c]] = 11^(n-1-c),
 // pow13[perm[r]] = 13^(n-1-r) modulo 1e9+7 (cfpq-cpp/Grammar.cpp:12-14),
-// and the subset sums of pow11 the hash kernel reads (built on stream s).
+// and the nibble tables of pow11 the hash kernel reads (built on stream s).
 static int make_pow_tables(uint32_t n, const uint32_t *perm, PowTables *t, cudaStream_t s) {
     const uint32_t np = tiles_for(n) * 64;
     std::vector<uint32_t> p11(np ? np : 1, 0), p13(np ? np : 1, 0);
@@ -156,8 +156,8 @@ static int make_pow_tables(uint32_t n, const uint32_t *perm, PowTables *t, cudaS
     CUDA_TRY(cudaMemcpy(t->d_pow11, p11.data(), p11.size() * 4, cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(t->d_pow13, p13.data(), p13.size() * 4, cudaMemcpyHostToDevice));
     const uint32_t T = tiles_for(n);
-    CUDA_TRY(cudaMalloc(&t->d_sub11, (size_t)(T ? T : 1) * 2048 * 4));
-    if (T) CUDA_TRY(launch_pow_subsets(t->d_pow11, T, t->d_sub11, s));
+    CUDA_TRY(cudaMalloc(&t->d_nib11, (size_t)(T ? T : 1) * 256 * 4));
+    if (T) CUDA_TRY(launch_pow_nibbles(t->d_pow11, T, t->d_nib11, s));
     return CFPQ_OK;
 }
 
@@ -215,7 +215,7 @@ extern "C" int cfpq_order_destroy(cfpq_ctx *ctx, cfpq_order *order) {
     if (order->d_perm) cudaFree(order->d_perm);
     if (order->pow.d_pow11) cudaFree(order->pow.d_pow11);
     if (order->pow.d_pow13) cudaFree(order->pow.d_pow13);
-    if (order->pow.d_sub11) cudaFree(order->pow.d_sub11);
+    if (order->pow.d_nib11) cudaFree(order->pow.d_nib11);
     delete order;
     return CFPQ_OK;
 }
@@ -293,7 +293,7 @@ extern "C" int cfpq_ctx_destroy(cfpq_ctx *ctx) {
     for (auto &kv : ctx->pow) {
         cudaFree(kv.second.d_pow11);
         cudaFree(kv.second.d_pow13);
-        cudaFree(kv.second.d_sub11);
+        cudaFree(kv.second.d_nib11);
     }
     for (DevBuf *b : {&ctx->stage, &ctx->items, &ctx->prods, &ctx->slots, &ctx->qtrack, &ctx->prod_seen,
                       &ctx->mats_desc, &ctx->edge_buf, &ctx->phase_log, &ctx->clear_desc, &ctx->diag_desc,
@@ -718,7 +718,7 @@ static int enqueue_hash_many(cfpq_ctx *ctx, cfpq_matrix *const *mats, size_t nma
             TRY(get_pow_tables(ctx, mats[i], &pt));
             const uint32_t k = hb.count++;
             hb.m[k] = mats[i]->d;
-            hb.sub11[k] = pt.d_sub11;
+            hb.nib11[k] = pt.d_nib11;
             hb.pow13[k] = pt.d_pow13;
             hb.start[k + 1] = hb.start[k] + mats[i]->d.T;  // one block per tile-row
         }

@@ -70,7 +70,7 @@ struct DevBuf {
 struct PowTables {
     uint32_t *d_pow11 = nullptr;
     uint32_t *d_pow13 = nullptr;
-    uint32_t *d_sub11 = nullptr;  // per tile column and byte: the 256 subset sums of pow11 (launch_pow_subsets)
+    uint32_t *d_nib11 = nullptr;  // per tile column and nibble: the 16 subset sums of pow11 (launch_pow_nibbles)
 };
 
 struct GraphCache {

@@ -199,38 +199,47 @@ __global__ void k_rows_scatter(DevMat m, const uint64_t *__restrict__ rows) {
 //
 // Column terms of one occupied tile (ti, tj) (one warp): lane l takes rows
 // l and l + 32.  A row's column term, Sum over its set bits c of
-// 11^(n-1-c), is the sum of 8 entries of the subset-sum table, one per byte
-// of the row's tile word (k_pow_subsets): one round of independent loads
-// after the tile words.  The row power 13^(n-1-r) is the same for every
-// tile of the row, so the column terms are only added here (acc0 / acc1,
-// rows l and l + 32) and multiplied once per row by the caller.  Entries
-// are below p < 2^30, so a tile adds less than 2^33 to acc0 and acc1.
-__device__ __forceinline__ void hash_tile(const DevMat &m, const uint32_t *__restrict__ sub11, uint32_t ti,
+// 11^(n-1-c), is the sum over the 16 nibbles of its tile word of a nibble
+// table entry: sub[p * 16 + v] = Sum over the set bits b of v of
+// 11^(n-1-c) for column c = 64 tj + 4 p + b (k_pow_nibbles, 256 entries per
+// tile column).  The warp loads the column's table with 8 coalesced loads
+// (lane l of register k holds entry 32 k + l), so the lookup of nibble p is
+// one shuffle from register p / 2, lane 16 (p & 1) + v: a tile costs one
+// round of coalesced loads and 32 shuffles.  The row power 13^(n-1-r) is
+// the same for every tile of the row, so the column terms are only added
+// here (acc0 / acc1, rows l and l + 32) and multiplied once per row by the
+// caller.  Entries are below p < 2^30, so a tile adds less than 2^34 to
+// acc0 and acc1.
+__device__ __forceinline__ void hash_tile(const DevMat &m, const uint32_t *__restrict__ nib11, uint32_t ti,
                                           uint32_t tj, unsigned long long &acc0, unsigned long long &acc1,
                                           unsigned long long &cnt) {
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t *tile = m.bits + tile_offset(m.T, ti, tj);
+    const uint32_t *tab = nib11 + (size_t)tj * 256;
+    uint32_t t[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) t[k] = tab[k * 32 + lane];
     const uint64_t w0 = tile[lane], w1 = tile[lane + 32];
-    const uint32_t *sub = sub11 + (size_t)tj * 2048;
     cnt += __popcll(w0) + __popcll(w1);
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-        acc0 += sub[j * 256 + (uint32_t)((w0 >> (8 * j)) & 255u)];
-        acc1 += sub[j * 256 + (uint32_t)((w1 >> (8 * j)) & 255u)];
+    for (int p = 0; p < 16; ++p) {
+        const uint32_t hi = (uint32_t)(p & 1) << 4;
+        acc0 += __shfl_sync(kFull, t[p >> 1], (int)(hi | (uint32_t)((w0 >> (4 * p)) & 15u)));
+        acc1 += __shfl_sync(kFull, t[p >> 1], (int)(hi | (uint32_t)((w1 >> (4 * p)) & 15u)));
     }
 }
 
-// Subset sums of the column powers (one entry per thread):
-// sub[(tj * 8 + j) * 256 + v] = Sum over the set bits b of v of
-// pow11[64 tj + 8 j + b] mod p.
-__global__ void k_pow_subsets(const uint32_t *__restrict__ pow11, uint32_t T, uint32_t *__restrict__ sub) {
-    const size_t total = (size_t)T * 2048;
+// Nibble tables of the column powers (one entry per thread):
+// sub[tj * 256 + p * 16 + v] = Sum over the set bits b of v of
+// pow11[64 tj + 4 p + b] mod p.
+__global__ void k_pow_nibbles(const uint32_t *__restrict__ pow11, uint32_t T, uint32_t *__restrict__ sub) {
+    const size_t total = (size_t)T * 256;
     for (size_t x = blockIdx.x * (size_t)blockDim.x + threadIdx.x; x < total; x += (size_t)gridDim.x * blockDim.x) {
-        const uint32_t v = (uint32_t)(x & 255u);
-        const size_t col0 = (x >> 8) * 8;  // first column of byte j of tile column tj
+        const uint32_t v = (uint32_t)(x & 15u);
+        const size_t col0 = (x >> 4) * 4;  // first column of nibble p of tile column tj
         unsigned long long acc = 0;
 #pragma unroll
-        for (uint32_t b = 0; b < 8; ++b)
+        for (uint32_t b = 0; b < 4; ++b)
             if ((v >> b) & 1u) acc += pow11[col0 + b];
         sub[x] = (uint32_t)(acc % kHashMod);
     }
@@ -267,7 +276,7 @@ __device__ __forceinline__ void block_sum2(unsigned long long &h, unsigned long 
 // tiles), every thread's term and every row's partial are reduced mod p
 // (< 2^30) before they are added up, and a matrix has fewer than 2^26
 // tile-rows.
-__global__ void __launch_bounds__(256, 8) k_hash_lines(HashBatch hb, unsigned long long *__restrict__ partial,
+__global__ void __launch_bounds__(256, 6) k_hash_lines(HashBatch hb, unsigned long long *__restrict__ partial,
                                                        uint32_t *ticket, unsigned long long *out) {
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     uint32_t i = 0;
@@ -275,7 +284,7 @@ __global__ void __launch_bounds__(256, 8) k_hash_lines(HashBatch hb, unsigned lo
     const DevMat &m = hb.m[i];
     const uint32_t ti = blockIdx.x - hb.start[i];
     const uint32_t *orow = m.occ + (size_t)ti * m.ow;
-    const uint32_t *sub11 = hb.sub11[i];
+    const uint32_t *nib11 = hb.nib11[i];
     const uint32_t q0 = hb.pow13[i][(size_t)ti * 64 + lane], q1 = hb.pow13[i][(size_t)ti * 64 + lane + 32];
     unsigned long long acc0 = 0, acc1 = 0, cnt = 0;
     uint32_t k = 0;  // occupied tiles of the row seen so far (the deal order)
@@ -289,7 +298,7 @@ __global__ void __launch_bounds__(256, 8) k_hash_lines(HashBatch hb, unsigned lo
             while (bits) {
                 const uint32_t tj = (base + src) * 32 + (__ffs(bits) - 1);
                 bits &= bits - 1;
-                if (k++ % nw == warp) hash_tile(m, sub11, ti, tj, acc0, acc1, cnt);
+                if (k++ % nw == warp) hash_tile(m, nib11, ti, tj, acc0, acc1, cnt);
             }
         }
     }
@@ -662,9 +671,9 @@ cudaError_t launch_clear_matrix(const DevMat &m, cudaStream_t s) {
     return cudaMemsetAsync(m.occ, 0, (size_t)m.T * m.ow * 4, s);
 }
 
-cudaError_t launch_pow_subsets(const uint32_t *d_pow11, uint32_t T, uint32_t *d_sub, cudaStream_t s) {
+cudaError_t launch_pow_nibbles(const uint32_t *d_pow11, uint32_t T, uint32_t *d_sub, cudaStream_t s) {
     if (T == 0) return cudaSuccess;
-    k_pow_subsets<<<capped_grid((size_t)T * 2048, 256, 65535u), 256, 0, s>>>(d_pow11, T, d_sub);
+    k_pow_nibbles<<<capped_grid((size_t)T * 256, 256, 65535u), 256, 0, s>>>(d_pow11, T, d_sub);
     return cudaGetLastError();
 }
 

@@ -53,17 +53,17 @@ cudaError_t launch_clear_rows(const MatRows *d_tab, uint32_t nmats, uint32_t tot
 constexpr uint32_t kHashBatch = 16;
 struct HashBatch {
     DevMat m[kHashBatch];
-    const uint32_t *sub11[kHashBatch];  // subset sums of the column powers (launch_pow_subsets)
+    const uint32_t *nib11[kHashBatch];  // nibble tables of the column powers (launch_pow_nibbles)
     const uint32_t *pow13[kHashBatch];
     uint32_t start[kHashBatch + 1];  // prefix sums of the matrices' tile-rows (one block each)
     uint32_t count;
 };
 cudaError_t launch_hash_lines(const HashBatch &hb, unsigned long long *d_partial, uint32_t *d_ticket,
                               unsigned long long *out, cudaStream_t s);
-// sub[(tj * 8 + j) * 256 + v] = sum over the set bits b of v of pow11[64 tj + 8 j + b]
-// (mod 1e9+7) for the T tile columns: a row's column term is the sum of 8
-// entries, one per byte of its tile word.
-cudaError_t launch_pow_subsets(const uint32_t *d_pow11, uint32_t T, uint32_t *d_sub, cudaStream_t s);
+// sub[tj * 256 + p * 16 + v] = sum over the set bits b of v of pow11[64 tj + 4 p + b]
+// (mod 1e9+7) for the T tile columns: a row's column term is the sum of 16
+// entries, one per nibble of its tile word.
+cudaError_t launch_pow_nibbles(const uint32_t *d_pow11, uint32_t T, uint32_t *d_sub, cudaStream_t s);
 
 // Plain dense product (variant PLAIN): mode 0 ORs into c and sets *d_flag on
 // change; mode 1 writes the product into c (c must not alias a or b).
