@@ -166,3 +166,23 @@ def test_scatter_hub_vertices_exact_tile_stats(ctx):
     finally:
         m.destroy()
 
+
+
+def test_intersection_many_nonterminals(ctx, pkg, oracle, tmp_path):
+    """A grammar of 20 nonterminals against the oracle: the result lines take
+    two hash launches (16 matrices per launch), and the repeated call clears
+    the previous closure of all 20 matrices first."""
+    labels = ["a", "b", "c"]
+    g = pkg.workloads.uniform_graph(700, 2100, labels, 21)
+    gram = pkg.workloads.random_cnf(20, 40, labels, 21)
+    wl = pkg.workloads.Workload("random_cnf_20", gram, g, {})
+    exp = _oracle_lines(oracle, wl, tmp_path)
+    q = pkg.query.PreparedQuery(ctx, wl.grammar, wl.graph)
+    try:
+        assert len(q.mats) == 20
+        for _ in range(2):
+            st, lines = ctx.intersection(wl.grammar.rules, q.mats, g.src, g.label, g.dst, q.off, q.lm,
+                                         epsilon=wl.grammar.epsilon)
+            assert dict(zip(wl.grammar.nonterminals, lines)) == exp
+    finally:
+        q.close()
