@@ -186,3 +186,28 @@ def test_intersection_many_nonterminals(ctx, pkg, oracle, tmp_path):
             assert dict(zip(wl.grammar.nonterminals, lines)) == exp
     finally:
         q.close()
+
+
+def test_intersection_kernel_launch_count(ctx, pkg):
+    """kernel_launches counts every kernel the call launches: on the
+    persistent path the input phase's first kernel (clear + closure
+    prologue), the edge scatter and the closure kernel, plus one hash launch
+    when the result lines are asked for."""
+    import torch
+
+    wl = pkg.workloads.ontology_query(8192, 1)
+    g = wl.graph
+    q = pkg.query.PreparedQuery(ctx, wl.grammar, wl.graph)
+    try:
+        dev = [torch.from_numpy(a.view(np.int32)).cuda() for a in (g.src, g.label, g.dst)]
+        torch.cuda.synchronize()
+        ptrs = tuple(t.data_ptr() for t in dev)
+        st, _ = ctx.intersection(wl.grammar.rules, q.mats, *ptrs, q.off, q.lm, epsilon=wl.grammar.epsilon,
+                                 nedges=g.nedges, lines=False)
+        assert st["kernel_launches"] == 3
+        st, lines = ctx.intersection(wl.grammar.rules, q.mats, *ptrs, q.off, q.lm, epsilon=wl.grammar.epsilon,
+                                     nedges=g.nedges, lines=True)
+        assert st["kernel_launches"] == 4
+        assert len(lines) == len(q.mats)
+    finally:
+        q.close()
