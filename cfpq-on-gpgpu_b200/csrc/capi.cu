@@ -425,10 +425,6 @@ extern "C" int cfpq_load_edges_device(cfpq_ctx *ctx, cfpq_matrix *const *mats, s
 
 extern "C" void *cfpq_ctx_stream(const cfpq_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
 
-// Validates an edge list and stages it for the scatter: the small tables
-// (matrix descriptors, label offsets, label -> matrices) on the device, host
-// edge arrays copied (asynchronously) into the context's staging block.
-// Fills the edge fields of *in; launches nothing.  Nothing to scatter: in->nedges = 0.
 // The device address of host array a[0..n) when all of it is pinned and
 // mapped into this device's address space, else null.
 static const uint32_t *mapped_host_array(const uint32_t *a, size_t n) {
@@ -446,10 +442,14 @@ static const uint32_t *mapped_host_array(const uint32_t *a, size_t n) {
     return dev[1] == dev[0] + (n - 1) ? dev[0] : nullptr;
 }
 
-// The edge scatter's input.  Host edge arrays are copied into the context's
-// staging buffer, except with read_pinned_in_place, where arrays in pinned
-// mapped host memory are read by the scatter kernel itself over the bus (the
-// caller must keep them unchanged until the stream has run the kernel).
+// Validates an edge list and stages it for the scatter: the small tables
+// (matrix descriptors, label offsets, label -> matrices) on the device, host
+// edge arrays copied (asynchronously) into the context's staging block --
+// except with read_pinned_in_place, where arrays in pinned mapped host
+// memory are read by the scatter kernel itself over the bus (the caller must
+// keep them unchanged until the stream has run the kernel; *read_in_place
+// tells which happened).  Fills the edge fields of *in; launches nothing.
+// Nothing to scatter: in->nedges = 0.
 static int prepare_edges(cfpq_ctx *ctx, cfpq_matrix *const *mats, size_t nmats, const uint32_t *from,
                          const uint32_t *label, const uint32_t *to, size_t nedges, const uint32_t *label_offsets,
                          const uint32_t *label_mats, uint32_t nlabels, bool on_device, ClosureInput *in,
