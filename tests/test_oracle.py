@@ -125,3 +125,45 @@ def test_empty_graph(oracle, tmp_path):
         assert p.n == 0
         p.closure(oracle.M4RM, 1)
         assert p.results() == {"S": (0, 0), "A": (0, 0), "B": (0, 0)}
+
+
+def test_hash_nibble_table_decomposition(oracle):
+    """The decomposition the device hash uses equals the reference loop (the
+    oracle): under a vertex order perm, with pow11[perm[c]] = 11^(n-1-c) and
+    pow13[perm[r]] = 13^(n-1-r), a tile word's column term is the sum over
+    its 16 nibbles of sub[tj][p][nibble] (the subset sums of the 4 column
+    powers of nibble p), a row's terms add up over its tiles and are
+    multiplied once by the row power."""
+    p = 1000000007
+    rng = np.random.default_rng(11)
+    for n in (1, 63, 64, 130, 300):
+        rows = _rows(rng, n, 0.2)
+        bits = _dense(rows, n)
+        perm = rng.permutation(n)
+        T = (n + 63) // 64
+        pow11 = np.zeros(T * 64, dtype=np.int64)
+        pow13 = np.zeros(T * 64, dtype=np.int64)
+        a = b = 1
+        for c in range(n - 1, -1, -1):
+            pow11[perm[c]], pow13[perm[c]] = a, b
+            a, b = a * 11 % p, b * 13 % p
+        sub = np.zeros((T, 16, 16), dtype=np.int64)
+        for v in range(16):
+            for bit in range(4):
+                if (v >> bit) & 1:
+                    sub[:, :, v] += pow11.reshape(T, 16, 4)[:, :, bit]
+        sub %= p
+        internal = np.zeros((T * 64, T * 64), dtype=bool)  # bit (perm[r], perm[c]) for vertex pair (r, c)
+        rr, cc = np.nonzero(bits)
+        internal[perm[rr], perm[cc]] = True
+        h = 0
+        for ti in range(T):
+            for lane in range(64):
+                acc = 0
+                for tj in range(T):
+                    word = 0
+                    for k in np.nonzero(internal[ti * 64 + lane, tj * 64:(tj + 1) * 64])[0]:
+                        word |= 1 << int(k)
+                    acc += sum(int(sub[tj, q, (word >> (4 * q)) & 15]) for q in range(16))
+                h += (acc % p) * int(pow13[ti * 64 + lane]) % p
+        assert (h % p, int(bits.sum())) == oracle.hash_count(rows, n)
